@@ -1,0 +1,357 @@
+"""Benchmark of the Kerr ray tracer on the 2048^2 thermal-synchrotron scene (one B200 per rank).
+
+Workload: the synchrotron frame of spacetime-optics_b200/shots/synchrotron_1024.ini rendered at
+2048 x 2048 (a = 0.94, inclination 163 deg, field of view +-12 M, 230 GHz, analytic torus plasma with
+512 Fourier modes of turbulence, flux normalised to 0.6 Jy), one sample per pixel centre.
+One "step" = one frame traced end to end.
+
+  value  Mrays/s of the fastest path (mixed precision when built and selected, else plain FP64),
+         device buffers only (so_render_device), CUDA events on the renderer's stream.
+  e2e    the same frame through so_render with host buffers: the frame descriptor goes host->device
+         and the 2048 x 2048 x 4 float image comes back device->host every step.
+Multi-GPU: frames are independent, so N ranks each render their own frame (weak scaling, no
+collective on the data path); the max over ranks of the device time gives the job time.
+
+--impl reference times the reference's own CPU tracer (oracle/_ref, built from the reference
+sources) on the host cores over a bounded sample of the same pixels; see DESIGN.md for how its
+plasma maps onto this workload.
+"""
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "spacetime-optics_b200")
+METRIC = "Mrays/s at ≤1e-3 image error: surrogate/mixed vs plain FP64 kernel, 1 B200"
+
+# Algorithmic FP64 flops (FMA = 2, divide = 1, sqrt = 1; comparisons, fabs and fmin/fmax not counted),
+# counted from spacetime-optics_b200/csrc/so_kerr.cuh and so_emission.cuh:
+FLOPS_ATTEMPT = 469        # one DP5(4) attempt: 6 RHS (31 each) + stage sums + 5th-order sum + error norm
+FLOPS_ACCEPT = 49          # controller err^-1/5 (34) + projection (11) + psi bookkeeping excluded (radio)
+FLOPS_FLOW = 160           # flow_step without the turbulence sum (transcendentals counted as 20 each)
+FLOPS_MODE = 8 + 20        # one Fourier mode: 3 fma (k.X + phase) + fma accumulate + cos (20)
+
+
+def load_package():
+    if "spacetime_optics_b200" in sys.modules:
+        return sys.modules["spacetime_optics_b200"]
+    spec = importlib.util.spec_from_file_location("spacetime_optics_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["spacetime_optics_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_scene(so, W, flux_norm=True):
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    p = sh.plasma()
+    r.set_plasma(p)
+    scene = sh.scene
+    info = {}
+    if flux_norm and sh.info.radio_flux_target_jy > 0:
+        # flux normalisation (main.cpp:475-508) on a 160^2 frame of width flow.normalize_fov_m
+        fov = sh.num("flow.normalize_fov_m", 40.0)
+        tmp = so.Shot("synchrotron_1024.ini", ["camera.width=160", "camera.height=160", f"camera.fov_m={fov}"])
+        fw = tmp.frame(0, W=160, seed=1)
+        pix_sr = (fov / 160 * sh.info.rg_cm / sh.info.distance_cm) ** 2
+        n0, jy = r.normalize_flux(scene, fw, 160, pix_sr, sh.info.radio_flux_target_jy)
+        info = {"n0": n0, "flux_jy": jy}
+    return sh, r, info
+
+
+def run_ours(args, so, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    W = args.size
+    sh, r, norm = build_scene(so, W)
+    path = args.path
+    if path == "auto":
+        path = "mixed" if os.environ.get("SO_BENCH_MIXED", "0") == "1" and has_mixed(so, r) else "fp64"
+    f = sh.frame(rank)
+    f.t = sh.frame(0).t + 50.0 * rank  # every rank renders its own turbulence time offset
+    npix = W * W
+    d_img = torch.empty((W, W, 4), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(r.stream())
+
+    def set_prec(p):
+        r.set_precision(so.abi.SO_PREC_MIXED if p == "mixed" else so.abi.SO_PREC_FP64)
+
+    # plain FP64 reference image (for the image error of the mixed path) and its timing
+    set_prec("fp64")
+    st64 = r.render_device(f, d_img.data_ptr(), stats=True)
+    img64 = d_img.cpu().numpy().copy()
+    results = {"fp64": {"ms_kernel": st64.ms_kernel, "attempts": st64.attempts, "flow_steps": st64.flow_steps,
+                        "accepted": st64.accepted}}
+    set_prec(path)
+    for _ in range(args.warmup):
+        r.render_device(f, d_img.data_ptr())
+    torch.cuda.synchronize()
+    # larger-than-L2 buffer written between steps (the frame's inputs are tiny and stay cached;
+    # flushing keeps each step cold like a fresh frame)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
+            r.render_device(f, d_img.data_ptr())
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    ms_step = float(np.mean(ms))
+    barrier(world)
+    ms_step = allreduce_max(ms_step, world)
+    value = world * npix / (ms_step * 1e-3) / 1e6
+    # instrumented step: counters and the tracer kernel's own device time (CUDA events in the library)
+    st = r.render_device(f, d_img.data_ptr(), stats=True)
+    img = d_img.cpu().numpy()
+    err_l1 = float(np.abs(img[..., 0] - img64[..., 0]).sum() / max(np.abs(img64[..., 0]).sum(), 1e-300))
+    flux_err = float(abs(img[..., 0].astype(np.float64).sum() / img64[..., 0].astype(np.float64).sum() - 1.0))
+    fp64_mrays = npix / (st64.ms_kernel * 1e-3) / 1e6
+    # roofline of the dominant kernel (the tracer): algorithmic FP64 flops per launch / its duration
+    fp64_peak, fp32_peak = so.probe_fma_peak(local)
+    flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
+             st.flow_steps * (FLOPS_FLOW + sh.plasma().n_modes * FLOPS_MODE))
+    achieved = flops / (st.ms_kernel * 1e-3) / 1e12
+    peak = fp64_peak if path == "fp64" else fp64_peak
+    # e2e: host buffers through so_render (frame H2D, image D2H inside the timed region)
+    host = np.empty((W, W, 4), np.float32)
+    host_pinned = torch.empty((W, W, 4), dtype=torch.float32).pin_memory().numpy()
+    for _ in range(2):
+        r.render(f, out=host_pinned)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        r.render(f, out=host_pinned)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
+    e2e = world * npix / (e2e_step * 1e-3) / 1e6
+    del host
+    gpu_launches = args.steps * (2 if path == "fp64" else 2)  # tracer + resolve per frame (spp_max = spp)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if path == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"synchrotron torus frame {W}x{W}, a=0.94, i=163 deg, fov +-12 M, 230 GHz, "
+                               f"512 Fourier modes, 1 sample/pixel", "path": path,
+                   "plain_fp64_mrays_s": round(fp64_mrays, 4), "image_rel_l1_vs_fp64": err_l1,
+                   "total_flux_err_vs_fp64": flux_err, "frames_per_s": round(1e3 / ms_step * world, 4),
+                   "l2": "256 MiB buffer written between timed steps", **norm,
+                   "attempts_per_ray": st.attempts / npix, "flow_steps_per_ray": st.flow_steps / npix},
+        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)",
+                     "kernel_ms": st.ms_kernel, "flops_per_launch": flops},
+        "e2e": {"value": round(e2e, 4), "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(so.abi.Frame),
+                "d2h_bytes_per_step": W * W * 16},
+        "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(so, sh, f, W, budget_s=args.cpu_seconds)
+    r.close()
+    return line
+
+
+def has_mixed(so, r):
+    try:
+        r.set_precision(so.abi.SO_PREC_MIXED)
+        ok = True
+    except so.TracerError:
+        ok = False
+    r.set_precision(so.abi.SO_PREC_FP64)
+    return ok and os.path.exists(os.path.join(PKG_DIR, "libso_tracer.so"))
+
+
+def _sample_pixels(so, f, W, n):
+    X, Y = so.pixel_centres(f, W, W)
+    idx = np.linspace(0, W * W - 1, n).astype(np.int64)
+    return X[idx], Y[idx]
+
+
+def cpu_baseline(so, sh, f, W, budget_s=15.0):
+    """The oracle port (the reference's algorithm restated in C, same torus workload) on the host cores,
+    over a bounded, evenly strided sample of the frame's pixels."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    threads = os.cpu_count() or 1
+    p = sh.plasma()
+    modes = so.plasma_modes(p)
+    n = 256
+    t0 = time.perf_counter()
+    x, y = _sample_pixels(so, f, W, n)
+    _oracle.orc_trace(sh.scene, f, x, y, plasma=p, modes=modes, threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(max(n * budget_s / max(dt, 1e-3), n), 2_000_000))
+    x, y = _sample_pixels(so, f, W, n2)
+    t0 = time.perf_counter()
+    _oracle.orc_trace(sh.scene, f, x, y, plasma=p, modes=modes, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(n2 / dt / 1e6, 6), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"{n2} evenly strided pixel centres of the {W}x{W} frame, oracle/so_oracle.c, "
+                      f"{threads} threads, {dt:.1f} s"}
+
+
+def run_reference(args, so):
+    """The reference's own trace_ray (oracle/_ref/libbhref.so, built from the reference sources) on
+    this workload's geometry with the reference's own hot-flow model (the torus plasma and its
+    Fourier turbulence are not part of the reference), all host threads, bounded samples."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    if not _oracle.have_ref():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libbhref.so was not built (reference tree absent)"}
+    W = args.size
+    path = os.path.join(PKG_DIR, "shots", "synchrotron_1024.ini")
+    R = _oracle.RefShot(path, [f"camera.width={W}", f"camera.height={W}", "flow.n_index=1.5",
+                               "flow.theta0=16.86", "flow.h_over_r=0.3", "flow.keplerian_fraction=0.8",
+                               "flow.turbulence=0.3", "flow.n0=1e6"])
+    f = R.frame(0)
+    threads = os.cpu_count() or 1
+    X, Y = so.pixel_centres(f, W, W)
+    n = 256
+    idx = np.linspace(0, W * W - 1, n).astype(np.int64)
+    t0 = time.perf_counter()
+    _oracle.ref_trace(R.scene, f, X[idx], Y[idx], threads=threads)
+    dt = time.perf_counter() - t0
+    per_step = max(10.0, min(30.0, 90.0 / max(args.steps + args.warmup, 1)))
+    n2 = int(min(max(n * per_step / max(dt, 1e-3), n), W * W))
+    idx = np.linspace(0, W * W - 1, n2).astype(np.int64)
+    for _ in range(min(args.warmup, 1)):
+        _oracle.ref_trace(R.scene, f, X[idx[:256]], Y[idx[:256]], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _oracle.ref_trace(R.scene, f, X[idx], Y[idx], threads=threads)
+        times.append(time.perf_counter() - t0)
+    v = n2 / float(np.mean(times)) / 1e6
+    return {"metric": METRIC, "value": round(v, 6), "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(float(np.mean(times)) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"synchrotron frame {W}x{W}, a=0.94, i=163 deg, fov +-12 M, 230 GHz, "
+                                   "reference flow model (n ~ r^-1.5, Theta 16.86 (r)^-0.84, h/r 0.3, fBm turbulence "
+                                   "rms 0.3)", "path": "reference host FP64"},
+            "cpu_baseline": {"value": round(v, 6), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                             "sample": f"{n2} evenly strided pixel centres per step, reference trace_ray "
+                                       f"(oracle/_ref), {threads} threads"},
+            "e2e": {"value": round(v, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--path", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    so = load_package()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, so)), flush=True)
+        return 0
+    world, rank, local = dist_setup()
+    line = run_ours(args, so, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

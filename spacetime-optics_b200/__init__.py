@@ -1,0 +1,272 @@
+"""spacetime-optics_b200: B200-native Kerr ray tracer (the per-pixel tracer path of bhrt).
+
+The product is the shared library ``libso_tracer.so`` (CUDA kernels for sm_100a plus the C ABI of
+include/so_tracer.h).  This module is a thin ctypes binding over that ABI, mirroring the
+reference's Renderer (blackholes/src/renderer.hpp:72-88) and shot builders so that callers and
+tests read like the reference's own code.  There is no CPU fallback: if the library or a CUDA
+device is missing, every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import (Frame, HdrFrame, MixedOpts, Mode, Plasma, Post, RaysOut, Scene, SceneInfo, Settings, Stats,
+                  Tables)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libso_tracer.so")
+SHOTS = os.path.join(HERE, "shots")
+
+_lib = None
+
+
+class TracerError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """The loaded tracer library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TracerError(abi.SO_ERR_NO_DEVICE, f"{LIB_PATH} missing: build it first (__graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        vp = C.c_void_p
+        L.so_init.argtypes = [P(vp), C.c_int, P(Scene), P(Tables), P(Settings)]
+        L.so_update_scene.argtypes = [vp, P(Scene)]
+        L.so_render.argtypes = [vp, P(Frame), P(Post), C.c_double, P(HdrFrame), P(Stats)]
+        L.so_render_device.argtypes = [vp, P(Frame), vp, P(Stats)]
+        L.so_probe_fma_peak.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
+        L.so_radio_flux.argtypes = [vp, P(Frame), C.c_int, C.c_double, P(C.c_double)]
+        L.so_trace_rays.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
+        L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
+        L.so_set_precision.argtypes = [vp, C.c_int, P(MixedOpts)]
+        L.so_set_plasma.argtypes = [vp, P(Plasma), P(Mode)]
+        L.so_stream.argtypes = [vp]
+        L.so_stream.restype = vp
+        L.so_last_error.argtypes = [vp]
+        L.so_last_error.restype = C.c_char_p
+        L.so_destroy.argtypes = [vp]
+        L.so_destroy.restype = None
+        L.so_shot_load.argtypes = [C.c_char_p, P(C.c_char_p), C.c_int, P(vp)]
+        L.so_shot_scene.argtypes = [vp, P(Scene), P(Tables), P(SceneInfo)]
+        L.so_shot_settings.argtypes = [vp, P(Settings)]
+        L.so_shot_nframes.argtypes = [vp]
+        L.so_shot_frame.argtypes = [vp, C.c_int, C.c_int, C.c_uint32, P(Frame)]
+        L.so_find_critical_point.argtypes = [vp, C.c_int, C.c_double, C.c_double, P(C.c_double)]
+        L.so_shot_get.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
+        L.so_shot_free.argtypes = [vp]
+        L.so_shot_free.restype = None
+        L.so_normalize_flux.argtypes = [vp, P(Scene), P(Frame), C.c_int, C.c_double, C.c_double, P(C.c_double),
+                                        P(C.c_double)]
+        L.so_plasma_modes.argtypes = [P(Plasma), P(Mode)]
+        L.so_kerr_point_at.argtypes = [C.c_double, C.c_double, C.c_double, P(abi.KerrPoint)]
+        L.so_kerr_point_at.restype = None
+        L.so_critical_curve_point.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double), P(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def _check(rc, handle=None):
+    if rc != abi.SO_OK:
+        msg = lib().so_last_error(handle).decode(errors="replace")
+        raise TracerError(rc, msg)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Shot:
+    """A shot .ini (reference schema plus the [so] section), with --set style overrides."""
+
+    def __init__(self, path, overrides=()):
+        if not os.path.isabs(path) and not os.path.exists(path):
+            path = os.path.join(SHOTS, path)
+        self.path = path
+        arr = (C.c_char_p * max(1, len(overrides)))(*[s.encode() for s in overrides])
+        h = C.c_void_p()
+        rc = lib().so_shot_load(path.encode(), arr, len(overrides), C.byref(h))
+        if rc != abi.SO_OK:
+            raise TracerError(rc, f"cannot load shot {path}")
+        self.h = h
+        self.scene = Scene()
+        self.tables = Tables()
+        self.info = SceneInfo()
+        _check(lib().so_shot_scene(self.h, C.byref(self.scene), C.byref(self.tables), C.byref(self.info)))
+        self.settings = Settings()
+        _check(lib().so_shot_settings(self.h, C.byref(self.settings)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.so_shot_free(self.h)
+            self.h = None
+
+    def nframes(self):
+        return lib().so_shot_nframes(self.h)
+
+    def frame(self, i=0, W=None, seed=None):
+        f = Frame()
+        W = self.settings.W if W is None else W
+        seed = (0x9E3779B9 * (i + 1)) & 0xFFFFFFFF if seed is None else seed  # main.cpp:529
+        _check(lib().so_shot_frame(self.h, i, W, seed, C.byref(f)))
+        f.W, f.H, f.spp = self.settings.W, self.settings.H, self.settings.spp
+        return f
+
+    def get(self, key, default=None):
+        buf = C.create_string_buffer(4096)
+        if lib().so_shot_get(self.h, key.encode(), buf, 4096) != abi.SO_OK:
+            return default
+        return buf.value.decode()
+
+    def num(self, key, default):
+        v = self.get(key)
+        try:
+            return float(v) if v is not None else default
+        except ValueError:
+            return default
+
+    def find_critical_point(self, psi, i=0):
+        rho = C.c_double()
+        _check(lib().so_find_critical_point(self.h, i, self.scene.a, psi, C.byref(rho)))
+        return rho.value
+
+    def plasma(self):
+        """The [so] torus plasma of this shot, or None (reference flow model)."""
+        if self.get("so.plasma", "reference") != "torus":
+            return None
+        p = Plasma()
+        p.model = abi.SO_PLASMA_TORUS
+        p.ne_index = self.num("so.ne_index", 1.5)
+        p.te0_kelvin = self.num("so.te0_kelvin", 1e11)
+        p.te_index = self.num("so.te_index", 0.84)
+        p.h_sph = self.num("so.h_sph", 0.3)
+        p.n_modes = int(self.num("so.modes", 512))
+        p.turb_rms = self.num("so.turb_rms", 0.3)
+        p.k_min = self.num("so.k_min", 2 * np.pi / 20)
+        p.k_max = self.num("so.k_max", 2 * np.pi / 0.5)
+        p.spectral_index = self.num("so.spectral_index", -11.0 / 3.0)
+        p.turb_seed = int(self.num("so.turb_seed", 1))
+        return p
+
+
+def plasma_modes(p):
+    """Fourier modes of a torus plasma (so_plasma_modes), as a ctypes array of Mode."""
+    arr = (Mode * max(1, p.n_modes))()
+    _check(lib().so_plasma_modes(C.byref(p), arr))
+    return arr
+
+
+def modes_to_numpy(arr, n):
+    return np.ctypeslib.as_array(C.cast(arr, C.POINTER(C.c_double)), shape=(n, 5)).copy()
+
+
+class Renderer:
+    """Renderer (render.cu:477-809) through the C ABI."""
+
+    def __init__(self, scene, tables, settings, device=0):
+        h = C.c_void_p()
+        rc = lib().so_init(C.byref(h), device, C.byref(scene), C.byref(tables), C.byref(settings))
+        if rc != abi.SO_OK:
+            raise TracerError(rc, lib().so_last_error(None).decode(errors="replace"))
+        self.h = h
+        self.settings = settings
+        self.scene = scene
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().so_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update_scene(self, scene):
+        self.scene = scene
+        _check(lib().so_update_scene(self.h, C.byref(scene)), self.h)
+
+    def set_plasma(self, plasma, modes=None):
+        if plasma is None:
+            plasma = Plasma()
+            plasma.model = abi.SO_PLASMA_REFERENCE
+        if modes is None and plasma.model == abi.SO_PLASMA_TORUS and plasma.n_modes > 0:
+            modes = plasma_modes(plasma)
+        _check(lib().so_set_plasma(self.h, C.byref(plasma), modes), self.h)
+        return modes
+
+    def set_precision(self, precision, band_m=0.05, tol32=1e-6, turn_frac=1e-3, drift_tol=1e-6):
+        o = MixedOpts(band_m, tol32, turn_frac, drift_tol)
+        _check(lib().so_set_precision(self.h, precision, C.byref(o)), self.h)
+
+    def render(self, frame, percentile=0.995, hide_direct=0.0, out=None):
+        W, H = self.settings.W, self.settings.H
+        if out is None:
+            out = np.empty((H, W, 4), np.float32)
+        hdr = HdrFrame(W, H, out.ctypes.data_as(C.POINTER(C.c_float)), 0.0, 0.0)
+        st = Stats()
+        post = Post(0.0, 0.0, hide_direct)
+        _check(lib().so_render(self.h, C.byref(frame), C.byref(post), percentile, C.byref(hdr), C.byref(st)), self.h)
+        return out, hdr, st
+
+    def render_device(self, frame, d_px, stats=False):
+        """Trace into caller-owned device memory (an address, e.g. torch tensor.data_ptr()).  Without
+        stats the call is asynchronous on self.stream()."""
+        st = Stats() if stats else None
+        _check(lib().so_render_device(self.h, C.byref(frame), C.c_void_p(d_px), C.byref(st) if st else None),
+               self.h)
+        return st
+
+    def stream(self):
+        """The renderer's CUDA stream handle (cudaStream_t as an int)."""
+        return lib().so_stream(self.h)
+
+    def radio_flux(self, frame, n, pix_sr):
+        jy = C.c_double()
+        _check(lib().so_radio_flux(self.h, C.byref(frame), n, pix_sr, C.byref(jy)), self.h)
+        return jy.value
+
+    def trace_rays(self, frame, x, y, cross=False):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.ascontiguousarray(y, np.float64)
+        n = x.size
+        o = dict(fate=np.zeros(n, np.int8), ncross=np.zeros(n, np.int8), theta=np.zeros(n), phi=np.zeros(n),
+                 I=np.zeros((n, 4), np.float32), n_accepted=np.zeros(n, np.int32), n_attempts=np.zeros(n, np.int32))
+        if cross:
+            o["cross_r"] = np.zeros((n, 3))
+            o["cross_g"] = np.zeros((n, 3))
+        ro = RaysOut(*[_ptr(o.get(k)) for k in ("fate", "ncross", "theta", "phi", "I", "n_accepted", "n_attempts",
+                                                 "cross_r", "cross_g")])
+        _check(lib().so_trace_rays(self.h, C.byref(frame), n, _ptr(x), _ptr(y), C.byref(ro)), self.h)
+        return o
+
+    def normalize_flux(self, scene, frame_wide, n, pix_sr, target_jy):
+        n0 = C.c_double()
+        jy = C.c_double()
+        _check(lib().so_normalize_flux(self.h, C.byref(scene), C.byref(frame_wide), n, pix_sr, target_jy,
+                                       C.byref(n0), C.byref(jy)), self.h)
+        self.scene = scene
+        return n0.value, jy.value
+
+
+def probe_fma_peak(device=0):
+    """Measured FP64 and FP32 FMA-pipe peaks of the device, TFLOP/s (so_probe_fma_peak)."""
+    a, b = C.c_double(), C.c_double()
+    _check(lib().so_probe_fma_peak(device, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def pixel_centres(frame, W, H):
+    """Tangent-plane coordinates of the pixel centres of a W x H frame (render.cu:79-80, jitter 1/2)."""
+    px = np.arange(W, dtype=np.float64)
+    py = np.arange(H, dtype=np.float64)
+    X = (px[None, :] + 0.5 - 0.5 * W) * frame.pix
+    Y = (0.5 * H - (py[:, None] + 0.5)) * frame.pix
+    return np.broadcast_to(X, (H, W)).ravel().copy(), np.broadcast_to(Y, (H, W)).ravel().copy()

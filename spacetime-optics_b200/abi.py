@@ -1,0 +1,133 @@
+"""ctypes mirror of include/so_tracer.h (the C ABI of the tracer library).
+
+The struct layouts follow the header field for field; so_scene / so_frame in turn follow the
+reference's SceneGPU / FrameGPU (blackholes/src/scene.hpp:12-80), which tests check against the
+reference's own offsets.
+"""
+import ctypes as C
+
+SO_OK = 0
+SO_ERR_ARG, SO_ERR_CUDA, SO_ERR_ALLOC, SO_ERR_CONFIG, SO_ERR_NO_DEVICE = 1, 2, 3, 4, 5
+SO_ERR_STATE, SO_ERR_WATCHDOG, SO_ERR_SIZE, SO_ERR_UNSUPPORTED = 6, 7, 8, 9
+SO_MODE_VISIBLE, SO_MODE_RADIO = 0, 1
+SO_FATE_LIMIT, SO_FATE_ESCAPED, SO_FATE_CAPTURED = 0, 1, -1
+SO_PREC_FP64, SO_PREC_MIXED = 0, 1
+SO_PLASMA_REFERENCE, SO_PLASMA_TORUS = 0, 1
+SO_MAX_MODES = 1024
+
+
+class Vec3(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+class Mat3(C.Structure):
+    _fields_ = [("r0", Vec3), ("r1", Vec3), ("r2", Vec3)]
+
+
+class KerrPoint(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("r", "s", "c", "Sigma", "Delta", "A", "omega", "e_nu", "e_psi", "sqrtSigma", "sqrtSigmaDelta")]
+
+
+class Scene(C.Structure):
+    _fields_ = [
+        ("a", C.c_double), ("rh", C.c_double), ("r_isco", C.c_double), ("tol", C.c_double),
+        ("max_steps", C.c_int), ("r_escape", C.c_double), ("r_stop", C.c_double), ("step_frac", C.c_double),
+        ("mode", C.c_int),
+        ("disk_on", C.c_int), ("disk_rin", C.c_double), ("disk_rout", C.c_double),
+        ("disk_lnT", C.POINTER(C.c_float)), ("disk_n", C.c_int), ("disk_lr0", C.c_double), ("disk_dlr", C.c_double),
+        ("disk_turb_amp", C.c_float), ("disk_turb_scale", C.c_float), ("disk_tcorr", C.c_float),
+        ("disk_ld", C.c_float), ("disk_fcol", C.c_float), ("disk_plunge", C.c_float),
+        ("flow_on", C.c_int), ("n0", C.c_double), ("n_index", C.c_double), ("theta_index", C.c_double),
+        ("theta0", C.c_double), ("h_r", C.c_double), ("beta_p", C.c_double), ("r_flow_max", C.c_double),
+        ("nu_obs", C.c_double), ("rg_cm", C.c_double), ("flow_kep", C.c_double),
+        ("flow_turb_amp", C.c_float), ("flow_turb_scale", C.c_float), ("flow_tcorr", C.c_float),
+        ("turb_tex", C.c_ulonglong * 24), ("turb_nt", C.c_int),
+        ("turb_lr0", C.c_float), ("turb_lr1", C.c_float), ("turb_zmax", C.c_float), ("turb_d0", C.c_float),
+        ("turb_dd", C.c_float),
+        ("k2_lntab", C.POINTER(C.c_float)), ("k2_n", C.c_int), ("k2_l0", C.c_float), ("k2_dl", C.c_float),
+        ("sky_on", C.c_int), ("sky_tex", C.c_ulonglong), ("sky_scale", C.c_float), ("sky_rot", Mat3),
+        ("bb_xyz", C.POINTER(C.c_float)), ("bb_n", C.c_int), ("bb_l0", C.c_float), ("bb_dl", C.c_float),
+        ("seed", C.c_uint32),
+    ]
+
+
+class Frame(C.Structure):
+    _fields_ = [
+        ("r", C.c_double), ("th", C.c_double), ("ph", C.c_double), ("t", C.c_double), ("kp", KerrPoint),
+        ("F", Vec3), ("R", Vec3), ("U", Vec3), ("beta", Vec3), ("cx", C.c_double), ("cy", C.c_double),
+        ("pix", C.c_double), ("W", C.c_int), ("H", C.c_int), ("spp", C.c_int), ("seed", C.c_uint32),
+    ]
+
+
+class Tables(C.Structure):
+    _fields_ = [("disk_lnT", C.POINTER(C.c_float)), ("disk_n", C.c_int),
+                ("k2_ln", C.POINTER(C.c_float)), ("k2_n", C.c_int),
+                ("bb_xyz", C.POINTER(C.c_float)), ("bb_n", C.c_int)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("spp", C.c_int), ("spp_max", C.c_int), ("target_err", C.c_float)]
+
+
+class Post(C.Structure):
+    _fields_ = [("bloom", C.c_float), ("blur_sigma_px", C.c_double), ("hide_direct", C.c_float)]
+
+
+class HdrFrame(C.Structure):
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("px", C.POINTER(C.c_float)),
+                ("lum_percentile", C.c_double), ("lum_max", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_trace", C.c_double), ("ms_post", C.c_double), ("samples", C.c_longlong),
+                ("step_limited", C.c_longlong), ("attempts", C.c_longlong), ("accepted", C.c_longlong),
+                ("fp64_rays", C.c_longlong), ("flow_steps", C.c_longlong), ("ms_kernel", C.c_double)]
+
+
+class RaysOut(C.Structure):
+    _fields_ = [("fate", C.c_void_p), ("ncross", C.c_void_p), ("theta", C.c_void_p), ("phi", C.c_void_p),
+                ("I", C.c_void_p), ("n_accepted", C.c_void_p), ("n_attempts", C.c_void_p),
+                ("cross_r", C.c_void_p), ("cross_g", C.c_void_p)]
+
+
+class Plasma(C.Structure):
+    _fields_ = [("model", C.c_int), ("ne_index", C.c_double), ("te0_kelvin", C.c_double), ("te_index", C.c_double),
+                ("h_sph", C.c_double), ("n_modes", C.c_int), ("turb_rms", C.c_double), ("k_min", C.c_double),
+                ("k_max", C.c_double), ("spectral_index", C.c_double), ("turb_seed", C.c_uint32)]
+
+
+class Mode(C.Structure):
+    _fields_ = [("kx", C.c_double), ("ky", C.c_double), ("kz", C.c_double), ("phase", C.c_double),
+                ("amp", C.c_double)]
+
+
+class MixedOpts(C.Structure):
+    _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_frac", C.c_double), ("drift_tol", C.c_double)]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("mass_msun", "distance_cm", "rg_cm", "tg_s", "uas_per_m", "disk_tmax",
+                                          "disk_mdot_edd", "radio_flux_target_jy")]
+
+
+# Field names of so_scene / so_frame whose offsets the reference layout check compares, in the order
+# oracle/ref_shim.cpp's ref_layout() reports them (after the two sizeofs).
+LAYOUT_FIELDS = [
+    (Scene, "tol"), (Scene, "max_steps"), (Scene, "r_escape"), (Scene, "mode"), (Scene, "disk_on"),
+    (Scene, "disk_lnT"), (Scene, "disk_turb_amp"), (Scene, "disk_plunge"), (Scene, "flow_on"), (Scene, "n0"),
+    (Scene, "flow_kep"), (Scene, "flow_turb_amp"), (Scene, "turb_tex"), (Scene, "turb_nt"), (Scene, "turb_dd"),
+    (Scene, "k2_lntab"), (Scene, "k2_n"), (Scene, "k2_dl"), (Scene, "sky_on"), (Scene, "sky_tex"),
+    (Scene, "sky_rot"), (Scene, "bb_xyz"), (Scene, "bb_dl"), (Scene, "seed"), (Frame, "kp"), (Frame, "F"),
+    (Frame, "beta"), (Frame, "cx"), (Frame, "pix"), (Frame, "W"), (Frame, "spp"), (Frame, "seed"),
+]
+
+# Every entry point include/so_tracer.h declares (checked against the built library's exports).
+EXPORTS = [
+    "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
+    "so_trace_rays_device", "so_probe_fma_peak",
+    "so_set_precision", "so_set_plasma", "so_stream", "so_last_error", "so_destroy",
+    "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
+    "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",
+    "so_kerr_point_at", "so_critical_curve_point",
+]

@@ -1,0 +1,58 @@
+// k_probe.cu -- FMA-pipe peak probe: the measured denominator of the tracers' roofline.
+// Every thread runs 8 independent FMA chains (enough instruction-level parallelism to hide the
+// pipe latency), on 8 CTAs of 256 threads per SM, and the kernel is timed with CUDA events.
+#include <cuda_runtime.h>
+
+#include "../../include/so_tracer.h"
+
+namespace {
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_chains(T* out, int iters, T a, T b) {
+    T x0 = (T)threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == (T)-12345.678) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+template <typename T>
+int probe(int nsm, int iters, double* tflops) {
+    T* out = nullptr;
+    if (cudaMalloc(&out, 256 * sizeof(T)) != cudaSuccess) return SO_ERR_ALLOC;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = nsm * 8;
+    k_fma_chains<T><<<blocks, 256>>>(out, iters / 4, (T)0.999999, (T)1e-7);  // warm-up
+    cudaEventRecord(e0);
+    k_fma_chains<T><<<blocks, 256>>>(out, iters, (T)0.999999, (T)1e-7);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess || ms <= 0.f) return SO_ERR_CUDA;
+    double flops = 2.0 * 8.0 * 16.0 * (double)iters * blocks * 256.0;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return SO_OK;
+}
+}  // namespace
+
+extern "C" int so_probe_fma_peak(int device, double* fp64_tflops, double* fp32_tflops) {
+    if (!fp64_tflops || !fp32_tflops) return SO_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return SO_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return SO_ERR_CUDA;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    int rc = probe<double>(nsm, 2000, fp64_tflops);
+    if (!rc) rc = probe<float>(nsm, 4000, fp32_tflops);
+    return rc;
+}

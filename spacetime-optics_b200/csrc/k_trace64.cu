@@ -1,0 +1,382 @@
+// k_trace64.cu -- plain FP64 tracer: the drop-in path, bit-reproducible against the CPU oracle.
+//
+// Reference: trace_ray (blackholes/src/trace.cuh:62-165) run per sample by k_pass1 / k_pass2
+// (blackholes/src/render.cu:89-128, 196-224), which give one CUDA thread one pixel for all its
+// samples.  Step counts differ by 100x between neighbouring pixels near the critical curve, so a
+// fixed thread-to-pixel map leaves most lanes of a warp idle behind the slowest ray.
+//
+// Here the kernel is persistent: a grid sized to fill the SMs once, each lane owning one ray (or one
+// pixel and its samples) at a time.  A lane whose ray retires takes the next one from a global
+// queue head; lanes needing work are found with a warp vote (__ballot_sync) and served by a single
+// warp-aggregated atomicAdd.  One loop iteration is one DP5(4) attempt for every active lane, so
+// lanes stay converged through the stepper and diverge only in the short accept / emission code.
+// The loop ends when the queue is empty and every lane has retired; each ray is bounded by
+// max_steps attempts, so there is no unbounded wait anywhere.
+//
+// Compiled with -fmad=false: every fusion is an explicit fma() (so_kerr.cuh), matching the oracle.
+#include <cuda_runtime.h>
+
+#include "so_emission.cuh"
+#include "so_launch.h"
+
+namespace so {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+struct Ray64 {
+    RayC c;
+    double y[6], k1[6];
+    double h, trans, psi;
+    double pp0, pp1, pp2;
+    float acc[4];
+    int ncross, nacc, natt, it, nflow;
+};
+
+__device__ __forceinline__ void pixel_point(const TraceLaunch& L, const so_frame& F, long long q, int s, double* x,
+                                            double* yv) {  // s: absolute sample index
+    int px = (int)(q % L.W), py = (int)(q / L.W);
+    float jx = 0.5f, jy = 0.5f;
+    if (L.jitter) {
+        uint32_t h = pcg((uint32_t)q * 0x9E3779B9u ^ F.seed);  // pixel_seed, render.cu:70-74
+        float r0 = rnd(h), r1 = rnd(h);
+        r2_sample((uint32_t)s, r0, r1, &jx, &jy);
+    }
+    *x = (px + jx - 0.5 * L.W) * F.pix;  // sample_pixel, render.cu:79-80
+    *yv = (0.5 * L.H - (py + jy)) * F.pix;
+}
+
+template <int VAR>
+__device__ __forceinline__ void ray_init(Ray64& R, const so_scene& S, const so_frame& F, double x, double yv) {
+    so_vec3 d = view_dir(F, x, yv);
+    camera_photon(S.a, F.kp, F.ph, F.t, d, F.beta, R.c, R.y);
+    rhs(R.c, R.y, R.k1);
+    R.h = initial_step(R.y);
+    R.trans = 1.0;
+    R.psi = 0.0;
+    R.ncross = R.nacc = R.natt = R.it = R.nflow = 0;
+    R.acc[0] = R.acc[1] = R.acc[2] = R.acc[3] = 0.f;
+    if (VAR == VAR_RADIO) {
+        double sp = sqrt(fmax(fma(-R.y[2], R.y[2], 1.0), 0.0));
+        double s4, c4;
+        sincos(R.y[4], &s4, &c4);
+        R.pp0 = sp * c4;
+        R.pp1 = sp * s4;
+        R.pp2 = R.y[2];
+    }
+}
+
+// One loop iteration of trace_ray (trace.cuh:81-163).  Returns 1 when the ray is finished and sets
+// fate (and the escape angles for escaped rays).
+template <int VAR>
+__device__ __forceinline__ int ray_step(Ray64& R, const so_scene& S, const TorusParams& tp, const ModesSmem& md,
+                                        double rcam, int* fate, double* th, double* ph, double* cross_r,
+                                        double* cross_g) {
+    if (R.it >= S.max_steps) {
+        *fate = 0;
+        return 1;
+    }
+    ++R.it;
+    double hc = R.h;
+    if (VAR == VAR_RADIO && S.flow_on && R.y[0] < S.r_flow_max) {
+        double s = sqrt(fmax(fma(-R.y[2], R.y[2], 1.0), 0.0));
+        double cap = S.step_frac * fmin(R.y[0] / (fabs(R.y[1]) + 1e-30), fmax(s, 0.05) / (fabs(R.y[3]) + 1e-30));
+        hc = fmin(hc, cap);
+    } else if (VAR != VAR_VACUUM && S.disk_on) {
+        hc = fmin(hc, 0.3 / (fabs(R.y[3]) + 1e-30));
+    }
+    ++R.natt;
+    double yn[6], k7[6];
+    double err = dp54(R.c, R.y, R.k1, hc, S.tol, yn, k7);
+    if (!(err <= 1.0)) {
+        R.h = reject_step(hc, err);
+        return 0;
+    }
+    ++R.nacc;
+    if (VAR == VAR_RADIO) {
+        double sn = sqrt(fmax(fma(-yn[2], yn[2], 1.0), 0.0));
+        double s4, c4;
+        sincos(yn[4], &s4, &c4);
+        double pn0 = sn * c4, pn1 = sn * s4, pn2 = yn[2];
+        double cx = fma(R.pp1, pn2, -(R.pp2 * pn1));
+        double cy = fma(R.pp2, pn0, -(R.pp0 * pn2));
+        double cz = fma(R.pp0, pn1, -(R.pp1 * pn0));
+        double cc = fma(cz, cz, fma(cy, cy, cx * cx));
+        double dd = fma(R.pp2, pn2, fma(R.pp1, pn1, R.pp0 * pn0));
+        R.psi += atan2(sqrt(cc), dd);
+        R.pp0 = pn0;
+        R.pp1 = pn1;
+        R.pp2 = pn2;
+    }
+    if ((R.y[2] > 0.0) != (yn[2] > 0.0)) {
+        ++R.ncross;
+        const bool rec = cross_r != nullptr && R.ncross <= 3;
+        const bool disk = VAR != VAR_VACUUM && S.disk_on;
+        if (disk || rec) {
+            double lo = 0.0, hi = 1.0, u0 = R.y[2], u1 = yn[2], m0 = R.y[3] * hc, m1 = yn[3] * hc;
+            for (int b = 0; b < 40; ++b) {
+                double mid = 0.5 * (lo + hi);
+                double um = hermite(u0, u1, m0, m1, mid);
+                if ((um > 0.0) == (u0 > 0.0)) lo = mid;
+                else hi = mid;
+            }
+            double sc = 0.5 * (lo + hi);
+            double rc = hermite(R.y[0], yn[0], R.y[1] * hc, yn[1] * hc, sc);
+            if (rec) {
+                cross_r[R.ncross - 1] = rc;
+                cross_g[R.ncross - 1] = crossing_g(S, rc, R.c.lam, R.c.E);
+            }
+            if (disk) {
+                double pc = hermite(R.y[4], yn[4], R.k1[4] * hc, k7[4] * hc, sc);
+                double tc = hermite(R.y[5], yn[5], R.k1[5] * hc, k7[5] * hc, sc);
+                float cs[4];
+                disk_shade(S, rc, pc, tc, R.c.lam, R.c.eta, R.c.E, cs);
+                if (cs[3] > 0.f) {
+                    float tf = (float)R.trans;
+                    R.acc[0] += tf * cs[0];
+                    R.acc[1] += tf * cs[1];
+                    R.acc[2] += tf * cs[2];
+                    R.acc[3] += tf * cs[1] * (float)(R.ncross - 1);
+                    R.trans *= 1.0 - cs[3];
+                    if (R.trans < 1e-4) {
+                        *fate = -1;
+                        return 1;
+                    }
+                }
+            }
+        }
+    }
+    if (VAR == VAR_RADIO && S.flow_on && yn[0] < S.r_flow_max) {
+        double dI, dtau;
+        flow_step(S, tp, md, rcam, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+        float cc = (float)(R.trans * dI);
+        int n = (int)(R.psi * (1.0 / PI));
+        R.acc[0] += cc;
+        if (n == 1) R.acc[1] += cc;
+        else if (n == 2) R.acc[2] += cc;
+        else if (n >= 3) R.acc[3] += cc;
+        ++R.nflow;
+        R.trans *= exp(-dtau);
+        if (R.trans < 1e-5) {
+            *fate = -1;
+            return 1;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        R.y[i] = yn[i];
+        R.k1[i] = k7[i];
+    }
+    project_radial(R.c, R.y, R.k1);
+    R.h = accept_step(hc, err);
+    if (R.y[0] < S.r_stop) {
+        *fate = -1;
+        return 1;
+    }
+    if (R.y[0] > S.r_escape && R.y[1] > 0.0) {
+        *fate = 1;
+        escape_angles(R.y, R.k1, th, ph);
+        return 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    return v;
+}
+
+}  // namespace
+
+template <int VAR>
+__global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
+    extern __shared__ double smem[];
+    TorusParams tp;
+    tp.on = VAR == VAR_RADIO && L.torus;
+    tp.n_modes = L.n_modes;
+    tp.ne_index = L.ne_index;
+    tp.te_index = L.te_index;
+    tp.h_sph = L.h_sph;
+    tp.theta_e0 = L.theta_e0;
+    tp.half_var = L.half_var;
+    ModesSmem md = {smem, smem + L.n_modes, smem + 2 * L.n_modes, smem + 3 * L.n_modes, smem + 4 * L.n_modes};
+    if (VAR == VAR_RADIO && tp.on) {
+        // Stage the mode table once per CTA (SoA in shared memory, all lanes then read one mode at a
+        // time: a broadcast).
+        for (int i = threadIdx.x; i < L.n_modes; i += blockDim.x) {
+            so_mode m = L.modes[i];
+            smem[i] = m.kx;
+            smem[L.n_modes + i] = m.ky;
+            smem[2 * L.n_modes + i] = m.kz;
+            smem[3 * L.n_modes + i] = m.phase;
+            smem[4 * L.n_modes + i] = m.amp;
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const long long total = L.nrays;
+    long long job = 0, pix = 0;
+    int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
+    bool active = false, exhausted = false;
+    Ray64 R;
+    float pa[4] = {0.f, 0.f, 0.f, 0.f};
+    float ys = 0.f, yq = 0.f;
+    double cr[3], cg[3];
+    unsigned long long n_att = 0, n_acc = 0, n_lim = 0, n_flow = 0;
+    const so_scene* S = nullptr;
+    const so_frame* F = nullptr;
+    const bool radio_lum = VAR == VAR_RADIO;  // sample_lum, render.cu:87
+
+    for (;;) {
+        const bool need = !active && !exhausted;
+        const unsigned m = __ballot_sync(FULL, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&L.counters->next, (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, leader);
+            if (need) {
+                const unsigned long long j = base + __popc(m & ((1u << lane) - 1u));
+                if (j >= (unsigned long long)total) {
+                    exhausted = true;
+                } else {
+                    job = (long long)j;
+                    active = true;
+                    sample = 0;
+                    double x, yv;
+                    if (L.kind == RAYS_LIST) {
+                        fidx = 0;
+                        x = L.x[job];
+                        yv = L.y[job];
+                        jobs_n = 1;
+                    } else if (L.kind == RAYS_PIXELS) {
+                        const long long npix = (long long)L.W * L.H;
+                        fidx = (int)(job / npix);
+                        pix = job % npix;
+                        sbase = L.sample0;
+                        jobs_n = L.spp;
+                        pixel_point(L, L.frames[fidx], pix, sbase, &x, &yv);
+                    } else {
+                        // upper bound of job in the exclusive scan: the pixel owning chunk `job`
+                        long long lo = 0, hi = (long long)L.W * L.H;
+                        while (lo < hi) {
+                            long long mid = (lo + hi) >> 1;
+                            if ((long long)__ldg(L.offsets + mid) <= job) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        fidx = 0;
+                        pix = lo - 1;
+                        sbase = L.sample0 + (int)(job - (long long)__ldg(L.offsets + pix)) * L.chunk;
+                        jobs_n = L.chunk;
+                        pixel_point(L, L.frames[0], pix, sbase, &x, &yv);
+                    }
+                    S = &L.scenes[L.frame_scene[fidx]];
+                    F = &L.frames[fidx];
+                    pa[0] = pa[1] = pa[2] = pa[3] = 0.f;
+                    ys = yq = 0.f;
+                    cr[0] = cr[1] = cr[2] = 0.0;
+                    cg[0] = cg[1] = cg[2] = 0.0;
+                    ray_init<VAR>(R, *S, *F, x, yv);
+                }
+            }
+        }
+        if (__all_sync(FULL, !active)) break;
+        if (!active) continue;
+        int fate = 0;
+        double th = 0.0, ph = 0.0;
+        const bool rec = L.kind == RAYS_LIST && L.record_cross;
+        if (!ray_step<VAR>(R, *S, tp, md, F->r, &fate, &th, &ph, rec ? cr : nullptr, cg)) continue;
+        // sample finished
+        n_att += (unsigned long long)R.natt;
+        n_acc += (unsigned long long)R.nacc;
+        n_flow += (unsigned long long)R.nflow;
+        if (fate == 0) ++n_lim;
+        if (L.kind == RAYS_LIST) {
+            const so_rays_out& o = L.out;
+            if (o.fate) o.fate[job] = (int8_t)fate;
+            if (o.ncross) o.ncross[job] = (int8_t)(R.ncross > 127 ? 127 : R.ncross);
+            if (o.theta) o.theta[job] = fate == 1 ? th : 0.0;
+            if (o.phi) o.phi[job] = fate == 1 ? ph : 0.0;
+            if (o.I) reinterpret_cast<float4*>(o.I)[job] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
+            if (o.n_accepted) o.n_accepted[job] = R.nacc;
+            if (o.n_attempts) o.n_attempts[job] = R.natt;
+            if (o.cross_r) {
+                for (int c = 0; c < 3; ++c) {
+                    o.cross_r[3 * job + c] = cr[c];
+                    o.cross_g[3 * job + c] = cg[c];
+                }
+            }
+            active = false;
+        } else {
+            pa[0] += R.acc[0];
+            pa[1] += R.acc[1];
+            pa[2] += R.acc[2];
+            pa[3] += R.acc[3];
+            const float Y = radio_lum ? R.acc[0] : R.acc[1];
+            ys += Y;
+            yq += Y * Y;
+            if (++sample < jobs_n) {
+                double x, yv;
+                pixel_point(L, *F, pix, sbase + sample, &x, &yv);
+                ray_init<VAR>(R, *S, *F, x, yv);
+            } else if (L.kind == RAYS_PIXELS) {
+                reinterpret_cast<float4*>(L.accum)[job] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+                if (L.ystat) reinterpret_cast<float2*>(L.ystat)[job] = make_float2(ys, yq);
+                active = false;
+            } else {
+                reinterpret_cast<float4*>(L.chunk_acc)[job] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+                active = false;
+            }
+        }
+    }
+    n_att = warp_sum(n_att);
+    n_acc = warp_sum(n_acc);
+    n_lim = warp_sum(n_lim);
+    n_flow = warp_sum(n_flow);
+    if (lane == 0) {
+        atomicAdd(&L.counters->attempts, n_att);
+        atomicAdd(&L.counters->accepted, n_acc);
+        atomicAdd(&L.counters->step_limited, n_lim);
+        atomicAdd(&L.counters->flow_steps, n_flow);
+    }
+}
+
+// Host launcher: grid = SMs x resident CTAs per SM (persistent), dynamic shared memory for the
+// mode table.  Returns the CUDA error of the launch.
+cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaStream_t st) {
+    const int tpb = 128;
+    size_t smem = (variant == VAR_RADIO && L.torus) ? (size_t)5 * L.n_modes * sizeof(double) : 0;
+    int per_sm = 1;
+    cudaError_t e;
+    switch (variant) {
+        case VAR_VACUUM:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_VACUUM>, tpb, smem);
+            break;
+        case VAR_DISK:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_DISK>, tpb, smem);
+            break;
+        default:
+            if (smem > 48 * 1024) {
+                e = cudaFuncSetAttribute(k_trace64<VAR_RADIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+            }
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_RADIO>, tpb, smem);
+            break;
+    }
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long want = (L.nrays + tpb - 1) / tpb;
+    long long grid = (long long)num_sms * per_sm;
+    if (grid > want) grid = want;
+    if (grid < 1) grid = 1;
+    switch (variant) {
+        case VAR_VACUUM: k_trace64<VAR_VACUUM><<<(int)grid, tpb, smem, st>>>(L); break;
+        case VAR_DISK: k_trace64<VAR_DISK><<<(int)grid, tpb, smem, st>>>(L); break;
+        default: k_trace64<VAR_RADIO><<<(int)grid, tpb, smem, st>>>(L); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace so

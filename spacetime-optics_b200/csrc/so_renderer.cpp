@@ -1,0 +1,616 @@
+// so_renderer.cpp -- the Renderer of the reference (blackholes/src/renderer.hpp:72-88,
+// render.cu:477-809) behind the C ABI of include/so_tracer.h.
+//
+// Per frame (so_render, render.cu:677-730 + 755-795):
+//   frame descriptor -> device;  pass 1 (spp samples per pixel, persistent tracer kernel);
+//   adaptive pass 2 (k_adapt, k_dilate, single-pass scan, chunked samples, deterministic add);
+//   resolve;  device -> host copy of the HDR frame;  luminance percentile on the host.
+// Differences from the reference: every failure is a status code (no abort), reductions are
+// deterministic, per-frame scene data live in device memory (not __constant__), and there is no
+// sky texture / bloom / beam blur (outside this library: SO_ERR_UNSUPPORTED).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "so_kerr.cuh"
+#include "so_launch.h"
+
+namespace so {
+cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaStream_t st);
+cudaError_t launch_trace_mixed(const TraceLaunch& L, int variant, int num_sms, cudaStream_t st);
+cudaError_t launch_resolve(float4* img, const float4* accum, const uint32_t* nsamp, uint32_t nconst, long long npix,
+                           int visible, cudaStream_t st);
+cudaError_t launch_sum_channel(const float* v, int stride, long long n, double* part, double* out, int num_sms,
+                               cudaStream_t st);
+cudaError_t launch_adapt(const float2* ystat, uint32_t spp, long long npix, const double* fsum, double yscale,
+                         float target, int extra_max, uint32_t* extra, uint32_t* chunks, int W, int H, int chunk,
+                         cudaStream_t st);
+long long scan_tiles(long long n);
+cudaError_t launch_scan(const uint32_t* in, uint32_t* out, long long n, unsigned long long* tile_state,
+                        unsigned int* tile_counter, uint32_t* total, int* err, cudaStream_t st);
+cudaError_t launch_add_chunks(float4* accum, uint32_t* nsamp, const uint32_t* offsets, const uint32_t* chunks,
+                              const float4* chunk_acc, long long npix, int chunk, cudaStream_t st);
+cudaError_t launch_fill_u32(uint32_t* p, uint32_t v, long long n, cudaStream_t st);
+}  // namespace so
+
+using namespace so;
+
+namespace {
+constexpr int CHUNK = 8;  // samples per pass-2 job (render.cu:30)
+std::string g_init_error;
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+struct so_renderer {
+    int device = 0, num_sms = 148;
+    cudaStream_t st = nullptr;
+    so_scene S{};            // host copy, table pointers = device tables
+    so_settings rs{};
+    float *d_disk = nullptr, *d_k2 = nullptr, *d_bb = nullptr;
+    so_scene* d_scene = nullptr;
+    so_frame* d_frame = nullptr;
+    int* d_frame_scene = nullptr;
+    // frame buffers
+    long long npix = 0;
+    float4 *d_accum = nullptr, *d_img = nullptr, *d_chunk_acc = nullptr;
+    float2* d_ystat = nullptr;
+    uint32_t *d_nsamp = nullptr, *d_extra = nullptr, *d_chunks = nullptr, *d_offsets = nullptr, *d_total = nullptr;
+    unsigned long long* d_tiles = nullptr;
+    int* d_err = nullptr;
+    long long chunk_cap = 0;
+    double *d_part = nullptr, *d_fsum = nullptr;
+    Counters* d_cnt = nullptr;
+    // per-ray buffers of so_trace_rays (grown on demand)
+    long long ray_cap = 0;
+    double *d_x = nullptr, *d_y = nullptr;
+    void* d_rays = nullptr;  // packed outputs
+    // plasma / precision
+    so_plasma plasma{};
+    so_mode* d_modes = nullptr;
+    int precision = SO_PREC_FP64;
+    so_mixed_opts mixed{0.05, 1e-6, 1e-3, 1e-6};
+    std::string err;
+};
+
+namespace {
+
+int fail(so_renderer* r, int code, const std::string& msg) {
+    if (r) r->err = msg;
+    else g_init_error = msg;
+    return code;
+}
+int cuda_fail(so_renderer* r, cudaError_t e, const char* what) {
+    return fail(r, SO_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define SO_CK(r, x)                                      \
+    do {                                                 \
+        cudaError_t e_ = (x);                            \
+        if (e_ != cudaSuccess) return cuda_fail(r, e_, #x); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) {
+    return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+int variant_of(const so_scene& S) {
+    if (S.mode == SO_MODE_RADIO) return VAR_RADIO;
+    if (S.disk_on) return VAR_DISK;
+    return VAR_VACUUM;
+}
+
+void free_all(so_renderer* r) {
+    void* ps[] = {r->d_disk, r->d_k2, r->d_bb, r->d_scene, r->d_frame, r->d_frame_scene, r->d_accum, r->d_img,
+                  r->d_chunk_acc, r->d_ystat, r->d_nsamp, r->d_extra, r->d_chunks, r->d_offsets, r->d_total,
+                  r->d_tiles, r->d_err, r->d_part, r->d_fsum, r->d_cnt, r->d_x, r->d_y, r->d_rays, r->d_modes};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (r->st) cudaStreamDestroy(r->st);
+}
+
+int upload_scene(so_renderer* r) {
+    r->S.disk_lnT = r->d_disk;
+    r->S.k2_lntab = r->d_k2;
+    r->S.bb_xyz = r->d_bb;
+    SO_CK(r, cudaMemcpyAsync(r->d_scene, &r->S, sizeof(so_scene), cudaMemcpyHostToDevice, r->st));
+    return SO_OK;
+}
+
+// Fills the plasma / precision part of a launch descriptor.
+void launch_common(so_renderer* r, TraceLaunch& L) {
+    std::memset(&L, 0, sizeof L);
+    L.scenes = r->d_scene;
+    L.frames = r->d_frame;
+    L.frame_scene = r->d_frame_scene;
+    L.nframes = 1;
+    L.counters = r->d_cnt;
+    const so_plasma& p = r->plasma;
+    L.torus = p.model == SO_PLASMA_TORUS;
+    L.n_modes = L.torus ? p.n_modes : 0;
+    L.ne_index = p.ne_index;
+    L.te_index = p.te_index;
+    L.h_sph = p.h_sph;
+    L.theta_e0 = 1.380649e-16 * p.te0_kelvin / (9.1093837e-28 * 2.99792458e10 * 2.99792458e10);
+    L.half_var = 0.5 * p.turb_rms * p.turb_rms;
+    L.modes = r->d_modes;
+    L.band_m = r->mixed.band_m;
+    L.tol32 = r->mixed.tol32;
+    L.turn_frac = r->mixed.turn_frac;
+    L.drift_tol = r->mixed.drift_tol;
+}
+
+int run_tracer(so_renderer* r, const TraceLaunch& L) {
+    int var = variant_of(r->S);
+    cudaError_t e = r->precision == SO_PREC_MIXED ? launch_trace_mixed(L, var, r->num_sms, r->st)
+                                                  : launch_trace64(L, var, r->num_sms, r->st);
+    if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
+
+int read_counters(so_renderer* r, Counters* c) {
+    SO_CK(r, cudaMemcpyAsync(c, r->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, r->st));
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    return SO_OK;
+}
+
+// Impl::trace (render.cu:677-730): pass 1, optional adaptive pass 2, resolve into img (d_img by
+// default).  With stats == NULL nothing waits on the device except the adaptive pass's chunk count.
+int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stats, float4* img = nullptr) {
+    if (!img) img = r->d_img;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (stats)
+        for (auto& e : ev) cudaEventCreate(&e);
+    struct EvGuard {
+        cudaEvent_t* e;
+        ~EvGuard() {
+            for (int i = 0; i < 4; ++i)
+                if (e[i]) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+    SO_CK(r, cudaMemcpyAsync(r->d_frame, &f, sizeof f, cudaMemcpyHostToDevice, r->st));
+    SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    const long long n = (long long)f.W * f.H;
+    TraceLaunch L;
+    launch_common(r, L);
+    L.kind = RAYS_PIXELS;
+    L.nrays = n;
+    L.W = f.W;
+    L.H = f.H;
+    L.spp = f.spp;
+    L.jitter = 1;
+    L.sample0 = 0;
+    L.accum = (float*)r->d_accum;
+    L.ystat = (float*)r->d_ystat;
+    if (stats) cudaEventRecord(ev[0], r->st);
+    int rc = run_tracer(r, L);
+    if (rc) return rc;
+    if (stats) cudaEventRecord(ev[1], r->st);
+    long long samples = n * f.spp;
+    const int extra_max = std::max(r->rs.spp_max - f.spp, 0);
+    bool have_nsamp = false;
+    if (adaptive && extra_max > 0) {
+        // yref = 0.03 * fsum / (n spp) (render.cu:702), fsum = sum over pixels of sum_s Y.
+        SO_CK(r, launch_sum_channel((const float*)r->d_ystat, 2, n, r->d_part, r->d_fsum, r->num_sms, r->st));
+        SO_CK(r, launch_fill_u32(r->d_nsamp, (uint32_t)f.spp, n, r->st));
+        have_nsamp = true;
+        SO_CK(r, launch_adapt(r->d_ystat, (uint32_t)f.spp, n, r->d_fsum, 1.0 / ((double)n * f.spp), r->rs.target_err,
+                              extra_max, r->d_extra, r->d_chunks, f.W, f.H, CHUNK, r->st));
+        long long nt = scan_tiles(n);
+        SO_CK(r, cudaMemsetAsync(r->d_tiles, 0, (size_t)(nt + 1) * sizeof(unsigned long long), r->st));
+        SO_CK(r, cudaMemsetAsync(r->d_err, 0, sizeof(int), r->st));
+        SO_CK(r, launch_scan(r->d_chunks, r->d_offsets, n, r->d_tiles, (unsigned int*)(r->d_tiles + nt), r->d_total,
+                             r->d_err, r->st));
+        uint32_t total = 0;
+        int serr = 0;
+        SO_CK(r, cudaMemcpyAsync(&total, r->d_total, 4, cudaMemcpyDeviceToHost, r->st));
+        SO_CK(r, cudaMemcpyAsync(&serr, r->d_err, 4, cudaMemcpyDeviceToHost, r->st));
+        SO_CK(r, cudaStreamSynchronize(r->st));
+        if (serr) return fail(r, SO_ERR_WATCHDOG, "scan look-back gave up");
+        if (total > 0) {
+            if ((long long)total > r->chunk_cap) {
+                if (r->d_chunk_acc) cudaFree(r->d_chunk_acc);
+                r->d_chunk_acc = nullptr;
+                r->chunk_cap = 0;
+                SO_CK(r, dalloc(&r->d_chunk_acc, (size_t)total));
+                r->chunk_cap = total;
+            }
+            TraceLaunch L2 = L;
+            L2.kind = RAYS_CHUNKS;
+            L2.nrays = total;
+            L2.sample0 = f.spp;
+            L2.offsets = r->d_offsets;
+            L2.chunk_acc = (float*)r->d_chunk_acc;
+            L2.chunk = CHUNK;
+            L2.ystat = nullptr;
+            // the queue head restarts for pass 2; the sample counters keep accumulating
+            SO_CK(r, cudaMemsetAsync(&r->d_cnt->next, 0, sizeof(unsigned long long), r->st));
+            if (stats) cudaEventRecord(ev[2], r->st);
+            rc = run_tracer(r, L2);
+            if (rc) return rc;
+            if (stats) cudaEventRecord(ev[3], r->st);
+            SO_CK(r, launch_add_chunks(r->d_accum, r->d_nsamp, r->d_offsets, r->d_chunks, r->d_chunk_acc, n, CHUNK,
+                                       r->st));
+            samples += (long long)total * CHUNK;
+        }
+    }
+    SO_CK(r, launch_resolve(img, r->d_accum, have_nsamp ? r->d_nsamp : nullptr, (uint32_t)f.spp, n,
+                            r->S.mode == SO_MODE_VISIBLE, r->st));
+    if (stats) {
+        Counters c;
+        rc = read_counters(r, &c);
+        if (rc) return rc;
+        float ms1 = 0.f, ms2 = 0.f;
+        cudaEventElapsedTime(&ms1, ev[0], ev[1]);
+        if (cudaEventQuery(ev[3]) == cudaSuccess && cudaEventElapsedTime(&ms2, ev[2], ev[3]) != cudaSuccess) ms2 = 0.f;
+        cudaGetLastError();
+        stats->ms_kernel = (double)ms1 + (double)ms2;
+        stats->flow_steps = (long long)c.flow_steps;
+        stats->samples = samples;
+        stats->step_limited = (long long)c.step_limited;
+        stats->attempts = (long long)c.attempts;
+        stats->accepted = (long long)c.accepted;
+        stats->fp64_rays = (long long)c.fp64_rays;
+    }
+    return SO_OK;
+}
+
+int alloc_frame_buffers(so_renderer* r, int W, int H) {
+    r->npix = (long long)W * H;
+    const long long n = r->npix;
+    SO_CK(r, dalloc(&r->d_accum, n));
+    SO_CK(r, dalloc(&r->d_img, n));
+    SO_CK(r, dalloc(&r->d_ystat, n));
+    SO_CK(r, dalloc(&r->d_nsamp, n));
+    SO_CK(r, dalloc(&r->d_extra, n));
+    SO_CK(r, dalloc(&r->d_chunks, n));
+    SO_CK(r, dalloc(&r->d_offsets, n));
+    SO_CK(r, dalloc(&r->d_total, 1));
+    SO_CK(r, dalloc(&r->d_tiles, scan_tiles(n) + 2));
+    SO_CK(r, dalloc(&r->d_err, 1));
+    return SO_OK;
+}
+
+// Packed device storage for so_trace_rays outputs.
+struct RayBufs {
+    int8_t *fate, *ncross;
+    double *theta, *phi, *cross_r, *cross_g;
+    float* I;
+    int32_t *nacc, *natt;
+};
+size_t ray_bytes(long long n) { return (size_t)n * (2 + 8 * 2 + 16 + 4 * 2 + 48); }
+RayBufs carve(void* base, long long n) {
+    char* p = (char*)base;
+    RayBufs b;
+    b.theta = (double*)p;
+    p += 8 * n;
+    b.phi = (double*)p;
+    p += 8 * n;
+    b.cross_r = (double*)p;
+    p += 24 * n;
+    b.cross_g = (double*)p;
+    p += 24 * n;
+    b.I = (float*)p;
+    p += 16 * n;
+    b.nacc = (int32_t*)p;
+    p += 4 * n;
+    b.natt = (int32_t*)p;
+    p += 4 * n;
+    b.fate = (int8_t*)p;
+    p += n;
+    b.ncross = (int8_t*)p;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int so_init(so_renderer** out, int device, const so_scene* scene, const so_tables* tables, const so_settings* rs) {
+    if (!out) return fail(nullptr, SO_ERR_ARG, "so_init: out is NULL");
+    *out = nullptr;
+    if (!scene || !tables || !rs) return fail(nullptr, SO_ERR_ARG, "so_init: NULL argument");
+    if (rs->W <= 0 || rs->H <= 0 || rs->spp <= 0) return fail(nullptr, SO_ERR_ARG, "so_init: bad render settings");
+    if (scene->sky_on) return fail(nullptr, SO_ERR_UNSUPPORTED, "so_init: sky texture lookups are not supported");
+    if (!tables->k2_ln || tables->k2_n < 2 || !tables->bb_xyz || tables->bb_n < 2 || !tables->disk_lnT ||
+        tables->disk_n < 2)
+        return fail(nullptr, SO_ERR_ARG, "so_init: missing tables");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return fail(nullptr, SO_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(nullptr, SO_ERR_ARG, "so_init: bad device index");
+    so_renderer* r = new so_renderer;
+    r->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&r->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking);
+    int rc = SO_OK;
+    if (e != cudaSuccess) rc = cuda_fail(nullptr, e, "so_init device");
+    auto up = [&](float** d, const float* h, size_t n) -> int {
+        if (dalloc(d, n) != cudaSuccess) return SO_ERR_ALLOC;
+        if (cudaMemcpy(*d, h, n * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return SO_ERR_CUDA;
+        return SO_OK;
+    };
+    if (!rc) rc = up(&r->d_disk, tables->disk_lnT, (size_t)tables->disk_n);
+    if (!rc) rc = up(&r->d_k2, tables->k2_ln, (size_t)tables->k2_n);
+    if (!rc) rc = up(&r->d_bb, tables->bb_xyz, (size_t)tables->bb_n * 3);
+    if (!rc && (dalloc(&r->d_scene, 1) != cudaSuccess || dalloc(&r->d_frame, 1) != cudaSuccess ||
+                dalloc(&r->d_frame_scene, 1) != cudaSuccess || dalloc(&r->d_cnt, 1) != cudaSuccess ||
+                dalloc(&r->d_part, 600) != cudaSuccess || dalloc(&r->d_fsum, 1) != cudaSuccess))
+        rc = SO_ERR_ALLOC;
+    if (!rc && cudaMemset(r->d_frame_scene, 0, sizeof(int)) != cudaSuccess) rc = SO_ERR_CUDA;
+    if (!rc) {
+        r->S = *scene;
+        r->S.disk_n = tables->disk_n;
+        r->S.k2_n = tables->k2_n;
+        r->S.bb_n = tables->bb_n;
+        r->rs = *rs;
+        rc = upload_scene(r);
+    }
+    if (!rc) rc = alloc_frame_buffers(r, rs->W, rs->H);
+    if (!rc && cudaStreamSynchronize(r->st) != cudaSuccess) rc = SO_ERR_CUDA;
+    if (rc) {
+        if (g_init_error.empty()) g_init_error = r->err.empty() ? "so_init failed" : r->err;
+        free_all(r);
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return SO_OK;
+}
+
+int so_update_scene(so_renderer* r, const so_scene* scene) {
+    if (!r || !scene) return fail(r, SO_ERR_ARG, "so_update_scene: NULL argument");
+    if (scene->sky_on) return fail(r, SO_ERR_UNSUPPORTED, "sky texture lookups are not supported");
+    int dn = r->S.disk_n, kn = r->S.k2_n, bn = r->S.bb_n;
+    r->S = *scene;
+    r->S.disk_n = dn;
+    r->S.k2_n = kn;
+    r->S.bb_n = bn;
+    return upload_scene(r);
+}
+
+int so_render(so_renderer* r, const so_frame* f_in, const so_post* post, double percentile, so_hdr_frame* out,
+              so_stats* stats) {
+    if (!r || !f_in || !out || !out->px) return fail(r, SO_ERR_ARG, "so_render: NULL argument");
+    if (post && (post->bloom > 0.f || post->blur_sigma_px > 0.5))
+        return fail(r, SO_ERR_UNSUPPORTED, "so_render: bloom / beam blur are display post-processing");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    so_frame f = *f_in;
+    f.W = r->rs.W;
+    f.H = r->rs.H;
+    f.spp = r->rs.spp;
+    double t0 = now_ms();
+    int rc = trace_frame(r, f, true, stats);
+    if (rc) return rc;
+    double t1 = now_ms();
+    out->W = f.W;
+    out->H = f.H;
+    SO_CK(r, cudaMemcpyAsync(out->px, r->d_img, (size_t)r->npix * sizeof(float4), cudaMemcpyDeviceToHost, r->st));
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    // Luminance percentile over significant pixels (render.cu:771-790)
+    const float hide = post ? post->hide_direct : 0.f;
+    std::vector<float> lum;
+    lum.reserve((size_t)r->npix);
+    double mx = 0;
+    for (long long i = 0; i < r->npix; ++i) {
+        const float* c = &out->px[4 * i];
+        double Y = r->S.mode == SO_MODE_RADIO ? c[0] - hide * std::max(c[0] - c[1] - c[2] - c[3], 0.f)
+                                              : 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2];
+        if (Y > 0) {
+            lum.push_back((float)Y);
+            mx = std::max(mx, Y);
+        }
+    }
+    std::vector<float> sig;
+    for (float v : lum)
+        if (v > mx * 1e-5) sig.push_back(v);
+    double pv = 0;
+    if (!sig.empty()) {
+        size_t idx = std::min(sig.size() - 1, (size_t)(percentile * (sig.size() - 1)));
+        std::nth_element(sig.begin(), sig.begin() + idx, sig.end());
+        pv = sig[idx];
+    }
+    out->lum_percentile = pv;
+    out->lum_max = mx;
+    if (stats) {
+        stats->ms_trace = t1 - t0;
+        stats->ms_post = now_ms() - t1;
+    }
+    return SO_OK;
+}
+
+int so_render_device(so_renderer* r, const so_frame* f_in, float* d_px, so_stats* stats) {
+    if (!r || !f_in || !d_px) return fail(r, SO_ERR_ARG, "so_render_device: NULL argument");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    so_frame f = *f_in;
+    f.W = r->rs.W;
+    f.H = r->rs.H;
+    f.spp = r->rs.spp;
+    double t0 = now_ms();
+    int rc = trace_frame(r, f, true, stats, reinterpret_cast<float4*>(d_px));
+    if (rc) return rc;
+    if (stats) {
+        stats->ms_trace = now_ms() - t0;
+        stats->ms_post = 0.0;
+    }
+    return SO_OK;
+}
+
+int so_radio_flux(so_renderer* r, const so_frame* f_in, int n, double pix_sr, double* jy) {
+    if (!r || !f_in || !jy || n <= 0) return fail(r, SO_ERR_ARG, "so_radio_flux: bad argument");
+    if ((long long)n * n > r->npix) return fail(r, SO_ERR_SIZE, "so_radio_flux: n*n exceeds the frame buffers");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    so_frame f = *f_in;
+    f.W = n;
+    f.H = n;
+    f.spp = 2;
+    int rc = trace_frame(r, f, false, nullptr);
+    if (rc) return rc;
+    // sum of I_nu over the n x n image (render.cu:803-808), fixed-order FP64 sum on the device
+    SO_CK(r, launch_sum_channel((const float*)r->d_img, 4, (long long)n * n, r->d_part, r->d_fsum, r->num_sms, r->st));
+    double s = 0;
+    SO_CK(r, cudaMemcpyAsync(&s, r->d_fsum, sizeof s, cudaMemcpyDeviceToHost, r->st));
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    *jy = s * pix_sr / 1e-23;
+    return SO_OK;
+}
+
+static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
+                           const so_rays_out& d_out) {
+    SO_CK(r, cudaMemcpyAsync(r->d_frame, f, sizeof(so_frame), cudaMemcpyHostToDevice, r->st));
+    SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    TraceLaunch L;
+    launch_common(r, L);
+    L.kind = RAYS_LIST;
+    L.nrays = n;
+    L.x = d_x;
+    L.y = d_y;
+    L.out = d_out;
+    L.record_cross = d_out.cross_r != nullptr && d_out.cross_g != nullptr;
+    if (!L.record_cross) {
+        L.out.cross_r = nullptr;
+        L.out.cross_g = nullptr;
+    }
+    return run_tracer(r, L);
+}
+
+int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
+                         const so_rays_out* d_out) {
+    if (!r || !f || !d_out || n < 0 || (n > 0 && (!d_x || !d_y))) return fail(r, SO_ERR_ARG, "so_trace_rays_device");
+    if (n == 0) return SO_OK;
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    return trace_rays_impl(r, f, n, d_x, d_y, *d_out);
+}
+
+int so_trace_rays(so_renderer* r, const so_frame* f, int n, const double* x, const double* y, const so_rays_out* out) {
+    if (!r || !f || !out || n < 0 || (n > 0 && (!x || !y))) return fail(r, SO_ERR_ARG, "so_trace_rays");
+    if (n == 0) return SO_OK;
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    if (n > r->ray_cap) {
+        if (r->d_x) cudaFree(r->d_x);
+        if (r->d_y) cudaFree(r->d_y);
+        if (r->d_rays) cudaFree(r->d_rays);
+        r->d_x = r->d_y = nullptr;
+        r->d_rays = nullptr;
+        r->ray_cap = 0;
+        if (dalloc(&r->d_x, n) != cudaSuccess || dalloc(&r->d_y, n) != cudaSuccess ||
+            cudaMalloc(&r->d_rays, ray_bytes(n)) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "so_trace_rays: device allocation");
+        r->ray_cap = n;
+    }
+    SO_CK(r, cudaMemcpyAsync(r->d_x, x, (size_t)n * 8, cudaMemcpyHostToDevice, r->st));
+    SO_CK(r, cudaMemcpyAsync(r->d_y, y, (size_t)n * 8, cudaMemcpyHostToDevice, r->st));
+    RayBufs b = carve(r->d_rays, n);
+    so_rays_out d;
+    d.fate = out->fate ? b.fate : nullptr;
+    d.ncross = out->ncross ? b.ncross : nullptr;
+    d.theta = out->theta ? b.theta : nullptr;
+    d.phi = out->phi ? b.phi : nullptr;
+    d.I = out->I ? b.I : nullptr;
+    d.n_accepted = out->n_accepted ? b.nacc : nullptr;
+    d.n_attempts = out->n_attempts ? b.natt : nullptr;
+    const bool cross = out->cross_r && out->cross_g;
+    d.cross_r = cross ? b.cross_r : nullptr;
+    d.cross_g = cross ? b.cross_g : nullptr;
+    int rc = trace_rays_impl(r, f, n, r->d_x, r->d_y, d);
+    if (rc) return rc;
+    auto back = [&](void* h, const void* dv, size_t bytes) -> cudaError_t {
+        return h ? cudaMemcpyAsync(h, dv, bytes, cudaMemcpyDeviceToHost, r->st) : cudaSuccess;
+    };
+    SO_CK(r, back(out->fate, b.fate, (size_t)n));
+    SO_CK(r, back(out->ncross, b.ncross, (size_t)n));
+    SO_CK(r, back(out->theta, b.theta, (size_t)n * 8));
+    SO_CK(r, back(out->phi, b.phi, (size_t)n * 8));
+    SO_CK(r, back(out->I, b.I, (size_t)n * 16));
+    SO_CK(r, back(out->n_accepted, b.nacc, (size_t)n * 4));
+    SO_CK(r, back(out->n_attempts, b.natt, (size_t)n * 4));
+    if (cross) {
+        SO_CK(r, back(out->cross_r, b.cross_r, (size_t)n * 24));
+        SO_CK(r, back(out->cross_g, b.cross_g, (size_t)n * 24));
+    }
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    return SO_OK;
+}
+
+int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
+    if (!r) return SO_ERR_ARG;
+    if (precision != SO_PREC_FP64 && precision != SO_PREC_MIXED) return fail(r, SO_ERR_ARG, "bad precision");
+    r->precision = precision;
+    if (opts) r->mixed = *opts;
+    return SO_OK;
+}
+
+int so_set_plasma(so_renderer* r, const so_plasma* p, const so_mode* modes) {
+    if (!r || !p) return SO_ERR_ARG;
+    if (p->model != SO_PLASMA_REFERENCE && p->model != SO_PLASMA_TORUS) return fail(r, SO_ERR_ARG, "bad plasma model");
+    if (p->model == SO_PLASMA_TORUS) {
+        if (p->n_modes < 0 || p->n_modes > SO_MAX_MODES) return fail(r, SO_ERR_SIZE, "n_modes out of range");
+        if (p->n_modes > 0 && !modes) return fail(r, SO_ERR_ARG, "modes missing");
+        if (!(p->h_sph > 0)) return fail(r, SO_ERR_ARG, "h_sph must be > 0");
+    }
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    if (r->d_modes) {
+        cudaFree(r->d_modes);
+        r->d_modes = nullptr;
+    }
+    r->plasma = *p;
+    if (p->model == SO_PLASMA_TORUS && p->n_modes > 0) {
+        if (dalloc(&r->d_modes, (size_t)p->n_modes) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "modes alloc");
+        SO_CK(r, cudaMemcpy(r->d_modes, modes, (size_t)p->n_modes * sizeof(so_mode), cudaMemcpyHostToDevice));
+    }
+    return SO_OK;
+}
+
+void* so_stream(so_renderer* r) { return r ? (void*)r->st : nullptr; }
+
+const char* so_last_error(const so_renderer* r) { return r ? r->err.c_str() : g_init_error.c_str(); }
+
+void so_destroy(so_renderer* r) {
+    if (!r) return;
+    cudaSetDevice(r->device);
+    if (r->st) cudaStreamSynchronize(r->st);
+    free_all(r);
+    delete r;
+}
+
+// main.cpp:475-508: secant iteration on ln n0 so that radio_flux matches target_jy.
+int so_normalize_flux(so_renderer* r, so_scene* scene, const so_frame* f_wide, int n, double pix_sr, double target_jy,
+                      double* n0_out, double* jy_out) {
+    if (!r || !scene || !f_wide || n <= 0 || !(target_jy > 0)) return fail(r, SO_ERR_ARG, "so_normalize_flux");
+    double jy = 0;
+    int rc = so_update_scene(r, scene);
+    if (!rc) rc = so_radio_flux(r, f_wide, n, pix_sr, &jy);
+    if (rc) return rc;
+    double x0 = std::log(scene->n0), f0v = std::log(std::max(jy, 1e-30));
+    double target = std::log(target_jy);
+    double x1 = x0 + (target - f0v) / 1.5, f1v = 0;
+    for (int it = 0; it < 8; ++it) {
+        scene->n0 = std::exp(x1);
+        rc = so_update_scene(r, scene);
+        if (!rc) rc = so_radio_flux(r, f_wide, n, pix_sr, &jy);
+        if (rc) return rc;
+        f1v = std::log(std::max(jy, 1e-30));
+        if (std::fabs(f1v - target) < 0.01) break;
+        double slope = (f1v - f0v) / (x1 - x0);
+        if (!(slope > 0.2)) slope = 1.5;
+        x0 = x1;
+        f0v = f1v;
+        x1 = x1 + (target - f1v) / slope;
+    }
+    scene->n0 = std::exp(x1);
+    rc = so_update_scene(r, scene);
+    if (rc) return rc;
+    if (n0_out) *n0_out = scene->n0;
+    if (jy_out) *jy_out = std::exp(f1v);
+    return SO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+"""ctypes access to the CPU checkers under oracle/ (test infrastructure).
+
+libso_oracle.so is the C restatement of the reference tracer (oracle/so_oracle.c); _ref/libbhref.so
+is the reference's own host code compiled from its sources (oracle/ref_shim.cpp + oracle/Makefile).
+Only tests, the smoke check and bench.py's CPU baseline use these.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "libso_oracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libbhref.so")
+
+_pkg = sys.modules.get("spacetime_optics_b200")
+if _pkg is None:
+    import conftest  # noqa: F401  (registers the package)
+    _pkg = conftest.load_package()
+abi = _pkg.abi
+Scene, Frame, Plasma, Mode, RaysOut, Vec3, KerrPoint = abi.Scene, abi.Frame, abi.Plasma, abi.Mode, abi.RaysOut, abi.Vec3, abi.KerrPoint
+
+_orc = None
+_ref = None
+
+
+def oracle():
+    global _orc
+    if _orc is None:
+        L = C.CDLL(ORACLE_SO)
+        P, vp = C.POINTER, C.c_void_p
+        L.orc_trace_rays.argtypes = [P(Scene), vp, vp, P(Frame), C.c_int, vp, vp, P(RaysOut), C.c_int]
+        L.orc_render_pass1.argtypes = [P(Scene), vp, vp, P(Frame), C.c_int, vp, vp, P(C.c_longlong), P(C.c_longlong),
+                                       C.c_int]
+        L.orc_vacuum_fate.argtypes = [C.c_double, P(Frame), Vec3, C.c_double, C.c_double, C.c_int]
+        L.orc_find_critical_point.argtypes = [P(Frame), C.c_double, C.c_double, C.c_double]
+        L.orc_find_critical_point.restype = C.c_double
+        L.orc_critical_curve_point.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double), P(C.c_double)]
+        L.orc_kerr_point.argtypes = [C.c_double, C.c_double, C.c_double, P(KerrPoint)]
+        L.orc_kerr_point.restype = None
+        L.orc_radial_drift.argtypes = [C.c_double, C.c_double, C.c_double, Vec3, C.c_double, C.c_int, P(C.c_int)]
+        L.orc_radial_drift.restype = C.c_double
+        L.so_rpow5.argtypes = [C.c_double]
+        L.so_rpow5.restype = C.c_double
+        _orc = L
+    return _orc
+
+
+def have_ref():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_SO)
+        P, vp = C.POINTER, C.c_void_p
+        L.ref_layout.argtypes = [P(C.c_longlong), C.c_int]
+        L.ref_shot_load.argtypes = [C.c_char_p, P(C.c_char_p), C.c_int]
+        L.ref_shot_load.restype = vp
+        L.ref_shot_free.argtypes = [vp]
+        L.ref_shot_nframes.argtypes = [vp]
+        L.ref_shot_scene.argtypes = [vp, vp]
+        L.ref_shot_tables.argtypes = [vp] + [P(P(C.c_float)), P(C.c_int)] * 3
+        L.ref_shot_info.argtypes = [vp, P(C.c_double)]
+        L.ref_shot_settings.argtypes = [vp, P(C.c_int), P(C.c_float)]
+        L.ref_shot_frame.argtypes = [vp, C.c_int, C.c_int, C.c_uint32, vp]
+        L.ref_find_critical_point.argtypes = [vp, C.c_int, C.c_double, C.c_double]
+        L.ref_find_critical_point.restype = C.c_double
+        L.ref_find_critical_point_cam.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
+        L.ref_find_critical_point_cam.restype = C.c_double
+        L.ref_critical_curve_point.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double), P(C.c_double)]
+        L.ref_kerr_point.argtypes = [C.c_double, C.c_double, C.c_double, vp]
+        L.ref_radial_drift.argtypes = [P(C.c_int)]
+        L.ref_radial_drift.restype = C.c_double
+        L.ref_trace_rays.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, C.c_int]
+        L.ref_trace_vacuum.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int]
+        L.ref_render_pass1.argtypes = [vp, vp, vp, P(C.c_longlong), C.c_int]
+        _ref = L
+    return _ref
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def orc_trace(scene, frame, x, y, plasma=None, modes=None, threads=8, cross=False):
+    """trace_ray of the C oracle for tangent-plane points (x, y)."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    n = x.size
+    o = dict(fate=np.zeros(n, np.int8), ncross=np.zeros(n, np.int8), theta=np.zeros(n), phi=np.zeros(n),
+             I=np.zeros((n, 4), np.float32), n_accepted=np.zeros(n, np.int32), n_attempts=np.zeros(n, np.int32),
+             cross_r=np.zeros((n, 3)), cross_g=np.zeros((n, 3)))
+    ro = RaysOut(*[_p(o[k]) for k in ("fate", "ncross", "theta", "phi", "I", "n_accepted", "n_attempts", "cross_r",
+                                      "cross_g")])
+    pl = C.byref(plasma) if plasma is not None else None
+    rc = oracle().orc_trace_rays(C.byref(scene), pl, modes, C.byref(frame), n, _p(x), _p(y), C.byref(ro), threads)
+    assert rc == 0
+    if not cross:
+        o.pop("cross_r")
+        o.pop("cross_g")
+    return o
+
+
+def orc_pass1(scene, frame, plasma=None, modes=None, jitter=1, threads=8):
+    W, H = frame.W, frame.H
+    acc = np.zeros((H, W, 4), np.float32)
+    ys = np.zeros((H, W, 2), np.float32)
+    lim = C.c_longlong()
+    att = C.c_longlong()
+    pl = C.byref(plasma) if plasma is not None else None
+    rc = oracle().orc_render_pass1(C.byref(scene), pl, modes, C.byref(frame), jitter, _p(acc), _p(ys), C.byref(lim),
+                                   C.byref(att), threads)
+    assert rc == 0
+    return acc, ys, lim.value, att.value
+
+
+class RefShot:
+    """The reference's own Config/build_scene/build_shot/make_frame on a shot file."""
+
+    def __init__(self, path, overrides=()):
+        arr = (C.c_char_p * max(1, len(overrides)))(*[s.encode() for s in overrides])
+        self.h = ref().ref_shot_load(path.encode(), arr, len(overrides))
+        assert self.h, f"reference could not load {path}"
+        self.scene = Scene()
+        ref().ref_shot_scene(self.h, C.byref(self.scene))
+        d, k, b = P3 = (C.POINTER(C.c_float)(), C.POINTER(C.c_float)(), C.POINTER(C.c_float)())
+        nd, nk, nb = C.c_int(), C.c_int(), C.c_int()
+        ref().ref_shot_tables(self.h, C.byref(d), C.byref(nd), C.byref(k), C.byref(nk), C.byref(b), C.byref(nb))
+        self.disk = np.ctypeslib.as_array(d, shape=(nd.value,)).copy()
+        self.k2 = np.ctypeslib.as_array(k, shape=(nk.value,)).copy()
+        self.bb = np.ctypeslib.as_array(b, shape=(nb.value * 3,)).copy()
+        info = (C.c_double * 8)()
+        ref().ref_shot_info(self.h, info)
+        self.info = list(info)
+        s4 = (C.c_int * 4)()
+        te = C.c_float()
+        ref().ref_shot_settings(self.h, s4, C.byref(te))
+        self.settings = (s4[0], s4[1], s4[2], s4[3], te.value)
+
+    def frame(self, i=0, W=None, seed=None):
+        f = Frame()
+        W = self.settings[0] if W is None else W
+        seed = (0x9E3779B9 * (i + 1)) & 0xFFFFFFFF if seed is None else seed
+        ref().ref_shot_frame(self.h, i, W, seed, C.byref(f))
+        f.W, f.H, f.spp = self.settings[0], self.settings[1], self.settings[2]
+        return f
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.ref_shot_free(self.h)
+            self.h = None
+
+
+def ref_vacuum(scene, frame, x, y, threads=8):
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    n = x.size
+    o = dict(fate=np.zeros(n, np.int8), ncross=np.zeros(n, np.int8), theta=np.zeros(n), phi=np.zeros(n),
+             n_accepted=np.zeros(n, np.int32), n_attempts=np.zeros(n, np.int32))
+    ref().ref_trace_vacuum(C.byref(scene), C.byref(frame), n, _p(x), _p(y), _p(o["fate"]), _p(o["ncross"]),
+                           _p(o["theta"]), _p(o["phi"]), _p(o["n_accepted"]), _p(o["n_attempts"]), threads)
+    return o
+
+
+def ref_trace(scene, frame, x, y, threads=8):
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    n = x.size
+    fate = np.zeros(n, np.int8)
+    I = np.zeros((n, 4), np.float32)
+    ref().ref_trace_rays(C.byref(scene), C.byref(frame), n, _p(x), _p(y), _p(fate), _p(I), threads)
+    return dict(fate=fate, I=I)
+
+
+def ref_pass1(scene, frame, threads=8):
+    acc = np.zeros((frame.H, frame.W, 4), np.float32)
+    lim = C.c_longlong()
+    ref().ref_render_pass1(C.byref(scene), C.byref(frame), _p(acc), C.byref(lim), threads)
+    return acc, lim.value

@@ -1,0 +1,114 @@
+"""Generates the golden fixtures of tests/golden from the REFERENCE's own code.
+
+The reference (orrnithogalum/spacetime-optics, bhrt) has no test vectors of its own: its only check
+is `bhrt --selftest` (blackholes/src/main.cpp:323-372), which prints shadow-edge extents and a
+radial-constraint drift.  The fixtures here are therefore produced by running the reference's code
+itself, compiled for the host from its sources by oracle/Makefile into oracle/_ref/libbhref.so:
+trace.cuh's trace_ray (via oracle/ref_shim.cpp), kerr.hpp's integrator, scene_build.cpp,
+shot.cpp and config.cpp.
+
+Run from the repository root (needs the reference tree to build oracle/_ref):
+    make -f oracle/Makefile && python tests/golden/make_golden.py
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import conftest  # noqa: E402
+
+so = conftest.load_package()
+import _oracle as O  # noqa: E402
+
+SHOTS = os.path.join(ROOT, "spacetime-optics_b200", "shots")
+
+
+def scene_bytes(s):
+    return np.frombuffer(bytes(memoryview(s)), np.uint8).copy()
+
+
+def main():
+    lib = O.ref()
+    out = {}
+    # 1. Struct layout of SceneGPU / FrameGPU
+    buf = (C.c_longlong * 64)()
+    n = lib.ref_layout(buf, 64)
+    np.save(os.path.join(HERE, "layout.npy"), np.array(buf[:n], np.int64))
+
+    # 2. Shadow self-test scene: rays on a strided subset of the 256^2 pixel-centre grid
+    R = O.RefShot(os.path.join(SHOTS, "shadow_selftest_256.ini"))
+    f = R.frame(0)
+    X, Y = so.pixel_centres(f, 256, 256)
+    idx = np.arange(0, 256 * 256, 29)
+    v = O.ref_vacuum(R.scene, f, X[idx], Y[idx])
+    np.savez_compressed(os.path.join(HERE, "shadow_rays.npz"), idx=idx, x=X[idx], y=Y[idx], **v)
+
+    # 3. Host builders: scene / frame structs and tables for every shipped shot
+    for name in ("shadow_selftest_256", "synchrotron_1024", "m87_reference_flow", "thin_disk_4096"):
+        Rs = O.RefShot(os.path.join(SHOTS, name + ".ini"))
+        fr = Rs.frame(0)
+        np.savez_compressed(os.path.join(HERE, f"build_{name}.npz"), scene=scene_bytes(Rs.scene),
+                            frame=scene_bytes(fr), disk=Rs.disk, k2=Rs.k2, bb=Rs.bb,
+                            info=np.array(Rs.info), settings=np.array(Rs.settings[:4], np.int64),
+                            target_err=np.float32(Rs.settings[4]))
+
+    # 4. Hot flow, the reference's model without turbulence (its fBm time phase is ill-conditioned,
+    #    see DESIGN.md), 32 x 32 pixel centres, and pass 1 with R2 jitter at spp = 2
+    Rf = O.RefShot(os.path.join(SHOTS, "m87_reference_flow.ini"), ["flow.turbulence=0", "camera.width=32",
+                                                                    "camera.height=32"])
+    ff = Rf.frame(0)
+    Xf, Yf = so.pixel_centres(ff, 32, 32)
+    t = O.ref_trace(Rf.scene, ff, Xf, Yf)
+    acc, lim = O.ref_pass1(Rf.scene, ff)
+    np.savez_compressed(os.path.join(HERE, "flow_rays.npz"), x=Xf, y=Yf, fate=t["fate"], I=t["I"], pass1=acc,
+                        step_limited=np.int64(lim))
+
+    # 5. Thin disk (visible mode, XYZ), 40 x 40 pixel centres
+    Rd = O.RefShot(os.path.join(SHOTS, "thin_disk_4096.ini"), ["camera.width=40", "camera.height=40"])
+    fd = Rd.frame(0)
+    Xd, Yd = so.pixel_centres(fd, 40, 40)
+    t = O.ref_trace(Rd.scene, fd, Xd, Yd)
+    np.savez_compressed(os.path.join(HERE, "disk_rays.npz"), x=Xd, y=Yd, fate=t["fate"], I=t["I"])
+
+    # 6. The reference self-test (main.cpp:323-371): shadow edges vs the analytic Bardeen curve
+    rows = []
+    for a in (0.5, 0.94, 0.99):
+        for incl in (90.0, 17.0):
+            th = incl * np.pi / 180
+            rp0 = 2.0 * (1.0 + np.cos(2.0 / 3.0 * np.arccos(-a)))
+            rp1 = 2.0 * (1.0 + np.cos(2.0 / 3.0 * np.arccos(a)))
+            amin, amax = 1e9, -1e9
+            al, be = C.c_double(), C.c_double()
+            for i in range(0, 200001):
+                rp = rp0 + (rp1 - rp0) * i / 200000.0
+                if lib.ref_critical_curve_point(a, th, rp, C.byref(al), C.byref(be)):
+                    amin = min(amin, al.value)
+                    amax = max(amax, al.value)
+            xp = lib.ref_find_critical_point_cam(a, 1e7, th, 0.0)
+            xm = lib.ref_find_critical_point_cam(a, 1e7, th, np.pi)
+            rows.append((a, incl, -xm, xp, amin, amax))
+    steps = C.c_int()
+    drift = lib.ref_radial_drift(C.byref(steps))
+    # critical_curve_point samples
+    ccp = []
+    for a in (0.3, 0.94):
+        for incl in (17.0, 60.0, 163.0):
+            for rp in np.linspace(1.9, 3.9, 9):
+                ok = lib.ref_critical_curve_point(a, incl * np.pi / 180, rp, C.byref(al), C.byref(be))
+                ccp.append((a, incl, rp, ok, al.value if ok else 0.0, be.value if ok else 0.0))
+    kp = []
+    for a, r, th in ((0.94, 1000.0, 0.3), (0.5, 1e7, 2.8), (0.99, 6.0, 1.2)):
+        k = O.KerrPoint()
+        lib.ref_kerr_point(a, r, th, C.byref(k))
+        kp.append([a, r, th] + [getattr(k, n) for n, _ in O.KerrPoint._fields_])
+    np.savez_compressed(os.path.join(HERE, "selftest.npz"), edges=np.array(rows), drift=np.float64(drift),
+                        drift_steps=np.int64(steps.value), ccp=np.array(ccp), kerr_point=np.array(kp))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

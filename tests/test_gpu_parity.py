@@ -1,0 +1,250 @@
+"""Parity of the CUDA FP64 tracer with the CPU oracle and the reference's golden vectors.
+
+All calls go through the C ABI (libso_tracer.so).  Bars:
+  * kernel vs oracle (same operations, bit-reproducible trajectories): fate, winding order and step
+    counts exact for every ray; escape direction within 1e-13 relative (only libm vs libdevice acos
+    / atan2 differ); specific intensity within float-accumulation precision (1e-6 of the maximum).
+  * kernel vs the reference's own code (golden fixtures): fate / winding order exact, escape
+    direction within 1e-9 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def shadow(so):
+    sh = so.Shot("shadow_selftest_256.ini")
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    yield sh, r
+    r.close()
+
+
+def _cmp_geometry(o, k, rtol_dir=1e-13):
+    assert np.array_equal(o["fate"], k["fate"])
+    assert np.array_equal(o["ncross"], k["ncross"])
+    assert np.array_equal(o["n_accepted"], k["n_accepted"])
+    assert np.array_equal(o["n_attempts"], k["n_attempts"])
+    esc = o["fate"] == 1
+    for key in ("theta", "phi"):
+        rel = np.abs(o[key][esc] - k[key][esc]) / np.maximum(np.abs(o[key][esc]), 1e-300)
+        assert rel.max(initial=0.0) <= rtol_dir, (key, rel.max())
+
+
+def test_shadow_grid_bitexact_vs_oracle(so, orc, shadow):
+    """256^2 shadow self-test grid (every 5th pixel): kernel == oracle on every ray."""
+    sh, r = shadow
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 256, 256)
+    X, Y = X[::5], Y[::5]
+    k = r.trace_rays(f, X, Y)
+    o = orc.orc_trace(sh.scene, f, X, Y)
+    _cmp_geometry(o, k)
+    assert (k["fate"] == -1).sum() > 1000 and (k["fate"] == 1).sum() > 1000
+
+
+def test_shadow_vs_reference_golden(so, shadow):
+    g = np.load(os.path.join(GOLD, "shadow_rays.npz"))
+    sh, r = shadow
+    k = r.trace_rays(sh.frame(0), g["x"], g["y"])
+    assert np.array_equal(k["fate"], g["fate"])
+    assert np.array_equal(k["ncross"], g["ncross"])
+    esc = g["fate"] == 1
+    for key in ("theta", "phi"):
+        rel = np.abs(k[key][esc] - g[key][esc]) / np.maximum(np.abs(g[key][esc]), 1e-300)
+        assert rel.max() < 1e-9, (key, rel.max())
+
+
+def test_crossing_records_vs_oracle(so, orc, shadow):
+    """First three equatorial crossings (radius, circular-emitter redshift) recorded per ray."""
+    sh, r = shadow
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 256, 256)
+    X, Y = X[7::97], Y[7::97]
+    k = r.trace_rays(f, X, Y, cross=True)
+    o = orc.orc_trace(sh.scene, f, X, Y, cross=True)
+    assert np.array_equal(k["ncross"], o["ncross"])
+    assert np.array_equal(k["cross_r"], o["cross_r"])
+    np.testing.assert_allclose(k["cross_g"], o["cross_g"], rtol=1e-14, atol=0)
+    assert (k["cross_r"][:, 0] > 0).mean() > 0.5
+
+
+def test_analytic_shadow_edge(so, shadow):
+    """bhrt --selftest on the GPU: the fate transition along the horizontal image axis of a distant
+    camera (r = 1e7) sits on the analytic Bardeen critical curve (kerr.hpp:260-270)."""
+    import ctypes as C
+    for a, incl in ((0.94, 17.0), (0.5, 90.0), (0.99, 90.0)):
+        import tempfile
+        with tempfile.NamedTemporaryFile("w", suffix=".ini", delete=False) as fh:
+            fh.write(f"[bh]\nspin = {a}\n[render]\nmode = visible\ntolerance = 1e-12\nmax_steps = 2000000\n"
+                     f"r_escape = 200\nhorizon_margin = 0.001\n[disk]\nenabled = 0\n[sky]\nenabled = 0\n"
+                     f"[camera]\nr = 1e7\nincl = {incl}\nfov_m = 30\nwidth = 8\nheight = 8\n")
+            path = fh.name
+        try:
+            sh = so.Shot(path)
+            r = so.Renderer(sh.scene, sh.tables, sh.settings)
+            f = sh.frame(0)
+            th = incl * np.pi / 180
+            rp0 = 2.0 * (1.0 + np.cos(2.0 / 3.0 * np.arccos(-a)))
+            rp1 = 2.0 * (1.0 + np.cos(2.0 / 3.0 * np.arccos(a)))
+            al, be = C.c_double(), C.c_double()
+            alphas = []
+            for rp in np.linspace(rp0, rp1, 20001):
+                if so.lib().so_critical_curve_point(a, th, rp, C.byref(al), C.byref(be)):
+                    alphas.append(al.value)
+            amin, amax = min(alphas), max(alphas)
+            for edge, lo, hi in ((amax, amax - 0.05, amax + 0.05), (amin, amin - 0.05, amin + 0.05)):
+                xs = np.linspace(lo, hi, 4001)
+                k = r.trace_rays(f, xs / 1e7, np.zeros_like(xs))
+                fate = k["fate"]
+                cap = fate == -1
+                # one transition captured <-> escaped inside the window
+                trans = np.nonzero(cap[1:] != cap[:-1])[0]
+                assert len(trans) >= 1
+                x_edge = xs[trans[0]] if edge == amax else xs[trans[-1]]
+                assert abs(x_edge - edge) < 5e-4, (a, incl, x_edge, edge)
+            r.close()
+        finally:
+            os.unlink(path)
+
+
+def test_reference_flow_turbulent_vs_oracle(so, orc):
+    """The reference's hot flow with its fBm turbulence (radio mode), 48 x 48 pixel centres."""
+    sh = so.Shot("m87_reference_flow.ini", ["camera.width=48", "camera.height=48"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 48, 48)
+    k = r.trace_rays(f, X, Y)
+    o = orc.orc_trace(sh.scene, f, X, Y)
+    _cmp_geometry(o, k, rtol_dir=1e-12)
+    I0, I1 = o["I"].astype(np.float64), k["I"].astype(np.float64)
+    assert I0[:, 0].max() > 0
+    assert np.abs(I0 - I1).max() <= 1e-6 * I0[:, 0].max()
+    assert abs(I0[:, 0].sum() - I1[:, 0].sum()) <= 1e-6 * I0[:, 0].sum()
+    r.close()
+
+
+def test_reference_flow_vs_reference_golden(so):
+    g = np.load(os.path.join(GOLD, "flow_rays.npz"))
+    sh = so.Shot("m87_reference_flow.ini", ["flow.turbulence=0", "camera.width=32", "camera.height=32"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    k = r.trace_rays(sh.frame(0), g["x"], g["y"])
+    assert np.array_equal(k["fate"], g["fate"])
+    I0, I1 = g["I"].astype(np.float64), k["I"].astype(np.float64)
+    assert np.abs(I0 - I1).max() <= 1e-5 * I0[:, 0].max()
+    assert abs(I0[:, 0].sum() - I1[:, 0].sum()) <= 1e-7 * I0[:, 0].sum()
+    r.close()
+
+
+def test_torus_plasma_vs_oracle(so, orc):
+    """Synchrotron torus with 512 Fourier modes (FP64 everywhere), 40 x 40 over the +-12 M field."""
+    sh = so.Shot("synchrotron_1024.ini", ["camera.width=40", "camera.height=40"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    p = sh.plasma()
+    modes = r.set_plasma(p)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 40, 40)
+    k = r.trace_rays(f, X, Y)
+    o = orc.orc_trace(sh.scene, f, X, Y, plasma=p, modes=modes)
+    _cmp_geometry(o, k, rtol_dir=1e-12)
+    I0, I1 = o["I"].astype(np.float64), k["I"].astype(np.float64)
+    assert I0[:, 0].max() > 0
+    assert np.abs(I0 - I1).max() <= 1e-6 * I0[:, 0].max()
+    r.close()
+
+
+def test_thin_disk_vs_oracle_and_golden(so, orc):
+    g = np.load(os.path.join(GOLD, "disk_rays.npz"))
+    sh = so.Shot("thin_disk_4096.ini", ["camera.width=40", "camera.height=40"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    k = r.trace_rays(f, g["x"], g["y"])
+    o = orc.orc_trace(sh.scene, f, g["x"], g["y"])
+    _cmp_geometry(o, k, rtol_dir=1e-12)
+    scale = np.abs(g["I"]).max()
+    assert np.abs(k["I"].astype(np.float64) - o["I"]).max() <= 1e-6 * scale
+    assert np.array_equal(k["fate"], g["fate"])
+    assert np.abs(k["I"].astype(np.float64) - g["I"]).max() <= 1e-5 * scale
+    r.close()
+
+
+def test_render_pass1_jitter_vs_oracle(so, orc):
+    """so_render with spp = 2 R2-jittered samples and no adaptive pass == oracle pass 1 / spp."""
+    sh = so.Shot("m87_reference_flow.ini", ["camera.width=32", "camera.height=24", "render.spp=2",
+                                            "render.spp_max=2"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    img, hdr, st = r.render(f)
+    acc, ys, lim, att = orc.orc_pass1(sh.scene, f)
+    ref = acc / 2.0
+    assert np.abs(img - ref).max() <= 1e-6 * ref[..., 0].max()
+    assert st.samples == 32 * 24 * 2 and st.step_limited == lim and st.attempts == att
+    assert hdr.lum_max > 0 and 0 < hdr.lum_percentile <= hdr.lum_max
+    r.close()
+
+
+def test_adaptive_render_deterministic(so):
+    """Adaptive pass 2 (k_adapt, k_dilate, scan, chunked samples) is deterministic and adds samples."""
+    sh = so.Shot("m87_reference_flow.ini", ["camera.width=48", "camera.height=32", "render.spp=2",
+                                            "render.spp_max=34", "render.target_error=0.02"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    a, _, s1 = r.render(f)
+    b, _, s2 = r.render(f)
+    assert np.array_equal(a, b)
+    assert s1.samples > 48 * 32 * 2 and s1.samples == s2.samples
+    assert (s1.samples - 48 * 32 * 2) % 8 == 0
+    r.close()
+
+
+def test_radio_flux_matches_image_sum(so, orc):
+    sh = so.Shot("m87_reference_flow.ini", ["camera.width=64", "camera.height=64", "flow.turbulence=0"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0, W=24)
+    jy = r.radio_flux(f, 24, 1.0)
+    f.W, f.H, f.spp = 24, 24, 2
+    acc, _, _, _ = orc.orc_pass1(sh.scene, f)
+    ref = (acc[..., 0] / np.float32(2)).astype(np.float64).sum() / 1e-23
+    assert abs(jy - ref) <= 1e-6 * ref
+    r.close()
+
+
+def test_status_codes_on_gpu(so):
+    sh = so.Shot("shadow_selftest_256.ini")
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    import ctypes as C
+    L = so.lib()
+    out = np.zeros((256, 256, 4), np.float32)
+    hdr = so.abi.HdrFrame(256, 256, out.ctypes.data_as(C.POINTER(C.c_float)), 0, 0)
+    post = so.abi.Post(0.5, 0.0, 0.0)
+    assert L.so_render(r.h, C.byref(f), C.byref(post), 0.5, C.byref(hdr), None) == so.abi.SO_ERR_UNSUPPORTED
+    jy = C.c_double()
+    assert L.so_radio_flux(r.h, C.byref(f), 300, 1.0, C.byref(jy)) == so.abi.SO_ERR_SIZE
+    assert b"frame buffers" in L.so_last_error(r.h)
+    p = so.abi.Plasma()
+    p.model = so.abi.SO_PLASMA_TORUS
+    p.n_modes = 5000
+    p.h_sph = 0.3
+    assert L.so_set_plasma(r.h, C.byref(p), None) == so.abi.SO_ERR_SIZE
+    # the renderer stays usable after the rejected calls
+    k = r.trace_rays(f, np.array([0.0, 0.01]), np.array([0.0, 0.0]))
+    assert k["fate"][0] == -1 and k["fate"][1] == 1
+    r.close()
+
+
+def test_step_limit_counts(so, orc):
+    """max_steps bounds every ray; step-limited samples are reported (render.cu:83, 126)."""
+    sh = so.Shot("shadow_selftest_256.ini", ["render.max_steps=50", "camera.width=16", "camera.height=16"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 16, 16)
+    k = r.trace_rays(f, X, Y)
+    o = orc.orc_trace(sh.scene, f, X, Y)
+    assert np.array_equal(k["fate"], o["fate"]) and (k["fate"] == 0).all()
+    assert (k["n_attempts"] == 50).all()
+    r.close()

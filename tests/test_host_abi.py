@@ -1,0 +1,166 @@
+"""Host side of the product on CPU: the C ABI library loads and exports every declared entry point,
+its structs have the reference's layout, the shot builders reproduce the reference's scene / frame /
+tables, and calls fail loudly (status codes) where they must.  No GPU needed."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+SHOTS = ("shadow_selftest_256", "synchrotron_1024", "m87_reference_flow", "thin_disk_4096")
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "so_tracer.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(so_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_every_declared_symbol(so):
+    lib = so.lib()
+    declared = header_functions()
+    assert set(declared) == set(so.abi.EXPORTS), set(declared) ^ set(so.abi.EXPORTS)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_struct_layout_matches_reference(so):
+    ref = np.load(os.path.join(GOLD, "layout.npy"))
+    assert ref[0] == C.sizeof(so.abi.Scene)
+    assert ref[1] == C.sizeof(so.abi.Frame)
+    for (cls, field), off in zip(so.abi.LAYOUT_FIELDS, ref[2:]):
+        assert getattr(cls, field).offset == off, (cls.__name__, field)
+
+
+def _scene_bytes_no_ptrs(so, s):
+    b = bytearray(bytes(memoryview(s)))
+    for name in ("disk_lnT", "k2_lntab", "bb_xyz"):
+        off = getattr(so.abi.Scene, name).offset
+        b[off:off + 8] = bytes(8)
+    return bytes(b)
+
+
+@pytest.mark.parametrize("name", SHOTS)
+def test_shot_builders_match_reference(so, name):
+    """so_shot_load / so_shot_scene / so_shot_frame vs the reference's build_scene / make_frame."""
+    g = np.load(os.path.join(GOLD, f"build_{name}.npz"))
+    sh = so.Shot(f"{name}.ini")
+    ref_scene = so.abi.Scene()
+    C.memmove(C.byref(ref_scene), g["scene"].tobytes(), C.sizeof(ref_scene))
+    assert _scene_bytes_no_ptrs(so, sh.scene) == _scene_bytes_no_ptrs(so, ref_scene)
+    f = sh.frame(0)
+    ref_f = so.abi.Frame()
+    C.memmove(C.byref(ref_f), g["frame"].tobytes(), C.sizeof(ref_f))
+    for fld, _ in so.abi.Frame._fields_:
+        if fld in ("W", "H", "spp"):
+            continue
+        a, b = getattr(f, fld), getattr(ref_f, fld)
+        assert bytes(memoryview(a)) == bytes(memoryview(b)) if hasattr(a, "_fields_") else a == b, fld
+    n = sh.tables
+    assert np.array_equal(np.ctypeslib.as_array(n.k2_ln, (n.k2_n,)), g["k2"])
+    assert np.array_equal(np.ctypeslib.as_array(n.disk_lnT, (n.disk_n,)), g["disk"])
+    assert np.array_equal(np.ctypeslib.as_array(n.bb_xyz, (3 * n.bb_n,)), g["bb"])
+    assert np.array_equal(np.array([sh.settings.W, sh.settings.H, sh.settings.spp, sh.settings.spp_max]),
+                          g["settings"])
+    info = [getattr(sh.info, k) for k, _ in so.abi.SceneInfo._fields_]
+    assert np.array_equal(np.array(info), g["info"])
+
+
+def test_overrides_and_tracks(so, tmp_path):
+    p = tmp_path / "base.ini"
+    p.write_text("[bh]\nspin = 0.5\n[camera]\nr = 100\nincl = 30\nfov_m = 20\nwidth = 8\nheight = 8\n"
+                 "[shot]\nduration = 1\nfps = 4\n")
+    q = tmp_path / "shot.ini"
+    q.write_text("include = base.ini\n[bh]\nspin = 0.7   # comment\n[track]\ncamera.incl = 0:30, 1:60\n"
+                 "camera.r = 0:100, 1:1000\n")
+    sh = so.Shot(str(q), ["render.tolerance=1e-8", "camera.width=16"])
+    assert sh.scene.a == 0.7 and sh.scene.tol == 1e-8 and sh.settings.W == 16
+    assert sh.nframes() == 4
+    f0, f3 = sh.frame(0), sh.frame(3)
+    assert abs(f0.th - np.radians(30)) < 1e-15
+    assert np.radians(30) < f3.th < np.radians(60)
+    assert 100 < f3.r < 1000  # log-space monotone cubic
+    with pytest.raises(so.TracerError):
+        so.Shot(str(tmp_path / "missing.ini"))
+    bad = tmp_path / "bad.ini"
+    bad.write_text("[bh\nspin = 1\n")
+    with pytest.raises(so.TracerError):
+        so.Shot(str(bad))
+
+
+def test_spin_clamp(so, tmp_path):
+    p = tmp_path / "s.ini"
+    p.write_text("[bh]\nspin = 0\n")
+    assert so.Shot(str(p)).scene.a == 1e-6  # scene_build.cpp:86
+    p.write_text("[bh]\nspin = 1.5\n")
+    assert so.Shot(str(p)).scene.a == 0.9999
+
+
+def test_plasma_modes_spectrum(so):
+    sh = so.Shot("synchrotron_1024.ini")
+    p = sh.plasma()
+    assert p is not None and p.n_modes == 512
+    m = so.modes_to_numpy(so.plasma_modes(p), p.n_modes)
+    k = np.linalg.norm(m[:, :3], axis=1)
+    assert k.min() >= p.k_min * (1 - 1e-12) and k.max() <= p.k_max * (1 + 1e-12)
+    assert abs(np.sum(m[:, 4] ** 2) / 2 - p.turb_rms ** 2) < 1e-12
+    # amplitude^2 ~ k^(3 + index): log-log slope
+    slope = np.polyfit(np.log(k), np.log(m[:, 4] ** 2), 1)[0]
+    assert abs(slope - (3 + p.spectral_index)) < 1e-9
+    again = so.modes_to_numpy(so.plasma_modes(p), p.n_modes)
+    assert np.array_equal(m, again)  # deterministic from the seed
+    p.n_modes = 5000
+    with pytest.raises(so.TracerError):
+        so.plasma_modes(p)
+
+
+def test_kerr_point_and_critical_curve_exports(so):
+    g = np.load(os.path.join(GOLD, "selftest.npz"))
+    lib = so.lib()
+    for row in g["kerr_point"]:
+        k = so.abi.KerrPoint()
+        lib.so_kerr_point_at(row[0], row[1], row[2], C.byref(k))
+        assert np.array_equal(np.array([getattr(k, n) for n, _ in so.abi.KerrPoint._fields_]), row[3:])
+    al, be = C.c_double(), C.c_double()
+    for a, incl, rp, ok, a0, b0 in g["ccp"]:
+        assert lib.so_critical_curve_point(a, incl * np.pi / 180, rp, C.byref(al), C.byref(be)) == int(ok)
+        if ok:
+            assert al.value == a0 and be.value == b0
+
+
+def test_find_critical_point_matches_reference_selftest(so):
+    """so_find_critical_point reproduces the reference's find_critical_point edges (host FP64)."""
+    g = np.load(os.path.join(GOLD, "selftest.npz"))
+    a, incl, xm, xp = g["edges"][2][:4]  # a = 0.94, incl = 90
+    import tempfile
+    with tempfile.NamedTemporaryFile("w", suffix=".ini", delete=False) as fh:
+        fh.write(f"[bh]\nspin = {a}\n[camera]\nr = 1e7\nincl = {incl}\nfov_m = 30\n")
+        path = fh.name
+    try:
+        sh = so.Shot(path)
+        assert abs(sh.find_critical_point(0.0) - xp) < 1e-9
+        assert abs(-sh.find_critical_point(np.pi) - xm) < 1e-9
+    finally:
+        os.unlink(path)
+
+
+def test_init_fails_loudly_without_device_or_bad_args(so):
+    """No silent fallback: without a usable CUDA device so_init returns an error status."""
+    import torch
+    sh = so.Shot("shadow_selftest_256.ini")
+    if not torch.cuda.is_available():
+        with pytest.raises(so.TracerError) as e:
+            so.Renderer(sh.scene, sh.tables, sh.settings)
+        assert e.value.code in (so.abi.SO_ERR_NO_DEVICE, so.abi.SO_ERR_CUDA)
+    bad = so.abi.Settings(0, 0, 1, 1, 0.03)
+    with pytest.raises(so.TracerError) as e:
+        so.Renderer(sh.scene, sh.tables, bad)
+    assert e.value.code == so.abi.SO_ERR_ARG
+    lib = so.lib()
+    assert lib.so_init(None, 0, None, None, None) == so.abi.SO_ERR_ARG
+    assert lib.so_render(None, None, None, 0.5, None, None) == so.abi.SO_ERR_ARG
+    assert lib.so_trace_rays(None, None, 1, None, None, None) == so.abi.SO_ERR_ARG
+    assert lib.so_last_error(None)  # message of the last failed init
