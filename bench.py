@@ -39,6 +39,10 @@ FLOPS_ATTEMPT = 469        # one DP5(4) attempt: 6 RHS (31 each) + stage sums + 
 FLOPS_ACCEPT = 49          # controller err^-1/5 (34) + projection (11) + psi bookkeeping excluded (radio)
 FLOPS_FLOW = 160           # flow_step without the turbulence sum (transcendentals counted as 20 each)
 FLOPS_MODE = 8 + 20        # one Fourier mode: 3 fma (k.X + phase) + fma accumulate + cos (20)
+# SFU operations of the FP32 tracer (k_trace32): per attempt 7 RHS x 2 reciprocals + 5 error
+# divides + err^-0.2 (2); per flow step ~20 (exp, log, sincos, rsqrt, divides) + one cosine per mode
+SFU_ATTEMPT = 21
+SFU_FLOW = 20
 
 
 def load_package():
@@ -150,7 +154,7 @@ def run_ours(args, so, world, rank, local):
     sh, r, norm = build_scene(so, W)
     path = args.path
     if path == "auto":
-        path = "mixed" if os.environ.get("SO_BENCH_MIXED", "0") == "1" and has_mixed(so, r) else "fp64"
+        path = "mixed"
     f = sh.frame(rank)
     f.t = sh.frame(0).t + 50.0 * rank  # every rank renders its own turbulence time offset
     npix = W * W
@@ -196,12 +200,25 @@ def run_ours(args, so, world, rank, local):
     err_l1 = float(np.abs(img[..., 0] - img64[..., 0]).sum() / max(np.abs(img64[..., 0]).sum(), 1e-300))
     flux_err = float(abs(img[..., 0].astype(np.float64).sum() / img64[..., 0].astype(np.float64).sum() - 1.0))
     fp64_mrays = npix / (st64.ms_kernel * 1e-3) / 1e6
-    # roofline of the dominant kernel (the tracer): algorithmic FP64 flops per launch / its duration
+    # roofline of the dominant kernel: the FP64 tracer (plain path, FP64 pipe) or the FP32 tracer
+    # (mixed path, SFU-bound: one cosine per Fourier mode per flow step)
     fp64_peak, fp32_peak = so.probe_fma_peak(local)
-    flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
-             st.flow_steps * (FLOPS_FLOW + sh.plasma().n_modes * FLOPS_MODE))
-    achieved = flops / (st.ms_kernel * 1e-3) / 1e12
-    peak = fp64_peak if path == "fp64" else fp64_peak
+    n_modes = sh.plasma().n_modes
+    if path == "fp64":
+        flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
+                 st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
+        roof = {"bound": "fp64", "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
+                "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel": "k_trace64", "kernel_ms": st.ms_kernel,
+                "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
+    else:
+        sfu_peak = so.probe_sfu_peak(local)
+        ops = st.attempts_fp32 * SFU_ATTEMPT + st.flow_steps_fp32 * (SFU_FLOW + n_modes)
+        roof = {"bound": "sfu", "achieved": round(ops / (st.ms_fp32 * 1e-3) / 1e9, 3), "peak": round(sfu_peak, 3),
+                "unit": "Gop/s", "kernel": "k_trace32", "kernel_ms": st.ms_fp32, "per_launch": ops,
+                "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
+                "fp32_tflops_peak": round(fp32_peak, 3)}
+    roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
+    roof["traffic"] = None
     # e2e: host buffers through so_render (frame H2D, image D2H inside the timed region)
     host = np.empty((W, W, 4), np.float32)
     host_pinned = torch.empty((W, W, 4), dtype=torch.float32).pin_memory().numpy()
@@ -216,21 +233,22 @@ def run_ours(args, so, world, rank, local):
     e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
     e2e = world * npix / (e2e_step * 1e-3) / 1e6
     del host
-    gpu_launches = args.steps * (2 if path == "fp64" else 2)  # tracer + resolve per frame (spp_max = spp)
+    # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, re-trace, gather,
+    # resolve (mixed); spp_max = spp, so no adaptive pass
+    gpu_launches = args.steps * (2 if path == "fp64" else 7)
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if path == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": f"synchrotron torus frame {W}x{W}, a=0.94, i=163 deg, fov +-12 M, 230 GHz, "
-                               f"512 Fourier modes, 1 sample/pixel", "path": path,
+                               f"512 Fourier modes, 1 R2-jittered sample/pixel (k_pass1 sampling)", "path": path,
+                   "band_rays": st.band_rays if path == "mixed" else None,
+                   "fp64_rays": st.fp64_rays if path == "mixed" else None,
                    "plain_fp64_mrays_s": round(fp64_mrays, 4), "image_rel_l1_vs_fp64": err_l1,
                    "total_flux_err_vs_fp64": flux_err, "frames_per_s": round(1e3 / ms_step * world, 4),
                    "l2": "256 MiB buffer written between timed steps", **norm,
                    "attempts_per_ray": st.attempts / npix, "flow_steps_per_ray": st.flow_steps / npix},
-        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
-                     "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)",
-                     "kernel_ms": st.ms_kernel, "flops_per_launch": flops},
+        "roofline": roof,
         "e2e": {"value": round(e2e, 4), "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(so.abi.Frame),
                 "d2h_bytes_per_step": W * W * 16},
         "gpu_launches": gpu_launches,
@@ -240,16 +258,6 @@ def run_ours(args, so, world, rank, local):
         line["cpu_baseline"] = cpu_baseline(so, sh, f, W, budget_s=args.cpu_seconds)
     r.close()
     return line
-
-
-def has_mixed(so, r):
-    try:
-        r.set_precision(so.abi.SO_PREC_MIXED)
-        ok = True
-    except so.TracerError:
-        ok = False
-    r.set_precision(so.abi.SO_PREC_FP64)
-    return ok and os.path.exists(os.path.join(PKG_DIR, "libso_tracer.so"))
 
 
 def _sample_pixels(so, f, W, n):

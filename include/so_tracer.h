@@ -159,9 +159,13 @@ typedef struct so_stats {
     long long samples, step_limited;
     long long attempts;   /* DP5(4) step attempts over all samples */
     long long accepted;   /* accepted steps over all samples */
-    long long fp64_rays;  /* mixed precision: rays integrated in FP64 (critical band) */
+    long long fp64_rays;  /* mixed precision: rays integrated in FP64 end to end (band + re-traced) */
     long long flow_steps; /* accepted steps that evaluated the hot-flow transfer */
     double ms_kernel;     /* device time of the tracer launches (CUDA events), when measured */
+    long long attempts_fp32; /* mixed precision: attempts made by the FP32 tracer (the rest are FP64) */
+    long long band_rays;  /* mixed precision: rays routed to FP64 by the critical band */
+    long long flow_steps_fp32; /* mixed precision: flow steps evaluated by the FP32 tracer */
+    double ms_fp32;       /* mixed precision: device time of the FP32 tracer launch (CUDA events) */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -200,12 +204,16 @@ typedef struct so_plasma {
 /* One Fourier mode: wave vector (rad/M), phase (rad), amplitude. */
 typedef struct so_mode { double kx, ky, kz, phase, amp; } so_mode;
 
-/* Mixed-precision routing options (SO_PREC_MIXED). */
+/* Mixed-precision routing options (SO_PREC_MIXED).  A ray is integrated in FP64 from the camera
+ * down to r_switch, then in FP32 with two-sum compensated state; rays inside the critical band are
+ * FP64 throughout; an FP32 ray whose radial turning point falls inside turn_r, or whose
+ * Carter-constant drift (checked in FP64 at the end) exceeds drift_tol, is re-integrated in FP64. */
 typedef struct so_mixed_opts {
     double band_m;           /* FP64 for rays within this distance (M) of the analytic critical curve */
     double tol32;            /* FP32 integrator tolerance (reference error norm) */
-    double turn_frac;        /* promote a step to FP64 when R(r) < turn_frac * r^4 or U(u) < turn_frac */
-    double drift_tol;        /* Carter-constant drift check: re-trace in FP64 above this relative drift */
+    double turn_r;           /* radial turning point inside this radius (M): re-trace in FP64 */
+    double drift_tol;        /* relative drift of p_u^2 - U(u) and p_r^2 - R(r) that triggers FP64 */
+    double r_switch;         /* FP64 approach from the camera down to this radius (0 = automatic) */
 } so_mixed_opts;
 
 /* ---- renderer lifecycle ---------------------------------------------------------------------- */
@@ -278,6 +286,9 @@ int so_plasma_modes(const so_plasma* p, so_mode* modes);
 /* Peak FP64 / FP32 FMA throughput of `device` in TFLOP/s (FMA = 2 flops), measured by independent
  * FMA chains on every SM and timed with CUDA events: the roofline denominator for the tracers. */
 int so_probe_fma_peak(int device, double* fp64_tflops, double* fp32_tflops);
+/* Peak special-function-unit throughput (FP32 cosines, G ops/s) of `device`: the roofline of the
+ * FP32 tracer, whose turbulence sum issues one SFU cosine per Fourier mode. */
+int so_probe_sfu_peak(int device, double* gops);
 
 /* ---- analytic helpers (kerr.hpp) --------------------------------------------------------------- */
 /* kerr_point (kerr.hpp:77-92). */

@@ -42,6 +42,7 @@ def lib():
         L.so_render.argtypes = [vp, P(Frame), P(Post), C.c_double, P(HdrFrame), P(Stats)]
         L.so_render_device.argtypes = [vp, P(Frame), vp, P(Stats)]
         L.so_probe_fma_peak.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
+        L.so_probe_sfu_peak.argtypes = [C.c_int, P(C.c_double)]
         L.so_radio_flux.argtypes = [vp, P(Frame), C.c_int, C.c_double, P(C.c_double)]
         L.so_trace_rays.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
         L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
@@ -202,8 +203,8 @@ class Renderer:
         _check(lib().so_set_plasma(self.h, C.byref(plasma), modes), self.h)
         return modes
 
-    def set_precision(self, precision, band_m=0.05, tol32=1e-6, turn_frac=1e-3, drift_tol=1e-6):
-        o = MixedOpts(band_m, tol32, turn_frac, drift_tol)
+    def set_precision(self, precision, band_m=0.05, tol32=3e-6, turn_r=3.5, drift_tol=1e-4, r_switch=0.0):
+        o = MixedOpts(band_m, tol32, turn_r, drift_tol, r_switch)
         _check(lib().so_set_precision(self.h, precision, C.byref(o)), self.h)
 
     def render(self, frame, percentile=0.995, hide_direct=0.0, out=None):
@@ -261,6 +262,13 @@ def probe_fma_peak(device=0):
     a, b = C.c_double(), C.c_double()
     _check(lib().so_probe_fma_peak(device, C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+def probe_sfu_peak(device=0):
+    """Measured SFU cosine throughput of the device, G ops/s (so_probe_sfu_peak)."""
+    g = C.c_double()
+    _check(lib().so_probe_sfu_peak(device, C.byref(g)))
+    return g.value
 
 
 def pixel_centres(frame, W, H):

@@ -82,7 +82,9 @@ class HdrFrame(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("ms_trace", C.c_double), ("ms_post", C.c_double), ("samples", C.c_longlong),
                 ("step_limited", C.c_longlong), ("attempts", C.c_longlong), ("accepted", C.c_longlong),
-                ("fp64_rays", C.c_longlong), ("flow_steps", C.c_longlong), ("ms_kernel", C.c_double)]
+                ("fp64_rays", C.c_longlong), ("flow_steps", C.c_longlong), ("ms_kernel", C.c_double),
+                ("attempts_fp32", C.c_longlong), ("band_rays", C.c_longlong), ("flow_steps_fp32", C.c_longlong),
+                ("ms_fp32", C.c_double)]
 
 
 class RaysOut(C.Structure):
@@ -103,7 +105,8 @@ class Mode(C.Structure):
 
 
 class MixedOpts(C.Structure):
-    _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_frac", C.c_double), ("drift_tol", C.c_double)]
+    _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_r", C.c_double), ("drift_tol", C.c_double),
+                ("r_switch", C.c_double)]
 
 
 class SceneInfo(C.Structure):
@@ -125,7 +128,7 @@ LAYOUT_FIELDS = [
 # Every entry point include/so_tracer.h declares (checked against the built library's exports).
 EXPORTS = [
     "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
-    "so_trace_rays_device", "so_probe_fma_peak",
+    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak",
     "so_set_precision", "so_set_plasma", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
     "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",

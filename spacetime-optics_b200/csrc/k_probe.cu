@@ -45,6 +45,48 @@ int probe(int nsm, int iters, double* tflops) {
 }
 }  // namespace
 
+__global__ void __launch_bounds__(256) k_sfu_chains(float* out, int iters, float b) {
+    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 0.1f, x2 = x0 + 0.2f, x3 = x0 + 0.3f, x4 = x0 + 0.4f, x5 = x0 + 0.5f,
+          x6 = x0 + 0.6f, x7 = x0 + 0.7f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            x0 = __cosf(x0) + b; x1 = __cosf(x1) + b; x2 = __cosf(x2) + b; x3 = __cosf(x3) + b;
+            x4 = __cosf(x4) + b; x5 = __cosf(x5) + b; x6 = __cosf(x6) + b; x7 = __cosf(x7) + b;
+        }
+    }
+    float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == -12345.678f) out[threadIdx.x] = s;
+}
+
+extern "C" int so_probe_sfu_peak(int device, double* gops) {
+    if (!gops) return SO_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return SO_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return SO_ERR_CUDA;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    float* out = nullptr;
+    if (cudaMalloc(&out, 256 * sizeof(float)) != cudaSuccess) return SO_ERR_ALLOC;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = nsm * 8, iters = 500;
+    k_sfu_chains<<<blocks, 256>>>(out, iters / 4, 1e-3f);
+    cudaEventRecord(e0);
+    k_sfu_chains<<<blocks, 256>>>(out, iters, 1e-3f);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess || ms <= 0.f) return SO_ERR_CUDA;
+    *gops = 8.0 * 16.0 * (double)iters * blocks * 256.0 / (ms * 1e-3) / 1e9;
+    return SO_OK;
+}
+
 extern "C" int so_probe_fma_peak(int device, double* fp64_tflops, double* fp32_tflops) {
     if (!fp64_tflops || !fp32_tflops) return SO_ERR_ARG;
     int ndev = 0;

@@ -36,15 +36,7 @@ struct Ray64 {
 
 __device__ __forceinline__ void pixel_point(const TraceLaunch& L, const so_frame& F, long long q, int s, double* x,
                                             double* yv) {  // s: absolute sample index
-    int px = (int)(q % L.W), py = (int)(q / L.W);
-    float jx = 0.5f, jy = 0.5f;
-    if (L.jitter) {
-        uint32_t h = pcg((uint32_t)q * 0x9E3779B9u ^ F.seed);  // pixel_seed, render.cu:70-74
-        float r0 = rnd(h), r1 = rnd(h);
-        r2_sample((uint32_t)s, r0, r1, &jx, &jy);
-    }
-    *x = (px + jx - 0.5 * L.W) * F.pix;  // sample_pixel, render.cu:79-80
-    *yv = (0.5 * L.H - (py + jy)) * F.pix;
+    sample_point(L.W, L.H, L.jitter, F, q, s, x, yv);
 }
 
 template <int VAR>
@@ -216,7 +208,7 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
         __syncthreads();
     }
     const int lane = threadIdx.x & 31;
-    const long long total = L.nrays;
+    const long long total = L.nrays_dev ? (long long)*L.nrays_dev : L.nrays;
     long long job = 0, pix = 0;
     int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
     bool active = false, exhausted = false;
@@ -251,6 +243,13 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
                         x = L.x[job];
                         yv = L.y[job];
                         jobs_n = 1;
+                    } else if (L.kind == RAYS_SAMPLES) {
+                        const long long sid = (long long)__ldg(L.list + job);
+                        fidx = 0;
+                        pix = sid / L.spp;
+                        sbase = (int)(sid % L.spp);
+                        jobs_n = 1;
+                        pixel_point(L, L.frames[0], pix, sbase, &x, &yv);
                     } else if (L.kind == RAYS_PIXELS) {
                         const long long npix = (long long)L.W * L.H;
                         fidx = (int)(job / npix);
@@ -317,7 +316,12 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
             const float Y = radio_lum ? R.acc[0] : R.acc[1];
             ys += Y;
             yq += Y * Y;
-            if (++sample < jobs_n) {
+            if (L.kind == RAYS_SAMPLES) {
+                const long long sid = pix * L.spp + sbase;
+                L.sample_out[sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
+                if (L.sample_fate) L.sample_fate[sid] = (int8_t)fate;
+                active = false;
+            } else if (++sample < jobs_n) {
                 double x, yv;
                 pixel_point(L, *F, pix, sbase + sample, &x, &yv);
                 ray_init<VAR>(R, *S, *F, x, yv);

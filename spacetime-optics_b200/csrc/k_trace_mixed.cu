@@ -1,10 +1,711 @@
-// k_trace_mixed.cu -- mixed-precision tracer (FP32 far from the critical curve, FP64 in the band).
+// k_trace_mixed.cu -- mixed-precision tracer: FP32 far from the critical curve, FP64 where it matters.
+//
+// Same physics as the plain FP64 tracer (trace_ray, blackholes/src/trace.cuh:62-165; flow_step,
+// emission.cuh:99-175), re-arranged for throughput:
+//   k_route       per sample: distance of its image point from the analytic critical curve
+//                 (critical_curve_point, kerr.hpp:260-270, tabulated per frame on the host).  Inside
+//                 the band -> FP64 list; outside -> FP32 list.
+//   k_approach64  FP64 DP5(4) from the camera to r_switch (the far field, where the coordinate time
+//                 and radius are too large for FP32 increments), then parks the state in HBM as five
+//                 float4 SoA planes (two-float hi/lo pairs for r, r', u, u', phi, t).
+//   k_trace32     persistent FP32 tracer over the parked rays: compensated (two-sum) state update,
+//                 FP32 stages and error estimate with the reference's error norm at tol32, err^-0.2
+//                 on the SFU, torus turbulence with the mode table in shared memory and SFU cosines
+//                 of phases reduced in turns.  At the end the Carter-constant and radial constraints
+//                 are checked in FP64; a ray that fails, or whose radial turning point falls inside
+//                 turn_r, goes to the FP64 re-trace list.
+// The band and re-trace lists are then traced by the plain FP64 kernel (k_trace64, RAYS_SAMPLES).
+// Compiled with --use_fast_math (FP32 only; the FP64 code is unaffected).
 #include <cuda_runtime.h>
 
+#include "so_emission.cuh"
 #include "so_launch.h"
 
 namespace so {
 
-cudaError_t launch_trace_mixed(const TraceLaunch&, int, int, cudaStream_t) { return cudaErrorNotSupported; }
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ void push(uint32_t* list, unsigned long long* count, uint32_t v, bool want) {
+    const unsigned m = __ballot_sync(FULL, want);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+    base = __shfl_sync(FULL, base, leader);
+    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Bardeen coordinates (alpha, beta) of a viewing direction d in the camera's ZAMO frame
+// (e_r, e_theta, e_phi): image +x is +alpha (main.cpp:345), beta along -e_theta.
+__device__ __forceinline__ bool in_band(const TraceLaunch& L, const so_frame& F, double x, double yv) {
+    so_vec3 d = view_dir(F, x, yv);
+    if (!(d.x < 0.0)) return true;  // looking away from the hole: no critical curve to compare with
+    double al = F.r * d.z / (-d.x), be = F.r * (-d.y) / (-d.x);
+    double rho = sqrt(al * al + be * be);
+    double psi = atan2(be, al);
+    double u = (psi + PI) * (L.band_n / (2.0 * PI));
+    int i = (int)floor(u);
+    double f = u - i;
+    i = ((i % L.band_n) + L.band_n) % L.band_n;
+    int j = (i + 1) % L.band_n;
+    double rc = L.band_rho[i] + (L.band_rho[j] - L.band_rho[i]) * f;
+    return fabs(rho - rc) < L.band_m;
+}
+
+}  // namespace
+
+// ---- router ------------------------------------------------------------------------------------
+__global__ void k_route(const TraceLaunch L) {
+    const so_frame& F = L.frames[0];
+    const long long n = L.nsamples;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const long long sid = base + threadIdx.x;
+        const bool valid = sid < n;
+        bool band = false;
+        if (valid) {
+            double x, yv;
+            sample_point(L.W, L.H, L.jitter, F, sid / L.spp, (int)(sid % L.spp), &x, &yv);
+            band = in_band(L, F, x, yv);
+        }
+        push(L.list64, &L.nlists[1], (uint32_t)sid, valid && band);
+        push(L.list32, &L.nlists[0], (uint32_t)sid, valid && !band);
+    }
+}
+
+// ---- FP64 approach -----------------------------------------------------------------------------
+// State planes (nsamples each): P0 = (r_hi, r_lo, pr_hi, pr_lo), P1 = (u_hi, u_lo, pu_hi, pu_lo),
+// P2 = (phi_hi, phi_lo, t_hi, t_lo), P3 = (lam, eta, E, h), P4 = (psi, attempts, accepted, ncross).
+__device__ __forceinline__ float2 split(double v) {
+    float hi = (float)v;
+    return make_float2(hi, (float)(v - (double)hi));
+}
+
+__global__ void __launch_bounds__(128) k_approach64(const TraceLaunch L) {
+    const so_frame& F = L.frames[0];
+    const so_scene& S = L.scenes[0];
+    const long long n = (long long)L.nlists[0];
+    const long long ns = L.nsamples;
+    unsigned long long n_att = 0, n_acc = 0;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const long long j = base + threadIdx.x;
+        bool park = false;
+        uint32_t sid = 0;
+        if (j < n) {
+            sid = L.list32[j];
+            double x, yv;
+            sample_point(L.W, L.H, L.jitter, F, sid / L.spp, (int)(sid % L.spp), &x, &yv);
+            RayC c;
+            double y[6], k1[6], yn[6], k7[6];
+            camera_photon(S.a, F.kp, F.ph, F.t, view_dir(F, x, yv), F.beta, c, y);
+            rhs(c, y, k1);
+            double h = initial_step(y);
+            int fate = 0, it = 0, nacc = 0, ncross = 0;
+            double psi = 0.0;
+            const bool radio = S.mode == SO_MODE_RADIO;
+            double sp = sqrt(fmax(fma(-y[2], y[2], 1.0), 0.0));
+            double s4, c4;
+            sincos(y[4], &s4, &c4);
+            double pp0 = sp * c4, pp1 = sp * s4, pp2 = y[2];
+            bool done = false;
+            for (; it < S.max_steps;) {
+                ++it;
+                double err = dp54(c, y, k1, h, S.tol, yn, k7);
+                if (!(err <= 1.0)) {
+                    h = reject_step(h, err);
+                    continue;
+                }
+                ++nacc;
+                if (radio) {
+                    double sn = sqrt(fmax(fma(-yn[2], yn[2], 1.0), 0.0));
+                    sincos(yn[4], &s4, &c4);
+                    double pn0 = sn * c4, pn1 = sn * s4, pn2 = yn[2];
+                    double cx = fma(pp1, pn2, -(pp2 * pn1)), cy = fma(pp2, pn0, -(pp0 * pn2)),
+                           cz = fma(pp0, pn1, -(pp1 * pn0));
+                    psi += atan2(sqrt(fma(cz, cz, fma(cy, cy, cx * cx))), fma(pp2, pn2, fma(pp1, pn1, pp0 * pn0)));
+                    pp0 = pn0;
+                    pp1 = pn1;
+                    pp2 = pn2;
+                }
+                if ((y[2] > 0.0) != (yn[2] > 0.0)) ++ncross;
+                double hc = h;
+                for (int i = 0; i < 6; ++i) {
+                    y[i] = yn[i];
+                    k1[i] = k7[i];
+                }
+                project_radial(c, y, k1);
+                h = accept_step(hc, err);
+                if (y[0] < S.r_stop) {
+                    fate = -1;
+                    done = true;
+                    break;
+                }
+                if (y[0] > S.r_escape && y[1] > 0.0) {
+                    fate = 1;
+                    done = true;
+                    break;
+                }
+                if (y[0] < L.r_switch) break;
+            }
+            n_att += (unsigned long long)it;
+            n_acc += (unsigned long long)nacc;
+            if (!done && it >= S.max_steps) done = true;  // step limit: fate 0
+            if (done) {
+                L.sample_out[sid] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (L.sample_fate) L.sample_fate[sid] = (int8_t)fate;
+            } else {
+                park = true;
+                float2 r = split(y[0]), pr = split(y[1]), u = split(y[2]), pu = split(y[3]), ph = split(y[4]),
+                       t = split(y[5]);
+                L.state[0 * ns + sid] = make_float4(r.x, r.y, pr.x, pr.y);
+                L.state[1 * ns + sid] = make_float4(u.x, u.y, pu.x, pu.y);
+                L.state[2 * ns + sid] = make_float4(ph.x, ph.y, t.x, t.y);
+                L.state[3 * ns + sid] = make_float4((float)c.lam, (float)c.eta, (float)c.E, (float)h);
+                L.state[4 * ns + sid] = make_float4((float)psi, __int_as_float(it), __int_as_float(nacc),
+                                                    __int_as_float(ncross));
+            }
+        }
+        push(L.parked, &L.nlists[3], sid, park);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        n_att += __shfl_down_sync(FULL, n_att, o);
+        n_acc += __shfl_down_sync(FULL, n_acc, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&L.counters->pad[0], n_att);  // FP64 attempts of the approach
+        atomicAdd(&L.counters->accepted, n_acc);
+    }
+}
+
+// ---- FP32 tracer -----------------------------------------------------------------------------------
+namespace {
+
+struct C32 {
+    float a, lam, eta, E, A2, CP, K, Q3;
+};
+
+// geodesic_rhs in FP32 (kerr.hpp:153-166); s2 = (1-u)(1+u) keeps its relative precision at the poles.
+__device__ __forceinline__ void rhs32(const C32& c, float r, float pr, float u, float pu, float* d) {
+    float Delta = fmaf(r, r - 2.f, c.A2);
+    float P = fmaf(r, r, c.CP);
+    d[0] = pr;
+    d[1] = fmaf(2.f * r, P, -((r - 1.f) * c.K));
+    d[2] = pu;
+    float u2 = u * u;
+    d[3] = u * fmaf(c.A2, fmaf(-2.f, u2, 1.f), -c.Q3);
+    float s2 = fmaxf((1.f - u) * (1.f + u), 1e-30f);
+    float iD = __frcp_rn(Delta);
+    d[4] = c.a - fmaf(c.a * P, iD, __fdividef(c.lam, s2));
+    d[5] = -fmaf(fmaf(r, r, c.A2) * P, iD, c.a * fmaf(-c.a, s2, c.lam));
+}
+
+// Two-sum: hi + lo + d renormalised (Knuth), the compensated state update.
+__device__ __forceinline__ void acc2(float& hi, float& lo, float d) {
+    float s = hi + d;
+    float bp = s - hi;
+    float e = (hi - (s - bp)) + (d - bp);
+    lo += e;
+    float s2 = s + lo;
+    lo = lo - (s2 - s);
+    hi = s2;
+}
+
+struct Ray32 {
+    float rh, rl, prh, prl, uh, ul, puh, pul, phh, phl, th, tl;
+    float k1[6];
+    float h, trans, psi, pp0, pp1, pp2;
+    float acc[4];
+    int ncross, natt, nacc, nflow, it;
+    uint32_t sid;
+};
+
+struct Torus32 {
+    int on, n_modes;
+    float ne_index, te_index, h_sph, theta_e0, half_var;
+};
+
+// Turbulence sum with the modes in shared memory as turns: phase/2pi and k/2pi.
+__device__ __forceinline__ float torus_delta32(const float4* __restrict__ km, const float* __restrict__ amp, int n,
+                                               float X, float Y, float Z) {
+    float acc0 = 0.f, acc1 = 0.f;
+    int m = 0;
+#pragma unroll 4
+    for (; m + 1 < n; m += 2) {
+        float4 a = km[m], b = km[m + 1];
+        float p = fmaf(a.z, Z, fmaf(a.y, Y, fmaf(a.x, X, a.w)));
+        float q = fmaf(b.z, Z, fmaf(b.y, Y, fmaf(b.x, X, b.w)));
+        p -= rintf(p);
+        q -= rintf(q);
+        acc0 = fmaf(amp[m], __cosf(6.28318530718f * p), acc0);
+        acc1 = fmaf(amp[m + 1], __cosf(6.28318530718f * q), acc1);
+    }
+    if (m < n) {
+        float4 a = km[m];
+        float p = fmaf(a.z, Z, fmaf(a.y, Y, fmaf(a.x, X, a.w)));
+        p -= rintf(p);
+        acc0 = fmaf(amp[m], __cosf(6.28318530718f * p), acc0);
+    }
+    return acc0 + acc1;
+}
+
+// flow_step (emission.cuh:264-340) in FP32.  t_rel is the emission time counted from the radial
+// light-travel time to the camera (see so_emission.cuh).  The reference plasma's fBm turbulence is
+// evaluated in FP64 coordinates (sheared_noise), as in the FP64 tracer.
+__device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp, const float4* km, const float* amp,
+                                            float r, float u, float phi, float t_rel, double t_abs, float lam,
+                                            float Ecam, float h, float* dI, float* dtau) {
+    *dI = 0.f;
+    *dtau = 0.f;
+    const float a = (float)S.a;
+    float s2 = fmaxf((1.f - u) * (1.f + u), 1e-12f), s = sqrtf(s2);
+    float R = r * s, z = r * u;
+    if (r > (float)S.r_flow_max || R < 1e-3f) return;
+    const float risco = (float)S.r_isco, rh = (float)S.rh;
+    float ne, Th;
+    if (tp.on) {
+        float zh = __fdividef(u, tp.h_sph);
+        float vert = __expf(-0.5f * zh * zh);
+        if (vert < 1e-7f) return;
+        float lx = __logf(__fdividef(r, rh));
+        ne = (float)S.n0 * __expf(-tp.ne_index * lx) * vert;
+        if (tp.n_modes > 0) {
+            float Rk = fmaxf(R, risco);
+            float Omf = (float)S.flow_kep * __frcp_rn(fmaf(Rk, sqrtf(Rk), a));
+            float phc = phi - Omf * t_rel;
+            float sp, cp;
+            __sincosf(phc, &sp, &cp);
+            float d = torus_delta32(km, amp, tp.n_modes, R * cp, R * sp, z);
+            ne *= __expf(d - tp.half_var);
+        }
+        Th = tp.theta_e0 * __expf(-tp.te_index * lx);
+    } else {
+        float zh = __fdividef(z, (float)S.h_r * R);
+        float vert = __expf(-0.5f * zh * zh);
+        if (vert < 1e-7f) return;
+        ne = (float)S.n0 * __expf(-(float)S.n_index * __logf(r)) * vert;
+        if (S.flow_turb_amp > 0.f) {
+            float n = sheared_noise(S, (double)R, (double)phi, (double)z, t_abs, S.flow_turb_scale, S.flow_tcorr,
+                                    S.seed ^ 0x51f15eedu);
+            ne *= __expf(S.flow_turb_amp * n - 0.5f * S.flow_turb_amp * S.flow_turb_amp);
+        }
+        Th = (float)S.theta0 * __expf(-(float)S.theta_index * __logf(r));
+    }
+    float dr = r - rh;
+    ne *= 1.f - __expf(-(dr * dr) * 4.f);
+    if (ne < 1e-30f) return;
+    // B^2 / 8 pi = ne m_p c^2 / (6 r beta)
+    const float kB = (float)(8.0 * PI * cgs::MP * cgs::C * cgs::C / 6.0);
+    float B = sqrtf(kB * ne / (r * (float)S.beta_p));
+    float r2 = r * r, a2 = a * a;
+    float Sigma = fmaf(a2, u * u, r2), Delta = fmaf(r, r - 2.f, a2);
+    float rpa = r2 + a2;
+    float A = fmaf(rpa, rpa, -(a2 * Delta * s2));
+    float iS = __frcp_rn(Sigma);
+    float g_tt = -(1.f - 2.f * r * iS), g_tph = -2.f * a * r * s2 * iS, g_phph = A * s2 * iS;
+    float omz = __fdividef(2.f * a * r, A);
+    float Rk = fmaxf(R, risco);
+    float Om = (float)S.flow_kep * __frcp_rn(fmaf(Rk, sqrtf(Rk), a));
+    float vmax = sqrtf(__fdividef(Sigma * Delta, A)) * rsqrtf(g_phph) * 0.999f;
+    Om = omz + fmaxf(-vmax, fminf(vmax, Om - omz));
+    float norm = -fmaf(g_phph * Om, Om, fmaf(2.f * g_tph, Om, g_tt));
+    if (norm <= 0.f) return;
+    float ut = rsqrtf(norm);
+    float kdotu = ut * fmaf(-Om, lam, 1.f);
+    float nu_f = (float)S.nu_obs * Ecam * kdotu;
+    float g = __fdividef((float)S.nu_obs, nu_f);
+    float u_ph = ut * fmaf(g_phph, Om, g_tph);
+    float kb = fmaf(-kdotu, u_ph, lam);
+    float bb = fmaf(u_ph, u_ph, g_phph);
+    float cosb = __fdividef(kb, kdotu * sqrtf(bb));
+    float sinb = sqrtf(fmaxf(fmaf(-cosb, cosb, 1.f), 1e-6f));
+    const float knuc = (float)(cgs::QE / (2.0 * PI * cgs::ME * cgs::C));
+    float nus = (2.f / 9.f) * knuc * B * Th * Th * sinb;
+    float Xs = __fdividef(nu_f, nus);
+    float x3 = cbrtf(Xs);
+    float k2 = __expf(table_lerp(S.k2_lntab, S.k2_n, S.k2_l0, S.k2_dl, __logf(Th)));
+    float brk = fmaf(1.887748625363387f, sqrtf(x3), sqrtf(Xs));
+    const float kj = (float)(1.4142135623730951 * PI * cgs::QE * cgs::QE / (3.0 * cgs::C));
+    float j = __fdividef(ne * kj * nus, k2) * brk * brk * __expf(-x3);
+    const float kte = (float)(cgs::H / (cgs::ME * cgs::C * cgs::C));  // h nu / (k Te) = kte nu / Th
+    float hnu = __fdividef(kte * nu_f, Th);
+    // 2 h nu^3 / c^2 with nu in GHz (2 h / c^2 itself is below the FP32 range)
+    const float kbn = (float)(2.0 * cgs::H / (cgs::C * cgs::C) * 1e27);
+    const float nu_g = nu_f * 1e-9f;
+    float Bnu = __fdividef(kbn * nu_g * nu_g * nu_g, expm1f(hnu));
+    float alpha = __fdividef(j, Bnu);
+    float dl = kdotu * Sigma * h * (float)S.rg_cm;
+    float tau = alpha * dl;
+    *dtau = tau;
+    *dI = g * g * g * Bnu * (-expm1f(-tau));
+}
+
+}  // namespace
+
+template <int VAR>
+__global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
+    extern __shared__ float4 sm4[];
+    const so_scene& S = L.scenes[0];
+    const so_frame& F = L.frames[0];
+    Torus32 tp;
+    tp.on = VAR == VAR_RADIO && L.torus;
+    tp.n_modes = L.n_modes;
+    tp.ne_index = (float)L.ne_index;
+    tp.te_index = (float)L.te_index;
+    tp.h_sph = (float)L.h_sph;
+    tp.theta_e0 = (float)L.theta_e0;
+    tp.half_var = (float)L.half_var;
+    float4* km = sm4;
+    float* amp = reinterpret_cast<float*>(sm4 + L.n_modes);
+    if (tp.on) {
+        const double i2pi = 1.0 / (2.0 * PI);
+        for (int i = threadIdx.x; i < L.n_modes; i += blockDim.x) {
+            so_mode m = L.modes[i];
+            km[i] = make_float4((float)(m.kx * i2pi), (float)(m.ky * i2pi), (float)(m.kz * i2pi),
+                                (float)(m.phase * i2pi));
+            amp[i] = (float)m.amp;
+        }
+        __syncthreads();
+    }
+    const long long ns = L.nsamples;
+    const long long total = (long long)L.nlists[3];
+    const uint32_t* work = L.parked;
+    const int lane = threadIdx.x & 31;
+    const float tol = (float)L.tol32;
+    const float rstop = (float)S.r_stop, resc = (float)S.r_escape, rflow = (float)S.r_flow_max;
+    const float step_frac = (float)S.step_frac;
+    const float rcam_hi = (float)F.r, rcam_lo = (float)(F.r - (double)(float)F.r);
+    const bool radio = VAR == VAR_RADIO;
+    C32 c;
+    c.a = (float)S.a;
+    c.A2 = c.a * c.a;
+    Ray32 R;
+    bool active = false, exhausted = false;
+    unsigned long long n_att = 0, n_acc = 0, n_flow = 0, n_lim = 0, n_redo = 0;
+    for (;;) {
+        const bool need = !active && !exhausted;
+        const unsigned m = __ballot_sync(FULL, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&L.counters->next, (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, leader);
+            if (need) {
+                const unsigned long long j = base + __popc(m & ((1u << lane) - 1u));
+                if (j >= (unsigned long long)total) {
+                    exhausted = true;
+                } else {
+                    active = true;
+                    const uint32_t sid = work[j];
+                    R.sid = sid;
+                    float4 p0 = L.state[0 * ns + sid], p1 = L.state[1 * ns + sid], p2 = L.state[2 * ns + sid],
+                           p3 = L.state[3 * ns + sid], p4 = L.state[4 * ns + sid];
+                    R.rh = p0.x; R.rl = p0.y; R.prh = p0.z; R.prl = p0.w;
+                    R.uh = p1.x; R.ul = p1.y; R.puh = p1.z; R.pul = p1.w;
+                    R.phh = p2.x; R.phl = p2.y; R.th = p2.z; R.tl = p2.w;
+                    c.lam = p3.x;
+                    c.eta = p3.y;
+                    c.E = p3.z;
+                    R.h = p3.w;
+                    R.psi = p4.x;
+                    R.natt = __float_as_int(p4.y);
+                    R.nacc = __float_as_int(p4.z);
+                    R.ncross = __float_as_int(p4.w);
+                    R.it = R.natt;
+                    R.nflow = 0;
+                    c.CP = fmaf(-c.a, c.lam, c.A2);
+                    float lma = c.lam - c.a;
+                    c.K = fmaf(lma, lma, c.eta);
+                    c.Q3 = fmaf(c.lam, c.lam, c.eta);
+                    R.trans = 1.f;
+                    R.acc[0] = R.acc[1] = R.acc[2] = R.acc[3] = 0.f;
+                    rhs32(c, R.rh + R.rl, R.prh + R.prl, R.uh + R.ul, R.puh + R.pul, R.k1);
+                    float u = R.uh + R.ul, sp = sqrtf(fmaxf((1.f - u) * (1.f + u), 0.f)), s4, c4;
+                    __sincosf(R.phh + R.phl, &s4, &c4);
+                    R.pp0 = sp * c4;
+                    R.pp1 = sp * s4;
+                    R.pp2 = u;
+                }
+            }
+        }
+        if (__all_sync(FULL, !active)) break;
+        if (!active) continue;
+        // ---- one DP5(4) attempt in FP32 -----------------------------------------------------------
+        int fate = 2;  // 2 = running, 3 = re-trace in FP64
+        if (R.it >= S.max_steps) {
+            fate = 0;
+        } else {
+            ++R.it;
+            ++R.natt;
+            const float y0 = R.rh + R.rl, y1 = R.prh + R.prl, y2 = R.uh + R.ul, y3 = R.puh + R.pul;
+            float hc = R.h;
+            if (radio && S.flow_on && y0 < rflow) {
+                float s = sqrtf(fmaxf((1.f - y2) * (1.f + y2), 0.f));
+                float cap = step_frac * fminf(__fdividef(y0, fabsf(y1) + 1e-30f),
+                                              __fdividef(fmaxf(s, 0.05f), fabsf(y3) + 1e-30f));
+                hc = fminf(hc, cap);
+            } else if (VAR != VAR_VACUUM && S.disk_on) {
+                hc = fminf(hc, __fdividef(0.3f, fabsf(y3) + 1e-30f));
+            }
+            const float* k1 = R.k1;
+            float k2[6], k3[6], k4[6], k5[6], k6[6], k7[6];
+            const float yy[4] = {y0, y1, y2, y3};
+            float t[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, (float)A21 * k1[i], yy[i]);
+            rhs32(c, t[0], t[1], t[2], t[3], k2);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, fmaf((float)A32, k2[i], (float)A31 * k1[i]), yy[i]);
+            rhs32(c, t[0], t[1], t[2], t[3], k3);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                t[i] = fmaf(hc, fmaf((float)A43, k3[i], fmaf((float)A42, k2[i], (float)A41 * k1[i])), yy[i]);
+            rhs32(c, t[0], t[1], t[2], t[3], k4);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                t[i] = fmaf(hc, fmaf((float)A54, k4[i], fmaf((float)A53, k3[i], fmaf((float)A52, k2[i],
+                                                                                    (float)A51 * k1[i]))), yy[i]);
+            rhs32(c, t[0], t[1], t[2], t[3], k5);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                t[i] = fmaf(hc, fmaf((float)A65, k5[i], fmaf((float)A64, k4[i], fmaf((float)A63, k3[i],
+                               fmaf((float)A62, k2[i], (float)A61 * k1[i])))), yy[i]);
+            rhs32(c, t[0], t[1], t[2], t[3], k6);
+            float dy[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                dy[i] = hc * fmaf((float)B6, k6[i], fmaf((float)B5, k5[i], fmaf((float)B4, k4[i],
+                                  fmaf((float)B3, k3[i], (float)B1 * k1[i]))));
+            // candidate state (compensated), then k7 = f(y_new)
+            float nrh = R.rh, nrl = R.rl, nprh = R.prh, nprl = R.prl, nuh = R.uh, nul = R.ul, npuh = R.puh,
+                  npul = R.pul;
+            acc2(nrh, nrl, dy[0]);
+            acc2(nprh, nprl, dy[1]);
+            acc2(nuh, nul, dy[2]);
+            acc2(npuh, npul, dy[3]);
+            const float n0 = nrh + nrl, n1 = nprh + nprl, n2 = nuh + nul, n3 = npuh + npul;
+            rhs32(c, n0, n1, n2, n3, k7);
+            // error norm of kerr.hpp:193-205 at tol32, with a floor of a few ulp of each scale so the
+            // controller does not chase FP32 rounding
+            float sc[5];
+            sc[0] = tol * (1e-6f + fmaxf(fabsf(y0), fabsf(n0)));
+            sc[1] = tol * (1e-6f + fmaxf(fmaxf(fabsf(y1), fabsf(n1)), y0 * y0));
+            sc[2] = tol;
+            sc[3] = tol * fmaxf(1.f, fmaxf(fabsf(y3), fabsf(n3)));
+            sc[4] = tol * 4.f;
+            float err = 0.f;
+#pragma unroll
+            for (int i = 0; i < 5; ++i) {
+                float e = hc * fmaf((float)E7, k7[i], fmaf((float)E6, k6[i], fmaf((float)E5, k5[i],
+                                    fmaf((float)E4, k4[i], fmaf((float)E3, k3[i], (float)E1 * k1[i])))));
+                err = fmaxf(err, __fdividef(fabsf(e), sc[i]));
+            }
+            if (!(err <= 1.f)) {
+                R.h = hc * fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f));
+                if (!(err == err)) R.h = hc * 0.1f;
+            } else {
+                ++R.nacc;
+                if (radio) {
+                    float sn = sqrtf(fmaxf((1.f - n2) * (1.f + n2), 0.f)), s4, c4;
+                    float phn = (R.phh + R.phl) + dy[4];
+                    __sincosf(phn, &s4, &c4);
+                    float pn0 = sn * c4, pn1 = sn * s4, pn2 = n2;
+                    float cx = fmaf(R.pp1, pn2, -(R.pp2 * pn1)), cy = fmaf(R.pp2, pn0, -(R.pp0 * pn2)),
+                          cz = fmaf(R.pp0, pn1, -(R.pp1 * pn0));
+                    R.psi += atan2f(sqrtf(fmaf(cz, cz, fmaf(cy, cy, cx * cx))),
+                                    fmaf(R.pp2, pn2, fmaf(R.pp1, pn1, R.pp0 * pn0)));
+                    R.pp0 = pn0;
+                    R.pp1 = pn1;
+                    R.pp2 = pn2;
+                }
+                const bool crossed = (y2 > 0.f) != (n2 > 0.f);
+                if (crossed) ++R.ncross;
+                const bool turned = (y1 < 0.f) && (n1 >= 0.f) && n0 < (float)L.turn_r;
+                if (turned) fate = 3;
+                if (VAR != VAR_VACUUM && S.disk_on && crossed && fate == 2) {
+                    // rare: the disk shading of the FP64 tracer on the promoted endpoints
+                    double lo = 0.0, hi = 1.0, u0 = y2, u1 = n2, m0 = (double)y3 * hc, m1 = (double)n3 * hc;
+                    for (int b = 0; b < 40; ++b) {
+                        double mid = 0.5 * (lo + hi);
+                        double um = hermite(u0, u1, m0, m1, mid);
+                        if ((um > 0.0) == (u0 > 0.0)) lo = mid;
+                        else hi = mid;
+                    }
+                    double scr = 0.5 * (lo + hi);
+                    double rc = hermite(y0, n0, (double)y1 * hc, (double)n1 * hc, scr);
+                    double ph0 = (double)R.phh + R.phl, t0 = (double)R.th + R.tl;
+                    double pc = hermite(ph0, ph0 + dy[4], (double)k1[4] * hc, (double)k7[4] * hc, scr);
+                    double tcv = hermite(t0, t0 + dy[5], (double)k1[5] * hc, (double)k7[5] * hc, scr);
+                    float cs[4];
+                    disk_shade(S, rc, pc, tcv, c.lam, c.eta, c.E, cs);
+                    if (cs[3] > 0.f) {
+                        float tf = R.trans;
+                        R.acc[0] += tf * cs[0];
+                        R.acc[1] += tf * cs[1];
+                        R.acc[2] += tf * cs[2];
+                        R.acc[3] += tf * cs[1] * (float)(R.ncross - 1);
+                        R.trans *= 1.f - cs[3];
+                        if (R.trans < 1e-4f) fate = -1;
+                    }
+                }
+                if (radio && S.flow_on && n0 < rflow && fate == 2) {
+                    float ph_new_h = R.phh, ph_new_l = R.phl, t_new_h = R.th, t_new_l = R.tl;
+                    acc2(ph_new_h, ph_new_l, dy[4]);
+                    acc2(t_new_h, t_new_l, dy[5]);
+                    float t_rel = ((t_new_h + rcam_hi) + (t_new_l + rcam_lo)) - n0 +
+                                  2.f * __logf(__fdividef(rcam_hi, n0));
+                    float dI, dtau;
+                    flow_step32(S, tp, km, amp, n0, n2, ph_new_h + ph_new_l, t_rel, (double)t_new_h + t_new_l, c.lam,
+                                c.E, hc, &dI, &dtau);
+                    ++R.nflow;
+                    float cc = R.trans * dI;
+                    int nb = (int)(R.psi * (float)(1.0 / PI));
+                    R.acc[0] += cc;
+                    if (nb == 1) R.acc[1] += cc;
+                    else if (nb == 2) R.acc[2] += cc;
+                    else if (nb >= 3) R.acc[3] += cc;
+                    R.trans *= __expf(-dtau);
+                    if (R.trans < 1e-5f) fate = -1;
+                }
+                // commit the step
+                R.rh = nrh; R.rl = nrl; R.prh = nprh; R.prl = nprl;
+                R.uh = nuh; R.ul = nul; R.puh = npuh; R.pul = npul;
+                acc2(R.phh, R.phl, dy[4]);
+                acc2(R.th, R.tl, dy[5]);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) R.k1[i] = k7[i];
+                // project_radial (kerr.hpp:216-223) in FP32
+                {
+                    float r = n0, P = fmaf(r, r, c.CP), D = fmaf(r, r - 2.f, c.A2);
+                    float Rr = fmaf(P, P, -(D * c.K)), r2 = r * r;
+                    if (Rr > 0.25f * (r2 * r2)) {
+                        float v = sqrtf(Rr);
+                        float pr = n1 < 0.f ? -v : v;
+                        R.prh = pr;
+                        R.prl = 0.f;
+                        R.k1[0] = pr;
+                    }
+                }
+                R.h = hc * fminf(5.f, fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f)));
+                if (fate == 2) {
+                    if (n0 < rstop) fate = -1;
+                    else if (n0 > resc && R.prh > 0.f) fate = 1;
+                }
+            }
+        }
+        if (fate == 2) continue;
+        // ---- ray finished: FP64 Carter-constant / radial constraint check ------------------------
+        if (fate != 3 && fate != 0) {
+            double r = (double)R.rh + R.rl, pr = (double)R.prh + R.prl, u = (double)R.uh + R.ul,
+                   pu = (double)R.puh + R.pul;
+            double lam = c.lam, eta = c.eta, a = S.a;
+            double U = (1.0 - u * u) * (eta + a * a * u * u) - lam * lam * u * u;
+            double scaleU = eta + a * a + lam * lam + 1e-12;
+            double P = r * r + a * a - a * lam, D = r * r - 2.0 * r + a * a;
+            double Rr = P * P - D * (eta + (lam - a) * (lam - a));
+            double dU = fabs(pu * pu - U) / scaleU, dR = fabs(pr * pr - Rr) / (r * r * r * r);
+            if (dU > L.drift_tol || dR > L.drift_tol) fate = 3;
+        }
+        n_att += (unsigned long long)R.natt;
+        n_acc += (unsigned long long)R.nacc;
+        n_flow += (unsigned long long)R.nflow;
+        if (fate == 0) ++n_lim;
+        const bool redo = fate == 3;
+        if (!redo) {
+            L.sample_out[R.sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
+            if (L.sample_fate) L.sample_fate[R.sid] = (int8_t)fate;
+        }
+        n_redo += redo ? 1 : 0;
+        active = false;
+        // re-trace list: lanes finish at different iterations, so append without a warp vote
+        if (redo) L.redo[atomicAdd(&L.nlists[2], 1ull)] = R.sid;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        n_att += __shfl_down_sync(FULL, n_att, o);
+        n_acc += __shfl_down_sync(FULL, n_acc, o);
+        n_flow += __shfl_down_sync(FULL, n_flow, o);
+        n_lim += __shfl_down_sync(FULL, n_lim, o);
+        n_redo += __shfl_down_sync(FULL, n_redo, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&L.counters->attempts, n_att);
+        atomicAdd(&L.counters->pad[1], n_acc);  // FP32 accepted steps
+        atomicAdd(&L.counters->flow_steps, n_flow);
+        atomicAdd(&L.counters->step_limited, n_lim);
+        atomicAdd(&L.counters->fp64_rays, n_redo);
+    }
+}
+
+// Per pixel: sum of its spp samples in sample order, and (sum Y, sum Y^2) (k_pass1, render.cu:103-113).
+__global__ void k_gather_samples(const TraceLaunch L) {
+    const long long npix = (long long)L.W * L.H;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, ys = 0.f, yq = 0.f;
+    const bool radio = L.scenes[0].mode == SO_MODE_RADIO;
+    for (int s = 0; s < L.spp; ++s) {
+        float4 v = L.sample_out[p * L.spp + s];
+        a0 += v.x;
+        a1 += v.y;
+        a2 += v.z;
+        a3 += v.w;
+        float Y = radio ? v.x : v.y;
+        ys += Y;
+        yq += Y * Y;
+    }
+    reinterpret_cast<float4*>(L.accum)[p] = make_float4(a0, a1, a2, a3);
+    if (L.ystat) reinterpret_cast<float2*>(L.ystat)[p] = make_float2(ys, yq);
+}
+
+// ---- launchers -----------------------------------------------------------------------------------
+cudaError_t launch_route(const TraceLaunch& L, cudaStream_t st) {
+    long long blocks = (L.nsamples + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_route<<<(int)(blocks > 0 ? blocks : 1), 256, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st) {
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_approach64, 128, 0);
+    if (e != cudaSuccess) return e;
+    long long grid = (long long)num_sms * (per_sm > 0 ? per_sm : 1);
+    long long want = (n + 127) / 128;
+    if (grid > want) grid = want > 0 ? want : 1;
+    k_approach64<<<(int)grid, 128, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st) {
+    const bool torus = L.torus && L.n_modes > 0;
+    size_t smem = torus ? (size_t)L.n_modes * (sizeof(float4) + sizeof(float)) : 0;
+    int per_sm = 1;
+    cudaError_t e;
+    auto go = [&](auto kern) -> cudaError_t {
+        if (smem > 48 * 1024) {
+            cudaError_t e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e2 != cudaSuccess) return e2;
+        }
+        cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem);
+        if (e2 != cudaSuccess) return e2;
+        long long grid = (long long)num_sms * (per_sm > 0 ? per_sm : 1);
+        long long want = (n + 127) / 128;
+        if (grid > want) grid = want > 0 ? want : 1;
+        kern<<<(int)grid, 128, smem, st>>>(L);
+        return cudaGetLastError();
+    };
+    switch (variant) {
+        case VAR_VACUUM: e = go(k_trace32<VAR_VACUUM>); break;
+        case VAR_DISK: e = go(k_trace32<VAR_DISK>); break;
+        default: e = go(k_trace32<VAR_RADIO>); break;
+    }
+    return e;
+}
+
+cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st) {
+    long long npix = (long long)L.W * L.H;
+    k_gather_samples<<<(int)((npix + 255) / 256), 256, 0, st>>>(L);
+    return cudaGetLastError();
+}
 
 }  // namespace so

@@ -39,6 +39,21 @@ __device__ __forceinline__ void r2_sample(uint32_t n, float r0, float r1, float*
 }
 __device__ __forceinline__ float lerpf_(float a, float b, float t) { return a + (b - a) * t; }
 
+// Tangent-plane point of sample s of pixel q in a W x H frame: pixel_seed + R2 jitter + sample_pixel
+// (render.cu:70-85), or the pixel centre when jitter == 0.
+__device__ __forceinline__ void sample_point(int W, int H, int jitter, const so_frame& F, long long q, int s,
+                                             double* x, double* yv) {
+    int px = (int)(q % W), py = (int)(q / W);
+    float jx = 0.5f, jy = 0.5f;
+    if (jitter) {
+        uint32_t h = pcg((uint32_t)q * 0x9E3779B9u ^ F.seed);
+        float r0 = rnd(h), r1 = rnd(h);
+        r2_sample((uint32_t)s, r0, r1, &jx, &jy);
+    }
+    *x = (px + jx - 0.5 * W) * F.pix;
+    *yv = (0.5 * H - (py + jy)) * F.pix;
+}
+
 __device__ __forceinline__ float grad3(int ix, int iy, int iz, uint32_t seed, float fx, float fy, float fz) {
     uint32_t h = pcg((uint32_t)ix * 73856093u ^ pcg((uint32_t)iy * 19349663u ^ pcg((uint32_t)iz * 83492791u ^ seed)));
     switch (h % 12u) {
@@ -47,7 +62,7 @@ __device__ __forceinline__ float grad3(int ix, int iy, int iz, uint32_t seed, fl
         case 8: return fy + fz;   case 9: return -fy + fz;  case 10: return fy - fz;  default: return -fy - fz;
     }
 }
-__device__ float gnoise(float x, float y, float z, uint32_t seed) {
+static __device__ float gnoise(float x, float y, float z, uint32_t seed) {
     float fx = floorf(x), fy = floorf(y), fz = floorf(z);
     int ix = (int)fx, iy = (int)fy, iz = (int)fz;
     float ux = x - fx, uy = y - fy, uz = z - fz;
@@ -66,7 +81,7 @@ __device__ float gnoise(float x, float y, float z, uint32_t seed) {
     float x01 = lerpf_(n001, n101, wx), x11 = lerpf_(n011, n111, wx);
     return lerpf_(lerpf_(x00, x10, wy), lerpf_(x01, x11, wy), wz);
 }
-__device__ float fbm3(float x, float y, float z, int oct, uint32_t seed) {
+static __device__ float fbm3(float x, float y, float z, int oct, uint32_t seed) {
     float s = 0.f, amp = 1.f, norm = 0.f;
     for (int i = 0; i < oct; ++i) {
         s += amp * gnoise(x, y, z, seed + 1013u * (uint32_t)i);
@@ -101,7 +116,7 @@ __device__ __forceinline__ void blackbody_xyz(const so_scene& S, float T, float*
 
 __device__ __forceinline__ double keplerian_omega(double a, double R) { return 1.0 / fma(R, sqrt(R), a); }
 
-__device__ float sheared_noise(const so_scene& S, double R, double phi, double z, double t, float scale, float tcorr,
+static __device__ float sheared_noise(const so_scene& S, double R, double phi, double z, double t, float scale, float tcorr,
                                uint32_t seed) {
     double Om = keplerian_omega(S.a, fmax(R, S.r_isco));
     double P = 6.283185307179586 / Om * (double)tcorr;
@@ -130,7 +145,7 @@ __device__ __forceinline__ double circ_ut(double a, double r) {
     return fma(r, sr, a) / (q * q * q * sqrt(fmax(fma(r, sr, -3.0 * sr) + 2.0 * a, 1e-12)));
 }
 
-__device__ void disk_shade(const so_scene& S, double r, double phi, double t, double lam, double eta, double Ecam,
+static __device__ void disk_shade(const so_scene& S, double r, double phi, double t, double lam, double eta, double Ecam,
                            float* out) {
     out[0] = out[1] = out[2] = out[3] = 0.f;
     if (r < S.disk_rin || r > S.disk_rout) return;
@@ -203,7 +218,7 @@ __device__ __forceinline__ double torus_delta(const ModesSmem& md, int n, double
 // t + (rcam - r + 2 ln(rcam / r)) (the retarded time of emission.cuh:26-28 plus the frame time):
 // the raw coordinate time is ~ -rcam at the hole, which would put a factor rcam on every rounding
 // error of the advected phase.
-__device__ void flow_step(const so_scene& S, const TorusParams& tp, const ModesSmem& md, double rcam, double r,
+static __device__ void flow_step(const so_scene& S, const TorusParams& tp, const ModesSmem& md, double rcam, double r,
                           double u, double phi, double t, double lam, double Ecam, double h, double* dI,
                           double* dtau) {
     *dI = 0.0;

@@ -1,5 +1,7 @@
 // so_launch.h -- launch descriptors shared by the host renderer and the CUDA kernels.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "../../include/so_tracer.h"
@@ -10,7 +12,8 @@ namespace so {
 enum RayKind : int {
     RAYS_LIST = 0,   // explicit tangent-plane points x[i], y[i] of frame 0, one sample each
     RAYS_PIXELS = 1, // every pixel of every frame, spp samples per pixel (frames share W, H, spp)
-    RAYS_CHUNKS = 2  // adaptive pass 2: job j = `chunk` more samples of the pixel owning chunk j
+    RAYS_CHUNKS = 2, // adaptive pass 2: job j = `chunk` more samples of the pixel owning chunk j
+    RAYS_SAMPLES = 3 // job j = sample list[j] (pixel * spp + s) of the pixel grid; result per sample
 };
 
 // Scene features a kernel instantiation supports (uniform over the frames of one launch).
@@ -53,13 +56,33 @@ struct TraceLaunch {
     float* accum;             // RAYS_PIXELS: W*H*nframes*4 sums
     float* ystat;             // RAYS_PIXELS: W*H*nframes*2 (sum Y, sum Y^2), or NULL
     Counters* counters;
+    const unsigned long long* nrays_dev;  // if set, the job count is read from device memory
     // RAYS_CHUNKS
     const uint32_t* offsets;  // exclusive scan of chunks per pixel (W*H)
     float* chunk_acc;         // per chunk: 4 float sums
     int chunk;                // samples per chunk
+    // RAYS_SAMPLES
+    const uint32_t* list;     // sample ids
+    float4* sample_out;       // per sample id: the sample's accumulated value
+    int8_t* sample_fate;      // per sample id, or NULL
     // mixed precision
-    double band_m, tol32, turn_frac, drift_tol;
-    const uint8_t* band_mask; // per ray: 1 = integrate in FP64 (critical band), or NULL
+    double band_m, tol32, turn_r, drift_tol;
+    double r_switch;          // FP64 approach down to this radius, FP32 inside
+    const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi
+    int band_n;
+    float4* state;            // parked ray state, 5 float4 per sample id (SoA planes of nsamples)
+    long long nsamples;       // W * H * spp
+    uint32_t* list32;         // FP32 work list (sample ids), filled by the router / approach
+    uint32_t* list64;         // FP64 work list (band rays), filled by the router
+    uint32_t* redo;           // FP64 re-trace list (drift check / radial turning point near the hole)
+    uint32_t* parked;         // rays parked at r_switch by the FP64 approach (the FP32 work list)
+    unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked counts
 };
+
+// Mixed-path kernels (k_trace_mixed.cu).
+cudaError_t launch_route(const TraceLaunch& L, cudaStream_t st);
+cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st);
+cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
+cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);
 
 }  // namespace so

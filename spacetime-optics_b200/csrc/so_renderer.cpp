@@ -77,7 +77,19 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 1e-6, 1e-3, 1e-6};
+    so_mixed_opts mixed{0.05, 3e-6, 3.5, 1e-4, 0.0};
+    // mixed-path buffers (grown on demand) and the critical-curve table of the current frame
+    long long mixed_cap = 0;
+    float4 *d_state = nullptr, *d_sample_out = nullptr;
+    int8_t* d_sample_fate = nullptr;
+    uint32_t *d_list32 = nullptr, *d_list64 = nullptr, *d_redo = nullptr, *d_parked = nullptr;
+    unsigned long long* d_nlists = nullptr;
+    Counters* d_cnt3 = nullptr;  // band and re-trace launches run on their own queue heads
+    float* d_band = nullptr;
+    double band_a = -1.0, band_th = -1.0;
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev32[2] = {nullptr, nullptr};  // around the FP32 tracer launch
     std::string err;
 };
 
@@ -114,7 +126,54 @@ void free_all(so_renderer* r) {
                   r->d_tiles, r->d_err, r->d_part, r->d_fsum, r->d_cnt, r->d_x, r->d_y, r->d_rays, r->d_modes};
     for (void* p : ps)
         if (p) cudaFree(p);
+    void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked,
+                  r->d_nlists, r->d_cnt3, r->d_band};
+    for (void* p : pm)
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : r->ev32)
+        if (e) cudaEventDestroy(e);
+    if (r->ev_fork) cudaEventDestroy(r->ev_fork);
+    if (r->ev_join) cudaEventDestroy(r->ev_join);
+    if (r->st2) cudaStreamDestroy(r->st2);
     if (r->st) cudaStreamDestroy(r->st);
+}
+
+constexpr int BAND_N = 2048;
+
+// Critical curve rho_c(psi) of a distant observer at inclination th (critical_curve_point,
+// kerr.hpp:260-270, both signs of beta), tabulated on BAND_N image angles psi in [-pi, pi).
+std::vector<float> band_table(double a, double th) {
+    std::vector<float> out(BAND_N);
+    if (a < 1e-4) {  // the 1/a parametrisation degenerates: Schwarzschild circle sqrt(27)
+        for (auto& v : out) v = (float)std::sqrt(27.0);
+        return out;
+    }
+    double rp0 = 2.0 * (1.0 + std::cos(2.0 / 3.0 * std::acos(-a))), rp1 = 2.0 * (1.0 + std::cos(2.0 / 3.0 * std::acos(a)));
+    std::vector<std::pair<double, double>> pts;
+    const int N = 40000;
+    for (int i = 0; i <= N; ++i) {
+        double rp = rp0 + (rp1 - rp0) * i / N, al, be;
+        if (!critical_curve_point(a, th, rp, &al, &be)) continue;
+        pts.push_back({std::atan2(be, al), std::hypot(al, be)});
+        pts.push_back({std::atan2(-be, al), std::hypot(al, be)});
+    }
+    if (pts.size() < 4) {
+        for (auto& v : out) v = (float)std::sqrt(27.0);
+        return out;
+    }
+    std::sort(pts.begin(), pts.end());
+    for (int j = 0; j < BAND_N; ++j) {
+        double psi = -PI + 2.0 * PI * j / BAND_N;
+        auto it = std::lower_bound(pts.begin(), pts.end(), std::make_pair(psi, -1.0));
+        const auto& hi = it == pts.end() ? pts.front() : *it;
+        const auto& lo = it == pts.begin() ? pts.back() : *(it - 1);
+        double p0 = lo.first, p1 = hi.first;
+        if (p1 < p0) p1 += 2.0 * PI;
+        double pj = psi < p0 ? psi + 2.0 * PI : psi;
+        double f = p1 > p0 ? (pj - p0) / (p1 - p0) : 0.0;
+        out[j] = (float)(lo.second + (hi.second - lo.second) * f);
+    }
+    return out;
 }
 
 int upload_scene(so_renderer* r) {
@@ -144,15 +203,101 @@ void launch_common(so_renderer* r, TraceLaunch& L) {
     L.modes = r->d_modes;
     L.band_m = r->mixed.band_m;
     L.tol32 = r->mixed.tol32;
-    L.turn_frac = r->mixed.turn_frac;
+    L.turn_r = r->mixed.turn_r;
     L.drift_tol = r->mixed.drift_tol;
 }
 
-int run_tracer(so_renderer* r, const TraceLaunch& L) {
-    int var = variant_of(r->S);
-    cudaError_t e = r->precision == SO_PREC_MIXED ? launch_trace_mixed(L, var, r->num_sms, r->st)
-                                                  : launch_trace64(L, var, r->num_sms, r->st);
+int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
+    cudaError_t e = launch_trace64(L, variant_of(r->S), r->num_sms, st ? st : r->st);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
+
+// Pass 1 of the mixed path into d_accum / d_ystat (see k_trace_mixed.cu):
+//   route (band / FP32 lists) -> FP64 approach to r_switch -> FP32 tracer, with the band list traced
+//   by the FP64 tracer on a second stream meanwhile, then the FP64 re-trace list, then the
+//   per-pixel gather of the samples.  Counts stay on the device: nothing waits on the host.
+int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
+    const long long ns = (long long)f.W * f.H * f.spp;
+    if (ns > 0xffffffffll) return fail(r, SO_ERR_SIZE, "mixed path: more than 2^32 samples per frame");
+    if (ns > r->mixed_cap) {
+        void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked};
+        for (void* p : pm)
+            if (p) cudaFree(p);
+        r->d_state = r->d_sample_out = nullptr;
+        r->d_sample_fate = nullptr;
+        r->d_list32 = r->d_list64 = r->d_redo = r->d_parked = nullptr;
+        r->mixed_cap = 0;
+        if (dalloc(&r->d_state, (size_t)ns * 5) != cudaSuccess || dalloc(&r->d_sample_out, (size_t)ns) != cudaSuccess ||
+            dalloc(&r->d_sample_fate, (size_t)ns) != cudaSuccess || dalloc(&r->d_list32, (size_t)ns) != cudaSuccess ||
+            dalloc(&r->d_list64, (size_t)ns) != cudaSuccess || dalloc(&r->d_redo, (size_t)ns) != cudaSuccess ||
+            dalloc(&r->d_parked, (size_t)ns) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "mixed path: device allocation");
+        r->mixed_cap = ns;
+    }
+    if (!r->d_nlists) {
+        if (dalloc(&r->d_nlists, 4) != cudaSuccess || dalloc(&r->d_cnt3, 2) != cudaSuccess ||
+            dalloc(&r->d_band, BAND_N) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "mixed path: device allocation");
+        SO_CK(r, cudaStreamCreateWithFlags(&r->st2, cudaStreamNonBlocking));
+        SO_CK(r, cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming));
+        SO_CK(r, cudaEventCreateWithFlags(&r->ev_join, cudaEventDisableTiming));
+        SO_CK(r, cudaEventCreate(&r->ev32[0]));
+        SO_CK(r, cudaEventCreate(&r->ev32[1]));
+    }
+    if (r->band_a != r->S.a || r->band_th != f.th) {
+        std::vector<float> tab = band_table(r->S.a, f.th);
+        SO_CK(r, cudaMemcpyAsync(r->d_band, tab.data(), BAND_N * sizeof(float), cudaMemcpyHostToDevice, r->st));
+        SO_CK(r, cudaStreamSynchronize(r->st));
+        r->band_a = r->S.a;
+        r->band_th = f.th;
+    }
+    double rsw = r->mixed.r_switch;
+    if (!(rsw > 0.0)) {
+        rsw = 100.0;
+        if (r->S.flow_on) rsw = std::max(rsw, 1.5 * r->S.r_flow_max);
+        if (r->S.disk_on) rsw = std::max(rsw, 1.2 * r->S.disk_rout);
+    }
+    L.r_switch = rsw;
+    L.band_rho = r->d_band;
+    L.band_n = BAND_N;
+    L.nsamples = ns;
+    L.state = r->d_state;
+    L.sample_out = r->d_sample_out;
+    L.sample_fate = r->d_sample_fate;
+    L.list32 = r->d_list32;
+    L.list64 = r->d_list64;
+    L.redo = r->d_redo;
+    L.parked = r->d_parked;
+    L.nlists = r->d_nlists;
+    SO_CK(r, cudaMemsetAsync(r->d_nlists, 0, 4 * sizeof(unsigned long long), r->st));
+    SO_CK(r, cudaMemsetAsync(r->d_cnt3, 0, 2 * sizeof(Counters), r->st));
+    SO_CK(r, launch_route(L, r->st));
+    // band rays: plain FP64 tracer on the second stream, concurrently with the FP32 work
+    SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
+    SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
+    TraceLaunch Lb = L;
+    Lb.kind = RAYS_SAMPLES;
+    Lb.list = r->d_list64;
+    Lb.nrays = ns;
+    Lb.nrays_dev = &r->d_nlists[1];
+    Lb.counters = &r->d_cnt3[0];
+    int rc = run_tracer(r, Lb, r->st2);
+    if (rc) return rc;
+    SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
+    SO_CK(r, launch_approach64(L, ns, r->num_sms, r->st));
+    SO_CK(r, cudaEventRecord(r->ev32[0], r->st));
+    SO_CK(r, launch_trace32(L, ns, variant_of(r->S), r->num_sms, r->st));
+    SO_CK(r, cudaEventRecord(r->ev32[1], r->st));
+    // FP64 re-trace of the rays the FP32 tracer handed back
+    TraceLaunch Lr = Lb;
+    Lr.list = r->d_redo;
+    Lr.nrays_dev = &r->d_nlists[2];
+    Lr.counters = &r->d_cnt3[1];
+    rc = run_tracer(r, Lr, r->st);
+    if (rc) return rc;
+    SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
+    SO_CK(r, launch_gather_samples(L, r->st));
     return SO_OK;
 }
 
@@ -191,7 +336,8 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
     L.accum = (float*)r->d_accum;
     L.ystat = (float*)r->d_ystat;
     if (stats) cudaEventRecord(ev[0], r->st);
-    int rc = run_tracer(r, L);
+    const bool mixed = r->precision == SO_PREC_MIXED;
+    int rc = mixed ? trace_pass1_mixed(r, f, L) : run_tracer(r, L);
     if (rc) return rc;
     if (stats) cudaEventRecord(ev[1], r->st);
     long long samples = n * f.spp;
@@ -248,6 +394,34 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
         Counters c;
         rc = read_counters(r, &c);
         if (rc) return rc;
+        if (mixed) {
+            Counters c3[2];
+            SO_CK(r, cudaMemcpy(c3, r->d_cnt3, sizeof c3, cudaMemcpyDeviceToHost));
+            stats->flow_steps_fp32 = (long long)c.flow_steps;
+            float ms32 = 0.f;
+            cudaEventElapsedTime(&ms32, r->ev32[0], r->ev32[1]);
+            stats->ms_fp32 = ms32;
+            for (const Counters& x : c3) {
+                c.attempts += x.attempts;
+                c.accepted += x.accepted;
+                c.step_limited += x.step_limited;
+                c.flow_steps += x.flow_steps;
+            }
+            unsigned long long nl[4];
+            SO_CK(r, cudaMemcpy(nl, r->d_nlists, sizeof nl, cudaMemcpyDeviceToHost));
+            // c.attempts now holds FP32 attempts (k_trace32) + band + re-trace FP64 attempts;
+            // the FP64 approach's attempts are in pad[0]
+            stats->attempts_fp32 = (long long)(c.attempts - c3[0].attempts - c3[1].attempts);
+            c.attempts += c.pad[0];
+            c.fp64_rays = nl[1] + nl[2];  // band + re-traced rays
+            stats->band_rays = (long long)nl[1];
+        } else {
+            stats->attempts_fp32 = 0;
+            stats->band_rays = 0;
+            stats->flow_steps_fp32 = 0;
+            stats->ms_fp32 = 0.0;
+            c.fp64_rays = 0;
+        }
         float ms1 = 0.f, ms2 = 0.f;
         cudaEventElapsedTime(&ms1, ev[0], ev[1]);
         if (cudaEventQuery(ev[3]) == cudaSuccess && cudaEventElapsedTime(&ms2, ev[2], ev[3]) != cudaSuccess) ms2 = 0.f;

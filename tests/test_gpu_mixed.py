@@ -1,0 +1,100 @@
+"""Mixed-precision path (FP32 far from the critical curve, FP64 in the band, at the far-field
+approach and for re-traced rays) against the plain FP64 kernel on the same frames.
+
+Bar (the synchrotron scene's target): relative L1 image error <= 1e-3 and total-flux error <= 0.1%
+against the FP64 render; the band and re-trace lists are exercised.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _render_pair(so, shot, overrides, plasma=True, **mixed):
+    sh = so.Shot(shot, overrides)
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    if plasma:
+        r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, st64 = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED, **mixed)
+    img32, _, st32 = r.render(f)
+    r.close()
+    return img64, img32, st64, st32
+
+
+def _errors(img64, img32):
+    a, b = img64[..., 0].astype(np.float64), img32[..., 0].astype(np.float64)
+    l1 = np.abs(a - b).sum() / np.abs(a).sum()
+    flux = abs(b.sum() / a.sum() - 1.0)
+    return l1, flux
+
+
+def test_mixed_synchrotron_image_error(so):
+    """Torus plasma with 512 modes at 192^2 over the +-12 M field: L1 <= 1e-3, flux <= 0.1%."""
+    img64, img32, st64, st32 = _render_pair(so, "synchrotron_1024.ini", ["camera.width=192", "camera.height=192"])
+    l1, flux = _errors(img64, img32)
+    assert img64[..., 0].max() > 0
+    assert l1 <= 1e-3, l1
+    assert flux <= 1e-3, flux
+    assert st32.band_rays > 0 and st32.attempts_fp32 > 0
+    assert st32.samples == st64.samples == 192 * 192
+
+
+def test_mixed_reference_flow_image_error(so):
+    """The reference's own flow model with its fBm turbulence (noise in FP64 coordinates)."""
+    img64, img32, _, st32 = _render_pair(so, "m87_reference_flow.ini", ["camera.width=96", "camera.height=96",
+                                                                         "render.spp=1", "render.spp_max=1"],
+                                         plasma=False)
+    l1, flux = _errors(img64, img32)
+    assert l1 <= 2e-3, l1
+    assert flux <= 1e-3, flux
+
+
+def test_mixed_band_width_zero_and_all_fp64(so):
+    """band 0: every ray starts FP32; a band covering the field: every ray is FP64 and the image is
+    the FP64 kernel's bit for bit."""
+    sh = so.Shot("synchrotron_1024.ini", ["camera.width=64", "camera.height=64"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+    imgb, _, stb = r.render(f)
+    assert stb.band_rays == 64 * 64 and stb.attempts_fp32 == 0
+    assert np.array_equal(img64, imgb)
+    r.set_precision(so.abi.SO_PREC_MIXED, band_m=0.0)
+    img0, _, st0 = r.render(f)
+    assert st0.band_rays == 0
+    l1, flux = _errors(img64, img0)
+    assert l1 < 1e-2 and flux < 1e-2
+    r.close()
+
+
+def test_mixed_retrace_list(so):
+    """A tiny drift tolerance sends every FP32 ray back to FP64: the image then equals the FP64 one."""
+    sh = so.Shot("synchrotron_1024.ini", ["camera.width=48", "camera.height=48"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED, drift_tol=0.0)
+    imgm, _, st = r.render(f)
+    assert st.fp64_rays == 48 * 48
+    assert np.array_equal(img64, imgm)
+    r.close()
+
+
+def test_mixed_deterministic(so):
+    sh = so.Shot("synchrotron_1024.ini", ["camera.width=64", "camera.height=64"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    f = sh.frame(0)
+    a, _, _ = r.render(f)
+    b, _, _ = r.render(f)
+    assert np.array_equal(a, b)
+    r.close()
