@@ -166,6 +166,8 @@ typedef struct so_stats {
     long long band_rays;  /* mixed precision: rays routed to FP64 by the critical band */
     long long flow_steps_fp32; /* mixed precision: flow steps evaluated by the FP32 tracer */
     double ms_fp32;       /* mixed precision: device time of the FP32 tracer launch (CUDA events) */
+    long long redo_turn;  /* mixed precision: FP32 rays re-traced for a radial turning point inside turn_r */
+    long long redo_drift; /* mixed precision: FP32 rays re-traced for constraint drift above drift_tol */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -211,7 +213,7 @@ typedef struct so_mode { double kx, ky, kz, phase, amp; } so_mode;
 typedef struct so_mixed_opts {
     double band_m;           /* FP64 for rays within this distance (M) of the analytic critical curve */
     double tol32;            /* FP32 integrator tolerance (reference error norm) */
-    double turn_r;           /* radial turning point inside this radius (M): re-trace in FP64 */
+    double turn_r;           /* radial turning point inside this radius (M): re-trace in FP64 (0 = off) */
     double drift_tol;        /* relative drift of p_u^2 - U(u) and p_r^2 - R(r) that triggers FP64 */
     double r_switch;         /* FP64 approach from the camera down to this radius (0 = automatic) */
 } so_mixed_opts;

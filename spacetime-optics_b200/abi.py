@@ -84,7 +84,7 @@ class Stats(C.Structure):
                 ("step_limited", C.c_longlong), ("attempts", C.c_longlong), ("accepted", C.c_longlong),
                 ("fp64_rays", C.c_longlong), ("flow_steps", C.c_longlong), ("ms_kernel", C.c_double),
                 ("attempts_fp32", C.c_longlong), ("band_rays", C.c_longlong), ("flow_steps_fp32", C.c_longlong),
-                ("ms_fp32", C.c_double)]
+                ("ms_fp32", C.c_double), ("redo_turn", C.c_longlong), ("redo_drift", C.c_longlong)]
 
 
 class RaysOut(C.Structure):

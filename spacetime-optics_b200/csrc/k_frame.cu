@@ -202,6 +202,35 @@ __global__ void k_add_chunks(float4* __restrict__ accum, uint32_t* __restrict__ 
     nsamp[p] += c * (uint32_t)chunk;
 }
 
+// Per pixel: the sum of its spp samples in sample order and (sum Y, sum Y^2), as k_pass1 accumulates
+// them (render.cu:103-113); the mixed path writes one result per sample first.  Compiled without
+// flush-to-zero, so an all-FP64 mixed frame equals the plain FP64 frame bit for bit.
+__global__ void k_gather_samples(const TraceLaunch L) {
+    const long long npix = (long long)L.W * L.H;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, ys = 0.f, yq = 0.f;
+    const bool radio = L.scenes[0].mode == SO_MODE_RADIO;
+    for (int s = 0; s < L.spp; ++s) {
+        float4 v = L.sample_out[p * L.spp + s];
+        a0 += v.x;
+        a1 += v.y;
+        a2 += v.z;
+        a3 += v.w;
+        float Y = radio ? v.x : v.y;
+        ys += Y;
+        yq += Y * Y;
+    }
+    reinterpret_cast<float4*>(L.accum)[p] = make_float4(a0, a1, a2, a3);
+    if (L.ystat) reinterpret_cast<float2*>(L.ystat)[p] = make_float2(ys, yq);
+}
+
+cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st) {
+    long long npix = (long long)L.W * L.H;
+    k_gather_samples<<<(int)((npix + 255) / 256), 256, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
 __global__ void k_fill_u32(uint32_t* __restrict__ p, uint32_t v, long long n) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;

@@ -10,12 +10,18 @@
 //                 float4 SoA planes (two-float hi/lo pairs for r, r', u, u', phi, t).
 //   k_trace32     persistent FP32 tracer over the parked rays: compensated (two-sum) state update,
 //                 FP32 stages and error estimate with the reference's error norm at tol32, err^-0.2
-//                 on the SFU, torus turbulence with the mode table in shared memory and SFU cosines
-//                 of phases reduced in turns.  At the end the Carter-constant and radial constraints
-//                 are checked in FP64; a ray that fails, or whose radial turning point falls inside
-//                 turn_r, goes to the FP64 re-trace list.
+//                 on the SFU, torus turbulence with the mode table in shared memory, its 512-mode sum
+//                 split across the 32 lanes of the warp for every lane that needs one (SFU cosines of
+//                 phases reduced in turns).  At the end the Carter-constant and radial constraints are
+//                 checked in FP64; a ray that fails, or whose radial turning point falls inside turn_r,
+//                 goes to the FP64 re-trace list.
 // The band and re-trace lists are then traced by the plain FP64 kernel (k_trace64, RAYS_SAMPLES).
-// Compiled with --use_fast_math (FP32 only; the FP64 code is unaffected).
+// Scenes whose emission depends on the raw coordinate time at a generation boundary (the reference's
+// sheared fBm turbulence of the flow or the disk: noise phase ~ t / P with t ~ -r_cam) are
+// ill-conditioned for any integrator that differs from the FP64 one, so the router sends all of
+// their rays to FP64.
+// Compiled with -ftz=true -prec-div=false -prec-sqrt=false -fmad=false: FP32 fusions are the explicit
+// fmaf calls; the FP64 approach keeps the fma placement of so_kerr.cuh.
 #include <cuda_runtime.h>
 
 #include "so_emission.cuh"
@@ -57,14 +63,14 @@ __device__ __forceinline__ bool in_band(const TraceLaunch& L, const so_frame& F,
 }  // namespace
 
 // ---- router ------------------------------------------------------------------------------------
-__global__ void k_route(const TraceLaunch L) {
+__global__ void k_route(const TraceLaunch L, int all64) {
     const so_frame& F = L.frames[0];
     const long long n = L.nsamples;
     for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
         const long long sid = base + threadIdx.x;
         const bool valid = sid < n;
-        bool band = false;
-        if (valid) {
+        bool band = all64 != 0;
+        if (valid && !band) {
             double x, yv;
             sample_point(L.W, L.H, L.jitter, F, sid / L.spp, (int)(sid % L.spp), &x, &yv);
             band = in_band(L, F, x, yv);
@@ -225,36 +231,38 @@ struct Torus32 {
     float ne_index, te_index, h_sph, theta_e0, half_var;
 };
 
-// Turbulence sum with the modes in shared memory as turns: phase/2pi and k/2pi.
-__device__ __forceinline__ float torus_delta32(const float4* __restrict__ km, const float* __restrict__ amp, int n,
-                                               float X, float Y, float Z) {
-    float acc0 = 0.f, acc1 = 0.f;
-    int m = 0;
+// Turbulence sums of the lanes in `want` (positions X, Y, Z per lane), each split across the warp:
+// lane l takes modes l, l+32, ...; a butterfly shuffle reduction gives every lane the total, which
+// the owning lane keeps.  All 32 lanes must call this.  Modes in shared memory as turns
+// (k / 2 pi, phase / 2 pi), so the reduced phase p - rint(p) feeds the SFU cosine on [-pi, pi].
+__device__ __forceinline__ float warp_turbulence(const float4* __restrict__ km, const float* __restrict__ amp, int n,
+                                                 bool want, float X, float Y, float Z) {
+    const int lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(FULL, want);
+    float mine = 0.f;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const float x = __shfl_sync(FULL, X, src), y = __shfl_sync(FULL, Y, src), z = __shfl_sync(FULL, Z, src);
+        float acc = 0.f;
 #pragma unroll 4
-    for (; m + 1 < n; m += 2) {
-        float4 a = km[m], b = km[m + 1];
-        float p = fmaf(a.z, Z, fmaf(a.y, Y, fmaf(a.x, X, a.w)));
-        float q = fmaf(b.z, Z, fmaf(b.y, Y, fmaf(b.x, X, b.w)));
-        p -= rintf(p);
-        q -= rintf(q);
-        acc0 = fmaf(amp[m], __cosf(6.28318530718f * p), acc0);
-        acc1 = fmaf(amp[m + 1], __cosf(6.28318530718f * q), acc1);
+        for (int i = lane; i < n; i += 32) {
+            const float4 k = km[i];
+            float p = fmaf(k.z, z, fmaf(k.y, y, fmaf(k.x, x, k.w)));
+            p -= rintf(p);
+            acc = fmaf(amp[i], __cosf(6.28318530718f * p), acc);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (lane == src) mine = acc;
     }
-    if (m < n) {
-        float4 a = km[m];
-        float p = fmaf(a.z, Z, fmaf(a.y, Y, fmaf(a.x, X, a.w)));
-        p -= rintf(p);
-        acc0 = fmaf(amp[m], __cosf(6.28318530718f * p), acc0);
-    }
-    return acc0 + acc1;
+    return mine;
 }
 
-// flow_step (emission.cuh:264-340) in FP32.  t_rel is the emission time counted from the radial
-// light-travel time to the camera (see so_emission.cuh).  The reference plasma's fBm turbulence is
-// evaluated in FP64 coordinates (sheared_noise), as in the FP64 tracer.
-__device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp, const float4* km, const float* amp,
-                                            float r, float u, float phi, float t_rel, double t_abs, float lam,
-                                            float Ecam, float h, float* dI, float* dtau) {
+// flow_step (emission.cuh:264-340) in FP32, given the turbulence sum delta at this point (torus
+// model).  The reference plasma enters only without its fBm turbulence (see the router).
+__device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp, float delta, float r, float u,
+                                            float lam, float Ecam, float h, float* dI, float* dtau) {
     *dI = 0.f;
     *dtau = 0.f;
     const float a = (float)S.a;
@@ -269,26 +277,13 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
         if (vert < 1e-7f) return;
         float lx = __logf(__fdividef(r, rh));
         ne = (float)S.n0 * __expf(-tp.ne_index * lx) * vert;
-        if (tp.n_modes > 0) {
-            float Rk = fmaxf(R, risco);
-            float Omf = (float)S.flow_kep * __frcp_rn(fmaf(Rk, sqrtf(Rk), a));
-            float phc = phi - Omf * t_rel;
-            float sp, cp;
-            __sincosf(phc, &sp, &cp);
-            float d = torus_delta32(km, amp, tp.n_modes, R * cp, R * sp, z);
-            ne *= __expf(d - tp.half_var);
-        }
+        if (tp.n_modes > 0) ne *= __expf(delta - tp.half_var);
         Th = tp.theta_e0 * __expf(-tp.te_index * lx);
     } else {
         float zh = __fdividef(z, (float)S.h_r * R);
         float vert = __expf(-0.5f * zh * zh);
         if (vert < 1e-7f) return;
         ne = (float)S.n0 * __expf(-(float)S.n_index * __logf(r)) * vert;
-        if (S.flow_turb_amp > 0.f) {
-            float n = sheared_noise(S, (double)R, (double)phi, (double)z, t_abs, S.flow_turb_scale, S.flow_tcorr,
-                                    S.seed ^ 0x51f15eedu);
-            ne *= __expf(S.flow_turb_amp * n - 0.5f * S.flow_turb_amp * S.flow_turb_amp);
-        }
         Th = (float)S.theta0 * __expf(-(float)S.theta_index * __logf(r));
     }
     float dr = r - rh;
@@ -342,6 +337,8 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
 
 }  // namespace
 
+// FP32 tracer.  One loop iteration = one DP5(4) attempt for every active lane.  The loop body is
+// split in two around the warp-cooperative turbulence sum, so every lane reaches the shuffles.
 template <int VAR>
 __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
     extern __shared__ float4 sm4[];
@@ -349,17 +346,17 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
     const so_frame& F = L.frames[0];
     Torus32 tp;
     tp.on = VAR == VAR_RADIO && L.torus;
-    tp.n_modes = L.n_modes;
+    tp.n_modes = tp.on ? L.n_modes : 0;
     tp.ne_index = (float)L.ne_index;
     tp.te_index = (float)L.te_index;
     tp.h_sph = (float)L.h_sph;
     tp.theta_e0 = (float)L.theta_e0;
     tp.half_var = (float)L.half_var;
     float4* km = sm4;
-    float* amp = reinterpret_cast<float*>(sm4 + L.n_modes);
-    if (tp.on) {
+    float* amp = reinterpret_cast<float*>(sm4 + tp.n_modes);
+    if (tp.n_modes > 0) {
         const double i2pi = 1.0 / (2.0 * PI);
-        for (int i = threadIdx.x; i < L.n_modes; i += blockDim.x) {
+        for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
             so_mode m = L.modes[i];
             km[i] = make_float4((float)(m.kx * i2pi), (float)(m.ky * i2pi), (float)(m.kz * i2pi),
                                 (float)(m.phase * i2pi));
@@ -375,13 +372,14 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
     const float rstop = (float)S.r_stop, resc = (float)S.r_escape, rflow = (float)S.r_flow_max;
     const float step_frac = (float)S.step_frac;
     const float rcam_hi = (float)F.r, rcam_lo = (float)(F.r - (double)(float)F.r);
+    const float risco = (float)S.r_isco, flow_kep = (float)S.flow_kep;
     const bool radio = VAR == VAR_RADIO;
     C32 c;
     c.a = (float)S.a;
     c.A2 = c.a * c.a;
     Ray32 R;
     bool active = false, exhausted = false;
-    unsigned long long n_att = 0, n_acc = 0, n_flow = 0, n_lim = 0, n_redo = 0;
+    unsigned long long n_att = 0, n_acc = 0, n_flow = 0, n_lim = 0, n_turn = 0, n_drift = 0;
     for (;;) {
         const bool need = !active && !exhausted;
         const unsigned m = __ballot_sync(FULL, need);
@@ -429,173 +427,200 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
             }
         }
         if (__all_sync(FULL, !active)) break;
-        if (!active) continue;
-        // ---- one DP5(4) attempt in FP32 -----------------------------------------------------------
-        int fate = 2;  // 2 = running, 3 = re-trace in FP64
-        if (R.it >= S.max_steps) {
-            fate = 0;
-        } else {
-            ++R.it;
-            ++R.natt;
-            const float y0 = R.rh + R.rl, y1 = R.prh + R.prl, y2 = R.uh + R.ul, y3 = R.puh + R.pul;
-            float hc = R.h;
-            if (radio && S.flow_on && y0 < rflow) {
-                float s = sqrtf(fmaxf((1.f - y2) * (1.f + y2), 0.f));
-                float cap = step_frac * fminf(__fdividef(y0, fabsf(y1) + 1e-30f),
-                                              __fdividef(fmaxf(s, 0.05f), fabsf(y3) + 1e-30f));
-                hc = fminf(hc, cap);
-            } else if (VAR != VAR_VACUUM && S.disk_on) {
-                hc = fminf(hc, __fdividef(0.3f, fabsf(y3) + 1e-30f));
-            }
-            const float* k1 = R.k1;
-            float k2[6], k3[6], k4[6], k5[6], k6[6], k7[6];
-            const float yy[4] = {y0, y1, y2, y3};
-            float t[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, (float)A21 * k1[i], yy[i]);
-            rhs32(c, t[0], t[1], t[2], t[3], k2);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, fmaf((float)A32, k2[i], (float)A31 * k1[i]), yy[i]);
-            rhs32(c, t[0], t[1], t[2], t[3], k3);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                t[i] = fmaf(hc, fmaf((float)A43, k3[i], fmaf((float)A42, k2[i], (float)A41 * k1[i])), yy[i]);
-            rhs32(c, t[0], t[1], t[2], t[3], k4);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                t[i] = fmaf(hc, fmaf((float)A54, k4[i], fmaf((float)A53, k3[i], fmaf((float)A52, k2[i],
-                                                                                    (float)A51 * k1[i]))), yy[i]);
-            rhs32(c, t[0], t[1], t[2], t[3], k5);
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                t[i] = fmaf(hc, fmaf((float)A65, k5[i], fmaf((float)A64, k4[i], fmaf((float)A63, k3[i],
-                               fmaf((float)A62, k2[i], (float)A61 * k1[i])))), yy[i]);
-            rhs32(c, t[0], t[1], t[2], t[3], k6);
-            float dy[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i)
-                dy[i] = hc * fmaf((float)B6, k6[i], fmaf((float)B5, k5[i], fmaf((float)B4, k4[i],
-                                  fmaf((float)B3, k3[i], (float)B1 * k1[i]))));
-            // candidate state (compensated), then k7 = f(y_new)
-            float nrh = R.rh, nrl = R.rl, nprh = R.prh, nprl = R.prl, nuh = R.uh, nul = R.ul, npuh = R.puh,
-                  npul = R.pul;
-            acc2(nrh, nrl, dy[0]);
-            acc2(nprh, nprl, dy[1]);
-            acc2(nuh, nul, dy[2]);
-            acc2(npuh, npul, dy[3]);
-            const float n0 = nrh + nrl, n1 = nprh + nprl, n2 = nuh + nul, n3 = npuh + npul;
-            rhs32(c, n0, n1, n2, n3, k7);
-            // error norm of kerr.hpp:193-205 at tol32, with a floor of a few ulp of each scale so the
-            // controller does not chase FP32 rounding
-            float sc[5];
-            sc[0] = tol * (1e-6f + fmaxf(fabsf(y0), fabsf(n0)));
-            sc[1] = tol * (1e-6f + fmaxf(fmaxf(fabsf(y1), fabsf(n1)), y0 * y0));
-            sc[2] = tol;
-            sc[3] = tol * fmaxf(1.f, fmaxf(fabsf(y3), fabsf(n3)));
-            sc[4] = tol * 4.f;
-            float err = 0.f;
-#pragma unroll
-            for (int i = 0; i < 5; ++i) {
-                float e = hc * fmaf((float)E7, k7[i], fmaf((float)E6, k6[i], fmaf((float)E5, k5[i],
-                                    fmaf((float)E4, k4[i], fmaf((float)E3, k3[i], (float)E1 * k1[i])))));
-                err = fmaxf(err, __fdividef(fabsf(e), sc[i]));
-            }
-            if (!(err <= 1.f)) {
-                R.h = hc * fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f));
-                if (!(err == err)) R.h = hc * 0.1f;
+        // ---- part 1 (active lanes): one DP5(4) attempt in FP32 ----------------------------------
+        int fate = 2;  // 2 = running, 3 = re-trace: radial turning point, 4 = re-trace: drift
+        bool accepted = false, want_flow = false, want_turb = false;
+        float nrh = 0.f, nrl = 0.f, nprh = 0.f, nprl = 0.f, nuh = 0.f, nul = 0.f, npuh = 0.f, npul = 0.f;
+        float n0 = 0.f, n1 = 0.f, n2 = 0.f, hc = 0.f, err = 0.f, TX = 0.f, TY = 0.f, TZ = 0.f;
+        float k7[6], dy[6];
+        if (active) {
+            if (R.it >= S.max_steps) {
+                fate = 0;
             } else {
-                ++R.nacc;
-                if (radio) {
-                    float sn = sqrtf(fmaxf((1.f - n2) * (1.f + n2), 0.f)), s4, c4;
-                    float phn = (R.phh + R.phl) + dy[4];
-                    __sincosf(phn, &s4, &c4);
-                    float pn0 = sn * c4, pn1 = sn * s4, pn2 = n2;
-                    float cx = fmaf(R.pp1, pn2, -(R.pp2 * pn1)), cy = fmaf(R.pp2, pn0, -(R.pp0 * pn2)),
-                          cz = fmaf(R.pp0, pn1, -(R.pp1 * pn0));
-                    R.psi += atan2f(sqrtf(fmaf(cz, cz, fmaf(cy, cy, cx * cx))),
-                                    fmaf(R.pp2, pn2, fmaf(R.pp1, pn1, R.pp0 * pn0)));
-                    R.pp0 = pn0;
-                    R.pp1 = pn1;
-                    R.pp2 = pn2;
+                ++R.it;
+                ++R.natt;
+                const float y0 = R.rh + R.rl, y1 = R.prh + R.prl, y2 = R.uh + R.ul, y3 = R.puh + R.pul;
+                hc = R.h;
+                if (radio && S.flow_on && y0 < rflow) {
+                    float s = sqrtf(fmaxf((1.f - y2) * (1.f + y2), 0.f));
+                    float cap = step_frac * fminf(__fdividef(y0, fabsf(y1) + 1e-30f),
+                                                  __fdividef(fmaxf(s, 0.05f), fabsf(y3) + 1e-30f));
+                    hc = fminf(hc, cap);
+                } else if (VAR == VAR_DISK && S.disk_on) {
+                    hc = fminf(hc, __fdividef(0.3f, fabsf(y3) + 1e-30f));
                 }
-                const bool crossed = (y2 > 0.f) != (n2 > 0.f);
-                if (crossed) ++R.ncross;
-                const bool turned = (y1 < 0.f) && (n1 >= 0.f) && n0 < (float)L.turn_r;
-                if (turned) fate = 3;
-                if (VAR != VAR_VACUUM && S.disk_on && crossed && fate == 2) {
-                    // rare: the disk shading of the FP64 tracer on the promoted endpoints
-                    double lo = 0.0, hi = 1.0, u0 = y2, u1 = n2, m0 = (double)y3 * hc, m1 = (double)n3 * hc;
-                    for (int b = 0; b < 40; ++b) {
-                        double mid = 0.5 * (lo + hi);
-                        double um = hermite(u0, u1, m0, m1, mid);
-                        if ((um > 0.0) == (u0 > 0.0)) lo = mid;
-                        else hi = mid;
-                    }
-                    double scr = 0.5 * (lo + hi);
-                    double rc = hermite(y0, n0, (double)y1 * hc, (double)n1 * hc, scr);
-                    double ph0 = (double)R.phh + R.phl, t0 = (double)R.th + R.tl;
-                    double pc = hermite(ph0, ph0 + dy[4], (double)k1[4] * hc, (double)k7[4] * hc, scr);
-                    double tcv = hermite(t0, t0 + dy[5], (double)k1[5] * hc, (double)k7[5] * hc, scr);
-                    float cs[4];
-                    disk_shade(S, rc, pc, tcv, c.lam, c.eta, c.E, cs);
-                    if (cs[3] > 0.f) {
-                        float tf = R.trans;
-                        R.acc[0] += tf * cs[0];
-                        R.acc[1] += tf * cs[1];
-                        R.acc[2] += tf * cs[2];
-                        R.acc[3] += tf * cs[1] * (float)(R.ncross - 1);
-                        R.trans *= 1.f - cs[3];
-                        if (R.trans < 1e-4f) fate = -1;
-                    }
-                }
-                if (radio && S.flow_on && n0 < rflow && fate == 2) {
-                    float ph_new_h = R.phh, ph_new_l = R.phl, t_new_h = R.th, t_new_l = R.tl;
-                    acc2(ph_new_h, ph_new_l, dy[4]);
-                    acc2(t_new_h, t_new_l, dy[5]);
-                    float t_rel = ((t_new_h + rcam_hi) + (t_new_l + rcam_lo)) - n0 +
-                                  2.f * __logf(__fdividef(rcam_hi, n0));
-                    float dI, dtau;
-                    flow_step32(S, tp, km, amp, n0, n2, ph_new_h + ph_new_l, t_rel, (double)t_new_h + t_new_l, c.lam,
-                                c.E, hc, &dI, &dtau);
-                    ++R.nflow;
-                    float cc = R.trans * dI;
-                    int nb = (int)(R.psi * (float)(1.0 / PI));
-                    R.acc[0] += cc;
-                    if (nb == 1) R.acc[1] += cc;
-                    else if (nb == 2) R.acc[2] += cc;
-                    else if (nb >= 3) R.acc[3] += cc;
-                    R.trans *= __expf(-dtau);
-                    if (R.trans < 1e-5f) fate = -1;
-                }
-                // commit the step
-                R.rh = nrh; R.rl = nrl; R.prh = nprh; R.prl = nprl;
-                R.uh = nuh; R.ul = nul; R.puh = npuh; R.pul = npul;
-                acc2(R.phh, R.phl, dy[4]);
-                acc2(R.th, R.tl, dy[5]);
+                const float* k1 = R.k1;
+                float k2[6], k3[6], k4[6], k5[6], k6[6];
+                const float yy[4] = {y0, y1, y2, y3};
+                float t[4];
 #pragma unroll
-                for (int i = 0; i < 6; ++i) R.k1[i] = k7[i];
-                // project_radial (kerr.hpp:216-223) in FP32
-                {
-                    float r = n0, P = fmaf(r, r, c.CP), D = fmaf(r, r - 2.f, c.A2);
-                    float Rr = fmaf(P, P, -(D * c.K)), r2 = r * r;
-                    if (Rr > 0.25f * (r2 * r2)) {
-                        float v = sqrtf(Rr);
-                        float pr = n1 < 0.f ? -v : v;
-                        R.prh = pr;
-                        R.prl = 0.f;
-                        R.k1[0] = pr;
+                for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, (float)A21 * k1[i], yy[i]);
+                rhs32(c, t[0], t[1], t[2], t[3], k2);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) t[i] = fmaf(hc, fmaf((float)A32, k2[i], (float)A31 * k1[i]), yy[i]);
+                rhs32(c, t[0], t[1], t[2], t[3], k3);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    t[i] = fmaf(hc, fmaf((float)A43, k3[i], fmaf((float)A42, k2[i], (float)A41 * k1[i])), yy[i]);
+                rhs32(c, t[0], t[1], t[2], t[3], k4);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    t[i] = fmaf(hc, fmaf((float)A54, k4[i], fmaf((float)A53, k3[i], fmaf((float)A52, k2[i],
+                                                                                        (float)A51 * k1[i]))), yy[i]);
+                rhs32(c, t[0], t[1], t[2], t[3], k5);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    t[i] = fmaf(hc, fmaf((float)A65, k5[i], fmaf((float)A64, k4[i], fmaf((float)A63, k3[i],
+                                   fmaf((float)A62, k2[i], (float)A61 * k1[i])))), yy[i]);
+                rhs32(c, t[0], t[1], t[2], t[3], k6);
+#pragma unroll
+                for (int i = 0; i < 6; ++i)
+                    dy[i] = hc * fmaf((float)B6, k6[i], fmaf((float)B5, k5[i], fmaf((float)B4, k4[i],
+                                      fmaf((float)B3, k3[i], (float)B1 * k1[i]))));
+                nrh = R.rh; nrl = R.rl; nprh = R.prh; nprl = R.prl; nuh = R.uh; nul = R.ul; npuh = R.puh; npul = R.pul;
+                acc2(nrh, nrl, dy[0]);
+                acc2(nprh, nprl, dy[1]);
+                acc2(nuh, nul, dy[2]);
+                acc2(npuh, npul, dy[3]);
+                n0 = nrh + nrl;
+                n1 = nprh + nprl;
+                n2 = nuh + nul;
+                const float n3 = npuh + npul;
+                rhs32(c, n0, n1, n2, n3, k7);
+                // error norm of kerr.hpp:193-205 at tol32
+                float sc[5];
+                sc[0] = tol * (1e-6f + fmaxf(fabsf(y0), fabsf(n0)));
+                sc[1] = tol * (1e-6f + fmaxf(fmaxf(fabsf(y1), fabsf(n1)), y0 * y0));
+                sc[2] = tol;
+                sc[3] = tol * fmaxf(1.f, fmaxf(fabsf(y3), fabsf(n3)));
+                sc[4] = tol * 4.f;
+#pragma unroll
+                for (int i = 0; i < 5; ++i) {
+                    float e = hc * fmaf((float)E7, k7[i], fmaf((float)E6, k6[i], fmaf((float)E5, k5[i],
+                                        fmaf((float)E4, k4[i], fmaf((float)E3, k3[i], (float)E1 * k1[i])))));
+                    err = fmaxf(err, __fdividef(fabsf(e), sc[i]));
+                }
+                if (!(err <= 1.f)) {
+                    R.h = hc * fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f));
+                    if (!(err == err)) R.h = hc * 0.1f;
+                } else {
+                    accepted = true;
+                    ++R.nacc;
+                    if (radio) {
+                        float sn = sqrtf(fmaxf((1.f - n2) * (1.f + n2), 0.f)), s4, c4;
+                        float phn = (R.phh + R.phl) + dy[4];
+                        __sincosf(phn, &s4, &c4);
+                        float pn0 = sn * c4, pn1 = sn * s4, pn2 = n2;
+                        float cx = fmaf(R.pp1, pn2, -(R.pp2 * pn1)), cy = fmaf(R.pp2, pn0, -(R.pp0 * pn2)),
+                              cz = fmaf(R.pp0, pn1, -(R.pp1 * pn0));
+                        R.psi += atan2f(sqrtf(fmaf(cz, cz, fmaf(cy, cy, cx * cx))),
+                                        fmaf(R.pp2, pn2, fmaf(R.pp1, pn1, R.pp0 * pn0)));
+                        R.pp0 = pn0;
+                        R.pp1 = pn1;
+                        R.pp2 = pn2;
+                    }
+                    if ((y2 > 0.f) != (n2 > 0.f)) ++R.ncross;
+                    if ((y1 < 0.f) && (n1 >= 0.f) && n0 < (float)L.turn_r) fate = 3;
+                    want_flow = radio && S.flow_on && n0 < rflow && fate == 2;
+                    if (want_flow && tp.n_modes > 0) {
+                        // torus turbulence position: the flow-advected azimuth at the emission time
+                        // counted from the radial light-travel time to the camera (so_emission.cuh)
+                        float s2 = fmaxf((1.f - n2) * (1.f + n2), 1e-12f), s = sqrtf(s2);
+                        float Rc = n0 * s, zh = __fdividef(n2, tp.h_sph);
+                        if (Rc >= 1e-3f && __expf(-0.5f * zh * zh) >= 1e-7f) {
+                            float ph_h = R.phh, ph_l = R.phl, t_h = R.th, t_l = R.tl;
+                            acc2(ph_h, ph_l, dy[4]);
+                            acc2(t_h, t_l, dy[5]);
+                            float t_rel = ((t_h + rcam_hi) + (t_l + rcam_lo)) - n0 +
+                                          2.f * __logf(__fdividef(rcam_hi, n0));
+                            float Rk = fmaxf(Rc, risco);
+                            float Omf = flow_kep * __frcp_rn(fmaf(Rk, sqrtf(Rk), c.a));
+                            float phc = (ph_h + ph_l) - Omf * t_rel;
+                            float sp, cp;
+                            __sincosf(phc, &sp, &cp);
+                            TX = Rc * cp;
+                            TY = Rc * sp;
+                            TZ = n0 * n2;
+                            want_turb = true;
+                        }
                     }
                 }
-                R.h = hc * fminf(5.f, fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f)));
-                if (fate == 2) {
-                    if (n0 < rstop) fate = -1;
-                    else if (n0 > resc && R.prh > 0.f) fate = 1;
+            }
+        }
+        // ---- all lanes: turbulence sums of the lanes that need one ------------------------------
+        float delta = 0.f;
+        if (VAR == VAR_RADIO && tp.n_modes > 0) delta = warp_turbulence(km, amp, tp.n_modes, want_turb, TX, TY, TZ);
+        // ---- part 2 (active lanes): emission, commit, termination ------------------------------
+        if (!active) continue;
+        if (accepted) {
+            if (VAR == VAR_DISK && S.disk_on && fate == 2 && ((R.uh + R.ul > 0.f) != (n2 > 0.f))) {
+                // rare: the disk shading of the FP64 tracer on the crossing found in FP64
+                const float y0 = R.rh + R.rl, y1 = R.prh + R.prl, y2 = R.uh + R.ul, y3 = R.puh + R.pul;
+                double lo = 0.0, hi = 1.0, u0 = y2, u1 = n2, m0 = (double)y3 * hc, m1 = (double)(npuh + npul) * hc;
+                for (int b = 0; b < 40; ++b) {
+                    double mid = 0.5 * (lo + hi);
+                    double um = hermite(u0, u1, m0, m1, mid);
+                    if ((um > 0.0) == (u0 > 0.0)) lo = mid;
+                    else hi = mid;
                 }
+                double scr = 0.5 * (lo + hi);
+                double rc = hermite(y0, n0, (double)y1 * hc, (double)n1 * hc, scr);
+                double ph0 = (double)R.phh + R.phl, t0 = (double)R.th + R.tl;
+                double pc = hermite(ph0, ph0 + dy[4], (double)R.k1[4] * hc, (double)k7[4] * hc, scr);
+                double tcv = hermite(t0, t0 + dy[5], (double)R.k1[5] * hc, (double)k7[5] * hc, scr);
+                float cs[4];
+                disk_shade(S, rc, pc, tcv, c.lam, c.eta, c.E, cs);
+                if (cs[3] > 0.f) {
+                    float tf = R.trans;
+                    R.acc[0] += tf * cs[0];
+                    R.acc[1] += tf * cs[1];
+                    R.acc[2] += tf * cs[2];
+                    R.acc[3] += tf * cs[1] * (float)(R.ncross - 1);
+                    R.trans *= 1.f - cs[3];
+                    if (R.trans < 1e-4f) fate = -1;
+                }
+            }
+            if (want_flow) {
+                float dI, dtau;
+                flow_step32(S, tp, delta, n0, n2, c.lam, c.E, hc, &dI, &dtau);
+                ++R.nflow;
+                float cc = R.trans * dI;
+                int nb = (int)(R.psi * (float)(1.0 / PI));
+                R.acc[0] += cc;
+                if (nb == 1) R.acc[1] += cc;
+                else if (nb == 2) R.acc[2] += cc;
+                else if (nb >= 3) R.acc[3] += cc;
+                R.trans *= __expf(-dtau);
+                if (R.trans < 1e-5f) fate = -1;
+            }
+            // commit the step
+            R.rh = nrh; R.rl = nrl; R.prh = nprh; R.prl = nprl;
+            R.uh = nuh; R.ul = nul; R.puh = npuh; R.pul = npul;
+            acc2(R.phh, R.phl, dy[4]);
+            acc2(R.th, R.tl, dy[5]);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) R.k1[i] = k7[i];
+            // project_radial (kerr.hpp:216-223) in FP32
+            {
+                float r = n0, P = fmaf(r, r, c.CP), D = fmaf(r, r - 2.f, c.A2);
+                float Rr = fmaf(P, P, -(D * c.K)), r2 = r * r;
+                if (Rr > 0.25f * (r2 * r2)) {
+                    float v = sqrtf(Rr);
+                    float pr = n1 < 0.f ? -v : v;
+                    R.prh = pr;
+                    R.prl = 0.f;
+                    R.k1[0] = pr;
+                }
+            }
+            R.h = hc * fminf(5.f, fmaxf(0.2f, 0.9f * __powf(fmaxf(err, 1e-30f), -0.2f)));
+            if (fate == 2) {
+                if (n0 < rstop) fate = -1;
+                else if (n0 > resc && R.prh > 0.f) fate = 1;
             }
         }
         if (fate == 2) continue;
         // ---- ray finished: FP64 Carter-constant / radial constraint check ------------------------
-        if (fate != 3 && fate != 0) {
+        if (fate == -1 || fate == 1) {
             double r = (double)R.rh + R.rl, pr = (double)R.prh + R.prl, u = (double)R.uh + R.ul,
                    pu = (double)R.puh + R.pul;
             double lam = c.lam, eta = c.eta, a = S.a;
@@ -604,18 +629,19 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
             double P = r * r + a * a - a * lam, D = r * r - 2.0 * r + a * a;
             double Rr = P * P - D * (eta + (lam - a) * (lam - a));
             double dU = fabs(pu * pu - U) / scaleU, dR = fabs(pr * pr - Rr) / (r * r * r * r);
-            if (dU > L.drift_tol || dR > L.drift_tol) fate = 3;
+            if (dU > L.drift_tol || dR > L.drift_tol) fate = 4;
         }
         n_att += (unsigned long long)R.natt;
         n_acc += (unsigned long long)R.nacc;
         n_flow += (unsigned long long)R.nflow;
         if (fate == 0) ++n_lim;
-        const bool redo = fate == 3;
+        const bool redo = fate >= 3;
+        n_turn += fate == 3 ? 1 : 0;
+        n_drift += fate == 4 ? 1 : 0;
         if (!redo) {
             L.sample_out[R.sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
             if (L.sample_fate) L.sample_fate[R.sid] = (int8_t)fate;
         }
-        n_redo += redo ? 1 : 0;
         active = false;
         // re-trace list: lanes finish at different iterations, so append without a warp vote
         if (redo) L.redo[atomicAdd(&L.nlists[2], 1ull)] = R.sid;
@@ -625,43 +651,24 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
         n_acc += __shfl_down_sync(FULL, n_acc, o);
         n_flow += __shfl_down_sync(FULL, n_flow, o);
         n_lim += __shfl_down_sync(FULL, n_lim, o);
-        n_redo += __shfl_down_sync(FULL, n_redo, o);
+        n_turn += __shfl_down_sync(FULL, n_turn, o);
+        n_drift += __shfl_down_sync(FULL, n_drift, o);
     }
     if (lane == 0) {
         atomicAdd(&L.counters->attempts, n_att);
         atomicAdd(&L.counters->pad[1], n_acc);  // FP32 accepted steps
         atomicAdd(&L.counters->flow_steps, n_flow);
         atomicAdd(&L.counters->step_limited, n_lim);
-        atomicAdd(&L.counters->fp64_rays, n_redo);
+        atomicAdd(&L.counters->redo_turn, n_turn);
+        atomicAdd(&L.counters->redo_drift, n_drift);
     }
-}
-
-// Per pixel: sum of its spp samples in sample order, and (sum Y, sum Y^2) (k_pass1, render.cu:103-113).
-__global__ void k_gather_samples(const TraceLaunch L) {
-    const long long npix = (long long)L.W * L.H;
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npix) return;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, ys = 0.f, yq = 0.f;
-    const bool radio = L.scenes[0].mode == SO_MODE_RADIO;
-    for (int s = 0; s < L.spp; ++s) {
-        float4 v = L.sample_out[p * L.spp + s];
-        a0 += v.x;
-        a1 += v.y;
-        a2 += v.z;
-        a3 += v.w;
-        float Y = radio ? v.x : v.y;
-        ys += Y;
-        yq += Y * Y;
-    }
-    reinterpret_cast<float4*>(L.accum)[p] = make_float4(a0, a1, a2, a3);
-    if (L.ystat) reinterpret_cast<float2*>(L.ystat)[p] = make_float2(ys, yq);
 }
 
 // ---- launchers -----------------------------------------------------------------------------------
-cudaError_t launch_route(const TraceLaunch& L, cudaStream_t st) {
+cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st) {
     long long blocks = (L.nsamples + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    k_route<<<(int)(blocks > 0 ? blocks : 1), 256, 0, st>>>(L);
+    k_route<<<(int)(blocks > 0 ? blocks : 1), 256, 0, st>>>(L, all64);
     return cudaGetLastError();
 }
 
@@ -677,7 +684,7 @@ cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cu
 }
 
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st) {
-    const bool torus = L.torus && L.n_modes > 0;
+    const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;
     size_t smem = torus ? (size_t)L.n_modes * (sizeof(float4) + sizeof(float)) : 0;
     int per_sm = 1;
     cudaError_t e;
@@ -700,12 +707,6 @@ cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int n
         default: e = go(k_trace32<VAR_RADIO>); break;
     }
     return e;
-}
-
-cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st) {
-    long long npix = (long long)L.W * L.H;
-    k_gather_samples<<<(int)((npix + 255) / 256), 256, 0, st>>>(L);
-    return cudaGetLastError();
 }
 
 }  // namespace so

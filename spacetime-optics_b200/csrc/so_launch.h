@@ -31,7 +31,9 @@ struct Counters {
     unsigned long long accepted;      // accepted steps
     unsigned long long fp64_rays;     // mixed precision: rays (or restarts) integrated in FP64
     unsigned long long flow_steps;    // accepted steps that evaluated the hot-flow transfer
-    unsigned long long pad[2];
+    unsigned long long pad[2];        // [0] FP64 approach attempts, [1] FP32 accepted steps
+    unsigned long long redo_turn;     // mixed: FP32 rays re-traced for a radial turning point inside turn_r
+    unsigned long long redo_drift;    // mixed: FP32 rays re-traced for constraint drift
 };
 
 struct TraceLaunch {
@@ -80,7 +82,7 @@ struct TraceLaunch {
 };
 
 // Mixed-path kernels (k_trace_mixed.cu).
-cudaError_t launch_route(const TraceLaunch& L, cudaStream_t st);
+cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st);
 cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st);
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);

@@ -77,7 +77,7 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 3.5, 1e-4, 0.0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0};
     // mixed-path buffers (grown on demand) and the critical-curve table of the current frame
     long long mixed_cap = 0;
     float4 *d_state = nullptr, *d_sample_out = nullptr;
@@ -272,7 +272,13 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     L.nlists = r->d_nlists;
     SO_CK(r, cudaMemsetAsync(r->d_nlists, 0, 4 * sizeof(unsigned long long), r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt3, 0, 2 * sizeof(Counters), r->st));
-    SO_CK(r, launch_route(L, r->st));
+    // The reference's sheared fBm turbulence (flow or disk) is evaluated at a noise generation
+    // k = floor(t / P) of the raw coordinate time t ~ -r_cam: a relative change eps of the radius moves
+    // its phase by ~ (t / P) eps, so any integrator that is not the FP64 one decorrelates it.  Such
+    // scenes, and radio scenes with a disk (not in the FP32 tracer), go to FP64 entirely.
+    const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f) ||
+                       (r->S.disk_on && r->S.disk_turb_amp > 0.f) || (r->S.mode == SO_MODE_RADIO && r->S.disk_on);
+    SO_CK(r, launch_route(L, all64 ? 1 : 0, r->st));
     // band rays: plain FP64 tracer on the second stream, concurrently with the FP32 work
     SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
     SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
@@ -398,6 +404,8 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             Counters c3[2];
             SO_CK(r, cudaMemcpy(c3, r->d_cnt3, sizeof c3, cudaMemcpyDeviceToHost));
             stats->flow_steps_fp32 = (long long)c.flow_steps;
+            stats->redo_turn = (long long)c.redo_turn;
+            stats->redo_drift = (long long)c.redo_drift;
             float ms32 = 0.f;
             cudaEventElapsedTime(&ms32, r->ev32[0], r->ev32[1]);
             stats->ms_fp32 = ms32;
@@ -420,6 +428,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->band_rays = 0;
             stats->flow_steps_fp32 = 0;
             stats->ms_fp32 = 0.0;
+            stats->redo_turn = stats->redo_drift = 0;
             c.fp64_rays = 0;
         }
         float ms1 = 0.f, ms2 = 0.f;
