@@ -243,6 +243,22 @@ int so_trace_rays(so_renderer* r, const so_frame* f, int n, const double* x, con
  * call does not synchronise; with stats it waits and fills the counters and ms_trace (device time
  * of the tracer launches, CUDA events). */
 int so_render_device(so_renderer* r, const so_frame* f, float* d_px, so_stats* stats);
+/* Renderer::radio_flux for callers that cannot allocate device memory (a process whose device
+ * memory belongs to a pool or arena, a real-time loop that allocates only up front, a plugin host
+ * that forbids allocation in its callbacks).  No reference counterpart: it needs no renderer and
+ * calls no cudaMalloc / cudaFree.  The caller passes, in memory it owns: d_scene (device so_scene of
+ * a radio scene whose table pointers are device pointers), d_frame (device so_frame built for width
+ * n), plasma (host; NULL = the reference flow model) with its device modes d_modes, and d_jy (device
+ * double that receives the flux density in Jy).  The n x n frame is traced at 2 samples per pixel,
+ * as so_radio_flux does, asynchronously on `stream` (a cudaStream_t; NULL = default stream).
+ * Working memory is a fixed device array of the library, SO_NOALLOC_MAX_PIXELS float4 plus 5.4 KB,
+ * held by every GPU that loads the library until the process exits: n*n above SO_NOALLOC_MAX_PIXELS
+ * returns SO_ERR_SIZE (message in so_last_error(NULL)).  The first call on a device looks the array
+ * up (cudaGetSymbolAddress) with that device current; make it before any stream capture.  All calls
+ * share the array, so calls that overlap on the GPU race: order them on one stream. */
+#define SO_NOALLOC_MAX_PIXELS 65536
+int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_frame, int n, double pix_sr,
+                          const so_plasma* plasma, const so_mode* d_modes, double* d_jy, void* stream);
 /* Same as so_trace_rays with x, y and the outputs already in device memory (device pointers). */
 int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
                          const so_rays_out* d_out);

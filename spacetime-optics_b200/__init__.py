@@ -43,6 +43,7 @@ def lib():
         L.so_render_device.argtypes = [vp, P(Frame), vp, P(Stats)]
         L.so_probe_fma_peak.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
         L.so_probe_sfu_peak.argtypes = [C.c_int, P(C.c_double)]
+        L.so_radio_flux_noalloc.argtypes = [vp, vp, C.c_int, C.c_double, P(Plasma), vp, vp, vp]
         L.so_radio_flux.argtypes = [vp, P(Frame), C.c_int, C.c_double, P(C.c_double)]
         L.so_trace_rays.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
         L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]

@@ -128,7 +128,7 @@ LAYOUT_FIELDS = [
 # Every entry point include/so_tracer.h declares (checked against the built library's exports).
 EXPORTS = [
     "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
-    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak",
+    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak", "so_radio_flux_noalloc",
     "so_set_precision", "so_set_plasma", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
     "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",

@@ -495,6 +495,11 @@ RayBufs carve(void* base, long long n) {
 
 }  // namespace
 
+namespace so {
+// Message returned by so_last_error(NULL), for entry points that have no renderer handle.
+void set_global_error(const std::string& msg) { g_init_error = msg; }
+}  // namespace so
+
 extern "C" {
 
 int so_init(so_renderer** out, int device, const so_scene* scene, const so_tables* tables, const so_settings* rs) {
