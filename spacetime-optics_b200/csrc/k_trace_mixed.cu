@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_approach64(const TraceLaunch L) {
             bool done = false;
             for (; it < S.max_steps;) {
                 ++it;
-                double err = dp54(c, y, k1, h, S.tol, yn, k7);
+                double err = dp54(c, y, k1, h, L.tol_approach, yn, k7);
                 if (!(err <= 1.0)) {
                     h = reject_step(h, err);
                     continue;
@@ -339,8 +339,8 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
 
 // FP32 tracer.  One loop iteration = one DP5(4) attempt for every active lane.  The loop body is
 // split in two around the warp-cooperative turbulence sum, so every lane reaches the shuffles.
-template <int VAR>
-__global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
+template <int VAR, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     extern __shared__ float4 sm4[];
     const so_scene& S = L.scenes[0];
     const so_frame& F = L.frames[0];
@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
     const float step_frac = (float)S.step_frac;
     const float rcam_hi = (float)F.r, rcam_lo = (float)(F.r - (double)(float)F.r);
     const float risco = (float)S.r_isco, flow_kep = (float)S.flow_kep;
+    const float r_out = (float)L.r_emit;
     const bool radio = VAR == VAR_RADIO;
     C32 c;
     c.a = (float)S.a;
@@ -616,6 +617,11 @@ __global__ void __launch_bounds__(128) k_trace32(const TraceLaunch L) {
             if (fate == 2) {
                 if (n0 < rstop) fate = -1;
                 else if (n0 > resc && R.prh > 0.f) fate = 1;
+                // outgoing beyond every emitter and beyond the largest radial turning point the
+                // constants of motion allow (R(r) ~ r^4 - (eta + lam^2) r^2 + ...): no more emission,
+                // the ray escapes; its escape direction is not part of the FP32 outputs
+                else if (r_out > 0.f && R.prh > 0.f && n0 > r_out && n0 * n0 > 4.f * (c.eta + c.lam * c.lam + c.A2) + 16.f)
+                    fate = 1;
             }
         }
         if (fate == 2) continue;
@@ -701,10 +707,15 @@ cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int n
         kern<<<(int)grid, 128, smem, st>>>(L);
         return cudaGetLastError();
     };
+    // register budget: 4 CTAs of 128 per SM (128 registers, no spills) or 5 / 6 (96 / 80 registers,
+    // a few spills to L1); chosen by the caller or the autotuner
     switch (variant) {
-        case VAR_VACUUM: e = go(k_trace32<VAR_VACUUM>); break;
-        case VAR_DISK: e = go(k_trace32<VAR_DISK>); break;
-        default: e = go(k_trace32<VAR_RADIO>); break;
+        case VAR_VACUUM: e = go(k_trace32<VAR_VACUUM, 4>); break;
+        case VAR_DISK: e = go(k_trace32<VAR_DISK, 4>); break;
+        default:
+            e = L.t32_min_blocks >= 6 ? go(k_trace32<VAR_RADIO, 6>)
+                : L.t32_min_blocks == 5 ? go(k_trace32<VAR_RADIO, 5>) : go(k_trace32<VAR_RADIO, 4>);
+            break;
     }
     return e;
 }

@@ -70,6 +70,9 @@ struct TraceLaunch {
     // mixed precision
     double band_m, tol32, turn_r, drift_tol;
     double r_switch;          // FP64 approach down to this radius, FP32 inside
+    double tol_approach;      // tolerance of the FP64 approach
+    double r_emit;            // FP32 tracer: outgoing beyond this radius = escaped (0 = off)
+    int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
     const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi
     int band_n;
     float4* state;            // parked ray state, 5 float4 per sample id (SoA planes of nsamples)

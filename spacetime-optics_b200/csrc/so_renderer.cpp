@@ -77,7 +77,7 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0};
     // mixed-path buffers (grown on demand) and the critical-curve table of the current frame
     long long mixed_cap = 0;
     float4 *d_state = nullptr, *d_sample_out = nullptr;
@@ -259,6 +259,13 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         if (r->S.disk_on) rsw = std::max(rsw, 1.2 * r->S.disk_rout);
     }
     L.r_switch = rsw;
+    L.tol_approach = r->mixed.tol_approach > 0.0 ? r->mixed.tol_approach : r->S.tol;
+    L.t32_min_blocks = r->mixed.t32_blocks > 0 ? r->mixed.t32_blocks : 4;
+    // outgoing rays beyond every emitter cannot come back: the FP32 tracer ends them as escaped
+    double r_emit = 0.0;
+    if (r->S.mode == SO_MODE_RADIO && r->S.flow_on) r_emit = std::max(r_emit, r->S.r_flow_max);
+    if (r->S.disk_on) r_emit = std::max(r_emit, r->S.disk_rout);
+    L.r_emit = r_emit > 0.0 ? std::max(r_emit, 10.0) : 0.0;
     L.band_rho = r->d_band;
     L.band_n = BAND_N;
     L.nsamples = ns;
