@@ -274,6 +274,30 @@ void* so_stream(so_renderer* r);
 const char* so_last_error(const so_renderer* r);
 void so_destroy(so_renderer* r);
 
+/* ---- batched frames: the persistent wavefront (no reference counterpart) --------------------- */
+/* A batch of nframes frames of W x H pixels x spp samples, traced by ONE persistent FP64 launch:
+ * the rays of all frames share one work queue, so frames of very different cost (spins, photon-ring
+ * zooms, turbulence times) keep every lane busy until the last ray.  Frame i uses
+ * scenes[frame_scene[i]]; every scene must have the same mode and use the renderer's tables (those
+ * of so_init: the K2 and blackbody tables do not depend on the scene, the disk table depends on the
+ * spin, so disk scenes must share a spin).  The plasma is the renderer's (so_set_plasma).  The launch
+ * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed. */
+typedef struct so_batch so_batch;
+/* Launch shape of the batch: resident CTAs per SM of the persistent grid (0 = as many as fit), and
+ * the job order (0 = frame after frame, 1 = frames interleaved ray by ray). */
+typedef struct so_tune { int ctas_per_sm; int interleave; double ms; } so_tune;
+int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const so_frame* frames,
+                    const int* frame_scene, int nframes, int W, int H, int spp, so_batch** out);
+/* Traces the batch into d_px (device memory, nframes * W * H * 4 floats, frame after frame) by
+ * replaying the batch's CUDA graph on so_stream(r).  With stats: waits, fills the counters and
+ * ms_kernel (graph time, CUDA events); without: asynchronous. */
+int so_batch_render(so_batch* b, float* d_px, so_stats* stats);
+/* Autotuner: times every launch shape (CTAs per SM from 1 to the occupancy limit, both job orders)
+ * on the batch, keeps the fastest for later so_batch_render calls and returns it in *best. */
+int so_batch_autotune(so_batch* b, float* d_px, so_tune* best);
+int so_batch_set_tune(so_batch* b, const so_tune* t);
+void so_batch_free(so_batch* b);
+
 /* ---- shot / scene builders (host only) --------------------------------------------------------- */
 typedef struct so_shot so_shot;
 /* Scene information that does not go to the device (SceneInfo, scene_build.hpp:7-17). */

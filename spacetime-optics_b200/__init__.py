@@ -44,6 +44,13 @@ def lib():
         L.so_probe_fma_peak.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
         L.so_probe_sfu_peak.argtypes = [C.c_int, P(C.c_double)]
         L.so_radio_flux_noalloc.argtypes = [vp, vp, C.c_int, C.c_double, P(Plasma), vp, vp, vp]
+        L.so_batch_create.argtypes = [vp, P(Scene), C.c_int, P(Frame), P(C.c_int), C.c_int, C.c_int, C.c_int,
+                                      C.c_int, P(vp)]
+        L.so_batch_render.argtypes = [vp, vp, P(Stats)]
+        L.so_batch_autotune.argtypes = [vp, vp, P(abi.Tune)]
+        L.so_batch_set_tune.argtypes = [vp, P(abi.Tune)]
+        L.so_batch_free.argtypes = [vp]
+        L.so_batch_free.restype = None
         L.so_radio_flux.argtypes = [vp, P(Frame), C.c_int, C.c_double, P(C.c_double)]
         L.so_trace_rays.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
         L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
@@ -257,6 +264,47 @@ class Renderer:
                                        C.byref(n0), C.byref(jy)), self.h)
         self.scene = scene
         return n0.value, jy.value
+
+
+class Batch:
+    """Many frames traced by one persistent launch (so_batch_*), replayed as a CUDA graph."""
+
+    def __init__(self, renderer, scenes, frames, frame_scene, W, H, spp=1):
+        self.r = renderer
+        sc = (Scene * len(scenes))(*scenes)
+        fr = (Frame * len(frames))(*frames)
+        fs = (C.c_int * len(frame_scene))(*frame_scene)
+        h = C.c_void_p()
+        _check(lib().so_batch_create(renderer.h, sc, len(scenes), fr, fs, len(frames), W, H, spp, C.byref(h)),
+               renderer.h)
+        self.h = h
+        self.n = len(frames)
+        self.W, self.H = W, H
+
+    def render(self, d_px, stats=False):
+        st = Stats() if stats else None
+        _check(lib().so_batch_render(self.h, C.c_void_p(d_px), C.byref(st) if st else None), self.r.h)
+        return st
+
+    def autotune(self, d_px):
+        t = abi.Tune()
+        _check(lib().so_batch_autotune(self.h, C.c_void_p(d_px), C.byref(t)), self.r.h)
+        return t
+
+    def set_tune(self, ctas_per_sm, interleave):
+        t = abi.Tune(ctas_per_sm, interleave, 0.0)
+        _check(lib().so_batch_set_tune(self.h, C.byref(t)), self.r.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().so_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def probe_fma_peak(device=0):

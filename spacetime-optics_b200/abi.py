@@ -109,6 +109,10 @@ class MixedOpts(C.Structure):
                 ("r_switch", C.c_double), ("tol_approach", C.c_double), ("t32_blocks", C.c_int)]
 
 
+class Tune(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int), ("interleave", C.c_int), ("ms", C.c_double)]
+
+
 class SceneInfo(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("mass_msun", "distance_cm", "rg_cm", "tg_s", "uas_per_m", "disk_tmax",
                                           "disk_mdot_edd", "radio_flux_target_jy")]
@@ -129,6 +133,7 @@ LAYOUT_FIELDS = [
 EXPORTS = [
     "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
     "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak", "so_radio_flux_noalloc",
+    "so_batch_create", "so_batch_render", "so_batch_autotune", "so_batch_set_tune", "so_batch_free",
     "so_set_precision", "so_set_plasma", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
     "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",

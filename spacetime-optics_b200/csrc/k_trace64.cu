@@ -13,6 +13,13 @@
 // The loop ends when the queue is empty and every lane has retired; each ray is bounded by
 // max_steps attempts, so there is no unbounded wait anywhere.
 //
+// The torus turbulence (a 512-mode Fourier sum per flow step) is evaluated cooperatively: the
+// iteration is split around it, every lane that needs a sum has its modes spread over the 32 lanes
+// of the warp, and a shuffle reduction returns it.  The geometry and the rest of the emission are
+// per lane.  EMIT32 evaluates that sum with FP32 SFU cosines (the geometry stays FP64): used where
+// the geometry must be FP64 (critical band, photon-ring batches) but the emission needs no more
+// than FP32.
+//
 // Compiled with -fmad=false: every fusion is an explicit fma() (so_kerr.cuh), matching the oracle.
 #include <cuda_runtime.h>
 
@@ -59,15 +66,17 @@ __device__ __forceinline__ void ray_init(Ray64& R, const so_scene& S, const so_f
     }
 }
 
-// One loop iteration of trace_ray (trace.cuh:81-163).  Returns 1 when the ray is finished and sets
-// fate (and the escape angles for escaped rays).
+enum Stage : int { ST_REJECTED = 0, ST_ACCEPTED = 1, ST_DONE = 2 };
+
+// First half of one loop iteration of trace_ray (trace.cuh:81-129): step cap, DP5(4) attempt,
+// controller on rejection, swept angle, equatorial crossing (with the disk).  On acceptance the new
+// state is in yn / k7 and the ray continues in ray_commit.
 template <int VAR>
-__device__ __forceinline__ int ray_step(Ray64& R, const so_scene& S, const TorusParams& tp, const ModesSmem& md,
-                                        double rcam, int* fate, double* th, double* ph, double* cross_r,
-                                        double* cross_g) {
+__device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, double* yn, double* k7, double* hc_out,
+                                           double* err_out, int* fate, double* cross_r, double* cross_g) {
     if (R.it >= S.max_steps) {
         *fate = 0;
-        return 1;
+        return ST_DONE;
     }
     ++R.it;
     double hc = R.h;
@@ -79,11 +88,12 @@ __device__ __forceinline__ int ray_step(Ray64& R, const so_scene& S, const Torus
         hc = fmin(hc, 0.3 / (fabs(R.y[3]) + 1e-30));
     }
     ++R.natt;
-    double yn[6], k7[6];
     double err = dp54(R.c, R.y, R.k1, hc, S.tol, yn, k7);
+    *hc_out = hc;
+    *err_out = err;
     if (!(err <= 1.0)) {
         R.h = reject_step(hc, err);
-        return 0;
+        return ST_REJECTED;
     }
     ++R.nacc;
     if (VAR == VAR_RADIO) {
@@ -133,22 +143,31 @@ __device__ __forceinline__ int ray_step(Ray64& R, const so_scene& S, const Torus
                     R.trans *= 1.0 - cs[3];
                     if (R.trans < 1e-4) {
                         *fate = -1;
-                        return 1;
+                        return ST_DONE;
                     }
                 }
             }
         }
     }
+    return ST_ACCEPTED;
+}
+
+// Second half (trace.cuh:130-163): hot-flow transfer with the turbulence sum delta, commit,
+// projection, controller, termination.  Returns 1 when the ray is finished.
+template <int VAR>
+__device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const TorusParams& tp, double delta,
+                                          const double* yn, const double* k7, double hc, double err, int* fate,
+                                          double* th, double* ph) {
     if (VAR == VAR_RADIO && S.flow_on && yn[0] < S.r_flow_max) {
         double dI, dtau;
-        flow_step(S, tp, md, rcam, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+        flow_step(S, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+        ++R.nflow;
         float cc = (float)(R.trans * dI);
         int n = (int)(R.psi * (1.0 / PI));
         R.acc[0] += cc;
         if (n == 1) R.acc[1] += cc;
         else if (n == 2) R.acc[2] += cc;
         else if (n >= 3) R.acc[3] += cc;
-        ++R.nflow;
         R.trans *= exp(-dtau);
         if (R.trans < 1e-5) {
             *fate = -1;
@@ -174,6 +193,70 @@ __device__ __forceinline__ int ray_step(Ray64& R, const so_scene& S, const Torus
     return 0;
 }
 
+// Turbulence sums of the lanes in `want`, each split over the warp (lane l takes modes l, l+32, ...)
+// and reduced with butterfly shuffles; two positions are served per pass so each mode read feeds two
+// cosines.  All 32 lanes must call this.  FP64: modes in shared memory as SoA doubles.
+__device__ __forceinline__ double warp_turbulence64(const ModesSmem& md, int n, bool want, double X, double Y,
+                                                    double Z) {
+    const int lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(FULL, want);
+    double mine = 0.0;
+    while (m) {
+        const int s0 = __ffs(m) - 1;
+        m &= m - 1;
+        const int s1 = m ? __ffs(m) - 1 : s0;
+        if (m) m &= m - 1;
+        const double x0 = __shfl_sync(FULL, X, s0), y0 = __shfl_sync(FULL, Y, s0), z0 = __shfl_sync(FULL, Z, s0);
+        const double x1 = __shfl_sync(FULL, X, s1), y1 = __shfl_sync(FULL, Y, s1), z1 = __shfl_sync(FULL, Z, s1);
+        double a = 0.0, b = 0.0;
+        for (int i = lane; i < n; i += 32) {
+            const double kx = md.kx[i], ky = md.ky[i], kz = md.kz[i], p0 = md.ph[i], w = md.amp[i];
+            a = fma(w, cos(fma(kz, z0, fma(ky, y0, fma(kx, x0, p0)))), a);
+            b = fma(w, cos(fma(kz, z1, fma(ky, y1, fma(kx, x1, p0)))), b);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(FULL, a, o);
+            b += __shfl_xor_sync(FULL, b, o);
+        }
+        if (lane == s0) mine = a;
+        if (lane == s1) mine = b;
+    }
+    return mine;
+}
+
+// Same with FP32 SFU cosines (modes as float4 (k, phase) and float amplitude in shared memory).
+__device__ __forceinline__ double warp_turbulence32(const float4* __restrict__ km, const float* __restrict__ amp, int n,
+                                                    bool want, double X, double Y, double Z) {
+    const int lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(FULL, want);
+    float mine = 0.f;
+    const float Xf = (float)X, Yf = (float)Y, Zf = (float)Z;
+    while (m) {
+        const int s0 = __ffs(m) - 1;
+        m &= m - 1;
+        const int s1 = m ? __ffs(m) - 1 : s0;
+        if (m) m &= m - 1;
+        const float x0 = __shfl_sync(FULL, Xf, s0), y0 = __shfl_sync(FULL, Yf, s0), z0 = __shfl_sync(FULL, Zf, s0);
+        const float x1 = __shfl_sync(FULL, Xf, s1), y1 = __shfl_sync(FULL, Yf, s1), z1 = __shfl_sync(FULL, Zf, s1);
+        float a = 0.f, b = 0.f;
+        for (int i = lane; i < n; i += 32) {
+            const float4 k = km[i];
+            const float w = amp[i];
+            a = fmaf(w, __cosf(fmaf(k.z, z0, fmaf(k.y, y0, fmaf(k.x, x0, k.w)))), a);
+            b = fmaf(w, __cosf(fmaf(k.z, z1, fmaf(k.y, y1, fmaf(k.x, x1, k.w)))), b);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(FULL, a, o);
+            b += __shfl_xor_sync(FULL, b, o);
+        }
+        if (lane == s0) mine = a;
+        if (lane == s1) mine = b;
+    }
+    return (double)mine;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
@@ -182,28 +265,35 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 
 }  // namespace
 
-template <int VAR>
+template <int VAR, bool EMIT32>
 __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
     extern __shared__ double smem[];
     TorusParams tp;
     tp.on = VAR == VAR_RADIO && L.torus;
-    tp.n_modes = L.n_modes;
+    tp.n_modes = tp.on ? L.n_modes : 0;
     tp.ne_index = L.ne_index;
     tp.te_index = L.te_index;
     tp.h_sph = L.h_sph;
     tp.theta_e0 = L.theta_e0;
     tp.half_var = L.half_var;
-    ModesSmem md = {smem, smem + L.n_modes, smem + 2 * L.n_modes, smem + 3 * L.n_modes, smem + 4 * L.n_modes};
-    if (VAR == VAR_RADIO && tp.on) {
-        // Stage the mode table once per CTA (SoA in shared memory, all lanes then read one mode at a
-        // time: a broadcast).
-        for (int i = threadIdx.x; i < L.n_modes; i += blockDim.x) {
+    ModesSmem md = {smem, smem + tp.n_modes, smem + 2 * tp.n_modes, smem + 3 * tp.n_modes, smem + 4 * tp.n_modes};
+    float4* km = reinterpret_cast<float4*>(smem);
+    float* kamp = reinterpret_cast<float*>(km + tp.n_modes);
+    if (tp.n_modes > 0) {
+        // Stage the mode table once per CTA; every lane then reads the modes of its share
+        for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
             so_mode m = L.modes[i];
-            smem[i] = m.kx;
-            smem[L.n_modes + i] = m.ky;
-            smem[2 * L.n_modes + i] = m.kz;
-            smem[3 * L.n_modes + i] = m.phase;
-            smem[4 * L.n_modes + i] = m.amp;
+            if (EMIT32) {
+                double p = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
+                km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)p);
+                kamp[i] = (float)m.amp;
+            } else {
+                smem[i] = m.kx;
+                smem[tp.n_modes + i] = m.ky;
+                smem[2 * tp.n_modes + i] = m.kz;
+                smem[3 * tp.n_modes + i] = m.phase;
+                smem[4 * tp.n_modes + i] = m.amp;
+            }
         }
         __syncthreads();
     }
@@ -220,6 +310,7 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
     const so_scene* S = nullptr;
     const so_frame* F = nullptr;
     const bool radio_lum = VAR == VAR_RADIO;  // sample_lum, render.cu:87
+    const bool rec = L.kind == RAYS_LIST && L.record_cross;
 
     for (;;) {
         const bool need = !active && !exhausted;
@@ -252,8 +343,15 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
                         pixel_point(L, L.frames[0], pix, sbase, &x, &yv);
                     } else if (L.kind == RAYS_PIXELS) {
                         const long long npix = (long long)L.W * L.H;
-                        fidx = (int)(job / npix);
-                        pix = job % npix;
+                        if (L.interleave && L.nframes > 1) {
+                            // consecutive jobs cycle through the frames: cheap and expensive frames
+                            // (different spins, zooms) mix in every warp instead of queueing up
+                            fidx = (int)(job % L.nframes);
+                            pix = job / L.nframes;
+                        } else {
+                            fidx = (int)(job / npix);
+                            pix = job % npix;
+                        }
                         sbase = L.sample0;
                         jobs_n = L.spp;
                         pixel_point(L, L.frames[fidx], pix, sbase, &x, &yv);
@@ -282,11 +380,25 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
             }
         }
         if (__all_sync(FULL, !active)) break;
-        if (!active) continue;
-        int fate = 0;
+        // ---- first half: the attempt (active lanes) ------------------------------------------
+        int fate = 0, stage = ST_REJECTED;
+        double yn[6], k7[6], hc = 0.0, err = 0.0;
+        bool want = false;
+        double TX = 0.0, TY = 0.0, TZ = 0.0;
+        if (active) {
+            stage = ray_attempt<VAR>(R, *S, yn, k7, &hc, &err, &fate, rec ? cr : nullptr, cg);
+            if (VAR == VAR_RADIO && stage == ST_ACCEPTED && S->flow_on && yn[0] < S->r_flow_max)
+                want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
+        }
+        // ---- all lanes: turbulence sums --------------------------------------------------------
+        double delta = 0.0;
+        if (VAR == VAR_RADIO && tp.n_modes > 0)
+            delta = EMIT32 ? warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ)
+                           : warp_turbulence64(md, tp.n_modes, want, TX, TY, TZ);
+        // ---- second half: emission and commit (active lanes) ----------------------------------
+        if (!active || stage == ST_REJECTED) continue;
         double th = 0.0, ph = 0.0;
-        const bool rec = L.kind == RAYS_LIST && L.record_cross;
-        if (!ray_step<VAR>(R, *S, tp, md, F->r, &fate, &th, &ph, rec ? cr : nullptr, cg)) continue;
+        if (stage == ST_ACCEPTED && !ray_commit<VAR>(R, *S, tp, delta, yn, k7, hc, err, &fate, &th, &ph)) continue;
         // sample finished
         n_att += (unsigned long long)R.natt;
         n_acc += (unsigned long long)R.nacc;
@@ -326,8 +438,9 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
                 pixel_point(L, *F, pix, sbase + sample, &x, &yv);
                 ray_init<VAR>(R, *S, *F, x, yv);
             } else if (L.kind == RAYS_PIXELS) {
-                reinterpret_cast<float4*>(L.accum)[job] = make_float4(pa[0], pa[1], pa[2], pa[3]);
-                if (L.ystat) reinterpret_cast<float2*>(L.ystat)[job] = make_float2(ys, yq);
+                const long long o = (long long)fidx * L.W * L.H + pix;
+                reinterpret_cast<float4*>(L.accum)[o] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+                if (L.ystat) reinterpret_cast<float2*>(L.ystat)[o] = make_float2(ys, yq);
                 active = false;
             } else {
                 reinterpret_cast<float4*>(L.chunk_acc)[job] = make_float4(pa[0], pa[1], pa[2], pa[3]);
@@ -347,40 +460,36 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
     }
 }
 
-// Host launcher: grid = SMs x resident CTAs per SM (persistent), dynamic shared memory for the
-// mode table.  Returns the CUDA error of the launch.
+// Host launcher: grid = SMs x resident CTAs per SM (persistent; capped by L.ctas_per_sm), dynamic
+// shared memory for the mode table.  Returns the CUDA error of the launch.
 cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaStream_t st) {
     const int tpb = 128;
-    size_t smem = (variant == VAR_RADIO && L.torus) ? (size_t)5 * L.n_modes * sizeof(double) : 0;
+    const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;
+    const bool emit32 = torus && L.emit32;
+    size_t smem = torus ? (size_t)L.n_modes * (emit32 ? sizeof(float4) + sizeof(float) : 5 * sizeof(double)) : 0;
     int per_sm = 1;
-    cudaError_t e;
+    auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t e;
+        if (smem > 48 * 1024) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tpb, smem);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        if (L.ctas_per_sm > 0 && L.ctas_per_sm < per_sm) per_sm = L.ctas_per_sm;
+        long long want = (L.nrays + tpb - 1) / tpb;
+        long long grid = (long long)num_sms * per_sm;
+        if (grid > want) grid = want;
+        if (grid < 1) grid = 1;
+        kern<<<(int)grid, tpb, smem, st>>>(L);
+        return cudaGetLastError();
+    };
     switch (variant) {
-        case VAR_VACUUM:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_VACUUM>, tpb, smem);
-            break;
-        case VAR_DISK:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_DISK>, tpb, smem);
-            break;
-        default:
-            if (smem > 48 * 1024) {
-                e = cudaFuncSetAttribute(k_trace64<VAR_RADIO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                if (e != cudaSuccess) return e;
-            }
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace64<VAR_RADIO>, tpb, smem);
-            break;
+        case VAR_VACUUM: return go(k_trace64<VAR_VACUUM, false>);
+        case VAR_DISK: return go(k_trace64<VAR_DISK, false>);
+        default: return emit32 ? go(k_trace64<VAR_RADIO, true>) : go(k_trace64<VAR_RADIO, false>);
     }
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    long long want = (L.nrays + tpb - 1) / tpb;
-    long long grid = (long long)num_sms * per_sm;
-    if (grid > want) grid = want;
-    if (grid < 1) grid = 1;
-    switch (variant) {
-        case VAR_VACUUM: k_trace64<VAR_VACUUM><<<(int)grid, tpb, smem, st>>>(L); break;
-        case VAR_DISK: k_trace64<VAR_DISK><<<(int)grid, tpb, smem, st>>>(L); break;
-        default: k_trace64<VAR_RADIO><<<(int)grid, tpb, smem, st>>>(L); break;
-    }
-    return cudaGetLastError();
 }
 
 }  // namespace so

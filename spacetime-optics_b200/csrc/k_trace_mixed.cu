@@ -233,28 +233,46 @@ struct Torus32 {
 
 // Turbulence sums of the lanes in `want` (positions X, Y, Z per lane), each split across the warp:
 // lane l takes modes l, l+32, ...; a butterfly shuffle reduction gives every lane the total, which
-// the owning lane keeps.  All 32 lanes must call this.  Modes in shared memory as turns
-// (k / 2 pi, phase / 2 pi), so the reduced phase p - rint(p) feeds the SFU cosine on [-pi, pi].
+// the owning lane keeps.  Positions are served two at a time, so each mode read from shared memory
+// feeds two cosines, with two independent accumulators per position.  All 32 lanes must call this.
+// Modes in shared memory in radians (k, phase) and amplitude; the SFU cosine reduces the phase in
+// turns itself, so the argument's FP32 rounding (|phase| <~ 1e3 rad: ~5e-5 rad) is the only error.
 __device__ __forceinline__ float warp_turbulence(const float4* __restrict__ km, const float* __restrict__ amp, int n,
                                                  bool want, float X, float Y, float Z) {
     const int lane = threadIdx.x & 31;
     unsigned m = __ballot_sync(FULL, want);
     float mine = 0.f;
     while (m) {
-        const int src = __ffs(m) - 1;
+        const int s0 = __ffs(m) - 1;
         m &= m - 1;
-        const float x = __shfl_sync(FULL, X, src), y = __shfl_sync(FULL, Y, src), z = __shfl_sync(FULL, Z, src);
-        float acc = 0.f;
-#pragma unroll 4
-        for (int i = lane; i < n; i += 32) {
-            const float4 k = km[i];
-            float p = fmaf(k.z, z, fmaf(k.y, y, fmaf(k.x, x, k.w)));
-            p -= rintf(p);
-            acc = fmaf(amp[i], __cosf(6.28318530718f * p), acc);
+        const int s1 = m ? __ffs(m) - 1 : s0;
+        if (m) m &= m - 1;
+        const float x0 = __shfl_sync(FULL, X, s0), y0 = __shfl_sync(FULL, Y, s0), z0 = __shfl_sync(FULL, Z, s0);
+        const float x1 = __shfl_sync(FULL, X, s1), y1 = __shfl_sync(FULL, Y, s1), z1 = __shfl_sync(FULL, Z, s1);
+        float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+        int i = lane;
+        for (; i + 32 < n; i += 64) {
+            const float4 k = km[i], q = km[i + 32];
+            const float w = amp[i], v = amp[i + 32];
+            a0 = fmaf(w, __cosf(fmaf(k.z, z0, fmaf(k.y, y0, fmaf(k.x, x0, k.w)))), a0);
+            b0 = fmaf(w, __cosf(fmaf(k.z, z1, fmaf(k.y, y1, fmaf(k.x, x1, k.w)))), b0);
+            a1 = fmaf(v, __cosf(fmaf(q.z, z0, fmaf(q.y, y0, fmaf(q.x, x0, q.w)))), a1);
+            b1 = fmaf(v, __cosf(fmaf(q.z, z1, fmaf(q.y, y1, fmaf(q.x, x1, q.w)))), b1);
         }
+        if (i < n) {
+            const float4 k = km[i];
+            const float w = amp[i];
+            a0 = fmaf(w, __cosf(fmaf(k.z, z0, fmaf(k.y, y0, fmaf(k.x, x0, k.w)))), a0);
+            b0 = fmaf(w, __cosf(fmaf(k.z, z1, fmaf(k.y, y1, fmaf(k.x, x1, k.w)))), b0);
+        }
+        float a = a0 + a1, b = b0 + b1;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
-        if (lane == src) mine = acc;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(FULL, a, o);
+            b += __shfl_xor_sync(FULL, b, o);
+        }
+        if (lane == s0) mine = a;
+        if (lane == s1) mine = b;
     }
     return mine;
 }
@@ -355,11 +373,11 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     float4* km = sm4;
     float* amp = reinterpret_cast<float*>(sm4 + tp.n_modes);
     if (tp.n_modes > 0) {
-        const double i2pi = 1.0 / (2.0 * PI);
         for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
             so_mode m = L.modes[i];
-            km[i] = make_float4((float)(m.kx * i2pi), (float)(m.ky * i2pi), (float)(m.kz * i2pi),
-                                (float)(m.phase * i2pi));
+            // phase folded into (-pi, pi]: its FP32 rounding then stays small
+            double ph = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
+            km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)ph);
             amp[i] = (float)m.amp;
         }
         __syncthreads();
@@ -407,10 +425,10 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                     c.E = p3.z;
                     R.h = p3.w;
                     R.psi = p4.x;
-                    R.natt = __float_as_int(p4.y);
-                    R.nacc = __float_as_int(p4.z);
+                    R.it = __float_as_int(p4.y);  // attempts so far (max_steps covers the whole ray)
+                    R.natt = 0;                   // FP32 attempts / accepted steps of this kernel
+                    R.nacc = 0;
                     R.ncross = __float_as_int(p4.w);
-                    R.it = R.natt;
                     R.nflow = 0;
                     c.CP = fmaf(-c.a, c.lam, c.A2);
                     float lma = c.lam - c.a;

@@ -202,14 +202,6 @@ struct ModesSmem {
     const double* ph;
     const double* amp;
 };
-__device__ __forceinline__ double torus_delta(const ModesSmem& md, int n, double X, double Y, double Z) {
-    double acc = 0.0;
-    for (int m = 0; m < n; ++m) {
-        double p = fma(md.kz[m], Z, fma(md.ky[m], Y, fma(md.kx[m], X, md.ph[m])));
-        acc = fma(md.amp[m], cos(p), acc);
-    }
-    return acc;
-}
 
 // flow_step (emission.cuh:264-340): source term g^3 S (1 - e^-dtau) and optical depth of a Mino
 // step h at (r, u, phi, t).  The torus model replaces the density / temperature / turbulence
@@ -218,9 +210,30 @@ __device__ __forceinline__ double torus_delta(const ModesSmem& md, int n, double
 // t + (rcam - r + 2 ln(rcam / r)) (the retarded time of emission.cuh:26-28 plus the frame time):
 // the raw coordinate time is ~ -rcam at the hole, which would put a factor rcam on every rounding
 // error of the advected phase.
-static __device__ void flow_step(const so_scene& S, const TorusParams& tp, const ModesSmem& md, double rcam, double r,
-                          double u, double phi, double t, double lam, double Ecam, double h, double* dI,
-                          double* dtau) {
+//
+// Where the torus turbulence is needed for a flow step at (r, u, phi, t): false when flow_step
+// returns before using it; else the advected Cartesian position (X, Y, Z) of the sum.
+__device__ __forceinline__ bool torus_position(const so_scene& S, const TorusParams& tp, double rcam, double r,
+                                               double u, double phi, double t, double* X, double* Y, double* Z) {
+    if (!tp.on || tp.n_modes <= 0) return false;
+    double s2 = fmax(fma(-u, u, 1.0), 1e-12), s = sqrt(s2);
+    double R = r * s;
+    if (r > S.r_flow_max || R < 1e-3) return false;
+    double zh = u / tp.h_sph;
+    if (exp(-0.5 * zh * zh) < 1e-7) return false;
+    double Omf = S.flow_kep * keplerian_omega(S.a, fmax(R, S.r_isco));
+    double phc = phi - Omf * (t + (rcam - r + 2.0 * log(rcam / r)));
+    double sp, cp;
+    sincos(phc, &sp, &cp);
+    *X = R * cp;
+    *Y = R * sp;
+    *Z = r * u;
+    return true;
+}
+
+// flow_step with the torus turbulence sum `delta` at this point already evaluated (torus_position).
+static __device__ void flow_step(const so_scene& S, const TorusParams& tp, double delta, double r, double u,
+                                 double phi, double t, double lam, double Ecam, double h, double* dI, double* dtau) {
     *dI = 0.0;
     *dtau = 0.0;
     const double a = S.a;
@@ -234,14 +247,7 @@ static __device__ void flow_step(const so_scene& S, const TorusParams& tp, const
         if (vert < 1e-7) return;
         double lx = log(r / S.rh);
         ne = S.n0 * exp(-tp.ne_index * lx) * vert;
-        if (tp.n_modes > 0) {
-            double Omf = S.flow_kep * keplerian_omega(a, fmax(R, S.r_isco));
-            double phc = phi - Omf * (t + (rcam - r + 2.0 * log(rcam / r)));
-            double sp, cp;
-            sincos(phc, &sp, &cp);
-            double d = torus_delta(md, tp.n_modes, R * cp, R * sp, z);
-            ne *= exp(d - tp.half_var);
-        }
+        if (tp.n_modes > 0) ne *= exp(delta - tp.half_var);
         Th = tp.theta_e0 * exp(-tp.te_index * lx);
     } else {
         double zh = z / (S.h_r * R);

@@ -73,6 +73,10 @@ struct TraceLaunch {
     double tol_approach;      // tolerance of the FP64 approach
     double r_emit;            // FP32 tracer: outgoing beyond this radius = escaped (0 = off)
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
+    // batched frames (RAYS_PIXELS over nframes)
+    int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
+    int ctas_per_sm;          // persistent grid: CTAs per SM (0 = as many as fit)
+    int emit32;               // FP64 tracer: torus turbulence sums in FP32 (geometry stays FP64)
     const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi
     int band_n;
     float4* state;            // parked ray state, 5 float4 per sample id (SoA planes of nsamples)

@@ -295,6 +295,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     Lb.nrays = ns;
     Lb.nrays_dev = &r->d_nlists[1];
     Lb.counters = &r->d_cnt3[0];
+    Lb.emit32 = 1;  // FP64 geometry in the band; the emission needs no more than FP32
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
     SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
@@ -806,6 +807,234 @@ int so_normalize_flux(so_renderer* r, so_scene* scene, const so_frame* f_wide, i
     if (n0_out) *n0_out = scene->n0;
     if (jy_out) *jy_out = std::exp(f1v);
     return SO_OK;
+}
+
+}  // extern "C"
+
+// ---- batched frames (the persistent wavefront) -----------------------------------------------------
+struct so_batch {
+    so_renderer* r = nullptr;
+    int nframes = 0, nscenes = 0, W = 0, H = 0, spp = 1, variant = VAR_VACUUM;
+    so_scene* d_scenes = nullptr;
+    so_frame* d_frames = nullptr;
+    int* d_frame_scene = nullptr;
+    Counters* d_cnt = nullptr;
+    so_tune tune{0, 1, 0.0};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    float* graph_px = nullptr;  // output buffer baked into the graph
+    so_tune graph_tune{-1, -1, 0.0};
+};
+
+namespace {
+
+void batch_drop_graph(so_batch* b) {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->gexec = nullptr;
+    b->graph = nullptr;
+    b->graph_px = nullptr;
+}
+
+// The launch sequence of one batch: counter reset, persistent tracer over all frames, resolve.
+int batch_enqueue(so_batch* b, float* d_px) {
+    so_renderer* r = b->r;
+    SO_CK(r, cudaMemsetAsync(b->d_cnt, 0, sizeof(Counters), r->st));
+    TraceLaunch L;
+    launch_common(r, L);
+    L.scenes = b->d_scenes;
+    L.frames = b->d_frames;
+    L.frame_scene = b->d_frame_scene;
+    L.nframes = b->nframes;
+    L.counters = b->d_cnt;
+    L.kind = RAYS_PIXELS;
+    L.W = b->W;
+    L.H = b->H;
+    L.spp = b->spp;
+    L.jitter = 1;
+    L.nrays = (long long)b->W * b->H * b->nframes;
+    L.accum = d_px;
+    L.interleave = b->tune.interleave;
+    L.ctas_per_sm = b->tune.ctas_per_sm;
+    // mixed precision on a batch: FP64 geometry everywhere (photon-ring windows lie in the critical
+    // band), FP32 turbulence sums
+    L.emit32 = r->precision == SO_PREC_MIXED;
+    cudaError_t e = launch_trace64(L, b->variant, r->num_sms, r->st);
+    if (e != cudaSuccess) return cuda_fail(r, e, "batch tracer launch");
+    SO_CK(r, launch_resolve(reinterpret_cast<float4*>(d_px), reinterpret_cast<const float4*>(d_px), nullptr,
+                            (uint32_t)b->spp, L.nrays, r->S.mode == SO_MODE_VISIBLE, r->st));
+    return SO_OK;
+}
+
+int batch_capture(so_batch* b, float* d_px) {
+    so_renderer* r = b->r;
+    batch_drop_graph(b);
+    SO_CK(r, cudaStreamBeginCapture(r->st, cudaStreamCaptureModeRelaxed));
+    int rc = batch_enqueue(b, d_px);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(r->st, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(r, e, "batch graph capture");
+    b->graph = g;
+    SO_CK(r, cudaGraphInstantiate(&b->gexec, g, 0));
+    b->graph_px = d_px;
+    b->graph_tune = b->tune;
+    return SO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const so_frame* frames, const int* frame_scene,
+                    int nframes, int W, int H, int spp, so_batch** out) {
+    if (!out) return fail(r, SO_ERR_ARG, "so_batch_create: out is NULL");
+    *out = nullptr;
+    if (!r || !scenes || !frames || !frame_scene || nscenes <= 0 || nframes <= 0 || W <= 0 || H <= 0 || spp <= 0)
+        return fail(r, SO_ERR_ARG, "so_batch_create: bad argument");
+    if ((long long)W * H * nframes > 0x7fffffffll) return fail(r, SO_ERR_SIZE, "so_batch_create: too many rays");
+    for (int i = 0; i < nframes; ++i)
+        if (frame_scene[i] < 0 || frame_scene[i] >= nscenes) return fail(r, SO_ERR_ARG, "so_batch_create: frame_scene");
+    const int var = variant_of(scenes[0]);
+    for (int s = 0; s < nscenes; ++s) {
+        if (scenes[s].sky_on) return fail(r, SO_ERR_UNSUPPORTED, "so_batch_create: sky texture lookups");
+        if (variant_of(scenes[s]) != var) return fail(r, SO_ERR_ARG, "so_batch_create: scenes of different modes");
+        if (scenes[s].disk_on && scenes[s].a != r->S.a)
+            return fail(r, SO_ERR_UNSUPPORTED, "so_batch_create: disk scenes need the renderer's spin (disk table)");
+    }
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    so_batch* b = new so_batch;
+    b->r = r;
+    b->nframes = nframes;
+    b->nscenes = nscenes;
+    b->W = W;
+    b->H = H;
+    b->spp = spp;
+    b->variant = var;
+    std::vector<so_scene> sc(scenes, scenes + nscenes);
+    for (so_scene& s : sc) {  // the renderer's device tables
+        s.disk_lnT = r->d_disk;
+        s.k2_lntab = r->d_k2;
+        s.bb_xyz = r->d_bb;
+        s.disk_n = r->S.disk_n;
+        s.k2_n = r->S.k2_n;
+        s.bb_n = r->S.bb_n;
+    }
+    std::vector<so_frame> fr(frames, frames + nframes);
+    for (so_frame& f : fr) {
+        f.W = W;
+        f.H = H;
+        f.spp = spp;
+    }
+    int rc = SO_OK;
+    if (dalloc(&b->d_scenes, (size_t)nscenes) != cudaSuccess || dalloc(&b->d_frames, (size_t)nframes) != cudaSuccess ||
+        dalloc(&b->d_frame_scene, (size_t)nframes) != cudaSuccess || dalloc(&b->d_cnt, 1) != cudaSuccess)
+        rc = fail(r, SO_ERR_ALLOC, "so_batch_create: device allocation");
+    if (!rc && (cudaMemcpy(b->d_scenes, sc.data(), sc.size() * sizeof(so_scene), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_frames, fr.data(), fr.size() * sizeof(so_frame), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(b->d_frame_scene, frame_scene, (size_t)nframes * sizeof(int), cudaMemcpyHostToDevice) !=
+                    cudaSuccess))
+        rc = fail(r, SO_ERR_CUDA, "so_batch_create: upload");
+    if (rc) {
+        so_batch_free(b);
+        return rc;
+    }
+    *out = b;
+    return SO_OK;
+}
+
+int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
+    if (!b || !d_px) return SO_ERR_ARG;
+    so_renderer* r = b->r;
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    if (!b->gexec || b->graph_px != d_px || b->graph_tune.ctas_per_sm != b->tune.ctas_per_sm ||
+        b->graph_tune.interleave != b->tune.interleave) {
+        int rc = batch_capture(b, d_px);
+        if (rc) return rc;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, r->st);
+    }
+    cudaError_t e = cudaGraphLaunch(b->gexec, r->st);
+    if (e != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        return cuda_fail(r, e, "so_batch_render graph launch");
+    }
+    if (stats) {
+        cudaEventRecord(e1, r->st);
+        Counters c;
+        e = cudaMemcpyAsync(&c, b->d_cnt, sizeof c, cudaMemcpyDeviceToHost, r->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(r->st);
+        float ms = 0.f;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e != cudaSuccess) return cuda_fail(r, e, "so_batch_render");
+        std::memset(stats, 0, sizeof *stats);
+        stats->samples = (long long)b->W * b->H * b->nframes * b->spp;
+        stats->step_limited = (long long)c.step_limited;
+        stats->attempts = (long long)c.attempts;
+        stats->accepted = (long long)c.accepted;
+        stats->flow_steps = (long long)c.flow_steps;
+        stats->ms_kernel = ms;
+        stats->ms_trace = ms;
+    }
+    return SO_OK;
+}
+
+int so_batch_set_tune(so_batch* b, const so_tune* t) {
+    if (!b || !t || t->ctas_per_sm < 0 || (t->interleave != 0 && t->interleave != 1)) return SO_ERR_ARG;
+    b->tune.ctas_per_sm = t->ctas_per_sm;
+    b->tune.interleave = t->interleave;
+    return SO_OK;
+}
+
+int so_batch_autotune(so_batch* b, float* d_px, so_tune* best) {
+    if (!b || !d_px) return SO_ERR_ARG;
+    // warm-up with the full grid; then CTAs per SM from 1 up (the launcher caps the value at the
+    // kernel's occupancy limit, so the sweep stops once a larger cap no longer helps)
+    const int per_sm = 8;
+    {
+        so_tune keep = b->tune;
+        b->tune.ctas_per_sm = 0;
+        so_stats st;
+        int rc = so_batch_render(b, d_px, &st);
+        if (rc) return rc;
+        b->tune = keep;
+    }
+    so_tune winner{0, 1, 1e300};
+    for (int inter = 0; inter <= 1; ++inter) {
+        for (int c = 1; c <= per_sm; ++c) {
+            so_tune t{c, inter, 0.0};
+            b->tune = t;
+            so_stats st;
+            int rc = so_batch_render(b, d_px, &st);
+            if (rc) return rc;
+            if (st.ms_kernel < winner.ms) winner = {c, inter, st.ms_kernel};
+            // a larger cap than the occupancy limit launches the same grid: stop early
+            if (c >= 2 && st.ms_kernel > 1.5 * winner.ms) break;
+        }
+    }
+    b->tune = winner;
+    if (best) *best = winner;
+    return SO_OK;
+}
+
+void so_batch_free(so_batch* b) {
+    if (!b) return;
+    if (b->r) cudaSetDevice(b->r->device);
+    batch_drop_graph(b);
+    void* ps[] = {b->d_scenes, b->d_frames, b->d_frame_scene, b->d_cnt};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    delete b;
 }
 
 }  // extern "C"

@@ -79,8 +79,8 @@ def test_mixed_reference_flow_without_turbulence(so):
 
 
 def test_mixed_band_width_zero_and_all_fp64(so):
-    """band 0: every ray starts FP32; a band covering the field: every ray is FP64 and the image is
-    the FP64 kernel's bit for bit."""
+    """band 0: every ray starts FP32; a band covering the field: every ray has FP64 geometry (its
+    turbulence sums are FP32, so the image is the FP64 one to FP32 emission precision)."""
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=64", "camera.height=64", N0])
     r = so.Renderer(sh.scene, sh.tables, sh.settings)
     r.set_plasma(sh.plasma())
@@ -90,7 +90,8 @@ def test_mixed_band_width_zero_and_all_fp64(so):
     r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
     imgb, _, stb = r.render(f)
     assert stb.band_rays == 64 * 64 and stb.attempts_fp32 == 0
-    assert np.array_equal(img64, imgb)
+    l1, flux = _errors(img64, imgb)
+    assert l1 < 1e-4 and flux < 1e-5, (l1, flux)
     r.set_precision(so.abi.SO_PREC_MIXED, band_m=0.0)
     img0, _, st0 = r.render(f)
     assert st0.band_rays == 0
@@ -100,7 +101,8 @@ def test_mixed_band_width_zero_and_all_fp64(so):
 
 
 def test_mixed_retrace_list(so):
-    """A tiny drift tolerance sends every FP32 ray back to FP64: the image then equals the FP64 one."""
+    """A zero drift tolerance sends every FP32 ray back to FP64 geometry: the image then is the FP64
+    one to FP32 emission precision."""
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=48", "camera.height=48", N0])
     r = so.Renderer(sh.scene, sh.tables, sh.settings)
     r.set_plasma(sh.plasma())
@@ -110,7 +112,8 @@ def test_mixed_retrace_list(so):
     r.set_precision(so.abi.SO_PREC_MIXED, drift_tol=0.0)
     imgm, _, st = r.render(f)
     assert st.fp64_rays == 48 * 48
-    assert np.array_equal(img64, imgm)
+    l1, flux = _errors(img64, imgm)
+    assert l1 < 1e-4 and flux < 1e-5, (l1, flux)
     r.close()
 
 
