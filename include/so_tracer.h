@@ -298,6 +298,102 @@ int so_batch_autotune(so_batch* b, float* d_px, so_tune* best);
 int so_batch_set_tune(so_batch* b, const so_tune* t);
 void so_batch_free(so_batch* b);
 
+/* ---- ray surrogate (no reference counterpart) ------------------------------------------------- */
+/* A small MLP that maps an image-plane ray of a static camera -- Bardeen coordinates alpha, beta
+ * (M), spin a, inclination (degrees) -- to what the FP64 integrator reports for it: termination
+ * class, escape direction, and the radius and redshift of its first three equatorial crossings.
+ * 64 Gaussian random frequencies of the inputs scaled to [-1, 1] give 128 features (sin, cos);
+ * 4 hidden layers of 256 with tanh-form GELU; 12 outputs.  BF16 weights and activations with FP32
+ * accumulation in tensor memory (tcgen05 kernels of this library), FP32 master weights, AdamW.
+ * All pointers named d_* are device memory. */
+#define SO_SUR_NFREQ 64
+#define SO_SUR_HIDDEN 256
+#define SO_SUR_LAYERS 4
+#define SO_SUR_NOUT 12
+#define SO_SUR_LDOUT 16 /* floats per output row (12 used) */
+#define SO_SUR_NPARAMS 234512
+typedef struct so_surrogate so_surrogate;
+typedef struct so_sur_ray { float alpha, beta, spin, incl_deg; } so_sur_ray;
+/* What the integrator reported for a ray.  Output row of the network: [0..2] class logits,
+ * [3..5] direction, [6..8] u, [9..11] g. */
+typedef struct so_sur_target {
+    float cls;    /* 0 escaped, 1 captured, 2 step limit */
+    float dir[3]; /* escape direction (sin th cos ph, sin th sin ph, cos th); 0 unless escaped */
+    float u[3];   /* 1/r of the first three equatorial crossings; 0 where there is none */
+    float g[3];   /* redshift of a circular prograde emitter at those radii; 0 inside the ISCO / none */
+    float pad[2];
+} so_sur_target;
+typedef struct so_sur_opts {
+    float fourier_sigma;   /* std of the frequencies per unit of the scaled inputs */
+    uint32_t seed;         /* frequencies and initial weights */
+    int batch;             /* rays per optimiser step, a multiple of 128 */
+    float lr, lr_final;    /* cosine schedule over the steps of one so_sur_train call */
+    int warmup;            /* linear warm-up steps of that schedule */
+    float beta1, beta2, eps, weight_decay;
+    float w_dir, w_u, w_g; /* loss weights of direction, 1/r and redshift (class cross-entropy: 1) */
+} so_sur_opts;
+/* Mean loss terms per ray; accuracy = fraction of rays whose largest class logit is the target's. */
+typedef struct so_sur_loss { double total, ce, dir, u, g, accuracy; long long rays; } so_sur_loss;
+void so_sur_default_opts(so_sur_opts* o);
+int so_sur_create(int device, const so_sur_opts* o, so_surrogate** out);
+void so_sur_destroy(so_surrogate* s);
+/* Master parameters (host, SO_SUR_NPARAMS floats: per layer weight [N x K] row-major then bias;
+ * layer 0 256 x 128, layers 1-3 256 x 256, head 16 x 256 with rows 12-15 zero) and frequencies
+ * (host, SO_SUR_NFREQ x 4).  Either pointer may be NULL. */
+int so_sur_get_params(so_surrogate* s, float* params, float* freqs);
+int so_sur_set_params(so_surrogate* s, const float* params, const float* freqs);
+/* `steps` AdamW steps over n device rays / targets, batches taken cyclically (ray i of step k is
+ * (k * batch + i) mod n); *last gets the loss of the last step. */
+int so_sur_train(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_target* d_tgt, long long n, int steps,
+                 so_sur_loss* last);
+/* Loss over the first n - n % 128 rays, no update. */
+int so_sur_evaluate(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_target* d_tgt, long long n,
+                    so_sur_loss* loss);
+/* One forward and backward pass over n rays (n % 128 == 0) at the current parameters, no update:
+ * gradient of the mean loss in the master-parameter layout (host, SO_SUR_NPARAMS floats). */
+int so_sur_gradients(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_target* d_tgt, int n, float* grads,
+                     so_sur_loss* loss);
+/* Network outputs for n rays: d_out, n x SO_SUR_LDOUT floats.  Queued on `stream` (NULL = the
+ * surrogate's own stream); the call returns once the work is queued. */
+int so_sur_infer(so_surrogate* s, const so_sur_ray* d_rays, long long n, float* d_out, void* stream);
+/* Training set from the FP64 integrator of renderer r: `groups` (spin, inclination) pairs drawn
+ * uniformly from the ranges, n / groups rays each with alpha, beta uniform in [-xy_max, xy_max],
+ * traced in vacuum from a static camera at f->r.  Stored interleaved (ray j of group g at
+ * j * groups + g) so that consecutive rays come from different groups.  The renderer's scene is
+ * restored afterwards. */
+typedef struct so_sur_ranges { double a_min, a_max, incl_min, incl_max, xy_max; } so_sur_ranges;
+int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, uint32_t seed,
+                   const so_sur_ranges* ranges, so_sur_ray* d_rays, so_sur_target* d_tgt, so_stats* stats);
+/* Thin-disk frame through the surrogate: every pixel centre inside band_m of the analytic critical
+ * curve goes to the FP64 integrator; of the others a random audit_frac sample (seeded) goes to the
+ * integrator as well, and the surrogate shades the rest from its predicted crossing radii (the
+ * redshift is the exact one of that radius and the ray's constants of motion).  The integrator
+ * judges the surrogate on the audit rays.  Renderer r holds a visible-mode disk scene (no disk
+ * turbulence); d_px is W x H x 4 floats of device memory, the same quantity so_trace_rays reports
+ * as I at the pixel centres. */
+typedef struct so_sur_frame_opts { double band_m, audit_frac; uint32_t audit_seed; } so_sur_frame_opts;
+typedef struct so_sur_report {
+    long long rays, surrogate_rays, band_rays, audit_rays;
+    double ms_total, ms_route, ms_mlp, ms_shade, ms_integrator;
+    /* surrogate against the integrator on the audit rays */
+    long long audit_class_mismatch;
+    double audit_dir_err;   /* mean angle between escape directions (rad), rays both call escaped */
+    double audit_u_err;     /* mean |u - u_true| over the crossings the integrator found */
+    double audit_r_err;     /* mean |r - r_true| / r_true over the crossings inside r = 50 */
+    double audit_g_err;     /* mean |g - g_true| of the network's redshift head over those crossings */
+    double audit_l1;        /* sum |I - I_true| / sum |I_true| of the Y channel */
+    double audit_flux;      /* sum I / sum I_true - 1 of the Y channel */
+} so_sur_report;
+int so_sur_render(so_surrogate* s, so_renderer* r, const so_frame* f, const so_sur_frame_opts* o, float* d_px,
+                  so_sur_report* rep);
+/* The surrogate's tensor-core GEMM on its own, for numerics checks.  A [M x K] and B [N x K] are
+ * BF16 row-major device arrays; M % 128 == 0, N <= 256 with N % 16 == 0 or N % 256 == 0,
+ * (K / splits) % 16 == 0.  layout 0: d_c[m * N + n] = (A B^T)[m, n] + bias[n] (splits must be 1,
+ * bias may be NULL); layout 1: d_c[s * M * N + m * N + n] = slice s of the reduction; layout 2:
+ * d_c[s * M * N + n * M + m] = the same, transposed.  Synchronous; status as elsewhere. */
+int so_sur_gemm(const void* d_a, const void* d_b, const float* d_bias, float* d_c, int M, int N, int K, int splits,
+                int layout);
+
 /* ---- shot / scene builders (host only) --------------------------------------------------------- */
 typedef struct so_shot so_shot;
 /* Scene information that does not go to the device (SceneInfo, scene_build.hpp:7-17). */

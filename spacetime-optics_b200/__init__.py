@@ -77,6 +77,21 @@ def lib():
         L.so_kerr_point_at.argtypes = [C.c_double, C.c_double, C.c_double, P(abi.KerrPoint)]
         L.so_kerr_point_at.restype = None
         L.so_critical_curve_point.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double), P(C.c_double)]
+        L.so_sur_default_opts.argtypes = [P(abi.SurOpts)]
+        L.so_sur_default_opts.restype = None
+        L.so_sur_create.argtypes = [C.c_int, P(abi.SurOpts), P(vp)]
+        L.so_sur_destroy.argtypes = [vp]
+        L.so_sur_destroy.restype = None
+        L.so_sur_get_params.argtypes = [vp, vp, vp]
+        L.so_sur_set_params.argtypes = [vp, vp, vp]
+        L.so_sur_train.argtypes = [vp, vp, vp, C.c_longlong, C.c_int, P(abi.SurLoss)]
+        L.so_sur_evaluate.argtypes = [vp, vp, vp, C.c_longlong, P(abi.SurLoss)]
+        L.so_sur_gradients.argtypes = [vp, vp, vp, C.c_int, vp, P(abi.SurLoss)]
+        L.so_sur_infer.argtypes = [vp, vp, C.c_longlong, vp, vp]
+        L.so_sur_dataset.argtypes = [vp, P(Frame), C.c_longlong, C.c_int, C.c_uint32, P(abi.SurRanges), vp, vp,
+                                     P(Stats)]
+        L.so_sur_render.argtypes = [vp, vp, P(Frame), P(abi.SurFrameOpts), vp, P(abi.SurReport)]
+        L.so_sur_gemm.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -319,6 +334,106 @@ def probe_sfu_peak(device=0):
     g = C.c_double()
     _check(lib().so_probe_sfu_peak(device, C.byref(g)))
     return g.value
+
+
+class Surrogate:
+    """The ray surrogate (so_sur_*): an MLP from (alpha, beta, spin, inclination) to the integrator's
+    termination class, escape direction and first three equatorial crossings, trained and run by the
+    library's tensor-core kernels.  Device arrays are torch CUDA tensors (float32): rays [n, 4],
+    targets [n, 12], outputs [n, 16]."""
+
+    def __init__(self, device=0, **opts):
+        o = abi.SurOpts()
+        lib().so_sur_default_opts(C.byref(o))
+        for k, v in opts.items():
+            setattr(o, k, v)
+        h = C.c_void_p()
+        _check(lib().so_sur_create(device, C.byref(o), C.byref(h)))
+        self.h = h
+        self.opts = o
+        self.device = device
+
+    def params(self):
+        p = np.empty(abi.SUR_NPARAMS, np.float32)
+        f = np.empty((abi.SUR_NFREQ, 4), np.float32)
+        _check(lib().so_sur_get_params(self.h, _ptr(p), _ptr(f)))
+        return p, f
+
+    def set_params(self, p=None, f=None):
+        p = None if p is None else np.ascontiguousarray(p, np.float32)
+        f = None if f is None else np.ascontiguousarray(f, np.float32)
+        _check(lib().so_sur_set_params(self.h, _ptr(p), _ptr(f)))
+
+    def dataset(self, renderer, frame, n, groups, seed=1, a=(0.0, 0.99), incl=(5.0, 175.0), xy_max=12.0):
+        """(rays, targets, stats): n rays from the FP64 integrator of `renderer` (camera at frame.r)."""
+        import torch
+        rays = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{self.device}")
+        tgt = torch.empty((n, 12), dtype=torch.float32, device=f"cuda:{self.device}")
+        rg = abi.SurRanges(a[0], a[1], incl[0], incl[1], xy_max)
+        st = Stats()
+        _check(lib().so_sur_dataset(renderer.h, C.byref(frame), n, groups, seed, C.byref(rg), rays.data_ptr(),
+                                    tgt.data_ptr(), C.byref(st)), renderer.h)
+        return rays, tgt, st
+
+    def train(self, rays, tgt, steps):
+        loss = abi.SurLoss()
+        _check(lib().so_sur_train(self.h, rays.data_ptr(), tgt.data_ptr(), rays.shape[0], steps, C.byref(loss)))
+        return loss
+
+    def evaluate(self, rays, tgt):
+        loss = abi.SurLoss()
+        _check(lib().so_sur_evaluate(self.h, rays.data_ptr(), tgt.data_ptr(), rays.shape[0], C.byref(loss)))
+        return loss
+
+    def gradients(self, rays, tgt):
+        g = np.empty(abi.SUR_NPARAMS, np.float32)
+        loss = abi.SurLoss()
+        _check(lib().so_sur_gradients(self.h, rays.data_ptr(), tgt.data_ptr(), rays.shape[0], _ptr(g),
+                                      C.byref(loss)))
+        return g, loss
+
+    def infer(self, rays):
+        """Outputs [n, 16], queued on torch's current stream."""
+        import torch
+        out = torch.empty((rays.shape[0], abi.SUR_LDOUT), dtype=torch.float32, device=rays.device)
+        st = torch.cuda.current_stream(rays.device).cuda_stream
+        _check(lib().so_sur_infer(self.h, rays.data_ptr(), rays.shape[0], out.data_ptr(), C.c_void_p(st)))
+        return out
+
+    def render(self, renderer, frame, band_m=0.5, audit_frac=0.01, audit_seed=2, out=None):
+        """Surrogate thin-disk frame into out (torch [H, W, 4] float32 on the device) and its report."""
+        import torch
+        W, H = renderer.settings.W, renderer.settings.H
+        if out is None:
+            out = torch.zeros((H, W, 4), dtype=torch.float32, device=f"cuda:{self.device}")
+        o = abi.SurFrameOpts(band_m, audit_frac, audit_seed)
+        rep = abi.SurReport()
+        _check(lib().so_sur_render(self.h, renderer.h, C.byref(frame), C.byref(o), out.data_ptr(), C.byref(rep)))
+        return out, rep
+
+    def close(self):
+        if self.h:
+            lib().so_sur_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sur_gemm(a, b, bias=None, splits=1, layout=0):
+    """so_sur_gemm on torch bf16 CUDA tensors a [M, K], b [N, K]: the float32 product [M, N]
+    (layout 0), or its per-slice planes [splits, M, N] (layout 1) or transposed [splits, N, M] (2)."""
+    import torch
+    M, K = a.shape
+    N = b.shape[0]
+    shape = {0: (M, N), 1: (splits, M, N), 2: (splits, N, M)}[layout]
+    c = torch.zeros(shape, dtype=torch.float32, device=a.device)
+    _check(lib().so_sur_gemm(a.data_ptr(), b.data_ptr(), None if bias is None else bias.data_ptr(), c.data_ptr(),
+                             M, N, K, splits, layout))
+    return c
 
 
 def pixel_centres(frame, W, H):

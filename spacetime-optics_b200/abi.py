@@ -113,6 +113,51 @@ class Tune(C.Structure):
     _fields_ = [("ctas_per_sm", C.c_int), ("interleave", C.c_int), ("ms", C.c_double)]
 
 
+class SurRay(C.Structure):
+    _fields_ = [("alpha", C.c_float), ("beta", C.c_float), ("spin", C.c_float), ("incl_deg", C.c_float)]
+
+
+class SurTarget(C.Structure):
+    _fields_ = [("cls", C.c_float), ("dir", C.c_float * 3), ("u", C.c_float * 3), ("g", C.c_float * 3),
+                ("pad", C.c_float * 2)]
+
+
+class SurOpts(C.Structure):
+    _fields_ = [("fourier_sigma", C.c_float), ("seed", C.c_uint32), ("batch", C.c_int), ("lr", C.c_float),
+                ("lr_final", C.c_float), ("warmup", C.c_int), ("beta1", C.c_float), ("beta2", C.c_float),
+                ("eps", C.c_float), ("weight_decay", C.c_float), ("w_dir", C.c_float), ("w_u", C.c_float),
+                ("w_g", C.c_float)]
+
+
+class SurLoss(C.Structure):
+    _fields_ = [("total", C.c_double), ("ce", C.c_double), ("dir", C.c_double), ("u", C.c_double),
+                ("g", C.c_double), ("accuracy", C.c_double), ("rays", C.c_longlong)]
+
+
+class SurRanges(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("a_min", "a_max", "incl_min", "incl_max", "xy_max")]
+
+
+class SurFrameOpts(C.Structure):
+    _fields_ = [("band_m", C.c_double), ("audit_frac", C.c_double), ("audit_seed", C.c_uint32)]
+
+
+class SurReport(C.Structure):
+    _fields_ = ([(n, C.c_longlong) for n in ("rays", "surrogate_rays", "band_rays", "audit_rays")] +
+                [(n, C.c_double) for n in ("ms_total", "ms_route", "ms_mlp", "ms_shade", "ms_integrator")] +
+                [("audit_class_mismatch", C.c_longlong)] +
+                [(n, C.c_double) for n in ("audit_dir_err", "audit_u_err", "audit_r_err", "audit_g_err",
+                                           "audit_l1", "audit_flux")])
+
+
+SUR_NFREQ = 64
+SUR_HIDDEN = 256
+SUR_LAYERS = 4
+SUR_NOUT = 12
+SUR_LDOUT = 16
+SUR_NPARAMS = 234512
+
+
 class SceneInfo(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("mass_msun", "distance_cm", "rg_cm", "tg_s", "uas_per_m", "disk_tmax",
                                           "disk_mdot_edd", "radio_flux_target_jy")]
@@ -138,4 +183,7 @@ EXPORTS = [
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
     "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",
     "so_kerr_point_at", "so_critical_curve_point",
+    "so_sur_default_opts", "so_sur_create", "so_sur_destroy", "so_sur_get_params", "so_sur_set_params",
+    "so_sur_train", "so_sur_evaluate", "so_sur_gradients", "so_sur_infer", "so_sur_dataset", "so_sur_render",
+    "so_sur_gemm",
 ]

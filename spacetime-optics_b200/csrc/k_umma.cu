@@ -1,0 +1,313 @@
+// BF16 GEMM tile on the fifth-generation tensor cores: tcgen05.mma with both operands in shared
+// memory and the FP32 accumulator in tensor memory (TMEM), read back with tcgen05.ld for the
+// epilogue.  One CTA of 128 threads owns a 128 x BN output tile (BN <= 256 TMEM columns):
+//   * all threads stage A and B K-slices into shared memory (two buffers), in the K-major
+//     no-swizzle canonical layout: an 8-row x 16-byte "core matrix" is 128 contiguous bytes, the
+//     K-neighbouring core matrices of one 8-row group sit 128 B apart (leading byte offset) and the
+//     8-row groups BK*16 B apart (stride byte offset);
+//   * thread 0 issues BK/16 tcgen05.mma (M=128, N=BN, K=16) per slice and commits them to the
+//     slice's mbarrier, so the next slice loads while the tensor core works;
+//   * after the last commit every warp reads its 32 TMEM lanes (= 32 output rows) with tcgen05.ld
+//     and applies the epilogue.
+// Every mbarrier wait is bounded (about one second of %globaltimer); a wait that gives up writes
+// SO_ERR_WATCHDOG into *err, skips the epilogue and still frees the TMEM columns.
+#include "so_mlp.h"
+
+namespace so {
+namespace mlp {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int NT = 128;  // threads per CTA
+constexpr unsigned long long WAIT_NS = 1000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Shared-memory matrix descriptor (sm_100 format: version 1, no swizzle, base offset 0).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: D = F32 (bits 4-5 = 1), A = B = BF16 (bits 7-9, 10-12 = 1),
+// both K-major (bits 15, 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void bar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool bar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the completion of phase `parity`; false after about a second.
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
+    if (bar_try(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+        if (bar_try(bar, parity)) return true;
+        if (now_ns() - t0 > WAIT_NS) return false;
+    }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float* f) {
+    uint32_t v[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(v[i]);
+}
+
+// Stage rows [0, rows) x K-slice [k0, k0 + BK) of a K-major global matrix into the canonical
+// layout.  One item moves 32 bytes (two core-matrix rows along K); a warp's 32 items cover
+// 8 rows x 4 K-pairs, so each 16-byte store instruction touches every bank once per 128 bytes.
+__device__ __forceinline__ void stage(uint8_t* sm, const bf16* g, long ld, int rows, int k0, int BK, int tid) {
+    const int nkq = BK >> 4;
+    const int items = rows * nkq;
+    for (int w = tid; w < items; w += NT) {
+        const int rr = w & 7, kq = (w >> 3) % nkq, rg = (w >> 3) / nkq;
+        const uint4* src = reinterpret_cast<const uint4*>(g + (long)(rg * 8 + rr) * ld + k0 + kq * 16);
+        const uint4 v0 = __ldg(src), v1 = __ldg(src + 1);
+        uint8_t* dst = sm + rg * (BK * 16) + kq * 256 + rr * 16;
+        *reinterpret_cast<uint4*>(dst) = v0;
+        *reinterpret_cast<uint4*>(dst + 128) = v1;
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(NT) k_gemm_bf16(GemmArgs g, int BN, int BK, int tmem_cols) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    const int kps = g.K / g.splits, kbeg = blockIdx.z * kps;
+    const int nk = kps / BK;
+    const int a_bytes = BM * BK * 2, b_bytes = BN * BK * 2;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(tmem_cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        bar_init(&bars[0], 1);
+        bar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = idesc_bf16(BM, BN);
+    bool ok = true;
+
+    for (int s = 0; s < nk; ++s) {
+        const int buf = s & 1;
+        // the MMAs that read this buffer two slices ago must be done; the verdict is made
+        // block-uniform so that no thread leaves the loop alone
+        const bool freed = s < 2 || bar_wait(&bars[buf], ((s - 2) >> 1) & 1);
+        if (!__syncthreads_and(freed)) {
+            ok = false;
+            break;
+        }
+        const int k0 = kbeg + s * BK;
+        uint8_t* sa = smem + buf * (a_bytes + b_bytes);
+        uint8_t* sb = sa + a_bytes;
+        stage(sa, g.A + (long)m0 * g.lda, g.lda, BM, k0, BK, tid);
+        stage(sb, g.B + (long)n0 * g.ldb, g.ldb, BN, k0, BK, tid);
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            for (int j = 0; j < (BK >> 4); ++j) {
+                const uint64_t da = smem_desc(a0 + j * 256, 128, BK * 16);
+                const uint64_t db = smem_desc(b0 + j * 256, 128, BK * 16);
+                mma_bf16(tmem, da, db, idesc, (s > 0 || j > 0) ? 1u : 0u);
+            }
+            mma_commit(&bars[buf]);
+        }
+    }
+    // The last commit tracks every MMA issued before it.
+    if (ok && nk > 0) ok = bar_wait(&bars[(nk - 1) & 1], ((nk - 1) >> 1) & 1);
+    ok = __syncthreads_and(ok);
+    fence_after();
+
+    if (ok) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c = 0; c < BN; c += 16) {
+            float f[16];
+            tmem_ld16(lane_addr + c, f);
+            const int n = n0 + c;
+            if (EPI == EPI_F32) {
+                float* o = g.out_f + (long)row * g.ldf + n;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) o[i] = f[i] + (g.bias ? g.bias[n + i] : 0.f);
+            } else if (EPI == EPI_GELU) {
+                __align__(16) bf16 h[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float z = f[i] + (g.bias ? g.bias[n + i] : 0.f);
+                    if (g.z_out) g.z_out[(long)row * g.ldz + n + i] = z;
+                    h[i] = __float2bfloat16_rn(gelu_f(z));
+                }
+                if (g.out_b) {
+                    uint4* o = reinterpret_cast<uint4*>(g.out_b + (long)row * g.ldob + n);
+                    o[0] = reinterpret_cast<const uint4*>(h)[0];
+                    o[1] = reinterpret_cast<const uint4*>(h)[1];
+                }
+                if (g.out_t) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) g.out_t[(long)(n + i) * g.ldot + row] = h[i];
+                }
+            } else if (EPI == EPI_GELU_BWD) {
+                __align__(16) bf16 h[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    h[i] = __float2bfloat16_rn(f[i] * gelu_grad_f(g.z_in[(long)row * g.ldz + n + i]));
+                if (g.out_b) {
+                    uint4* o = reinterpret_cast<uint4*>(g.out_b + (long)row * g.ldob + n);
+                    o[0] = reinterpret_cast<const uint4*>(h)[0];
+                    o[1] = reinterpret_cast<const uint4*>(h)[1];
+                }
+                if (g.out_t) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) g.out_t[(long)(n + i) * g.ldot + row] = h[i];
+                }
+            } else if (EPI == EPI_SPLIT) {
+                float4* o = reinterpret_cast<float4*>(g.out_f + blockIdx.z * g.split_stride + (long)row * g.ldf + n);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) o[i] = make_float4(f[4 * i], f[4 * i + 1], f[4 * i + 2], f[4 * i + 3]);
+            } else {  // EPI_SPLIT_T
+                float* o = g.out_f + blockIdx.z * g.split_stride;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) o[(long)(n + i) * g.ldf + row] = f[i];
+            }
+        }
+    } else if (tid == 0 && g.err) {
+        atomicExch(g.err, SO_ERR_WATCHDOG);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
+    }
+}
+
+template <int EPI>
+int launch_epi(const GemmArgs& g, int BN, int BK, cudaStream_t st) {
+    const int smem = 2 * (BM + BN) * BK * 2;
+    const int cols = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    if (cudaFuncSetAttribute(k_gemm_bf16<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * (BM + 256) * 64 * 2) !=
+        cudaSuccess)
+        return SO_ERR_CUDA;
+    dim3 grid(g.M / BM, g.N / BN, g.splits);
+    k_gemm_bf16<EPI><<<grid, NT, smem, st>>>(g, BN, BK, cols);
+    return cudaGetLastError() == cudaSuccess ? SO_OK : SO_ERR_CUDA;
+}
+
+bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+
+int launch_gemm(const GemmArgs& g, cudaStream_t st, const char** why) {
+    auto bad = [&](const char* m) {
+        if (why) *why = m;
+        return SO_ERR_ARG;
+    };
+    if (!g.A || !g.B) return bad("gemm: null operand");
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0 || g.splits <= 0) return bad("gemm: empty shape");
+    if (g.M % BM) return bad("gemm: M must be a multiple of 128");
+    int BN;
+    if (g.N <= 256) {
+        if (g.N % 16) return bad("gemm: N <= 256 must be a multiple of 16");
+        BN = g.N;
+    } else {
+        if (g.N % 256) return bad("gemm: N > 256 must be a multiple of 256");
+        BN = 256;
+    }
+    if (g.K % g.splits) return bad("gemm: K must divide into the splits");
+    const int kps = g.K / g.splits;
+    if (kps % 16) return bad("gemm: K per split must be a multiple of 16");
+    const int BK = (kps % 64 == 0) ? 64 : 16;
+    if (g.lda % 8 || g.ldb % 8 || g.lda < g.K || g.ldb < g.K || !al16(g.A) || !al16(g.B))
+        return bad("gemm: operands need 16-byte aligned rows");
+    if (g.splits > 1 && g.epi != EPI_SPLIT && g.epi != EPI_SPLIT_T) return bad("gemm: split reductions need a split epilogue");
+    switch (g.epi) {
+        case EPI_F32:
+            if (!g.out_f || g.ldf < g.N) return bad("gemm: EPI_F32 needs out_f");
+            return launch_epi<EPI_F32>(g, BN, BK, st);
+        case EPI_GELU:
+            if ((!g.out_b && !g.out_t) || (g.out_b && (g.ldob % 8 || g.ldob < g.N || !al16(g.out_b))) ||
+                (g.out_t && g.ldot < g.M) || (g.z_out && g.ldz < g.N))
+                return bad("gemm: EPI_GELU outputs");
+            return launch_epi<EPI_GELU>(g, BN, BK, st);
+        case EPI_GELU_BWD:
+            if (!g.z_in || g.ldz < g.N || (!g.out_b && !g.out_t) ||
+                (g.out_b && (g.ldob % 8 || g.ldob < g.N || !al16(g.out_b))) || (g.out_t && g.ldot < g.M))
+                return bad("gemm: EPI_GELU_BWD operands");
+            return launch_epi<EPI_GELU_BWD>(g, BN, BK, st);
+        case EPI_SPLIT:
+            if (!g.out_f || g.ldf < g.N || g.ldf % 4 || !al16(g.out_f) ||
+                (g.splits > 1 && g.split_stride < (long)g.M * g.ldf) || g.split_stride % 4)
+                return bad("gemm: EPI_SPLIT needs out_f with 16-byte aligned rows and disjoint planes");
+            return launch_epi<EPI_SPLIT>(g, BN, BK, st);
+        case EPI_SPLIT_T:
+            if (!g.out_f || g.ldf < g.M || (g.splits > 1 && g.split_stride < (long)g.N * g.ldf))
+                return bad("gemm: EPI_SPLIT_T needs out_f with disjoint planes");
+            return launch_epi<EPI_SPLIT_T>(g, BN, BK, st);
+        default:
+            return bad("gemm: unknown epilogue");
+    }
+}
+
+}  // namespace mlp
+}  // namespace so

@@ -237,7 +237,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     }
     if (!r->d_nlists) {
         if (dalloc(&r->d_nlists, 4) != cudaSuccess || dalloc(&r->d_cnt3, 2) != cudaSuccess ||
-            dalloc(&r->d_band, BAND_N) != cudaSuccess)
+            (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess))
             return fail(r, SO_ERR_ALLOC, "mixed path: device allocation");
         SO_CK(r, cudaStreamCreateWithFlags(&r->st2, cudaStreamNonBlocking));
         SO_CK(r, cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming));
@@ -506,6 +506,55 @@ RayBufs carve(void* base, long long n) {
 namespace so {
 // Message returned by so_last_error(NULL), for entry points that have no renderer handle.
 void set_global_error(const std::string& msg) { g_init_error = msg; }
+
+// ---- services for the surrogate (so_surrogate.cpp) ----------------------------------------------
+int rend_device(so_renderer* r) { return r->device; }
+int rend_num_sms(so_renderer* r) { return r->num_sms; }
+cudaStream_t rend_stream(so_renderer* r) { return r->st; }
+const so_scene& rend_scene(so_renderer* r) { return r->S; }
+const so_settings& rend_settings(so_renderer* r) { return r->rs; }
+const so_scene* rend_scene_dev(so_renderer* r) { return r->d_scene; }
+int rend_fail(so_renderer* r, int code, const char* msg) { return fail(r, code, msg); }
+
+int rend_band_table(so_renderer* r, double th, const float** d_band, int* n) {
+    if (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "band table allocation");
+    if (r->band_a != r->S.a || r->band_th != th) {
+        std::vector<float> tab = band_table(r->S.a, th);
+        SO_CK(r, cudaMemcpyAsync(r->d_band, tab.data(), BAND_N * sizeof(float), cudaMemcpyHostToDevice, r->st));
+        SO_CK(r, cudaStreamSynchronize(r->st));
+        r->band_a = r->S.a;
+        r->band_th = th;
+    }
+    *d_band = r->d_band;
+    *n = BAND_N;
+    return SO_OK;
+}
+
+int rend_upload_frame(so_renderer* r, const so_frame& f, const so_frame** d_frame) {
+    SO_CK(r, cudaMemcpyAsync(r->d_frame, &f, sizeof(so_frame), cudaMemcpyHostToDevice, r->st));
+    *d_frame = r->d_frame;
+    return SO_OK;
+}
+
+int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum) {
+    if (n <= 0) return SO_OK;
+    SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    TraceLaunch L;
+    launch_common(r, L);
+    L.kind = RAYS_LIST;
+    L.nrays = n;
+    L.x = d_x;
+    L.y = d_y;
+    L.out = d_out;
+    L.record_cross = d_out.cross_r != nullptr && d_out.cross_g != nullptr;
+    if (!L.record_cross) {
+        L.out.cross_r = nullptr;
+        L.out.cross_g = nullptr;
+    }
+    cudaError_t e = launch_trace64(L, vacuum ? VAR_VACUUM : variant_of(r->S), r->num_sms, r->st);
+    if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
 }  // namespace so
 
 extern "C" {

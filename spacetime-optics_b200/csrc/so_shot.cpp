@@ -287,6 +287,18 @@ struct ShotFrame {
 };
 
 }  // namespace
+
+// Scene scalars of the vacuum geodesics for spin a (the scene builder's clamp, horizon, ISCO and
+// stopping radius with the same horizon margin); the tables and the emitters' parameters stay.
+void scene_set_spin(so_scene* S, double a) {
+    const double margin = S->r_stop - S->rh;
+    if (a <= 0.0) a = 1e-6;
+    if (a > 0.9999) a = 0.9999;
+    S->a = a;
+    S->rh = horizon_radius(a);
+    S->r_isco = isco_radius(a);
+    S->r_stop = S->rh + margin;
+}
 }  // namespace so
 
 using namespace so;

@@ -180,3 +180,15 @@ def ref_pass1(scene, frame, threads=8):
     lim = C.c_longlong()
     ref().ref_render_pass1(C.byref(scene), C.byref(frame), _p(acc), C.byref(lim), threads)
     return acc, lim.value
+
+
+def mlp():
+    """oracle/so_mlp.py: the float64 restatement of the ray surrogate network."""
+    import importlib.util
+    name = "so_mlp_oracle"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "oracle", "so_mlp.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
