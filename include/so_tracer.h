@@ -319,8 +319,10 @@ typedef struct so_sur_ray { float alpha, beta, spin, incl_deg; } so_sur_ray;
 typedef struct so_sur_target {
     float cls;    /* 0 escaped, 1 captured, 2 step limit */
     float dir[3]; /* escape direction (sin th cos ph, sin th sin ph, cos th); 0 unless escaped */
-    float u[3];   /* 1/r of the first three equatorial crossings; 0 where there is none */
-    float g[3];   /* redshift of a circular prograde emitter at those radii; 0 inside the ISCO / none */
+    float u[3];   /* 1/r of the first three equatorial crossings; where there is none: 0 for a ray
+                   * that escapes, 1/r_stop (where the integrator stopped) for one that is captured */
+    float g[3];   /* redshift of a circular prograde emitter at those radii (0 inside the ISCO);
+                   * -1 where there is no crossing (not trained on) */
     float pad[2];
 } so_sur_target;
 typedef struct so_sur_opts {

@@ -6,7 +6,7 @@ the surrogate network that the library trains and runs on the tensor cores (incl
 loss (class cross-entropy plus weighted squared errors of direction, 1/r and redshift) and its
 gradient in the library's flat parameter layout.  The surrogate has no reference counterpart (the
 reference renders with the integrator only), so its parity is pinned two ways: the analytic gradient
-here is checked against central finite differences in float64 (tests/test_oracle_golden.py), and
+here is checked against central finite differences in float64 (tests/test_oracle_mlp.py), and
 the GPU gradient is checked against this oracle.
 
 Two arithmetic modes:
@@ -114,7 +114,7 @@ def loss_grad_outputs(O, tgt, w_dir, w_u, w_g):
     d[:, 3:6] = np.where(esc, 2.0 * w_dir * dd, 0.0)
     du = O[:, 6:9] - t[:, 4:7]
     d[:, 6:9] = 2.0 * w_u * du
-    has = t[:, 4:7] > 0.0
+    has = t[:, 7:10] >= 0.0
     dg = O[:, 9:12] - t[:, 7:10]
     d[:, 9:12] = np.where(has, 2.0 * w_g * dg, 0.0)
     ld = np.where(esc, dd * dd, 0.0).sum(axis=1)

@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(128) k_loss(const float* __restrict__ O, const
             const float du = o[6 + k] - t.u[k];
             lu += du * du;
             dl[6 + k] = 2.f * w.u * du;
-            if (t.u[k] > 0.f) {
+            if (t.g[k] >= 0.f) {
                 const float dg = o[9 + k] - t.g[k];
                 lg += dg * dg;
                 dl[9 + k] = 2.f * w.g * dg;
@@ -275,9 +275,9 @@ __global__ void k_sample(int g, int groups, int per_group, uint32_t seed, double
     rays[(long)j * groups + g] = r;
 }
 
-__global__ void k_targets(int g, int groups, int per_group, const int8_t* __restrict__ fate, const double* __restrict__ th,
-                          const double* __restrict__ ph, const double* __restrict__ cr, const double* __restrict__ cg,
-                          so_sur_target* __restrict__ tgt) {
+__global__ void k_targets(int g, int groups, int per_group, double r_stop, const int8_t* __restrict__ fate,
+                          const double* __restrict__ th, const double* __restrict__ ph, const double* __restrict__ cr,
+                          const double* __restrict__ cg, so_sur_target* __restrict__ tgt) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= per_group) return;
     so_sur_target t;
@@ -293,10 +293,13 @@ __global__ void k_targets(int g, int groups, int per_group, const int8_t* __rest
     } else {
         t.dir[0] = t.dir[1] = t.dir[2] = 0.f;
     }
+    // A crossing that does not happen lies at infinity for a ray that escapes and at the stopping
+    // radius for one that is captured: the target then moves continuously as a crossing appears.
+    const float u_none = f == SO_FATE_CAPTURED ? (float)(1.0 / r_stop) : 0.f;
     for (int k = 0; k < 3; ++k) {
         const double r = cr[3 * (long)j + k];
-        t.u[k] = r > 0.0 ? (float)(1.0 / r) : 0.f;
-        t.g[k] = r > 0.0 ? (float)cg[3 * (long)j + k] : 0.f;
+        t.u[k] = r > 0.0 ? (float)(1.0 / r) : u_none;
+        t.g[k] = r > 0.0 ? (float)cg[3 * (long)j + k] : -1.f;
     }
     t.pad[0] = t.pad[1] = 0.f;
     tgt[(long)j * groups + g] = t;
@@ -477,9 +480,9 @@ void launch_sample(int g, int groups, int per_group, uint32_t seed, double xy_ma
     k_sample<<<(per_group + 255) / 256, 256, 0, st>>>(g, groups, per_group, seed, xy_max, a, incl, r_cam, x, y, rays);
 }
 
-void launch_targets(int g, int groups, int per_group, const int8_t* fate, const double* th, const double* ph,
-                    const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st) {
-    k_targets<<<(per_group + 255) / 256, 256, 0, st>>>(g, groups, per_group, fate, th, ph, cr, cg, tgt);
+void launch_targets(int g, int groups, int per_group, double r_stop, const int8_t* fate, const double* th,
+                    const double* ph, const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st) {
+    k_targets<<<(per_group + 255) / 256, 256, 0, st>>>(g, groups, per_group, r_stop, fate, th, ph, cr, cg, tgt);
 }
 
 void launch_route(const Route& R, int num_sms, cudaStream_t st) { k_route<<<num_sms * 8, 256, 0, st>>>(R); }

@@ -130,5 +130,34 @@ void launch_adam(float* p, const float* g, float* m, float* v, long n, float lr,
 // BF16 weights and transposes from the master parameters (no update).
 void launch_pack(const float* p, long n, bf16* W, bf16* WT, cudaStream_t st);
 
+// ---- fused inference (k_mlp_fused.cu) --------------------------------------------------------
+// The weights of every layer cut into 64-wide K chunks, each stored as one contiguous tile in the
+// tensor cores' shared-memory layout, so that one bulk copy brings a chunk in.
+struct FusedChunk {
+    long offset;  // bytes from the start of the packed weights
+    int bytes;
+    int layer, row0, rows, k0;  // the weight rows [row0, row0 + rows) x columns [k0, k0 + 64) of layer
+};
+constexpr int FUSED_MAX_CHUNKS = 64;
+struct FusedArgs {
+    const so_sur_ray* rays;
+    long long n;
+    float* out;            // n x LDO floats
+    const float* params;   // FP32 master parameters (biases)
+    long bias_off[NLAYER];
+    const float* freq;     // NFREQ x 4
+    const uint8_t* wpack;  // packed BF16 weights
+    FusedChunk chunks[FUSED_MAX_CHUNKS];
+    int nchunks;
+    int* err;
+};
+// Fills the chunk table (in the order the kernel consumes it, at most FUSED_MAX_CHUNKS entries)
+// and the packed size in elements; returns the number of chunks, or -1 if the table is too small.
+int fused_chunks(FusedChunk* chunks, long* pack_elems);
+// Packs the BF16 weights into the chunks of a.chunks.
+void launch_pack_chunks(const bf16* W, const FusedArgs& a, bf16* wpack, cudaStream_t st);
+// Persistent launch, one CTA per SM (at most one per 256-ray tile).
+int launch_mlp_fused(const FusedArgs& a, int num_sms, cudaStream_t st);
+
 }  // namespace mlp
 }  // namespace so

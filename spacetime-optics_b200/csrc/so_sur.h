@@ -46,8 +46,8 @@ struct Audit {
 
 void launch_sample(int g, int groups, int per_group, uint32_t seed, double xy_max, float a, float incl, double r_cam,
                    double* x, double* y, so_sur_ray* rays, cudaStream_t st);
-void launch_targets(int g, int groups, int per_group, const int8_t* fate, const double* th, const double* ph,
-                    const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st);
+void launch_targets(int g, int groups, int per_group, double r_stop, const int8_t* fate, const double* th,
+                    const double* ph, const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st);
 void launch_route(const Route& R, int num_sms, cudaStream_t st);
 void launch_xy(const so_frame* F, int W, int H, const uint32_t* list_b, int nb, const uint32_t* list_a, int na, double* x,
                double* y, cudaStream_t st);

@@ -73,10 +73,12 @@ struct so_surrogate {
     bf16 *A[mlp::NHID] = {}, *AT[mlp::NHID] = {}, *dZ[2] = {}, *dZT[2] = {};
     float *Z[mlp::NHID] = {}, *O = nullptr, *part = nullptr, *part_gb = nullptr;
     double* part_acc = nullptr;
-    // inference buffers for ib rows
-    int ib = 0;
-    bf16 *iX = nullptr, *iA[2] = {};
-    float* iO = nullptr;
+    // fused inference: packed weight chunks, rebuilt when the parameters change
+    bf16* d_wpack = nullptr;
+    long pack_elems = 0;
+    mlp::FusedChunk chunks[mlp::FUSED_MAX_CHUNKS];
+    int nchunks = 0, num_sms = 148;
+    long long version = 1, packed_version = 0;
     // frame buffers for fcap pixels
     long long fcap = 0;
     uint32_t *list_s = nullptr, *list_b = nullptr, *list_a = nullptr, *audit_j = nullptr;
@@ -127,16 +129,6 @@ void free_train(so_surrogate* s) {
     s->tb = 0;
 }
 
-void free_infer(so_surrogate* s) {
-    if (s->iX) cudaFree(s->iX);
-    if (s->iA[0]) cudaFree(s->iA[0]);
-    if (s->iA[1]) cudaFree(s->iA[1]);
-    if (s->iO) cudaFree(s->iO);
-    s->iX = s->iA[0] = s->iA[1] = nullptr;
-    s->iO = nullptr;
-    s->ib = 0;
-}
-
 void free_frame(so_surrogate* s) {
     void* ps[] = {s->list_s, s->list_b, s->list_a, s->audit_j, s->rays_s, s->counts, s->out, s->fx, s->fy,
                   s->fth, s->fph, s->fcr, s->fcg, s->fI, s->ffate, s->facc};
@@ -183,19 +175,6 @@ int ensure_train(so_surrogate* s, int rows) {
     return SO_OK;
 }
 
-int ensure_infer(so_surrogate* s) {
-    if (s->ib) return SO_OK;
-    const size_t R = 1u << 17;
-    bool ok = dalloc(&s->iX, R * mlp::NFEAT) == cudaSuccess && dalloc(&s->iA[0], R * mlp::HID) == cudaSuccess &&
-              dalloc(&s->iA[1], R * mlp::HID) == cudaSuccess && dalloc(&s->iO, R * mlp::LDO) == cudaSuccess;
-    if (!ok) {
-        free_infer(s);
-        return fail(s, SO_ERR_ALLOC, "surrogate: inference buffers");
-    }
-    s->ib = (int)R;
-    return SO_OK;
-}
-
 int gemm(so_surrogate* s, const mlp::GemmArgs& g0, cudaStream_t st) {
     mlp::GemmArgs g = g0;
     g.err = s->d_err;
@@ -220,30 +199,26 @@ mlp::GemmArgs args(const bf16* A, long lda, const bf16* B, long ldb, int M, int 
     return g;
 }
 
-// Forward pass of `rows` rays starting at `off`.  Training keeps the pre-activations Z, the
-// activations and their transposes; inference ping-pongs two activation buffers.  The head's FP32
-// outputs go to O (ldo floats per row).
-int forward(so_surrogate* s, const so_sur_ray* rays, long long n, long long off, int rows, int wrap, bool train,
-            float* O, cudaStream_t st) {
+// Training forward pass of `rows` rays starting at `off` (layer by layer, keeping the
+// pre-activations Z, the activations and their transposes for the backward pass).  The head's FP32
+// outputs go to O (16 floats per row).
+int forward(so_surrogate* s, const so_sur_ray* rays, long long n, long long off, int rows, int wrap, float* O,
+            cudaStream_t st) {
     const mlp::Layout& L = s->L;
-    bf16* X = train ? s->X : s->iX;
-    mlp::launch_features(rays, off, n, rows, wrap, s->d_freq, X, train ? s->XT : nullptr, rows, st);
-    const bf16* in = X;
+    mlp::launch_features(rays, off, n, rows, wrap, s->d_freq, s->X, s->XT, rows, st);
+    const bf16* in = s->X;
     for (int l = 0; l < mlp::NHID; ++l) {
         mlp::GemmArgs g = args(in, L.k[l], s->d_W + L.w[l], L.k[l], rows, L.n[l], L.k[l], mlp::EPI_GELU);
         g.bias = s->d_p + L.b[l];
-        bf16* outb = train ? s->A[l] : s->iA[l & 1];
-        g.out_b = outb;
+        g.out_b = s->A[l];
         g.ldob = mlp::HID;
-        if (train) {
-            g.out_t = s->AT[l];
-            g.ldot = rows;
-            g.z_out = s->Z[l];
-            g.ldz = mlp::HID;
-        }
+        g.out_t = s->AT[l];
+        g.ldot = rows;
+        g.z_out = s->Z[l];
+        g.ldz = mlp::HID;
         int rc = gemm(s, g, st);
         if (rc) return rc;
-        in = outb;
+        in = s->A[l];
     }
     mlp::GemmArgs g = args(in, mlp::HID, s->d_W + L.w[mlp::NHID], mlp::HID, rows, mlp::LDO, mlp::HID, mlp::EPI_F32);
     g.bias = s->d_p + L.b[mlp::NHID];
@@ -395,6 +370,11 @@ int so_sur_create(int device, const so_sur_opts* opts, so_surrogate** out) {
         return bad(SO_ERR_ALLOC, "so_sur_create: device allocation");
     for (auto& e : s->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bad(SO_ERR_CUDA, "so_sur_create: events");
+    s->nchunks = mlp::fused_chunks(s->chunks, &s->pack_elems);
+    if (s->nchunks <= 0) return bad(SO_ERR_ARG, "so_sur_create: weight chunk table overflow");
+    if (dalloc(&s->d_wpack, (size_t)s->pack_elems)) return bad(SO_ERR_ALLOC, "so_sur_create: device allocation");
+    if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return bad(SO_ERR_CUDA, "so_sur_create: device attributes");
     // initial parameters: U(-1/sqrt(K), 1/sqrt(K)) for weights and biases; head rows 12-15 zero
     std::vector<float> p(P, 0.f), f((size_t)mlp::NFREQ * 4);
     Rng rng(((uint64_t)o.seed << 1) | 1u);
@@ -421,9 +401,8 @@ void so_sur_destroy(so_surrogate* s) {
     cudaSetDevice(s->device);
     if (s->st) cudaStreamSynchronize(s->st);
     free_train(s);
-    free_infer(s);
     free_frame(s);
-    void* ps[] = {s->d_p, s->d_g, s->d_m, s->d_v, s->d_freq, s->d_W, s->d_WT, s->d_err, s->d_acc};
+    void* ps[] = {s->d_p, s->d_g, s->d_m, s->d_v, s->d_freq, s->d_W, s->d_WT, s->d_err, s->d_acc, s->d_wpack};
     for (void* p : ps)
         if (p) cudaFree(p);
     for (auto e : s->ev)
@@ -453,6 +432,7 @@ int so_sur_set_params(so_surrogate* s, const float* params, const float* freqs) 
         mlp::launch_pack(s->d_p, SO_SUR_NPARAMS, s->d_W, s->d_WT, s->st);
         SUR_CK(s, cudaGetLastError());
         s->t = 0;
+        ++s->version;
     }
     if (freqs) SUR_CK(s, cudaMemcpy(s->d_freq, freqs, mlp::NFREQ * 4 * sizeof(float), cudaMemcpyHostToDevice));
     SUR_CK(s, cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st));
@@ -469,13 +449,14 @@ int so_sur_train(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_target*
     for (int k = 0; k < steps; ++k) {
         const long long off = s->cursor % n;
         SUR_CK(s, cudaMemsetAsync(s->d_acc, 0, 8 * sizeof(double), s->st));
-        int rc = forward(s, d_rays, n, off, B, 1, true, s->O, s->st);
+        int rc = forward(s, d_rays, n, off, B, 1, s->O, s->st);
         if (!rc) rc = backward(s, d_tgt, n, off, B, s->st);
         if (rc) return rc;
         ++s->t;
         mlp::launch_adam(s->d_p, s->d_g, s->d_m, s->d_v, SO_SUR_NPARAMS, schedule(s->o, k, steps), s->o.beta1,
                          s->o.beta2, s->o.eps, s->o.weight_decay, s->t, s->d_W, s->d_WT, s->st);
         SUR_CK(s, cudaGetLastError());
+        ++s->version;
         s->cursor = (off + B) % n;
     }
     return read_loss(s, steps > 0 ? B : 0, last);
@@ -491,7 +472,7 @@ int so_sur_evaluate(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_targ
     SUR_CK(s, cudaMemsetAsync(s->d_acc, 0, 8 * sizeof(double), s->st));
     for (long long off = 0; off < m; off += B) {
         const int rows = (int)std::min<long long>(B, m - off);
-        int rc = forward(s, d_rays, n, off, rows, 0, true, s->O, s->st);
+        int rc = forward(s, d_rays, n, off, rows, 0, s->O, s->st);
         if (rc) return rc;
         mlp::LossWeights w{s->o.w_dir, s->o.w_u, s->o.w_g};
         // the loss kernel scales gradients by 1/rows; the loss sums themselves are unscaled
@@ -507,7 +488,7 @@ int so_sur_gradients(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_tar
     if (int rc = set_device(s)) return rc;
     if (int rc = ensure_train(s, n)) return rc;
     SUR_CK(s, cudaMemsetAsync(s->d_acc, 0, 8 * sizeof(double), s->st));
-    int rc = forward(s, d_rays, n, 0, n, 0, true, s->O, s->st);
+    int rc = forward(s, d_rays, n, 0, n, 0, s->O, s->st);
     if (!rc) rc = backward(s, d_tgt, n, 0, n, s->st);
     if (rc) return rc;
     rc = read_loss(s, n, loss);
@@ -519,19 +500,27 @@ int so_sur_gradients(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_tar
 int so_sur_infer(so_surrogate* s, const so_sur_ray* d_rays, long long n, float* d_out, void* stream) {
     if (!s || n < 0 || (n > 0 && (!d_rays || !d_out))) return fail(s, SO_ERR_ARG, "so_sur_infer: bad arguments");
     if (n == 0) return SO_OK;
+    if (((uintptr_t)d_out & 15u) != 0) return fail(s, SO_ERR_ARG, "so_sur_infer: d_out must be 16-byte aligned");
     if (int rc = set_device(s)) return rc;
-    if (int rc = ensure_infer(s)) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->st;
-    for (long long off = 0; off < n; off += s->ib) {
-        const long long valid = std::min<long long>(s->ib, n - off);
-        const int rows = (int)((valid + 127) / 128 * 128);
-        float* O = rows == valid ? d_out + off * mlp::LDO : s->iO;
-        int rc = forward(s, d_rays, n, off, rows, 0, false, O, st);
-        if (rc) return rc;
-        if (O == s->iO)
-            SUR_CK(s, cudaMemcpyAsync(d_out + off * mlp::LDO, s->iO, (size_t)valid * mlp::LDO * sizeof(float),
-                                      cudaMemcpyDeviceToDevice, st));
+    mlp::FusedArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.rays = d_rays;
+    a.n = n;
+    a.out = d_out;
+    a.params = s->d_p;
+    for (int l = 0; l < mlp::NLAYER; ++l) a.bias_off[l] = s->L.b[l];
+    a.freq = s->d_freq;
+    a.wpack = reinterpret_cast<const uint8_t*>(s->d_wpack);
+    for (int q = 0; q < s->nchunks; ++q) a.chunks[q] = s->chunks[q];
+    a.nchunks = s->nchunks;
+    a.err = s->d_err;
+    if (s->packed_version != s->version) {
+        mlp::launch_pack_chunks(s->d_W, a, s->d_wpack, st);
+        SUR_CK(s, cudaGetLastError());
+        s->packed_version = s->version;
     }
+    if (mlp::launch_mlp_fused(a, s->num_sms, st)) return fail(s, SO_ERR_CUDA, "so_sur_infer: launch");
     return SO_OK;
 }
 
@@ -595,7 +584,7 @@ int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, u
         sur::launch_sample(g, groups, (int)per, seed, rg->xy_max, (float)S.a, (float)incl, F.r, x, y, d_rays, st);
         rc = rend_trace_list(r, (int)per, x, y, o, 1);
         if (rc) break;
-        sur::launch_targets(g, groups, (int)per, fate, th, ph, cr, cg, d_tgt, st);
+        sur::launch_targets(g, groups, (int)per, S.r_stop, fate, th, ph, cr, cg, d_tgt, st);
         if (cudaGetLastError() != cudaSuccess) rc = rend_fail(r, SO_ERR_CUDA, "so_sur_dataset: kernel launch");
     }
     cudaEventRecord(e1, st);

@@ -120,9 +120,17 @@ def test_dataset_matches_integrator(so):
         # both fates agree and the records are far from a crossing-count change
         agree = cls == T[sel, 0]
         assert agree.mean() > 0.99
-        u = np.where(o["cross_r"] > 0, 1.0 / np.where(o["cross_r"] > 0, o["cross_r"], 1.0), 0.0)
+        has = o["cross_r"] > 0
+        u = np.where(has, 1.0 / np.where(has, o["cross_r"], 1.0), 0.0)
         close = np.abs(u - T[sel, 4:7]) < 1e-4
-        assert close.mean() > 0.98
+        assert close[has].mean() > 0.98
+        # no crossing: 0 for escaped rays, 1/r_stop for captured ones; redshift target -1
+        none = ~has & agree[:, None]
+        cap = (T[sel, 0] == 1)[:, None]
+        r_stop = sh2.scene.r_stop
+        want = np.where(cap, 1.0 / r_stop, 0.0) * np.ones_like(u)
+        assert np.allclose(T[sel, 4:7][none], want[none], rtol=1e-6, atol=0)
+        assert np.all(T[sel, 7:10][none] == -1.0)
         r2.close()
     sur.close()
     r.close()

@@ -24,7 +24,7 @@ def _random_case(m, n=96, seed=3):
     tgt[:, 1:4] = d / np.linalg.norm(d, axis=1, keepdims=True) * (tgt[:, :1] == 0)
     u = rng.uniform(0, 0.5, (n, 3)) * (rng.uniform(size=(n, 3)) < 0.7)
     tgt[:, 4:7] = u
-    tgt[:, 7:10] = np.where(u > 0, rng.uniform(0.3, 1.4, (n, 3)), 0.0)
+    tgt[:, 7:10] = np.where(u > 0, rng.uniform(0.3, 1.4, (n, 3)), -1.0)
     return p, freq, rays, tgt
 
 
