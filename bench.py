@@ -260,6 +260,214 @@ def run_ours(args, so, world, rank, local):
     return line
 
 
+# surrogate network: forward FLOPs per ray (FMA = 2; the head is 16 wide on the tensor cores)
+SUR_FLOPS_RAY = 2 * (128 * 256 + 3 * 256 * 256 + 256 * 16)
+SUR_SIGMA = 0.35           # std of the random Fourier frequencies per unit of the scaled inputs
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return d, "MEASURED_PEAKS.json (measured on this pool's B200s)"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback figures"
+
+
+def run_surrogate(args, so, world, rank, local):
+    """Thin-disk frame through the ray surrogate: network trained on the GPU on rays of the FP64
+    integrator, fused tensor-core inference, FP64 integrator in the critical band and on a 1% audit
+    sample.  Compared with the same frame traced by the FP64 integrator for every pixel."""
+    import torch
+    torch.cuda.set_device(local)
+    W = args.size or 4096
+    sh = so.Shot("thin_disk_4096.ini", [f"camera.width={W}", f"camera.height={W}"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    sur = so.Surrogate(local, batch=65536, lr=2e-3, lr_final=5e-5, warmup=100, seed=1 + rank,
+                       fourier_sigma=SUR_SIGMA)
+    t0 = time.perf_counter()
+    rays, tgt, st = sur.dataset(r, f, args.train_rays, 4096, seed=1 + rank)
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    last = sur.train(rays, tgt, args.train_steps)
+    t_train = time.perf_counter() - t0
+    del rays, tgt
+    hr, ht, _ = sur.dataset(r, f, 1 << 18, 256, seed=1000 + rank)
+    held = sur.evaluate(hr, ht)
+    del hr, ht
+    stream = torch.cuda.ExternalStream(r.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(band_m, audit, n):
+        out = torch.zeros((W, W, 4), dtype=torch.float32, device="cuda")
+        ms, rep = [], None
+        for i in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            out, rep = sur.render(r, f, band_m=band_m, audit_frac=audit, audit_seed=2, out=out)
+            with torch.cuda.stream(stream):
+                b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return out, rep, ms
+
+    # the FP64 integrator on every pixel (same tracer, routing and scatter kernels)
+    img64, rep64, ms64 = timed(1e9, 0.0, 2)
+    ref = img64.cpu().numpy().astype(np.float64)
+    for _ in range(args.warmup):
+        timed(args.band, 0.01, 1)
+    barrier(world)
+    with ClockSampler(local) as clk:
+        img, rep, ms = timed(args.band, 0.01, args.steps)
+    ms_step = allreduce_max(float(np.mean(ms)), world)
+    npix = W * W
+    value = world * npix / (ms_step * 1e-3) / 1e6
+    fp64_ms = float(np.mean(ms64))
+    a = img.cpu().numpy().astype(np.float64)
+    l1 = float(np.abs(a[..., 1] - ref[..., 1]).sum() / max(np.abs(ref[..., 1]).sum(), 1e-300))
+    flux = float(a[..., 1].sum() / ref[..., 1].sum() - 1.0)
+    peaks, src = measured_peaks()
+    n_mlp = rep.surrogate_rays + rep.audit_rays
+    flops = n_mlp * SUR_FLOPS_RAY
+    achieved = flops / (rep.ms_mlp * 1e-3) / 1e12
+    roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+            "frac": round(achieved / peaks["bf16_tflops"], 4), "traffic": None, "kernel": "k_mlp_fused",
+            "kernel_ms": rep.ms_mlp, "per_launch": flops, "peak_source": src + ", dense bf16 burst"}
+    # e2e: the frame into host memory (descriptor in, 4 floats per pixel out)
+    host = torch.empty((W, W, 4), dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        out, _ = sur.render(r, f, band_m=args.band, audit_frac=0.01, audit_seed=2, out=img)
+        host.copy_(out)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16+f64", "data": "synthetic",
+        "config": {"workload": f"thin Novikov-Thorne disk frame {W}x{W}, a=0.9, i=60 deg, r_cam=1000 M, fov +-12 M, "
+                               "pixel centres; surrogate outside the critical band, FP64 integrator inside it and "
+                               "on a 1% audit sample",
+                   "band_m": args.band, "plain_fp64_mrays_s": round(npix / (fp64_ms * 1e-3) / 1e6, 4),
+                   "plain_fp64_ms": round(fp64_ms, 3), "speedup_vs_fp64": round(fp64_ms / ms_step, 3),
+                   "image_rel_l1_vs_fp64": l1, "total_flux_err_vs_fp64": flux,
+                   "rays": rep.rays, "surrogate_rays": rep.surrogate_rays, "band_rays": rep.band_rays,
+                   "audit_rays": rep.audit_rays, "ms_route": rep.ms_route, "ms_mlp": rep.ms_mlp,
+                   "ms_shade": rep.ms_shade, "ms_integrator": rep.ms_integrator,
+                   "audit": {"class_mismatch": rep.audit_class_mismatch, "dir_err_rad": rep.audit_dir_err,
+                             "u_err": rep.audit_u_err, "r_rel_err": rep.audit_r_err, "g_err": rep.audit_g_err,
+                             "l1": rep.audit_l1, "flux": rep.audit_flux},
+                   "training": {"rays": args.train_rays, "steps": args.train_steps, "batch": 65536,
+                                "dataset_s": round(t_data, 2), "train_s": round(t_train, 2),
+                                "last_loss": last.total, "heldout_loss": held.total,
+                                "heldout_class_accuracy": held.accuracy},
+                   "l2": "256 MiB buffer written between timed steps", "frames_per_s": round(1e3 / ms_step * world, 3)},
+        "roofline": roof,
+        "e2e": {"value": round(world * npix / (e2e_step * 1e-3) / 1e6, 4), "unit": "Mrays/s",
+                "h2d_bytes_per_step": C.sizeof(so.abi.Frame), "d2h_bytes_per_step": W * W * 16},
+        "gpu_launches": args.steps * 8,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_disk(so, sh, f, W, budget_s=args.cpu_seconds)
+    sur.close()
+    r.close()
+    return line
+
+
+def cpu_baseline_disk(so, sh, f, W, budget_s=15.0):
+    """The oracle port on the thin-disk frame (FP64 integrator, disk emission), host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    threads = os.cpu_count() or 1
+    n = 4096
+    t0 = time.perf_counter()
+    x, y = _sample_pixels(so, f, W, n)
+    _oracle.orc_trace(sh.scene, f, x, y, threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(min(max(n * budget_s / max(dt, 1e-3), n), W * W))
+    x, y = _sample_pixels(so, f, W, n2)
+    t0 = time.perf_counter()
+    _oracle.orc_trace(sh.scene, f, x, y, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(n2 / dt / 1e6, 6), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"{n2} evenly strided pixel centres of the {W}x{W} thin-disk frame, oracle/so_oracle.c, "
+                      f"{threads} threads, {dt:.1f} s"}
+
+
+def run_wavefront(args, so, world, rank, local):
+    """The photon-ring batch: 4 spins x 2 inclinations x 8 turbulence times / zooms of the torus
+    plasma, W x W windows on the critical curve, all frames in one persistent launch replayed from a
+    CUDA graph, launch shape from the autotuner (run on a 128 x 128 copy of the batch)."""
+    import importlib
+    import torch
+    torch.cuda.set_device(local)
+    wf = importlib.import_module("spacetime_optics_b200.wavefront")
+    W = args.size or 512
+    prec = so.abi.SO_PREC_MIXED if args.path != "fp64" else so.abi.SO_PREC_FP64
+    shots = wf.photon_ring_shots(so, 128)
+    r = so.Renderer(shots[0].scene, shots[0].tables, shots[0].settings, device=local)
+    r.set_plasma(shots[0].plasma())
+    r.set_precision(prec)
+    b, _, scenes, frames, fs = wf.photon_ring_batch(so, r, 128)
+    small = torch.zeros((len(frames), 128, 128, 4), dtype=torch.float32, device="cuda")
+    tune = b.autotune(small.data_ptr())
+    b.close()
+    b, _, scenes, frames, fs = wf.photon_ring_batch(so, r, W)
+    b.set_tune(tune.ctas_per_sm, tune.interleave)
+    out = torch.zeros((len(frames), W, W, 4), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(r.stream())
+    for _ in range(args.warmup):
+        b.render(out.data_ptr())
+    torch.cuda.synchronize()
+    ms = []
+    barrier(world)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            b.render(out.data_ptr())
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    ms_step = allreduce_max(float(np.mean(ms)), world)
+    st = b.render(out.data_ptr(), stats=True)
+    nrays = len(frames) * W * W
+    value = world * nrays / (ms_step * 1e-3) / 1e6
+    fp64_peak, _ = so.probe_fma_peak(local)
+    n_modes = shots[0].plasma().n_modes
+    flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
+             st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
+    achieved = flops / (ms_step * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == so.abi.SO_PREC_FP64 else "f64+f32", "data": "synthetic",
+        "config": {"workload": f"photon-ring batch: {len(frames)} frames of {W}x{W} (spins 0/0.5/0.9/0.99, "
+                               "incl 17/60 deg, 8 turbulence times, zoom 1e3-4e4 on the critical curve), torus "
+                               "plasma with 512 modes, one persistent launch replayed from a CUDA graph",
+                   "tune": {"ctas_per_sm": tune.ctas_per_sm, "interleave": tune.interleave, "tuned_on": "128x128"},
+                   "frames_per_s": round(world * len(frames) / (ms_step * 1e-3), 4),
+                   "attempts_per_ray": st.attempts / nrays, "flow_steps_per_ray": st.flow_steps / nrays,
+                   "l2": "inputs (mode table, frame descriptors) are small; no flush (one step is seconds long)"},
+        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
+                     "frac": round(achieved / fp64_peak, 4), "traffic": None, "kernel": "k_trace64",
+                     "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"},
+        "e2e": None,
+        "gpu_launches": args.steps * 3,
+        "clocks": clk.summary(),
+    }
+    b.close()
+    r.close()
+    return line
+
+
 def _sample_pixels(so, f, W, n):
     X, Y = so.pixel_centres(f, W, W)
     idx = np.linspace(0, W * W - 1, n).astype(np.int64)
@@ -339,20 +547,31 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--workload", default="synchrotron", choices=["synchrotron", "surrogate", "wavefront"])
+    ap.add_argument("--size", type=int, default=0, help="frame width (default 2048 / 4096 / 512 per workload)")
+    ap.add_argument("--band", type=float, default=0.3, help="surrogate: critical band half-width (M)")
+    ap.add_argument("--train-rays", type=int, default=1 << 24)
+    ap.add_argument("--train-steps", type=int, default=40000)
     ap.add_argument("--path", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     so = load_package()
     if args.impl == "reference":
+        args.size = args.size or 2048
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return 0
         print(json.dumps(run_reference(args, so)), flush=True)
         return 0
     world, rank, local = dist_setup()
-    line = run_ours(args, so, world, rank, local)
+    if args.workload == "surrogate":
+        line = run_surrogate(args, so, world, rank, local)
+    elif args.workload == "wavefront":
+        line = run_wavefront(args, so, world, rank, local)
+    else:
+        args.size = args.size or 2048
+        line = run_ours(args, so, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

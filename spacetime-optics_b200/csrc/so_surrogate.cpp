@@ -324,7 +324,7 @@ extern "C" {
 
 void so_sur_default_opts(so_sur_opts* o) {
     if (!o) return;
-    o->fourier_sigma = 2.0f;
+    o->fourier_sigma = 0.35f;
     o->seed = 1;
     o->batch = 65536;
     o->lr = 2e-3f;
