@@ -102,25 +102,41 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU from the torchrun environment; a process group only when WORLD_SIZE > 1
+    (NCCL on GPUs; gloo for host-only runs of this logic)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
 def allreduce_max(x, world):
+    """Max over ranks of a per-rank time: the job's time is its slowest rank's."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_frame(sh, rank):
+    """Weak scaling: rank k renders frame 0 of the shot at turbulence time offset 50 k M."""
+    f = sh.frame(0)
+    f.t = f.t + 50.0 * rank
+    return f
+
+
+def job_rate(world, units_per_rank, ms_step):
+    """Whole-job throughput (units per second over all ranks) from the max-over-ranks step time."""
+    return world * units_per_rank / (ms_step * 1e-3)
 
 
 def barrier(world):
@@ -155,8 +171,7 @@ def run_ours(args, so, world, rank, local):
     path = args.path
     if path == "auto":
         path = "mixed"
-    f = sh.frame(rank)
-    f.t = sh.frame(0).t + 50.0 * rank  # every rank renders its own turbulence time offset
+    f = rank_frame(sh, rank)
     npix = W * W
     d_img = torch.empty((W, W, 4), dtype=torch.float32, device="cuda")
     stream = torch.cuda.ExternalStream(r.stream())
@@ -193,7 +208,7 @@ def run_ours(args, so, world, rank, local):
     ms_step = float(np.mean(ms))
     barrier(world)
     ms_step = allreduce_max(ms_step, world)
-    value = world * npix / (ms_step * 1e-3) / 1e6
+    value = job_rate(world, npix, ms_step) / 1e6
     # instrumented step: counters and the tracer kernel's own device time (CUDA events in the library)
     st = r.render_device(f, d_img.data_ptr(), stats=True)
     img = d_img.cpu().numpy()
@@ -324,7 +339,7 @@ def run_surrogate(args, so, world, rank, local):
         img, rep, ms = timed(args.band, 0.01, args.steps)
     ms_step = allreduce_max(float(np.mean(ms)), world)
     npix = W * W
-    value = world * npix / (ms_step * 1e-3) / 1e6
+    value = job_rate(world, npix, ms_step) / 1e6
     fp64_ms = float(np.mean(ms64))
     a = img.cpu().numpy().astype(np.float64)
     l1 = float(np.abs(a[..., 1] - ref[..., 1]).sum() / max(np.abs(ref[..., 1]).sum(), 1e-300))
@@ -439,7 +454,7 @@ def run_wavefront(args, so, world, rank, local):
     ms_step = allreduce_max(float(np.mean(ms)), world)
     st = b.render(out.data_ptr(), stats=True)
     nrays = len(frames) * W * W
-    value = world * nrays / (ms_step * 1e-3) / 1e6
+    value = job_rate(world, nrays, ms_step) / 1e6
     fp64_peak, _ = so.probe_fma_peak(local)
     n_modes = shots[0].plasma().n_modes
     flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
