@@ -11,9 +11,9 @@ the GPU gradient is checked against this oracle.
 
 Two arithmetic modes:
   exact    float64 everywhere, weights taken from the FP32 master parameters;
-  bf16     the GPU's rounding points: BF16 weights, features, activations and back-propagated
-           gradients (round to nearest even), FP32-valued pre-activations, head-bias gradient from
-           the unrounded dL/dO.  Products and sums are still float64 (the GPU sums BF16 products in
+  bf16     the GPU's rounding points: BF16 weights, features, activations, GELU derivatives and
+           back-propagated gradients (round to nearest even), FP32-valued pre-activations,
+           head-bias gradient from the unrounded dL/dO.  Products and sums are still float64 (the GPU sums BF16 products in
            FP32), so the two agree to the accumulation error plus rare one-ulp BF16 flips.
 """
 import numpy as np
@@ -138,7 +138,8 @@ def gradients(params, freq, rays, tgt, w_dir=1.0, w_u=10.0, w_g=1.0, rounding=Fa
     g[bh:bh + n] = dO.sum(axis=0)
     dOr = bf16(dO) if rounding else dO
     g[wh:wh + n * k] = (dOr.T @ acts[NHID]).ravel()
-    dz = (dOr @ W[NHID]) * gelu_grad(zs[NHID - 1])
+    gd = [bf16(gelu_grad(z)) if rounding else gelu_grad(z) for z in zs]
+    dz = (dOr @ W[NHID]) * gd[NHID - 1]
     if rounding:
         dz = bf16(dz)
     for l in range(NHID - 1, -1, -1):
@@ -146,7 +147,7 @@ def gradients(params, freq, rays, tgt, w_dir=1.0, w_u=10.0, w_g=1.0, rounding=Fa
         g[w:w + n * k] = (dz.T @ acts[l]).ravel()
         g[bo:bo + n] = dz.sum(axis=0)
         if l > 0:
-            dz = (dz @ W[l]) * gelu_grad(zs[l - 1])
+            dz = (dz @ W[l]) * gd[l - 1]
             if rounding:
                 dz = bf16(dz)
     return g, terms

@@ -139,26 +139,45 @@ __global__ void __launch_bounds__(128) k_loss(const float* __restrict__ O, const
             ((s_acc[0][threadIdx.x] + s_acc[1][threadIdx.x]) + s_acc[2][threadIdx.x]) + s_acc[3][threadIdx.x];
 }
 
-__global__ void k_loss_reduce(const float* __restrict__ part_gb, const double* __restrict__ part_acc, int nblk,
-                              float* __restrict__ gb, double* __restrict__ acc) {
-    const int k = threadIdx.x;
-    if (k < LDO) {
-        float s = 0.f;
-        for (int b = 0; b < nblk; ++b) s += part_gb[(long)b * LDO + k];
-        gb[k] = s;
-    } else if (k < LDO + 6) {
-        double s = 0.0;
-        for (int b = 0; b < nblk; ++b) s += part_acc[(long)b * 8 + (k - LDO)];
-        acc[k - LDO] += s;
+// Sum of the block partials in a fixed order and a fixed tree (deterministic): one block, each
+// output summed by 256 threads over strided partials, then a shared-memory tree.
+__global__ void __launch_bounds__(256) k_loss_reduce(const float* __restrict__ part_gb,
+                                                     const double* __restrict__ part_acc, int nblk,
+                                                     float* __restrict__ gb, double* __restrict__ acc) {
+    __shared__ double red[256];
+    for (int k = 0; k < LDO + 6; ++k) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+            v += k < LDO ? (double)part_gb[(long)b * LDO + k] : part_acc[(long)b * 8 + (k - LDO)];
+        red[threadIdx.x] = v;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            if (k < LDO) gb[k] = (float)red[0];
+            else acc[k - LDO] += red[0];
+        }
+        __syncthreads();
     }
 }
 
-// One block per row; fixed per-thread order and a fixed tree: deterministic.
-__global__ void __launch_bounds__(256) k_rowsum(const bf16* __restrict__ dT, int cols, float* __restrict__ gb) {
-    __shared__ float s[8];
-    const bf16* row = dT + (long)blockIdx.x * cols;
+// One block of 512 threads per row, 16-byte loads (8 values), fixed per-thread order and a fixed
+// tree: deterministic.  cols is a multiple of 8 and rows are 16-byte aligned.
+__global__ void __launch_bounds__(512) k_rowsum(const bf16* __restrict__ dT, int cols, float* __restrict__ gb) {
+    __shared__ float s[16];
+    const uint4* row = reinterpret_cast<const uint4*>(dT + (long)blockIdx.x * cols);
     float v = 0.f;
-    for (int c = threadIdx.x; c < cols; c += blockDim.x) v += __bfloat162float(row[c]);
+    for (int c = threadIdx.x; c < cols / 8; c += blockDim.x) {
+        const uint4 q = __ldg(row + c);
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            v += f.x + f.y;
+        }
+    }
     for (int sh = 16; sh > 0; sh >>= 1) v += __shfl_xor_sync(FULL, v, sh);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
     __syncthreads();
@@ -225,11 +244,11 @@ void launch_loss(const float* O, const so_sur_target* tgt, long off, long n, int
                  bf16* dOT, float* part_gb, double* part_acc, float* gb, double* acc, cudaStream_t st) {
     const int nblk = (rows + 127) / 128;
     k_loss<<<nblk, 128, 0, st>>>(O, tgt, off, n, rows, w, dO, dOT, part_gb, part_acc);
-    k_loss_reduce<<<1, 32, 0, st>>>(part_gb, part_acc, nblk, gb, acc);
+    k_loss_reduce<<<1, 256, 0, st>>>(part_gb, part_acc, nblk, gb, acc);
 }
 
 void launch_rowsum(const bf16* dT, int rows, int cols, float* gb, cudaStream_t st) {
-    k_rowsum<<<rows, 256, 0, st>>>(dT, cols, gb);
+    k_rowsum<<<rows, 512, 0, st>>>(dT, cols, gb);
 }
 
 void launch_sum_splits(const float* part, int splits, long count, float* out, cudaStream_t st) {

@@ -21,8 +21,8 @@ typedef __nv_bfloat16 bf16;
 
 enum Epilogue {
     EPI_F32 = 0,       // out_f[m, n] = acc + bias[n]
-    EPI_GELU = 1,      // z = acc + bias[n]; z_out[m, n] = z; out_b[m, n] = out_t[n, m] = gelu(z)
-    EPI_GELU_BWD = 2,  // d = acc * gelu'(z_in[m, n]); out_b[m, n] = out_t[n, m] = d
+    EPI_GELU = 1,      // z = acc + bias[n]; d_out[m, n] = gelu'(z); out_b[m, n] = out_t[n, m] = gelu(z)
+    EPI_GELU_BWD = 2,  // y = acc * d_in[m, n]; out_b[m, n] = out_t[n, m] = y   (all BF16)
     EPI_SPLIT = 3,     // out_f[z][m, n] = acc   (partial sums of split reductions, z = slice)
     EPI_SPLIT_T = 4,   // out_f[z][n, m] = acc
 };
@@ -43,9 +43,9 @@ struct GemmArgs {
     long ldob;
     bf16* out_t;
     long ldot;
-    float* z_out;
-    const float* z_in;
-    long ldz;
+    bf16* d_out;       // GELU derivative at the pre-activation, for the backward pass
+    const bf16* d_in;
+    long ldd;
     int* err;  // device status word: set to a nonzero code when a wait gives up
 };
 
@@ -54,16 +54,12 @@ struct GemmArgs {
 // N % 256 == 0; (K / splits) % 16 == 0; lda, ldb multiples of 8 elements; A, B 16-byte aligned.
 int launch_gemm(const GemmArgs& g, cudaStream_t st, const char** why);
 
-// tanh-form GELU and its derivative (float), shared by the epilogues.
-__host__ __device__ inline float gelu_f(float z) {
+// tanh-form GELU and its derivative (float) from one tanh, for the training epilogue.
+__host__ __device__ inline void gelu_and_grad_f(float z, float* y, float* d) {
     const float c = 0.7978845608028654f, k = 0.044715f;
-    float t = tanhf(c * (z + k * z * z * z));
-    return 0.5f * z * (1.f + t);
-}
-__host__ __device__ inline float gelu_grad_f(float z) {
-    const float c = 0.7978845608028654f, k = 0.044715f;
-    float t = tanhf(c * (z + k * z * z * z));
-    return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * c * (1.f + 3.f * k * z * z);
+    const float t = tanhf(c * (z + k * z * z * z));
+    *y = 0.5f * z * (1.f + t);
+    *d = 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * c * (1.f + 3.f * k * z * z);
 }
 
 // ---- network shape and parameter layout ------------------------------------------------------

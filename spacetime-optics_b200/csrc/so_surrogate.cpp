@@ -71,7 +71,8 @@ struct so_surrogate {
     int tb = 0;
     bf16 *X = nullptr, *XT = nullptr, *dO = nullptr, *dOT = nullptr;
     bf16 *A[mlp::NHID] = {}, *AT[mlp::NHID] = {}, *dZ[2] = {}, *dZT[2] = {};
-    float *Z[mlp::NHID] = {}, *O = nullptr, *part = nullptr, *part_gb = nullptr;
+    bf16* D[mlp::NHID] = {};  // GELU derivatives of the hidden layers
+    float *O = nullptr, *part = nullptr, *part_gb = nullptr;
     double* part_acc = nullptr;
     // fused inference: packed weight chunks, rebuilt when the parameters change
     bf16* d_wpack = nullptr;
@@ -114,9 +115,8 @@ void free_train(so_surrogate* s) {
     for (int l = 0; l < mlp::NHID; ++l) {
         if (s->A[l]) cudaFree(s->A[l]);
         if (s->AT[l]) cudaFree(s->AT[l]);
-        if (s->Z[l]) cudaFree(s->Z[l]);
-        s->A[l] = s->AT[l] = nullptr;
-        s->Z[l] = nullptr;
+        if (s->D[l]) cudaFree(s->D[l]);
+        s->A[l] = s->AT[l] = s->D[l] = nullptr;
     }
     for (int i = 0; i < 2; ++i) {
         if (s->dZ[i]) cudaFree(s->dZ[i]);
@@ -164,7 +164,7 @@ int ensure_train(so_surrogate* s, int rows) {
               dalloc(&s->part_acc, (R / 128 + 1) * 8) == cudaSuccess;
     for (int l = 0; ok && l < mlp::NHID; ++l)
         ok = dalloc(&s->A[l], R * mlp::HID) == cudaSuccess && dalloc(&s->AT[l], R * mlp::HID) == cudaSuccess &&
-             dalloc(&s->Z[l], R * mlp::HID) == cudaSuccess;
+             dalloc(&s->D[l], R * mlp::HID) == cudaSuccess;
     for (int i = 0; ok && i < 2; ++i)
         ok = dalloc(&s->dZ[i], R * mlp::HID) == cudaSuccess && dalloc(&s->dZT[i], R * mlp::HID) == cudaSuccess;
     if (!ok) {
@@ -199,8 +199,8 @@ mlp::GemmArgs args(const bf16* A, long lda, const bf16* B, long ldb, int M, int 
     return g;
 }
 
-// Training forward pass of `rows` rays starting at `off` (layer by layer, keeping the
-// pre-activations Z, the activations and their transposes for the backward pass).  The head's FP32
+// Training forward pass of `rows` rays starting at `off` (layer by layer, keeping the GELU
+// derivatives D, the activations and their transposes for the backward pass).  The head's FP32
 // outputs go to O (16 floats per row).
 int forward(so_surrogate* s, const so_sur_ray* rays, long long n, long long off, int rows, int wrap, float* O,
             cudaStream_t st) {
@@ -214,8 +214,8 @@ int forward(so_surrogate* s, const so_sur_ray* rays, long long n, long long off,
         g.ldob = mlp::HID;
         g.out_t = s->AT[l];
         g.ldot = rows;
-        g.z_out = s->Z[l];
-        g.ldz = mlp::HID;
+        g.d_out = s->D[l];
+        g.ldd = mlp::HID;
         int rc = gemm(s, g, st);
         if (rc) return rc;
         in = s->A[l];
@@ -249,8 +249,8 @@ int backward(so_surrogate* s, const so_sur_target* tgt, long long n, long long o
     int cur = 0;
     {
         mlp::GemmArgs g = args(s->dO, mlp::LDO, s->d_WT + L.w[mlp::NHID], mlp::LDO, rows, H, mlp::LDO, mlp::EPI_GELU_BWD);
-        g.z_in = s->Z[mlp::NHID - 1];
-        g.ldz = H;
+        g.d_in = s->D[mlp::NHID - 1];
+        g.ldd = H;
         g.out_b = s->dZ[cur];
         g.ldob = H;
         g.out_t = s->dZT[cur];
@@ -272,8 +272,8 @@ int backward(so_surrogate* s, const so_sur_target* tgt, long long n, long long o
         mlp::launch_rowsum(s->dZT[cur], H, rows, s->d_g + L.b[l], st);
         if (l > 0) {
             mlp::GemmArgs d = args(s->dZ[cur], H, s->d_WT + L.w[l], H, rows, K, H, mlp::EPI_GELU_BWD);
-            d.z_in = s->Z[l - 1];
-            d.ldz = H;
+            d.d_in = s->D[l - 1];
+            d.ldd = H;
             d.out_b = s->dZ[cur ^ 1];
             d.ldob = H;
             d.out_t = s->dZT[cur ^ 1];
