@@ -335,7 +335,7 @@ void so_sur_default_opts(so_sur_opts* o) {
     o->eps = 1e-8f;
     o->weight_decay = 0.0f;
     o->w_dir = 1.0f;
-    o->w_u = 10.0f;
+    o->w_u = 30.0f;
     o->w_g = 1.0f;
 }
 
