@@ -564,7 +564,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="synchrotron", choices=["synchrotron", "surrogate", "wavefront"])
     ap.add_argument("--size", type=int, default=0, help="frame width (default 2048 / 4096 / 512 per workload)")
-    ap.add_argument("--band", type=float, default=0.3, help="surrogate: critical band half-width (M)")
+    ap.add_argument("--band", type=float, default=0.1, help="surrogate: critical band half-width (M)")
     ap.add_argument("--train-rays", type=int, default=1 << 24)
     ap.add_argument("--train-steps", type=int, default=40000)
     ap.add_argument("--path", default="auto", choices=["auto", "fp64", "mixed"])

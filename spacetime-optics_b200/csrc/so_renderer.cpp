@@ -207,6 +207,15 @@ void launch_common(so_renderer* r, TraceLaunch& L) {
     L.drift_tol = r->mixed.drift_tol;
 }
 
+// The second queue: a stream, its fork / join events and the queue heads of launches made on it.
+int ensure_side_queue(so_renderer* r) {
+    if (!r->d_cnt3 && dalloc(&r->d_cnt3, 2) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "second queue: allocation");
+    if (!r->st2) SO_CK(r, cudaStreamCreateWithFlags(&r->st2, cudaStreamNonBlocking));
+    if (!r->ev_fork) SO_CK(r, cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming));
+    if (!r->ev_join) SO_CK(r, cudaEventCreateWithFlags(&r->ev_join, cudaEventDisableTiming));
+    return SO_OK;
+}
+
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
     cudaError_t e = launch_trace64(L, variant_of(r->S), r->num_sms, st ? st : r->st);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
@@ -236,12 +245,9 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         r->mixed_cap = ns;
     }
     if (!r->d_nlists) {
-        if (dalloc(&r->d_nlists, 4) != cudaSuccess || dalloc(&r->d_cnt3, 2) != cudaSuccess ||
-            (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess))
+        if (dalloc(&r->d_nlists, 4) != cudaSuccess || (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess))
             return fail(r, SO_ERR_ALLOC, "mixed path: device allocation");
-        SO_CK(r, cudaStreamCreateWithFlags(&r->st2, cudaStreamNonBlocking));
-        SO_CK(r, cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming));
-        SO_CK(r, cudaEventCreateWithFlags(&r->ev_join, cudaEventDisableTiming));
+        if (int rc = ensure_side_queue(r)) return rc;
         SO_CK(r, cudaEventCreate(&r->ev32[0]));
         SO_CK(r, cudaEventCreate(&r->ev32[1]));
     }
@@ -536,11 +542,22 @@ int rend_upload_frame(so_renderer* r, const so_frame& f, const so_frame** d_fram
     return SO_OK;
 }
 
-int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum) {
+int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum,
+                    int side) {
     if (n <= 0) return SO_OK;
-    SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    cudaStream_t st = r->st;
+    Counters* cnt = r->d_cnt;
+    if (side) {
+        if (int rc = ensure_side_queue(r)) return rc;
+        SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
+        SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
+        st = r->st2;
+        cnt = &r->d_cnt3[0];
+    }
+    SO_CK(r, cudaMemsetAsync(cnt, 0, sizeof(Counters), st));
     TraceLaunch L;
     launch_common(r, L);
+    L.counters = cnt;
     L.kind = RAYS_LIST;
     L.nrays = n;
     L.x = d_x;
@@ -551,8 +568,15 @@ int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y,
         L.out.cross_r = nullptr;
         L.out.cross_g = nullptr;
     }
-    cudaError_t e = launch_trace64(L, vacuum ? VAR_VACUUM : variant_of(r->S), r->num_sms, r->st);
+    cudaError_t e = launch_trace64(L, vacuum ? VAR_VACUUM : variant_of(r->S), r->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
+
+int rend_join_side(so_renderer* r) {
+    if (!r->st2) return SO_OK;
+    SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
+    SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
     return SO_OK;
 }
 }  // namespace so

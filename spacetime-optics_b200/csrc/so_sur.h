@@ -76,7 +76,11 @@ int rend_band_table(so_renderer* r, double th, const float** d_band, int* n);
 int rend_upload_frame(so_renderer* r, const so_frame& f, const so_frame** d_frame);
 // trace_ray over n device rays (x, y) of the frame already uploaded, with the tracer variant
 // `vacuum` = 1 (no emission, crossing records) or 0 (the scene's own variant), on the renderer's
-// stream.  Does not synchronise.
-int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum);
+// stream, or with side = 1 on its second stream (ordered after the work queued on the first so far,
+// own queue head).  Does not synchronise.
+int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum,
+                    int side = 0);
+// Orders the renderer's stream after everything queued on its second stream.
+int rend_join_side(so_renderer* r);
 
 }  // namespace so

@@ -680,12 +680,7 @@ int so_sur_render(so_surrogate* s, so_renderer* r, const so_frame* f, const so_s
     // integrator: band and audit rays with the scene's own (disk) tracer, then the audit rays again
     // in vacuum for their crossing records
     sur::launch_xy(dF, rs.W, rs.H, s->list_b, nb, s->list_a, na, s->fx, s->fy, st);
-    so_rays_out o;
-    std::memset(&o, 0, sizeof o);
-    o.I = reinterpret_cast<float*>(s->fI);
-    rc = rend_trace_list(r, nb + na, s->fx, s->fy, o, 0);
-    if (rc) return fail(s, rc, "so_sur_render: integrator");
-    if (na > 0) {
+    if (na > 0) {  // the audit rays' vacuum records, on the renderer's second stream meanwhile
         so_rays_out v;
         std::memset(&v, 0, sizeof v);
         v.fate = s->ffate;
@@ -693,8 +688,17 @@ int so_sur_render(so_surrogate* s, so_renderer* r, const so_frame* f, const so_s
         v.phi = s->fph;
         v.cross_r = s->fcr;
         v.cross_g = s->fcg;
-        rc = rend_trace_list(r, na, s->fx + nb, s->fy + nb, v, 1);
+        rc = rend_trace_list(r, na, s->fx + nb, s->fy + nb, v, 1, 1);
         if (rc) return fail(s, rc, "so_sur_render: audit integrator");
+    }
+    so_rays_out o;
+    std::memset(&o, 0, sizeof o);
+    o.I = reinterpret_cast<float*>(s->fI);
+    rc = rend_trace_list(r, nb + na, s->fx, s->fy, o, 0);
+    if (rc) return fail(s, rc, "so_sur_render: integrator");
+    if (na > 0) {
+        rc = rend_join_side(r);
+        if (rc) return fail(s, rc, "so_sur_render: stream join");
         sur::Audit A;
         A.na = na;
         A.nb = nb;
