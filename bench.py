@@ -212,6 +212,19 @@ def run_ours(args, so, world, rank, local):
     # instrumented step: counters and the tracer kernel's own device time (CUDA events in the library)
     st = r.render_device(f, d_img.data_ptr(), stats=True)
     img = d_img.cpu().numpy()
+    classes = None
+    if path == "mixed":
+        # termination class of every sample outside the critical band against FP64 geometry (the
+        # same samples with the band covering the field)
+        ns = npix * sh.settings.spp
+        fm, band = r.last_fates(ns)
+        r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+        r.render_device(f, d_img.data_ptr(), stats=True)
+        f64, _ = r.last_fates(ns)
+        set_prec("mixed")
+        out = ~band
+        classes = {"samples_outside_band": int(out.sum()), "class_mismatch_outside_band": int((fm[out] != f64[out]).sum()),
+                   "class_mismatch_in_band": int((fm[band] != f64[band]).sum())}
     err_l1 = float(np.abs(img[..., 0] - img64[..., 0]).sum() / max(np.abs(img64[..., 0]).sum(), 1e-300))
     flux_err = float(abs(img[..., 0].astype(np.float64).sum() / img64[..., 0].astype(np.float64).sum() - 1.0))
     fp64_mrays = npix / (st64.ms_kernel * 1e-3) / 1e6
@@ -262,7 +275,8 @@ def run_ours(args, so, world, rank, local):
                    "plain_fp64_mrays_s": round(fp64_mrays, 4), "image_rel_l1_vs_fp64": err_l1,
                    "total_flux_err_vs_fp64": flux_err, "frames_per_s": round(1e3 / ms_step * world, 4),
                    "l2": "256 MiB buffer written between timed steps", **norm,
-                   "attempts_per_ray": st.attempts / npix, "flow_steps_per_ray": st.flow_steps / npix},
+                   "attempts_per_ray": st.attempts / npix, "flow_steps_per_ray": st.flow_steps / npix,
+                   "termination_class": classes},
         "roofline": roof,
         "e2e": {"value": round(e2e, 4), "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(so.abi.Frame),
                 "d2h_bytes_per_step": W * W * 16},

@@ -168,6 +168,7 @@ typedef struct so_stats {
     double ms_fp32;       /* mixed precision: device time of the FP32 tracer launch (CUDA events) */
     long long redo_turn;  /* mixed precision: FP32 rays re-traced for a radial turning point inside turn_r */
     long long redo_drift; /* mixed precision: FP32 rays re-traced for constraint drift above drift_tol */
+    long long redo_limit; /* mixed precision: FP32 rays re-traced after reaching max_steps in FP32 */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -268,6 +269,11 @@ int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double*
  * the scene.hpp flow model). */
 int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts);
 int so_set_plasma(so_renderer* r, const so_plasma* plasma, const so_mode* modes);
+/* Termination class (SO_FATE_*) of every sample of the last mixed-precision frame (samples in
+ * pixel-major order, spp per pixel) and whether the sample was routed to FP64 by the critical band
+ * (1) or not (0); host arrays of n = W * H * spp entries, either may be NULL.  For checking that the
+ * mixed path's classes outside the band are the FP64 ones.  No reference counterpart. */
+int so_last_fates(so_renderer* r, int8_t* fate, uint8_t* in_band, long long n);
 /* CUDA stream used by the renderer (cudaStream_t, as void*), for callers that order work on it. */
 void* so_stream(so_renderer* r);
 /* Message of the last failed call on r (or of the last failed so_init when r is NULL). */

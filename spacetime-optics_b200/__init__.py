@@ -92,6 +92,7 @@ def lib():
                                      P(Stats)]
         L.so_sur_render.argtypes = [vp, vp, P(Frame), P(abi.SurFrameOpts), vp, P(abi.SurReport)]
         L.so_sur_gemm.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.so_last_fates.argtypes = [vp, vp, vp, C.c_longlong]
         _lib = L
     return _lib
 
@@ -248,6 +249,13 @@ class Renderer:
         _check(lib().so_render_device(self.h, C.byref(frame), C.c_void_p(d_px), C.byref(st) if st else None),
                self.h)
         return st
+
+    def last_fates(self, n):
+        """(fate int8[n], in_band bool[n]) of the last mixed-precision frame's samples."""
+        fate = np.zeros(n, np.int8)
+        band = np.zeros(n, np.uint8)
+        _check(lib().so_last_fates(self.h, _ptr(fate), _ptr(band), n), self.h)
+        return fate, band.astype(bool)
 
     def stream(self):
         """The renderer's CUDA stream handle (cudaStream_t as an int)."""

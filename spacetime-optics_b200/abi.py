@@ -84,7 +84,8 @@ class Stats(C.Structure):
                 ("step_limited", C.c_longlong), ("attempts", C.c_longlong), ("accepted", C.c_longlong),
                 ("fp64_rays", C.c_longlong), ("flow_steps", C.c_longlong), ("ms_kernel", C.c_double),
                 ("attempts_fp32", C.c_longlong), ("band_rays", C.c_longlong), ("flow_steps_fp32", C.c_longlong),
-                ("ms_fp32", C.c_double), ("redo_turn", C.c_longlong), ("redo_drift", C.c_longlong)]
+                ("ms_fp32", C.c_double), ("redo_turn", C.c_longlong), ("redo_drift", C.c_longlong),
+                ("redo_limit", C.c_longlong)]
 
 
 class RaysOut(C.Structure):
@@ -185,5 +186,5 @@ EXPORTS = [
     "so_kerr_point_at", "so_critical_curve_point",
     "so_sur_default_opts", "so_sur_create", "so_sur_destroy", "so_sur_get_params", "so_sur_set_params",
     "so_sur_train", "so_sur_evaluate", "so_sur_gradients", "so_sur_infer", "so_sur_dataset", "so_sur_render",
-    "so_sur_gemm",
+    "so_sur_gemm", "so_last_fates",
 ]

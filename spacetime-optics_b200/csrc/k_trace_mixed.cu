@@ -658,10 +658,12 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         n_att += (unsigned long long)R.natt;
         n_acc += (unsigned long long)R.nacc;
         n_flow += (unsigned long long)R.nflow;
-        if (fate == 0) ++n_lim;
-        const bool redo = fate >= 3;
+        // a ray that used up max_steps in FP32 (the FP32 controller can stall where FP64 does not)
+        // is decided by the FP64 tracer, like the constraint and turning-point failures
+        const bool redo = fate >= 3 || fate == 0;
         n_turn += fate == 3 ? 1 : 0;
         n_drift += fate == 4 ? 1 : 0;
+        n_lim += fate == 0 ? 1 : 0;
         if (!redo) {
             L.sample_out[R.sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
             if (L.sample_fate) L.sample_fate[R.sid] = (int8_t)fate;
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         atomicAdd(&L.counters->attempts, n_att);
         atomicAdd(&L.counters->pad[1], n_acc);  // FP32 accepted steps
         atomicAdd(&L.counters->flow_steps, n_flow);
-        atomicAdd(&L.counters->step_limited, n_lim);
+        atomicAdd(&L.counters->redo_limit, n_lim);
         atomicAdd(&L.counters->redo_turn, n_turn);
         atomicAdd(&L.counters->redo_drift, n_drift);
     }

@@ -34,6 +34,7 @@ struct Counters {
     unsigned long long pad[2];        // [0] FP64 approach attempts, [1] FP32 accepted steps
     unsigned long long redo_turn;     // mixed: FP32 rays re-traced for a radial turning point inside turn_r
     unsigned long long redo_drift;    // mixed: FP32 rays re-traced for constraint drift
+    unsigned long long redo_limit;    // mixed: FP32 rays re-traced because they reached max_steps
 };
 
 struct TraceLaunch {

@@ -33,6 +33,7 @@ namespace {
 constexpr size_t OFF_COUNTERS = 0;
 constexpr size_t OFF_PARTIALS = 256;
 constexpr size_t OFF_ACCUM = 256 + 5120;
+static_assert(sizeof(so::Counters) + sizeof(int) <= 256, "counters and scene index must fit the cleared header");
 constexpr size_t SCRATCH_BYTES = OFF_ACCUM + (size_t)SO_NOALLOC_MAX_PIXELS * 16;
 
 // Held by every GPU that loads the library, until the process exits.

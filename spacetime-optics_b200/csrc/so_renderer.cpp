@@ -90,6 +90,7 @@ struct so_renderer {
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev32[2] = {nullptr, nullptr};  // around the FP32 tracer launch
+    long long last_mixed_ns = 0;               // samples of the last mixed-precision pass 1
     std::string err;
 };
 
@@ -228,6 +229,7 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
 //   per-pixel gather of the samples.  Counts stay on the device: nothing waits on the host.
 int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     const long long ns = (long long)f.W * f.H * f.spp;
+    r->last_mixed_ns = 0;
     if (ns > 0xffffffffll) return fail(r, SO_ERR_SIZE, "mixed path: more than 2^32 samples per frame");
     if (ns > r->mixed_cap) {
         void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked};
@@ -318,6 +320,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     if (rc) return rc;
     SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
     SO_CK(r, launch_gather_samples(L, r->st));
+    r->last_mixed_ns = ns;
     return SO_OK;
 }
 
@@ -420,6 +423,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->flow_steps_fp32 = (long long)c.flow_steps;
             stats->redo_turn = (long long)c.redo_turn;
             stats->redo_drift = (long long)c.redo_drift;
+            stats->redo_limit = (long long)c.redo_limit;
             float ms32 = 0.f;
             cudaEventElapsedTime(&ms32, r->ev32[0], r->ev32[1]);
             stats->ms_fp32 = ms32;
@@ -442,7 +446,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->band_rays = 0;
             stats->flow_steps_fp32 = 0;
             stats->ms_fp32 = 0.0;
-            stats->redo_turn = stats->redo_drift = 0;
+            stats->redo_turn = stats->redo_drift = stats->redo_limit = 0;
             c.fp64_rays = 0;
         }
         float ms1 = 0.f, ms2 = 0.f;
@@ -806,6 +810,25 @@ int so_trace_rays(so_renderer* r, const so_frame* f, int n, const double* x, con
         SO_CK(r, back(out->cross_g, b.cross_g, (size_t)n * 24));
     }
     SO_CK(r, cudaStreamSynchronize(r->st));
+    return SO_OK;
+}
+
+int so_last_fates(so_renderer* r, int8_t* fate, uint8_t* in_band, long long n) {
+    if (!r || (!fate && !in_band) || n <= 0) return SO_ERR_ARG;
+    if (r->last_mixed_ns == 0) return fail(r, SO_ERR_STATE, "so_last_fates: no mixed-precision frame rendered");
+    if (n != r->last_mixed_ns) return fail(r, SO_ERR_ARG, "so_last_fates: n is not the frame's sample count");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    if (fate) SO_CK(r, cudaMemcpy(fate, r->d_sample_fate, (size_t)n, cudaMemcpyDeviceToHost));
+    if (in_band) {
+        unsigned long long nb = 0;
+        SO_CK(r, cudaMemcpy(&nb, &r->d_nlists[1], sizeof nb, cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> ids((size_t)nb);
+        if (nb) SO_CK(r, cudaMemcpy(ids.data(), r->d_list64, (size_t)nb * 4, cudaMemcpyDeviceToHost));
+        std::memset(in_band, 0, (size_t)n);
+        for (uint32_t id : ids)
+            if ((long long)id < n) in_band[id] = 1;
+    }
     return SO_OK;
 }
 

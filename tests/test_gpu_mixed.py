@@ -51,7 +51,8 @@ def test_mixed_turning_point_retrace(so):
     """turn_r > 0 re-traces the FP32 rays whose radial turning point falls inside it, in FP64."""
     img64, img32, _, st32 = _render_pair(so, "synchrotron_1024.ini", ["camera.width=96", "camera.height=96", N0],
                                          turn_r=3.5)
-    assert st32.redo_turn > 0 and st32.fp64_rays == st32.band_rays + st32.redo_turn + st32.redo_drift
+    assert st32.redo_turn > 0
+    assert st32.fp64_rays == st32.band_rays + st32.redo_turn + st32.redo_drift + st32.redo_limit
     l1, flux = _errors(img64, img32)
     assert l1 <= 1e-3 and flux <= 1e-3
 
@@ -126,4 +127,27 @@ def test_mixed_deterministic(so):
     a, _, _ = r.render(f)
     b, _, _ = r.render(f)
     assert np.array_equal(a, b)
+    r.close()
+
+
+def test_mixed_classes_exact_outside_band(so):
+    """Outside the critical band every sample of the mixed path ends with the FP64 termination class
+    (the same samples traced with the band covering the field: FP64 geometry throughout)."""
+    W = 192
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", N0])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    n = W * W * sh.settings.spp
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    r.render(f)
+    fm, band = r.last_fates(n)
+    r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+    r.render(f)
+    f64, allband = r.last_fates(n)
+    assert allband.all()
+    out = ~band
+    assert 0.9 * n < out.sum() < n
+    assert set(np.unique(f64)) >= {-1, 1}
+    assert np.array_equal(fm[out], f64[out]), int((fm[out] != f64[out]).sum())
     r.close()
