@@ -299,6 +299,14 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
     }
     const int lane = threadIdx.x & 31;
     const long long total = L.nrays_dev ? (long long)*L.nrays_dev : L.nrays;
+    // Short lists (re-trace lists, small ray lists) leave most lanes of the grid without a ray; then
+    // only every stride-th lane takes rays, so the rays spread over more warps and each warp's
+    // cooperative turbulence sums serve fewer lanes.  The same for every lane of the grid.
+    int stride = 1;
+    {
+        const long long lanes = (long long)gridDim.x * blockDim.x;
+        while (stride < 32 && total > 0 && (long long)(stride * 2) * total <= lanes) stride *= 2;
+    }
     long long job = 0, pix = 0;
     int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
     bool active = false, exhausted = false;
@@ -313,7 +321,7 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
     const bool rec = L.kind == RAYS_LIST && L.record_cross;
 
     for (;;) {
-        const bool need = !active && !exhausted;
+        const bool need = !active && !exhausted && (lane & (stride - 1)) == 0;
         const unsigned m = __ballot_sync(FULL, need);
         if (m) {
             const int leader = __ffs(m) - 1;
@@ -478,7 +486,7 @@ cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaS
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         if (L.ctas_per_sm > 0 && L.ctas_per_sm < per_sm) per_sm = L.ctas_per_sm;
-        long long want = (L.nrays + tpb - 1) / tpb;
+        long long want = (L.nrays * 32 + tpb - 1) / tpb;  // up to a warp per ray for short lists
         long long grid = (long long)num_sms * per_sm;
         if (grid > want) grid = want;
         if (grid < 1) grid = 1;
