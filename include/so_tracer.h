@@ -146,8 +146,9 @@ typedef struct so_tables {
 /* RenderSettings (renderer.hpp:25-29). */
 typedef struct so_settings { int W, H, spp, spp_max; float target_err; } so_settings;
 
-/* PostParams (renderer.hpp:31-35).  blur_sigma_px > 0.5 and bloom > 0 return SO_ERR_UNSUPPORTED
- * (display post-processing is outside this library). */
+/* PostParams (renderer.hpp:31-35), applied by so_render as the reference does (render.cu:766-767):
+ * bloom in [0, 1] (visible mode), blur_sigma_px (radio mode, applied above 0.5 pixel), hide_direct
+ * (radio luminance statistics).  Tone mapping, HUD and image files are outside this library. */
 typedef struct so_post { float bloom; double blur_sigma_px; float hide_direct; } so_post;
 
 /* HdrFrame (renderer.hpp:41-46) with caller-owned pixels: px holds W*H*4 floats. */

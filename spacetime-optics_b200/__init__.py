@@ -232,13 +232,13 @@ class Renderer:
         o = MixedOpts(band_m, tol32, turn_r, drift_tol, r_switch, tol_approach, t32_blocks)
         _check(lib().so_set_precision(self.h, precision, C.byref(o)), self.h)
 
-    def render(self, frame, percentile=0.995, hide_direct=0.0, out=None):
+    def render(self, frame, percentile=0.995, hide_direct=0.0, out=None, bloom=0.0, blur_sigma_px=0.0):
         W, H = self.settings.W, self.settings.H
         if out is None:
             out = np.empty((H, W, 4), np.float32)
         hdr = HdrFrame(W, H, out.ctypes.data_as(C.POINTER(C.c_float)), 0.0, 0.0)
         st = Stats()
-        post = Post(0.0, 0.0, hide_direct)
+        post = Post(bloom, blur_sigma_px, hide_direct)
         _check(lib().so_render(self.h, C.byref(frame), C.byref(post), percentile, C.byref(hdr), C.byref(st)), self.h)
         return out, hdr, st
 

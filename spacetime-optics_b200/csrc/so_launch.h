@@ -37,6 +37,16 @@ struct Counters {
     unsigned long long redo_limit;    // mixed: FP32 rays re-traced because they reached max_steps
 };
 
+// The frame's 2x2 box-filter pyramid for the post filters (level 0 is the frame itself).
+constexpr int POST_MAX_LEVELS = 9;
+struct PostLevels {
+    float4* p[POST_MAX_LEVELS];
+    int w[POST_MAX_LEVELS], h[POST_MAX_LEVELS];
+    int n;
+};
+cudaError_t post_bloom(const PostLevels& L, float strength, cudaStream_t st);
+cudaError_t post_radio_blur(const PostLevels& L, float4* tmp, double sigma, cudaStream_t st);
+
 struct TraceLaunch {
     const so_scene* scenes;   // device array, indexed by frame_scene[f]
     const so_frame* frames;   // device array

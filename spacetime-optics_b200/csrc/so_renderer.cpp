@@ -7,7 +7,7 @@
 //   resolve;  device -> host copy of the HDR frame;  luminance percentile on the host.
 // Differences from the reference: every failure is a status code (no abort), reductions are
 // deterministic, per-frame scene data live in device memory (not __constant__), and there is no
-// sky texture / bloom / beam blur (outside this library: SO_ERR_UNSUPPORTED).
+// sky texture (SO_ERR_UNSUPPORTED).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -91,6 +91,9 @@ struct so_renderer {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev32[2] = {nullptr, nullptr};  // around the FP32 tracer launch
     long long last_mixed_ns = 0;               // samples of the last mixed-precision pass 1
+    // post filters: pyramid levels 1.. of d_img and a scratch frame (allocated on first use)
+    PostLevels lev{};
+    float4* d_tmp = nullptr;
     std::string err;
 };
 
@@ -131,6 +134,9 @@ void free_all(so_renderer* r) {
                   r->d_nlists, r->d_cnt3, r->d_band};
     for (void* p : pm)
         if (p) cudaFree(p);
+    for (int k = 1; k < r->lev.n; ++k)
+        if (r->lev.p[k]) cudaFree(r->lev.p[k]);
+    if (r->d_tmp) cudaFree(r->d_tmp);
     for (cudaEvent_t e : r->ev32)
         if (e) cudaEventDestroy(e);
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
@@ -206,6 +212,32 @@ void launch_common(so_renderer* r, TraceLaunch& L) {
     L.tol32 = r->mixed.tol32;
     L.turn_r = r->mixed.turn_r;
     L.drift_tol = r->mixed.drift_tol;
+}
+
+// Pyramid of the frame for the post filters, level sizes as the reference's (render.cu:638-647).
+int ensure_post(so_renderer* r) {
+    if (r->lev.n) return SO_OK;
+    int w = r->rs.W, h = r->rs.H, n = 0;
+    PostLevels L{};
+    while (n < POST_MAX_LEVELS && w >= 2 && h >= 2) {
+        L.w[n] = w;
+        L.h[n] = h;
+        if (n == 0) L.p[0] = r->d_img;
+        else if (dalloc(&L.p[n], (size_t)w * h) != cudaSuccess) {
+            for (int k = 1; k < n; ++k) cudaFree(L.p[k]);
+            return fail(r, SO_ERR_ALLOC, "post filters: pyramid allocation");
+        }
+        ++n;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+    }
+    if (dalloc(&r->d_tmp, (size_t)r->npix) != cudaSuccess) {
+        for (int k = 1; k < n; ++k) cudaFree(L.p[k]);
+        return fail(r, SO_ERR_ALLOC, "post filters: scratch allocation");
+    }
+    L.n = n;
+    r->lev = L;
+    return SO_OK;
 }
 
 // The second queue: a stream, its fork / join events and the queue heads of launches made on it.
@@ -653,8 +685,8 @@ int so_update_scene(so_renderer* r, const so_scene* scene) {
 int so_render(so_renderer* r, const so_frame* f_in, const so_post* post, double percentile, so_hdr_frame* out,
               so_stats* stats) {
     if (!r || !f_in || !out || !out->px) return fail(r, SO_ERR_ARG, "so_render: NULL argument");
-    if (post && (post->bloom > 0.f || post->blur_sigma_px > 0.5))
-        return fail(r, SO_ERR_UNSUPPORTED, "so_render: bloom / beam blur are display post-processing");
+    if (post && (!(post->bloom >= 0.f && post->bloom <= 1.f) || !(post->blur_sigma_px >= 0.0)))
+        return fail(r, SO_ERR_ARG, "so_render: bloom must be in [0, 1] and blur_sigma_px >= 0");
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
     so_frame f = *f_in;
     f.W = r->rs.W;
@@ -664,6 +696,14 @@ int so_render(so_renderer* r, const so_frame* f_in, const so_post* post, double 
     int rc = trace_frame(r, f, true, stats);
     if (rc) return rc;
     double t1 = now_ms();
+    // post filters (render.cu:766-767): glare in visible mode, interferometer beam in radio mode
+    const bool bloom = post && r->S.mode == SO_MODE_VISIBLE && post->bloom > 0.f;
+    const bool blur = post && r->S.mode == SO_MODE_RADIO && post->blur_sigma_px > 0.5;
+    if (bloom || blur) {
+        if (int prc = ensure_post(r)) return prc;
+        cudaError_t e = bloom ? post_bloom(r->lev, post->bloom, r->st) : post_radio_blur(r->lev, r->d_tmp, post->blur_sigma_px, r->st);
+        if (e != cudaSuccess) return cuda_fail(r, e, "post filters");
+    }
     out->W = f.W;
     out->H = f.H;
     SO_CK(r, cudaMemcpyAsync(out->px, r->d_img, (size_t)r->npix * sizeof(float4), cudaMemcpyDeviceToHost, r->st));

@@ -182,13 +182,21 @@ def ref_pass1(scene, frame, threads=8):
     return acc, lim.value
 
 
-def mlp():
-    """oracle/so_mlp.py: the float64 restatement of the ray surrogate network."""
+def _module(name, fname):
     import importlib.util
-    name = "so_mlp_oracle"
     if name not in sys.modules:
-        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "oracle", "so_mlp.py"))
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "oracle", fname))
         mod = importlib.util.module_from_spec(spec)
         sys.modules[name] = mod
         spec.loader.exec_module(mod)
     return sys.modules[name]
+
+
+def mlp():
+    """oracle/so_mlp.py: the float64 restatement of the ray surrogate network."""
+    return _module("so_mlp_oracle", "so_mlp.py")
+
+
+def post():
+    """oracle/so_post.py: the pyramid post filters (bloom, radio beam)."""
+    return _module("so_post_oracle", "so_post.py")

@@ -226,8 +226,8 @@ def test_status_codes_on_gpu(so):
     L = so.lib()
     out = np.zeros((256, 256, 4), np.float32)
     hdr = so.abi.HdrFrame(256, 256, out.ctypes.data_as(C.POINTER(C.c_float)), 0, 0)
-    post = so.abi.Post(0.5, 0.0, 0.0)
-    assert L.so_render(r.h, C.byref(f), C.byref(post), 0.5, C.byref(hdr), None) == so.abi.SO_ERR_UNSUPPORTED
+    post = so.abi.Post(1.5, 0.0, 0.0)  # bloom strength outside [0, 1]
+    assert L.so_render(r.h, C.byref(f), C.byref(post), 0.5, C.byref(hdr), None) == so.abi.SO_ERR_ARG
     jy = C.c_double()
     assert L.so_radio_flux(r.h, C.byref(f), 300, 1.0, C.byref(jy)) == so.abi.SO_ERR_SIZE
     assert b"frame buffers" in L.so_last_error(r.h)
