@@ -299,7 +299,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         if (r->S.disk_on) rsw = std::max(rsw, 1.2 * r->S.disk_rout);
     }
     L.r_switch = rsw;
-    L.tol_approach = r->mixed.tol_approach > 0.0 ? r->mixed.tol_approach : r->S.tol;
+    L.tol_approach = r->mixed.tol_approach > 0.0 ? r->mixed.tol_approach : 10.0 * r->S.tol;
     L.t32_min_blocks = r->mixed.t32_blocks > 0 ? r->mixed.t32_blocks : 4;
     // outgoing rays beyond every emitter cannot come back: the FP32 tracer ends them as escaped
     double r_emit = 0.0;
