@@ -370,8 +370,8 @@ int so_sur_infer(so_surrogate* s, const so_sur_ray* d_rays, long long n, float* 
 /* Training set from the FP64 integrator of renderer r: `groups` (spin, inclination) pairs drawn
  * uniformly from the ranges, n / groups rays each with alpha, beta uniform in [-xy_max, xy_max],
  * traced in vacuum from a static camera at f->r.  Stored interleaved (ray j of group g at
- * j * groups + g) so that consecutive rays come from different groups.  The renderer's scene is
- * restored afterwards. */
+ * j * groups + g) so that consecutive rays come from different groups; all groups are traced by
+ * one persistent launch.  The renderer's own scene and frame are left as they are. */
 typedef struct so_sur_ranges { double a_min, a_max, incl_min, incl_max, xy_max; } so_sur_ranges;
 int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, uint32_t seed,
                    const so_sur_ranges* ranges, so_sur_ray* d_rays, so_sur_target* d_tgt, so_stats* stats);

@@ -278,50 +278,53 @@ __device__ __forceinline__ float unit_rand(uint32_t seed, uint32_t a, uint32_t b
     return (float)(h >> 8) * (1.0f / 16777216.0f);
 }
 
-__global__ void k_sample(int g, int groups, int per_group, uint32_t seed, double xy_max, float a, float incl,
-                         double r_cam, double* __restrict__ x, double* __restrict__ y, so_sur_ray* __restrict__ rays) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= per_group) return;
-    const double al = (2.0 * unit_rand(seed, (uint32_t)g, (uint32_t)(2 * j)) - 1.0) * xy_max;
-    const double be = (2.0 * unit_rand(seed, (uint32_t)g, (uint32_t)(2 * j + 1)) - 1.0) * xy_max;
-    x[j] = al / r_cam;
-    y[j] = be / r_cam;
-    so_sur_ray r;
-    r.alpha = (float)al;
-    r.beta = (float)be;
-    r.spin = a;
-    r.incl_deg = incl;
-    rays[(long)j * groups + g] = r;
+__global__ void k_sample(long long n, int groups, uint32_t seed, double xy_max, const float* __restrict__ spin,
+                         const float* __restrict__ incl, double r_cam, double* __restrict__ x,
+                         double* __restrict__ y, so_sur_ray* __restrict__ rays) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(i % groups);
+        const uint32_t j = (uint32_t)(i / groups);
+        const double al = (2.0 * unit_rand(seed, (uint32_t)g, 2 * j) - 1.0) * xy_max;
+        const double be = (2.0 * unit_rand(seed, (uint32_t)g, 2 * j + 1) - 1.0) * xy_max;
+        x[i] = al / r_cam;
+        y[i] = be / r_cam;
+        so_sur_ray r;
+        r.alpha = (float)al;
+        r.beta = (float)be;
+        r.spin = spin[g];
+        r.incl_deg = incl[g];
+        rays[i] = r;
+    }
 }
 
-__global__ void k_targets(int g, int groups, int per_group, double r_stop, const int8_t* __restrict__ fate,
+__global__ void k_targets(long long n, int groups, const double* __restrict__ r_stop, const int8_t* __restrict__ fate,
                           const double* __restrict__ th, const double* __restrict__ ph, const double* __restrict__ cr,
                           const double* __restrict__ cg, so_sur_target* __restrict__ tgt) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= per_group) return;
-    so_sur_target t;
-    const int f = fate[j];
-    t.cls = f == SO_FATE_ESCAPED ? 0.f : f == SO_FATE_CAPTURED ? 1.f : 2.f;
-    if (f == SO_FATE_ESCAPED) {
-        double s, c, sp, cp;
-        sincos(th[j], &s, &c);
-        sincos(ph[j], &sp, &cp);
-        t.dir[0] = (float)(s * cp);
-        t.dir[1] = (float)(s * sp);
-        t.dir[2] = (float)c;
-    } else {
-        t.dir[0] = t.dir[1] = t.dir[2] = 0.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        so_sur_target t;
+        const int f = fate[i];
+        t.cls = f == SO_FATE_ESCAPED ? 0.f : f == SO_FATE_CAPTURED ? 1.f : 2.f;
+        if (f == SO_FATE_ESCAPED) {
+            double s, c, sp, cp;
+            sincos(th[i], &s, &c);
+            sincos(ph[i], &sp, &cp);
+            t.dir[0] = (float)(s * cp);
+            t.dir[1] = (float)(s * sp);
+            t.dir[2] = (float)c;
+        } else {
+            t.dir[0] = t.dir[1] = t.dir[2] = 0.f;
+        }
+        // A crossing that does not happen lies at infinity for a ray that escapes and at the stopping
+        // radius for one that is captured: the target then moves continuously as a crossing appears.
+        const float u_none = f == SO_FATE_CAPTURED ? (float)(1.0 / r_stop[i % groups]) : 0.f;
+        for (int k = 0; k < 3; ++k) {
+            const double r = cr[3 * i + k];
+            t.u[k] = r > 0.0 ? (float)(1.0 / r) : u_none;
+            t.g[k] = r > 0.0 ? (float)cg[3 * i + k] : -1.f;
+        }
+        t.pad[0] = t.pad[1] = 0.f;
+        tgt[i] = t;
     }
-    // A crossing that does not happen lies at infinity for a ray that escapes and at the stopping
-    // radius for one that is captured: the target then moves continuously as a crossing appears.
-    const float u_none = f == SO_FATE_CAPTURED ? (float)(1.0 / r_stop) : 0.f;
-    for (int k = 0; k < 3; ++k) {
-        const double r = cr[3 * (long)j + k];
-        t.u[k] = r > 0.0 ? (float)(1.0 / r) : u_none;
-        t.g[k] = r > 0.0 ? (float)cg[3 * (long)j + k] : -1.f;
-    }
-    t.pad[0] = t.pad[1] = 0.f;
-    tgt[(long)j * groups + g] = t;
 }
 
 // ---- surrogate frame ---------------------------------------------------------------------------
@@ -494,14 +497,14 @@ __global__ void k_scatter(const uint32_t* __restrict__ list_b, int nb, const uin
 
 }  // namespace
 
-void launch_sample(int g, int groups, int per_group, uint32_t seed, double xy_max, float a, float incl, double r_cam,
-                   double* x, double* y, so_sur_ray* rays, cudaStream_t st) {
-    k_sample<<<(per_group + 255) / 256, 256, 0, st>>>(g, groups, per_group, seed, xy_max, a, incl, r_cam, x, y, rays);
+void launch_sample(long long n, int groups, uint32_t seed, double xy_max, const float* spin, const float* incl,
+                   double r_cam, double* x, double* y, so_sur_ray* rays, cudaStream_t st) {
+    k_sample<<<1184, 256, 0, st>>>(n, groups, seed, xy_max, spin, incl, r_cam, x, y, rays);
 }
 
-void launch_targets(int g, int groups, int per_group, double r_stop, const int8_t* fate, const double* th,
+void launch_targets(long long n, int groups, const double* r_stop, const int8_t* fate, const double* th,
                     const double* ph, const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st) {
-    k_targets<<<(per_group + 255) / 256, 256, 0, st>>>(g, groups, per_group, r_stop, fate, th, ph, cr, cg, tgt);
+    k_targets<<<1184, 256, 0, st>>>(n, groups, r_stop, fate, th, ph, cr, cg, tgt);
 }
 
 void launch_route(const Route& R, int num_sms, cudaStream_t st) { k_route<<<num_sms * 8, 256, 0, st>>>(R); }

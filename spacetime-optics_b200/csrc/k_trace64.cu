@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
                     sample = 0;
                     double x, yv;
                     if (L.kind == RAYS_LIST) {
-                        fidx = 0;
+                        fidx = L.list_frames > 0 ? (int)(job % L.list_frames) : 0;
                         x = L.x[job];
                         yv = L.y[job];
                         jobs_n = 1;

@@ -86,6 +86,7 @@ struct TraceLaunch {
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
     // batched frames (RAYS_PIXELS over nframes)
     int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
+    int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
     int ctas_per_sm;          // persistent grid: CTAs per SM (0 = as many as fit)
     int emit32;               // FP64 tracer: torus turbulence sums in FP32 (geometry stays FP64)
     const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi

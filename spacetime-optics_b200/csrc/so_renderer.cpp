@@ -609,6 +609,34 @@ int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y,
     return SO_OK;
 }
 
+int rend_trace_list_frames(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out,
+                           int vacuum, const so_scene* d_scenes, const so_frame* d_frames, const int* d_frame_scene,
+                           int nframes) {
+    if (n <= 0) return SO_OK;
+    if (nframes <= 0 || !d_scenes || !d_frames || !d_frame_scene) return fail(r, SO_ERR_ARG, "trace list: frames");
+    SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    TraceLaunch L;
+    launch_common(r, L);
+    L.scenes = d_scenes;
+    L.frames = d_frames;
+    L.frame_scene = d_frame_scene;
+    L.nframes = nframes;
+    L.list_frames = nframes;
+    L.kind = RAYS_LIST;
+    L.nrays = n;
+    L.x = d_x;
+    L.y = d_y;
+    L.out = d_out;
+    L.record_cross = d_out.cross_r != nullptr && d_out.cross_g != nullptr;
+    if (!L.record_cross) {
+        L.out.cross_r = nullptr;
+        L.out.cross_g = nullptr;
+    }
+    cudaError_t e = launch_trace64(L, vacuum ? VAR_VACUUM : variant_of(r->S), r->num_sms, r->st);
+    if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
+
 int rend_join_side(so_renderer* r) {
     if (!r->st2) return SO_OK;
     SO_CK(r, cudaEventRecord(r->ev_join, r->st2));

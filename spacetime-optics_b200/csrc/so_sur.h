@@ -44,9 +44,12 @@ struct Audit {
     double* acc;
 };
 
-void launch_sample(int g, int groups, int per_group, uint32_t seed, double xy_max, float a, float incl, double r_cam,
-                   double* x, double* y, so_sur_ray* rays, cudaStream_t st);
-void launch_targets(int g, int groups, int per_group, double r_stop, const int8_t* fate, const double* th,
+// Training rays: ray i belongs to group g = i % groups (spin spin[g], inclination incl[g] degrees,
+// camera at r_cam); alpha, beta uniform in [-xy_max, xy_max] from the seed.
+void launch_sample(long long n, int groups, uint32_t seed, double xy_max, const float* spin, const float* incl,
+                   double r_cam, double* x, double* y, so_sur_ray* rays, cudaStream_t st);
+// Targets from the integrator's records of those rays (r_stop[g]: the group's stopping radius).
+void launch_targets(long long n, int groups, const double* r_stop, const int8_t* fate, const double* th,
                     const double* ph, const double* cr, const double* cg, so_sur_target* tgt, cudaStream_t st);
 void launch_route(const Route& R, int num_sms, cudaStream_t st);
 void launch_xy(const so_frame* F, int W, int H, const uint32_t* list_b, int nb, const uint32_t* list_a, int na, double* x,
@@ -80,6 +83,11 @@ int rend_upload_frame(so_renderer* r, const so_frame& f, const so_frame** d_fram
 // own queue head).  Does not synchronise.
 int rend_trace_list(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out, int vacuum,
                     int side = 0);
+// The same over many frames in one launch: ray i uses frame i % nframes of the device arrays
+// d_frames / d_scenes (through d_frame_scene).
+int rend_trace_list_frames(so_renderer* r, int n, const double* d_x, const double* d_y, const so_rays_out& d_out,
+                           int vacuum, const so_scene* d_scenes, const so_frame* d_frames, const int* d_frame_scene,
+                           int nframes);
 // Orders the renderer's stream after everything queued on its second stream.
 int rend_join_side(so_renderer* r);
 

@@ -528,48 +528,24 @@ int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, u
                    so_sur_ray* d_rays, so_sur_target* d_tgt, so_stats* stats) {
     if (!r || !f || !rg || !d_rays || !d_tgt || groups <= 0 || n <= 0 || n % groups)
         return r ? rend_fail(r, SO_ERR_ARG, "so_sur_dataset: bad arguments (n must be a multiple of groups)") : SO_ERR_ARG;
-    const long long per = n / groups;
-    if (per > (1ll << 30)) return rend_fail(r, SO_ERR_SIZE, "so_sur_dataset: too many rays per group");
+    if (n > 0x7fffffffll) return rend_fail(r, SO_ERR_SIZE, "so_sur_dataset: more than 2^31 rays");
     if (cudaSetDevice(rend_device(r)) != cudaSuccess) return rend_fail(r, SO_ERR_CUDA, "cudaSetDevice");
     cudaStream_t st = rend_stream(r);
-    const so_scene S0 = rend_scene(r);
-    double *x = nullptr, *y = nullptr, *th = nullptr, *ph = nullptr, *cr = nullptr, *cg = nullptr;
-    int8_t* fate = nullptr;
-    int32_t *nacc = nullptr, *natt = nullptr;
-    auto cleanup = [&]() {
-        void* ps[] = {x, y, th, ph, cr, cg, fate, nacc, natt};
-        for (void* p : ps)
-            if (p) cudaFree(p);
-    };
-    if (dalloc(&x, per) || dalloc(&y, per) || dalloc(&th, per) || dalloc(&ph, per) || dalloc(&cr, 3 * per) ||
-        dalloc(&cg, 3 * per) || dalloc(&fate, per) || dalloc(&nacc, per) || dalloc(&natt, per)) {
-        cleanup();
-        return rend_fail(r, SO_ERR_ALLOC, "so_sur_dataset: device allocation");
-    }
-    so_rays_out o;
-    std::memset(&o, 0, sizeof o);
-    o.fate = fate;
-    o.theta = th;
-    o.phi = ph;
-    o.cross_r = cr;
-    o.cross_g = cg;
-    o.n_accepted = nacc;
-    o.n_attempts = natt;
+    const so_scene S0 = rend_scene(r);  // host copy; its table pointers are the renderer's device tables
+    // one scene and one camera frame per (spin, inclination) group
+    std::vector<so_scene> scenes((size_t)groups);
+    std::vector<so_frame> frames((size_t)groups);
+    std::vector<int> fscene((size_t)groups);
+    std::vector<float> spin((size_t)groups), incl((size_t)groups);
+    std::vector<double> r_stop((size_t)groups);
     Rng rng(((uint64_t)seed << 1) | 1u);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
-    int rc = SO_OK;
-    for (int g = 0; g < groups && !rc; ++g) {
+    for (int g = 0; g < groups; ++g) {
         const double a = rg->a_min + (rg->a_max - rg->a_min) * rng.uniform();
-        const double incl = rg->incl_min + (rg->incl_max - rg->incl_min) * rng.uniform();
+        const double i_deg = rg->incl_min + (rg->incl_max - rg->incl_min) * rng.uniform();
         so_scene S = S0;
         scene_set_spin(&S, a);
-        rc = so_update_scene(r, &S);
-        if (rc) break;
         so_frame F = *f;
-        F.th = incl * PI_D / 180.0;
+        F.th = i_deg * PI_D / 180.0;
         F.ph = 0.0;
         F.t = 0.0;
         kerr_point(S.a, F.r, F.th, &F.kp);
@@ -578,15 +554,58 @@ int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, u
         F.R = so_vec3{0, 0, 1};
         F.beta = so_vec3{0, 0, 0};
         F.cx = F.cy = 0.0;
-        const so_frame* dF = nullptr;
-        rc = rend_upload_frame(r, F, &dF);
-        if (rc) break;
-        sur::launch_sample(g, groups, (int)per, seed, rg->xy_max, (float)S.a, (float)incl, F.r, x, y, d_rays, st);
-        rc = rend_trace_list(r, (int)per, x, y, o, 1);
-        if (rc) break;
-        sur::launch_targets(g, groups, (int)per, S.r_stop, fate, th, ph, cr, cg, d_tgt, st);
-        if (cudaGetLastError() != cudaSuccess) rc = rend_fail(r, SO_ERR_CUDA, "so_sur_dataset: kernel launch");
+        scenes[g] = S;
+        frames[g] = F;
+        fscene[g] = g;
+        spin[g] = (float)S.a;
+        incl[g] = (float)i_deg;
+        r_stop[g] = S.r_stop;
     }
+    double *x = nullptr, *y = nullptr, *th = nullptr, *ph = nullptr, *cr = nullptr, *cg = nullptr, *d_rstop = nullptr;
+    int8_t* fate = nullptr;
+    so_scene* d_scenes = nullptr;
+    so_frame* d_frames = nullptr;
+    int* d_fscene = nullptr;
+    float *d_spin = nullptr, *d_incl = nullptr;
+    auto cleanup = [&]() {
+        void* ps[] = {x, y, th, ph, cr, cg, d_rstop, fate, d_scenes, d_frames, d_fscene, d_spin, d_incl};
+        for (void* p : ps)
+            if (p) cudaFree(p);
+    };
+    const size_t N = (size_t)n, G = (size_t)groups;
+    if (dalloc(&x, N) || dalloc(&y, N) || dalloc(&th, N) || dalloc(&ph, N) || dalloc(&cr, 3 * N) || dalloc(&cg, 3 * N) ||
+        dalloc(&fate, N) || dalloc(&d_scenes, G) || dalloc(&d_frames, G) || dalloc(&d_fscene, G) || dalloc(&d_spin, G) ||
+        dalloc(&d_incl, G) || dalloc(&d_rstop, G)) {
+        cleanup();
+        return rend_fail(r, SO_ERR_ALLOC, "so_sur_dataset: device allocation");
+    }
+    int rc = SO_OK;
+    auto up = [&](void* d, const void* h, size_t bytes) {
+        if (!rc && cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            rc = rend_fail(r, SO_ERR_CUDA, "so_sur_dataset: upload");
+    };
+    up(d_scenes, scenes.data(), G * sizeof(so_scene));
+    up(d_frames, frames.data(), G * sizeof(so_frame));
+    up(d_fscene, fscene.data(), G * sizeof(int));
+    up(d_spin, spin.data(), G * sizeof(float));
+    up(d_incl, incl.data(), G * sizeof(float));
+    up(d_rstop, r_stop.data(), G * sizeof(double));
+    so_rays_out o;
+    std::memset(&o, 0, sizeof o);
+    o.fate = fate;
+    o.theta = th;
+    o.phi = ph;
+    o.cross_r = cr;
+    o.cross_g = cg;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    if (!rc) sur::launch_sample(n, groups, seed, rg->xy_max, d_spin, d_incl, f->r, x, y, d_rays, st);
+    // every group in one persistent launch: ray i uses frame / scene i % groups
+    if (!rc) rc = rend_trace_list_frames(r, (int)n, x, y, o, 1, d_scenes, d_frames, d_fscene, groups);
+    if (!rc) sur::launch_targets(n, groups, d_rstop, fate, th, ph, cr, cg, d_tgt, st);
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = rend_fail(r, SO_ERR_CUDA, "so_sur_dataset: kernel launch");
     cudaEventRecord(e1, st);
     if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = rend_fail(r, SO_ERR_CUDA, "so_sur_dataset: trace");
     float ms = 0.f;
@@ -594,9 +613,6 @@ int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, u
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cleanup();
-    so_scene Sr = S0;
-    int rc2 = so_update_scene(r, &Sr);
-    if (!rc) rc = rc2;
     if (!rc && stats) {
         std::memset(stats, 0, sizeof *stats);
         stats->ms_trace = ms;
