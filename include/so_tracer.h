@@ -367,6 +367,11 @@ int so_sur_gradients(so_surrogate* s, const so_sur_ray* d_rays, const so_sur_tar
 /* Network outputs for n rays: d_out, n x SO_SUR_LDOUT floats.  Queued on `stream` (NULL = the
  * surrogate's own stream); the call returns once the work is queued. */
 int so_sur_infer(so_surrogate* s, const so_sur_ray* d_rays, long long n, float* d_out, void* stream);
+/* Form of the fused inference kernel: 1 CTA per SM (default; a 256-ray tile as two M=128 MMA
+ * halves) or 2 (cluster pairs issuing cta_group::2 MMAs of M=256, each SM streaming half of every
+ * weight chunk; measured slower on B200).  Both compute the same outputs to FP32 rounding; a
+ * refused cluster launch falls back to 1. */
+int so_sur_set_infer_ctas(so_surrogate* s, int ctas);
 /* Training set from the FP64 integrator of renderer r: `groups` (spin, inclination) pairs drawn
  * uniformly from the ranges, n / groups rays each with alpha, beta uniform in [-xy_max, xy_max],
  * traced in vacuum from a static camera at f->r.  Stored interleaved (ray j of group g at

@@ -88,6 +88,7 @@ def lib():
         L.so_sur_evaluate.argtypes = [vp, vp, vp, C.c_longlong, P(abi.SurLoss)]
         L.so_sur_gradients.argtypes = [vp, vp, vp, C.c_int, vp, P(abi.SurLoss)]
         L.so_sur_infer.argtypes = [vp, vp, C.c_longlong, vp, vp]
+        L.so_sur_set_infer_ctas.argtypes = [vp, C.c_int]
         L.so_sur_dataset.argtypes = [vp, P(Frame), C.c_longlong, C.c_int, C.c_uint32, P(abi.SurRanges), vp, vp,
                                      P(Stats)]
         L.so_sur_render.argtypes = [vp, vp, P(Frame), P(abi.SurFrameOpts), vp, P(abi.SurReport)]
@@ -407,6 +408,10 @@ class Surrogate:
         st = torch.cuda.current_stream(rays.device).cuda_stream
         _check(lib().so_sur_infer(self.h, rays.data_ptr(), rays.shape[0], out.data_ptr(), C.c_void_p(st)))
         return out
+
+    def set_infer_ctas(self, ctas):
+        """Fused inference kernel form: 1 CTA per tile (default) or 2 (cta_group::2 cluster pairs)."""
+        _check(lib().so_sur_set_infer_ctas(self.h, ctas))
 
     def render(self, renderer, frame, band_m=0.5, audit_frac=0.01, audit_seed=2, out=None):
         """Surrogate thin-disk frame into out (torch [H, W, 4] float32 on the device) and its report."""

@@ -185,6 +185,6 @@ EXPORTS = [
     "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",
     "so_kerr_point_at", "so_critical_curve_point",
     "so_sur_default_opts", "so_sur_create", "so_sur_destroy", "so_sur_get_params", "so_sur_set_params",
-    "so_sur_train", "so_sur_evaluate", "so_sur_gradients", "so_sur_infer", "so_sur_dataset", "so_sur_render",
+    "so_sur_train", "so_sur_evaluate", "so_sur_gradients", "so_sur_infer", "so_sur_set_infer_ctas", "so_sur_dataset", "so_sur_render",
     "so_sur_gemm", "so_last_fates",
 ]

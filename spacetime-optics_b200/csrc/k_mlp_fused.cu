@@ -417,6 +417,332 @@ __global__ void __launch_bounds__(NTHR, 1) k_mlp_fused(const FusedArgs a) {
     }
 }
 
+// ==== 2-SM form (cta_group::2) ==================================================================
+// A cluster of two CTAs on two SMs runs pairs of 256-ray tiles T0, T1; each CTA holds its 128 rays
+// of both tiles (activations 2 x 64 KB) and its half of every weight chunk (N/2 weight rows).  One
+// tcgen05.mma.cta_group::2 (M = 256, N = 256, K = 16), issued by the leader CTA, multiplies both
+// CTAs' rows by both halves of the weights; each CTA's TMEM receives its own rows (all 256
+// columns).  Per SM that is 8 KB of shared-memory operands per 128 tensor cycles, half of the 1-SM
+// form's share.  The tiles alternate on the tensor core, layer by layer (T0 layer l, T1 layer l,
+// T0 layer l+1, ...), so each tile's epilogue runs while the other tile's MMAs do, and each weight
+// chunk serves both tiles before its buffer is refilled.
+//
+// Cross-CTA hand-offs (bounded polls everywhere):
+//   weights   each CTA bulk-copies its half-chunk into its own ring slot; the leader's `full`
+//             barrier counts its own transaction bytes plus one arrival that the second CTA's
+//             control thread forwards (remote mbarrier arrive) once its half has landed;
+//   buffers   the leader's commit after a chunk's last use (tile T1) arrives on `empty` in both CTAs;
+//   MMA done  the commit after a tile's last chunk arrives on `acc` in both CTAs;
+//   epilogue  each CTA's 512 epilogue threads arrive on its local `epi_done`; the second CTA's
+//             control thread forwards each completion to the leader's `epi_pair`.
+constexpr int F2_RAYS = 512;   // rays per pair iteration (2 tiles x 256, 128 per CTA per tile)
+constexpr int F2_NBUF = 6;     // weight ring slots of 16 KB
+constexpr int F2_SLOT = 128 * CHUNK_K * 2;
+constexpr int F2_SMEM = 2 * ACT_HALF + F2_NBUF * F2_SLOT;
+constexpr int F2_CHUNKS = 2 + 3 * 4 + 4;  // weight chunks per iteration (K = 64 slices)
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void remote_arrive(uint64_t* bar, uint32_t rank) {
+    asm volatile(
+        "{\n\t.reg .b32 ra;\n\t"
+        "mapa.shared::cluster.u32 ra, %0, %1;\n\t"
+        "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}\n" ::"r"(smem_u32(bar)),
+        "r"(rank)
+        : "memory");
+}
+// Non-blocking phase tests for the control threads' polling loops (try_wait may suspend the thread
+// for a while, which would hold up the other events it serves).
+__device__ __forceinline__ bool bar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.test_wait.parity.acquire.cta.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_test_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void mma2_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z), "r"(z),
+          "r"(z));
+}
+__device__ __forceinline__ void commit2_both(uint64_t* bar) {
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.aligned;\n\tbarrier.cluster.wait.aligned;" ::: "memory");
+}
+
+// Chunk c (K slice of 64) of layer l within an iteration: its index in the iteration's stream.
+__device__ __forceinline__ int f2_chunk_index(int l, int c) { return l == 0 ? c : 2 + (l - 1) * 4 + c; }
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NTHR, 1) k_mlp_fused2(const FusedArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t full[F2_NBUF], empty[F2_NBUF], acc[2], epi_done[2], epi_pair[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+    __shared__ __half2 bias2[NHID][HID / 2];
+    uint8_t* act = smem;                   // tiles T0, T1: this CTA's 128 rows each
+    uint8_t* wbuf = smem + 2 * ACT_HALF;   // F2_NBUF half-chunks
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = cluster_rank();
+    const int cluster = blockIdx.x >> 1, nclusters = gridDim.x >> 1;
+    const long long iters = (a.n + F2_RAYS - 1) / F2_RAYS;
+    const int my_iters = cluster < iters ? (int)((iters - 1 - cluster) / nclusters + 1) : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int b = 0; b < F2_NBUF; ++b) {
+            bar_init(&full[b], rank == 0 ? 2 : 1);
+            bar_init(&empty[b], 1);
+        }
+        for (int t = 0; t < 2; ++t) {
+            bar_init(&acc[t], 1);
+            bar_init(&epi_done[t], NEPI);
+            bar_init(&epi_pair[t], 1);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < NHID * HID / 2; i += NTHR) {
+        const int l = i / (HID / 2), c = i % (HID / 2);
+        const float* b = a.params + a.bias_off[l] + 2 * c;
+        bias2[l][c] = __floats2half2_rn(b[0], b[1]);
+    }
+    fence_before();
+    __syncthreads();
+    cluster_sync();  // both CTAs' barriers exist before any remote arrive
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == NEPI / 32) {
+        if (lane == 0) {
+            // ---- control thread: weight loads of this CTA's halves; MMAs (leader) or forwarding ----
+            const long long total = (long long)my_iters * F2_CHUNKS;
+            const long long total_steps = (long long)my_iters * 2 * F2_CHUNKS;  // each chunk serves T0 and T1
+            long long issued = 0, step = 0, fwd = 0;
+            long long efwd[2] = {0, 0}, ecnt[2] = {0, 0};
+            const long long total_epi = (long long)my_iters * NLAYER;
+            bool ok = true;
+            const uint64_t wdesc = smem_desc(smem_u32(wbuf), 128, CHUNK_K * 16);
+            const uint64_t adesc128 = smem_desc(smem_u32(act), 128, NFEAT * 16);
+            const uint64_t adesc256 = smem_desc(smem_u32(act), 128, HID * 16);
+            // deadline on the SM clock (cheap to read, unlike %globaltimer): ~2 s without progress
+            long long t_last = clock64();
+            for (;;) {
+                bool progress = false;
+                // 1. next weight load into its ring slot once the slot's previous chunk is released
+                if (issued < total) {
+                    const int b = (int)(issued % F2_NBUF);
+                    if (issued < F2_NBUF || bar_test(&empty[b], (uint32_t)(((issued / F2_NBUF) - 1) & 1))) {
+                        const FusedChunk& c = a.chunks[2 * (issued % F2_CHUNKS) + rank];
+                        bar_expect_tx(&full[b], (uint32_t)c.bytes);
+                        bulk_g2s(wbuf + b * F2_SLOT, a.wpack + c.offset, (uint32_t)c.bytes, &full[b]);
+                        ++issued;
+                        progress = true;
+                    }
+                }
+                if (rank == 0) {
+                    // 2. next MMA step: iteration, layer, tile, chunk in the schedule's order
+                    if (step < total_steps) {
+                        const long long it = step / (2 * F2_CHUNKS);
+                        int r = (int)(step % (2 * F2_CHUNKS));
+                        int l = 0, c = 0, T = 0;
+                        for (l = 0; l < NLAYER; ++l) {  // per layer: T0's chunks, then T1's
+                            const int kc = (l == 0 ? NFEAT : HID) / CHUNK_K;
+                            if (r < 2 * kc) {
+                                T = r / kc;
+                                c = r % kc;
+                                break;
+                            }
+                            r -= 2 * kc;
+                        }
+                        const long long q = it * F2_CHUNKS + f2_chunk_index(l, c);
+                        const int b = (int)(q % F2_NBUF);
+                        bool ready = true;
+                        if (c == 0)  // the tile's input (features or the previous epilogue) in both CTAs
+                            ready = bar_test(&epi_done[T], (uint32_t)(ecnt[T] & 1)) &&
+                                    bar_test_cluster(&epi_pair[T], (uint32_t)(ecnt[T] & 1));
+                        ready = ready && bar_test_cluster(&full[b], (uint32_t)((q / F2_NBUF) & 1));
+                        if (ready) {
+                            if (c == 0) ++ecnt[T];
+                            fence_after();
+                            const bool head = l == NHID;
+                            const int K = l == 0 ? NFEAT : HID;
+                            const uint32_t idesc = idesc_bf16(256, head ? LDO : HID);
+                            const uint64_t ad = (K == NFEAT ? adesc128 : adesc256) + (uint64_t)(T * (ACT_HALF >> 4)) +
+                                                (uint64_t)(c * CHUNK_K);
+                            const uint64_t bd = wdesc + (uint64_t)(b * (F2_SLOT >> 4));
+#pragma unroll
+                            for (int j = 0; j < CHUNK_K / 16; ++j)
+                                mma2_bf16(tmem + T * 256, ad + j * 16, bd + j * 16, idesc, (c > 0 || j > 0) ? 1u : 0u);
+                            if (T == 1) commit2_both(&empty[b]);        // chunk done with: release its slot
+                            if (c == K / CHUNK_K - 1) commit2_both(&acc[T]);  // the tile's layer is done
+                            ++step;
+                            progress = true;
+                        }
+                    }
+                } else {
+                    // 2'. forward this CTA's landed weight halves and finished epilogues to the leader
+                    if (fwd < issued && bar_test(&full[fwd % F2_NBUF], (uint32_t)((fwd / F2_NBUF) & 1))) {
+                        remote_arrive(&full[fwd % F2_NBUF], 0);
+                        ++fwd;
+                        progress = true;
+                    }
+                    for (int T = 0; T < 2; ++T)
+                        if (efwd[T] < total_epi && bar_test(&epi_done[T], (uint32_t)(efwd[T] & 1))) {
+                            remote_arrive(&epi_pair[T], 0);
+                            ++efwd[T];
+                            progress = true;
+                        }
+                }
+                const bool done = issued == total &&
+                                  (rank == 0 ? step == total_steps : (fwd == total && efwd[0] == total_epi && efwd[1] == total_epi));
+                if (done) break;
+                const long long t = clock64();
+                if (progress) t_last = t;
+                else if (abort_flag || t - t_last > 4000000000ll) {
+                    abort_flag = 1;
+                    ok = false;
+                    break;
+                }
+            }
+            if (!ok) {  // let copies in flight land before the CTA can exit
+                const unsigned long long t0 = now_ns();
+                while (now_ns() - t0 < 20000ull) {
+                }
+                if (a.err) atomicExch(a.err, SO_ERR_WATCHDOG);
+            }
+        }
+    } else {
+        // ---- features and epilogues: 16 warps.  Warp w serves TMEM lanes 32 (w % 4) .. + 31 of
+        // this CTA's 128 rows; for features it takes tile w / 8 and half the frequencies
+        // ((w / 4) % 2), for epilogues 64 of the 256 columns (w / 4) of the current tile.
+        const int q4 = warp & 3, cg = warp >> 2;
+        const int row = q4 * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(q4 * 32) << 16);
+        uint32_t acnt[2] = {0, 0};
+        bool ok = true;
+        auto wait_acc = [&](int T) -> bool {
+            if (!bar_wait(&acc[T], acnt[T] & 1, &abort_flag)) return false;
+            ++acnt[T];
+            fence_after();
+            return true;
+        };
+        for (int t = 0; t < my_iters && ok; ++t) {
+            const long long it = cluster + (long long)t * nclusters;
+            {   // features of both tiles
+                const int T = warp >> 3, half = (warp >> 2) & 1;
+                const long long ray = it * F2_RAYS + T * 256 + rank * 128 + row;
+                float x[4] = {0.f, 0.f, 0.f, 0.f};
+                if (ray < a.n) {
+                    const so_sur_ray r = a.rays[ray];
+                    x[0] = r.alpha * (1.f / XY_SCALE);
+                    x[1] = r.beta * (1.f / XY_SCALE);
+                    x[2] = (r.spin - A_MID) * (1.f / A_MID);
+                    x[3] = (r.incl_deg - I_MID) * (1.f / I_HALF);
+                }
+                uint8_t* my_act = act + T * ACT_HALF;
+                for (int j0 = half * 32; j0 < half * 32 + 32; j0 += 8) {
+                    __align__(16) bf16 sv[8], cv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float4 fj = __ldg(reinterpret_cast<const float4*>(a.freq) + j0 + q);
+                        const float turns = fmaf(fj.w, x[3], fmaf(fj.z, x[2], fmaf(fj.y, x[1], fj.x * x[0])));
+                        const float rr = 6.283185307179586f * (turns - rintf(turns));
+                        sv[q] = __float2bfloat16_rn(__sinf(rr));
+                        cv[q] = __float2bfloat16_rn(__cosf(rr));
+                    }
+                    *reinterpret_cast<uint4*>(my_act + canon(row, j0, NFEAT)) = *reinterpret_cast<const uint4*>(sv);
+                    *reinterpret_cast<uint4*>(my_act + canon(row, NFREQ + j0, NFEAT)) = *reinterpret_cast<const uint4*>(cv);
+                }
+            }
+            fence_async_smem();
+            bar_arrive(&epi_done[0]);
+            bar_arrive(&epi_done[1]);
+            for (int l = 0; l < NHID && ok; ++l) {
+                for (int T = 0; T < 2 && ok; ++T) {
+                    if (!wait_acc(T)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* my_act = act + T * ACT_HALF;
+                    const int c0 = cg * 64;
+                    uint32_t va[32], vb[32];
+                    tmem_ld32_async(lane_base + T * 256 + c0, va);
+                    tmem_wait32(va);
+                    tmem_ld32_async(lane_base + T * 256 + c0 + 32, vb);
+                    epilogue32(va, bias2[l], c0, my_act, row);
+                    tmem_wait32(vb);
+                    epilogue32(vb, bias2[l], c0 + 32, my_act, row);
+                    fence_before();
+                    fence_async_smem();
+                    bar_arrive(&epi_done[T]);
+                }
+            }
+            for (int T = 0; T < 2 && ok; ++T) {  // head
+                if (!wait_acc(T)) {
+                    ok = false;
+                    break;
+                }
+                float f[16];
+                tmem_ld16(lane_base + T * 256, f);
+                fence_before();
+                const long long ray = it * F2_RAYS + T * 256 + rank * 128 + row;
+                if (cg == 0 && ray < a.n) {
+                    float4* o = reinterpret_cast<float4*>(a.out + ray * LDO);
+                    const float4* b4 = reinterpret_cast<const float4*>(a.params + a.bias_off[NHID]);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float4 b = __ldg(b4 + i);
+                        o[i] = make_float4(f[4 * i] + b.x, f[4 * i + 1] + b.y, f[4 * i + 2] + b.z, f[4 * i + 3] + b.w);
+                    }
+                }
+            }
+        }
+        if (!ok && a.err && tid == 0) atomicExch(a.err, SO_ERR_WATCHDOG);
+    }
+    fence_before();
+    __syncthreads();
+    cluster_sync();  // the leader's last MMAs read this CTA's shared memory and write its TMEM
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+    }
+}
+
 // Pack the BF16 weights (row-major [N x K] per layer, flat layout) into the chunks of the table,
 // each a [rows x 64] tile in the canonical layout (row groups 1024 B apart, K core matrices 128 B
 // apart), in the order the kernel consumes them.
@@ -468,6 +794,39 @@ int fused_chunks(FusedChunk* chunks, long* pack_elems) {
     }
     *pack_elems = off / 2;
     return q > FUSED_MAX_CHUNKS ? -1 : q;
+}
+
+int fused2_chunks(FusedChunk* chunks, long* pack_elems) {
+    const Layout L = param_layout();
+    int q = 0;
+    long off = 0;
+    for (int l = 0; l < NLAYER; ++l) {
+        const int K = L.k[l], N = L.n[l];
+        for (int c = 0; c < K / CHUNK_K; ++c)
+            for (int h = 0; h < 2; ++h) {  // the two CTAs' halves of the weight rows
+                if (q >= FUSED_MAX_CHUNKS) return -1;
+                chunks[q].offset = off;
+                chunks[q].bytes = (N / 2) * CHUNK_K * 2;
+                chunks[q].layer = l;
+                chunks[q].row0 = h * (N / 2);
+                chunks[q].rows = N / 2;
+                chunks[q].k0 = c * CHUNK_K;
+                off += chunks[q].bytes;
+                ++q;
+            }
+    }
+    *pack_elems = off / 2;
+    return q;
+}
+
+int launch_mlp_fused2(const FusedArgs& a, int num_sms, cudaStream_t st) {
+    if (a.n <= 0) return SO_OK;
+    if (cudaFuncSetAttribute(k_mlp_fused2, cudaFuncAttributeMaxDynamicSharedMemorySize, F2_SMEM) != cudaSuccess)
+        return SO_ERR_CUDA;
+    const long long iters = (a.n + F2_RAYS - 1) / F2_RAYS;
+    const int clusters = (int)(iters < num_sms / 2 ? iters : num_sms / 2);
+    k_mlp_fused2<<<2 * clusters, NTHR, F2_SMEM, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? SO_OK : SO_ERR_CUDA;
 }
 
 void launch_pack_chunks(const bf16* W, const FusedArgs& a, bf16* wpack, cudaStream_t st) {

@@ -154,6 +154,10 @@ int fused_chunks(FusedChunk* chunks, long* pack_elems);
 void launch_pack_chunks(const bf16* W, const FusedArgs& a, bf16* wpack, cudaStream_t st);
 // Persistent launch, one CTA per SM (at most one per 256-ray tile).
 int launch_mlp_fused(const FusedArgs& a, int num_sms, cudaStream_t st);
+// The 2-SM form (clusters of two CTAs, tcgen05.mma.cta_group::2): its chunk table has the two
+// CTAs' halves of every chunk as consecutive entries.
+int fused2_chunks(FusedChunk* chunks, long* pack_elems);
+int launch_mlp_fused2(const FusedArgs& a, int num_sms, cudaStream_t st);
 
 }  // namespace mlp
 }  // namespace so

@@ -74,12 +74,14 @@ struct so_surrogate {
     bf16* D[mlp::NHID] = {};  // GELU derivatives of the hidden layers
     float *O = nullptr, *part = nullptr, *part_gb = nullptr;
     double* part_acc = nullptr;
-    // fused inference: packed weight chunks, rebuilt when the parameters change
-    bf16* d_wpack = nullptr;
-    long pack_elems = 0;
-    mlp::FusedChunk chunks[mlp::FUSED_MAX_CHUNKS];
-    int nchunks = 0, num_sms = 148;
-    long long version = 1, packed_version = 0;
+    // fused inference: packed weight chunks of the 2-SM form (and of the 1-SM form, used where a
+    // cluster launch is refused), rebuilt when the parameters change
+    bf16 *d_wpack = nullptr, *d_wpack1 = nullptr;
+    long pack_elems = 0, pack_elems1 = 0;
+    mlp::FusedChunk chunks[mlp::FUSED_MAX_CHUNKS], chunks1[mlp::FUSED_MAX_CHUNKS];
+    int nchunks = 0, nchunks1 = 0, num_sms = 148;
+    bool use2 = false;  // 2-SM (cta_group::2) form on request: measured slower than the 1-SM form
+    long long version = 1, packed_version = 0, packed_version1 = 0;
     // frame buffers for fcap pixels
     long long fcap = 0;
     uint32_t *list_s = nullptr, *list_b = nullptr, *list_a = nullptr, *audit_j = nullptr;
@@ -370,9 +372,11 @@ int so_sur_create(int device, const so_sur_opts* opts, so_surrogate** out) {
         return bad(SO_ERR_ALLOC, "so_sur_create: device allocation");
     for (auto& e : s->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return bad(SO_ERR_CUDA, "so_sur_create: events");
-    s->nchunks = mlp::fused_chunks(s->chunks, &s->pack_elems);
-    if (s->nchunks <= 0) return bad(SO_ERR_ARG, "so_sur_create: weight chunk table overflow");
-    if (dalloc(&s->d_wpack, (size_t)s->pack_elems)) return bad(SO_ERR_ALLOC, "so_sur_create: device allocation");
+    s->nchunks = mlp::fused2_chunks(s->chunks, &s->pack_elems);
+    s->nchunks1 = mlp::fused_chunks(s->chunks1, &s->pack_elems1);
+    if (s->nchunks <= 0 || s->nchunks1 <= 0) return bad(SO_ERR_ARG, "so_sur_create: weight chunk table overflow");
+    if (dalloc(&s->d_wpack, (size_t)s->pack_elems) || dalloc(&s->d_wpack1, (size_t)s->pack_elems1))
+        return bad(SO_ERR_ALLOC, "so_sur_create: device allocation");
     if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return bad(SO_ERR_CUDA, "so_sur_create: device attributes");
     // initial parameters: U(-1/sqrt(K), 1/sqrt(K)) for weights and biases; head rows 12-15 zero
@@ -402,7 +406,7 @@ void so_sur_destroy(so_surrogate* s) {
     if (s->st) cudaStreamSynchronize(s->st);
     free_train(s);
     free_frame(s);
-    void* ps[] = {s->d_p, s->d_g, s->d_m, s->d_v, s->d_freq, s->d_W, s->d_WT, s->d_err, s->d_acc, s->d_wpack};
+    void* ps[] = {s->d_p, s->d_g, s->d_m, s->d_v, s->d_freq, s->d_W, s->d_WT, s->d_err, s->d_acc, s->d_wpack, s->d_wpack1};
     for (void* p : ps)
         if (p) cudaFree(p);
     for (auto e : s->ev)
@@ -511,16 +515,35 @@ int so_sur_infer(so_surrogate* s, const so_sur_ray* d_rays, long long n, float* 
     a.params = s->d_p;
     for (int l = 0; l < mlp::NLAYER; ++l) a.bias_off[l] = s->L.b[l];
     a.freq = s->d_freq;
-    a.wpack = reinterpret_cast<const uint8_t*>(s->d_wpack);
-    for (int q = 0; q < s->nchunks; ++q) a.chunks[q] = s->chunks[q];
-    a.nchunks = s->nchunks;
     a.err = s->d_err;
-    if (s->packed_version != s->version) {
-        mlp::launch_pack_chunks(s->d_W, a, s->d_wpack, st);
+    if (s->use2) {  // 2-SM form
+        a.wpack = reinterpret_cast<const uint8_t*>(s->d_wpack);
+        for (int q = 0; q < s->nchunks; ++q) a.chunks[q] = s->chunks[q];
+        a.nchunks = s->nchunks;
+        if (s->packed_version != s->version) {
+            mlp::launch_pack_chunks(s->d_W, a, s->d_wpack, st);
+            SUR_CK(s, cudaGetLastError());
+            s->packed_version = s->version;
+        }
+        if (mlp::launch_mlp_fused2(a, s->num_sms, st) == SO_OK) return SO_OK;
+        cudaGetLastError();  // a refused cluster launch: use the 1-SM form from now on
+        s->use2 = false;
+    }
+    a.wpack = reinterpret_cast<const uint8_t*>(s->d_wpack1);
+    for (int q = 0; q < s->nchunks1; ++q) a.chunks[q] = s->chunks1[q];
+    a.nchunks = s->nchunks1;
+    if (s->packed_version1 != s->version) {
+        mlp::launch_pack_chunks(s->d_W, a, s->d_wpack1, st);
         SUR_CK(s, cudaGetLastError());
-        s->packed_version = s->version;
+        s->packed_version1 = s->version;
     }
     if (mlp::launch_mlp_fused(a, s->num_sms, st)) return fail(s, SO_ERR_CUDA, "so_sur_infer: launch");
+    return SO_OK;
+}
+
+int so_sur_set_infer_ctas(so_surrogate* s, int ctas) {
+    if (!s || (ctas != 1 && ctas != 2)) return s ? fail(s, SO_ERR_ARG, "so_sur_set_infer_ctas: 1 or 2") : SO_ERR_ARG;
+    s->use2 = ctas == 2;
     return SO_OK;
 }
 

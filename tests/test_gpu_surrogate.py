@@ -5,6 +5,7 @@
     oracle/so_mlp.py, per parameter block, with the oracle at the GPU's BF16 rounding points
     (relative L2 error <= 2e-2) and in plain float64 (<= 6e-2);
   * training on rays of the FP64 integrator lowers the held-out loss, deterministically;
+  * the 1-SM and the 2-SM (cta_group::2) fused inference kernels agree (relative max <= 1e-5);
   * the surrogate thin-disk frame: band pixels are the integrator's bit for bit, and the trained
     network's image error against the FP64 frame is a fraction of the untrained one's.
 """
@@ -170,6 +171,26 @@ def test_infer_matches_training_forward(so, orc):
     O, _ = orc.mlp().forward(p, freq, rays[:n].cpu().numpy(), rounding=True)
     err = np.abs(out[:, :12] - O[:, :12]).max() / np.abs(O[:, :12]).max()
     assert err < 2e-2, err
+    sur.close()
+    r.close()
+
+
+def test_infer_forms_agree(so, orc):
+    """The 2-SM (cta_group::2) fused kernel gives the 1-SM kernel's outputs; a ragged tail that
+    leaves the last cluster pair half empty included."""
+    sh, r, f = _disk(so)
+    sur = so.Surrogate(batch=1024, seed=5)
+    rays, tgt, _ = sur.dataset(r, f, 4096, 16, seed=9)
+    sur.train(rays, tgt, 5)
+    with pytest.raises(so.TracerError):
+        sur.set_infer_ctas(3)
+    for n in (4096, 3000, 200):
+        o1 = sur.infer(rays[:n]).cpu().numpy()
+        sur.set_infer_ctas(2)
+        o2 = sur.infer(rays[:n]).cpu().numpy()
+        sur.set_infer_ctas(1)
+        err = np.abs(o1[:, :12] - o2[:, :12]).max() / np.abs(o1[:, :12]).max()
+        assert err < 1e-5, (n, err)
     sur.close()
     r.close()
 
