@@ -222,6 +222,10 @@ typedef struct so_mixed_opts {
                               * far field carries no emission, and the synchrotron frame's image moves
                               * by 2e-5 L1 and keeps every class for it, at 7 % less frame time) */
     int t32_blocks;          /* FP32 tracer: resident 128-thread CTAs per SM, 4, 5 or 6 (0 = 4) */
+    int approach;            /* FP64 approach integrator: 0 = DP5(4) in the inverse radius 1/r on ingoing
+                              * legs without a radial turning point above r_switch (a few steps where
+                              * Mino time takes hundreds from a distant camera; other rays as 1),
+                              * 1 = the reference's Mino-time DP5(4) for every ray */
 } so_mixed_opts;
 
 /* ---- renderer lifecycle ---------------------------------------------------------------------- */
@@ -428,6 +432,15 @@ int so_shot_nframes(const so_shot* s);
 int so_shot_frame(const so_shot* s, int i, int W, uint32_t seed, so_frame* f);
 /* find_critical_point on frame i's camera along image direction psi (rad); rho in M. */
 int so_find_critical_point(const so_shot* s, int i, double a, double psi, double* rho);
+/* State (r, r', u, u', phi, t) of the backward ray through image-plane point (x, y) of frame f
+ * where it reaches radius r1 (< f->r), on the host (no device): method 0 = the mixed path's
+ * far-field transport (DP5(4) in the inverse radius 1/r, landing exactly on r1), 1 = the reference's
+ * Mino-time DP5(4) at tolerance tol, its last step shortened to stop within 1e-12 r1 above r1 (the
+ * state then has that radius).  *attempts (may be NULL) gets the DP5 attempts.  SO_ERR_ARG where the
+ * method does not apply (an outgoing ray, a radial turning point above r1; for method 0 also a
+ * turning point near r1).  No reference counterpart: a check of the approach integrators. */
+int so_approach_state(const so_scene* s, const so_frame* f, double x, double y, double r1, double tol, int method,
+                      double* state, int* attempts);
 /* Configuration value lookup (string form), for callers mirroring main.cpp's cfg.* reads. */
 int so_shot_get(const so_shot* s, const char* key, char* buf, int buflen);
 void so_shot_free(so_shot* s);

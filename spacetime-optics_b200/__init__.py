@@ -68,6 +68,8 @@ def lib():
         L.so_shot_nframes.argtypes = [vp]
         L.so_shot_frame.argtypes = [vp, C.c_int, C.c_int, C.c_uint32, P(Frame)]
         L.so_find_critical_point.argtypes = [vp, C.c_int, C.c_double, C.c_double, P(C.c_double)]
+        L.so_approach_state.argtypes = [P(Scene), P(Frame), C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        P(C.c_double), P(C.c_int)]
         L.so_shot_get.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.so_shot_free.argtypes = [vp]
         L.so_shot_free.restype = None
@@ -181,6 +183,15 @@ class Shot:
         return p
 
 
+def approach_state(scene, frame, x, y, r1, tol, method):
+    """so_approach_state: (state [r, r', u, u', phi, t], attempts) of the backward ray through image
+    point (x, y) at radius r1; method 0 = far-field transport in 1/r, 1 = Mino-time DP5(4)."""
+    st = (C.c_double * 6)()
+    att = C.c_int(0)
+    _check(lib().so_approach_state(C.byref(scene), C.byref(frame), x, y, r1, tol, method, st, C.byref(att)))
+    return np.array(st[:]), att.value
+
+
 def plasma_modes(p):
     """Fourier modes of a torus plasma (so_plasma_modes), as a ctypes array of Mode."""
     arr = (Mode * max(1, p.n_modes))()
@@ -229,8 +240,8 @@ class Renderer:
         return modes
 
     def set_precision(self, precision, band_m=0.05, tol32=3e-6, turn_r=0.0, drift_tol=1e-4, r_switch=0.0,
-                      tol_approach=0.0, t32_blocks=0):
-        o = MixedOpts(band_m, tol32, turn_r, drift_tol, r_switch, tol_approach, t32_blocks)
+                      tol_approach=0.0, t32_blocks=0, approach=0):
+        o = MixedOpts(band_m, tol32, turn_r, drift_tol, r_switch, tol_approach, t32_blocks, approach)
         _check(lib().so_set_precision(self.h, precision, C.byref(o)), self.h)
 
     def render(self, frame, percentile=0.995, hide_direct=0.0, out=None, bloom=0.0, blur_sigma_px=0.0):

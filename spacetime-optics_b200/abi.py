@@ -107,7 +107,8 @@ class Mode(C.Structure):
 
 class MixedOpts(C.Structure):
     _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_r", C.c_double), ("drift_tol", C.c_double),
-                ("r_switch", C.c_double), ("tol_approach", C.c_double), ("t32_blocks", C.c_int)]
+                ("r_switch", C.c_double), ("tol_approach", C.c_double), ("t32_blocks", C.c_int),
+                ("approach", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -182,7 +183,7 @@ EXPORTS = [
     "so_batch_create", "so_batch_render", "so_batch_autotune", "so_batch_set_tune", "so_batch_free",
     "so_set_precision", "so_set_plasma", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",
-    "so_find_critical_point", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",
+    "so_find_critical_point", "so_approach_state", "so_shot_get", "so_shot_free", "so_normalize_flux", "so_plasma_modes",
     "so_kerr_point_at", "so_critical_curve_point",
     "so_sur_default_opts", "so_sur_create", "so_sur_destroy", "so_sur_get_params", "so_sur_set_params",
     "so_sur_train", "so_sur_evaluate", "so_sur_gradients", "so_sur_infer", "so_sur_set_infer_ctas", "so_sur_dataset", "so_sur_render",

@@ -5,9 +5,12 @@
 //   k_route       per sample: distance of its image point from the analytic critical curve
 //                 (critical_curve_point, kerr.hpp:260-270, tabulated per frame on the host).  Inside
 //                 the band -> FP64 list; outside -> FP32 list.
-//   k_approach64  FP64 DP5(4) from the camera to r_switch (the far field, where the coordinate time
-//                 and radius are too large for FP32 increments), then parks the state in HBM as five
-//                 float4 SoA planes (two-float hi/lo pairs for r, r', u, u', phi, t).
+//   k_approach64  FP64 from the camera to r_switch (the far field, where the coordinate time and
+//                 radius are too large for FP32 increments): DP5(4) in the inverse radius
+//                 (far_approach, so_kerr.cuh: a few steps where Mino time needs hundreds) on ingoing
+//                 legs without a radial turning point, the reference's Mino-time DP5(4) otherwise;
+//                 then parks the state in HBM as five float4 SoA planes (two-float hi/lo pairs for
+//                 r, r', u, u', phi, t).
 //   k_trace32     persistent FP32 tracer over the parked rays: compensated (two-sum) state update,
 //                 FP32 stages and error estimate with the reference's error norm at tol32, err^-0.2
 //                 on the SFU, torus turbulence with the mode table in shared memory, its 512-mode sum
@@ -110,12 +113,21 @@ __global__ void __launch_bounds__(128) k_approach64(const TraceLaunch L) {
             int fate = 0, it = 0, nacc = 0, ncross = 0;
             double psi = 0.0;
             const bool radio = S.mode == SO_MODE_RADIO;
+            bool done = false, far = false;
+            if (L.far_field && far_applies(c, y, L.r_switch)) {
+                const int att = far_approach(c, y, L.r_switch, fmin(S.tol, L.tol_approach), 256, &psi, &ncross, radio);
+                if (att >= 0) {
+                    far = true;
+                    n_att += (unsigned long long)att;
+                    it = nacc = L.approach_it;
+                    h = initial_step(y);
+                }
+            }
             double sp = sqrt(fmax(fma(-y[2], y[2], 1.0), 0.0));
             double s4, c4;
             sincos(y[4], &s4, &c4);
             double pp0 = sp * c4, pp1 = sp * s4, pp2 = y[2];
-            bool done = false;
-            for (; it < S.max_steps;) {
+            for (; !far && it < S.max_steps;) {
                 ++it;
                 double err = dp54(c, y, k1, h, L.tol_approach, yn, k7);
                 if (!(err <= 1.0)) {
@@ -154,8 +166,10 @@ __global__ void __launch_bounds__(128) k_approach64(const TraceLaunch L) {
                 }
                 if (y[0] < L.r_switch) break;
             }
-            n_att += (unsigned long long)it;
-            n_acc += (unsigned long long)nacc;
+            if (!far) {
+                n_att += (unsigned long long)it;
+                n_acc += (unsigned long long)nacc;
+            }
             if (!done && it >= S.max_steps) done = true;  // step limit: fate 0
             if (done) {
                 L.sample_out[sid] = make_float4(0.f, 0.f, 0.f, 0.f);

@@ -82,6 +82,9 @@ struct TraceLaunch {
     double band_m, tol32, turn_r, drift_tol;
     double r_switch;          // FP64 approach down to this radius, FP32 inside
     double tol_approach;      // tolerance of the FP64 approach
+    int far_field;            // FP64 approach: transport in 1/r (far_approach) where it applies
+    int approach_it;          // attempts credited to a ray brought to r_switch by far_approach
+                              // (the reference's Mino-time count there, for the max_steps limit)
     double r_emit;            // FP32 tracer: outgoing beyond this radius = escaped (0 = off)
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
     // batched frames (RAYS_PIXELS over nframes)

@@ -77,7 +77,10 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0};
+    // attempts of the reference's Mino-time approach of the central ray, for the key below
+    int approach_it = 0;
+    double approach_key[6] = {-1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     // mixed-path buffers (grown on demand) and the critical-curve table of the current frame
     long long mixed_cap = 0;
     float4 *d_state = nullptr, *d_sample_out = nullptr;
@@ -259,6 +262,37 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
 //   route (band / FP32 lists) -> FP64 approach to r_switch -> FP32 tracer, with the band list traced
 //   by the FP64 tracer on a second stream meanwhile, then the FP64 re-trace list, then the
 //   per-pixel gather of the samples.  Counts stay on the device: nothing waits on the host.
+// Attempts the reference's Mino-time integrator (trace.cuh:80-96, with its disk step cap) takes for
+// the frame's central ray from the camera down to r_sw.  Rays that far_approach brings to r_sw are
+// credited with this count, so that the max_steps limit of the FP32 tracer counts about the
+// reference's steps for the whole ray.
+int mino_approach_attempts(const so_scene& S, const so_frame& F, double r_sw) {
+    RayC c;
+    double y[6], k1[6], yn[6], k7[6];
+    camera_photon(S.a, F.kp, F.ph, F.t, view_dir(F, 0.0, 0.0), F.beta, c, y);
+    rhs(c, y, k1);
+    double h = initial_step(y);
+    int it = 0;
+    while (it < S.max_steps && y[0] >= r_sw) {
+        ++it;
+        double hc = h;
+        if (S.disk_on) hc = std::fmin(hc, 0.3 / (std::fabs(y[3]) + 1e-30));
+        double err = dp54(c, y, k1, hc, S.tol, yn, k7);
+        if (!(err <= 1.0)) {
+            h = reject_step(hc, err);
+            continue;
+        }
+        for (int i = 0; i < 6; ++i) {
+            y[i] = yn[i];
+            k1[i] = k7[i];
+        }
+        project_radial(c, y, k1);
+        h = accept_step(hc, err);
+        if (y[0] > S.r_escape && y[1] > 0.0) break;
+    }
+    return it;
+}
+
 int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     const long long ns = (long long)f.W * f.H * f.spp;
     r->last_mixed_ns = 0;
@@ -300,6 +334,13 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     }
     L.r_switch = rsw;
     L.tol_approach = r->mixed.tol_approach > 0.0 ? r->mixed.tol_approach : 10.0 * r->S.tol;
+    L.far_field = r->mixed.approach == 0 ? 1 : 0;
+    const double key[6] = {r->S.a, r->S.tol, (double)r->S.disk_on, rsw, f.r, f.th};
+    if (std::memcmp(key, r->approach_key, sizeof key) != 0) {
+        r->approach_it = mino_approach_attempts(r->S, f, rsw);
+        std::memcpy(r->approach_key, key, sizeof key);
+    }
+    L.approach_it = r->approach_it;
     L.t32_min_blocks = r->mixed.t32_blocks > 0 ? r->mixed.t32_blocks : 4;
     // outgoing rays beyond every emitter cannot come back: the FP32 tracer ends them as escaped
     double r_emit = 0.0;
@@ -903,6 +944,7 @@ int so_last_fates(so_renderer* r, int8_t* fate, uint8_t* in_band, long long n) {
 int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
     if (!r) return SO_ERR_ARG;
     if (precision != SO_PREC_FP64 && precision != SO_PREC_MIXED) return fail(r, SO_ERR_ARG, "bad precision");
+    if (opts && opts->approach != 0 && opts->approach != 1) return fail(r, SO_ERR_ARG, "so_mixed_opts.approach: 0 or 1");
     r->precision = precision;
     if (opts) r->mixed = *opts;
     return SO_OK;

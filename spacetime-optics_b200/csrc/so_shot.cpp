@@ -627,6 +627,52 @@ int so_critical_curve_point(double a, double theta_o, double rp, double* alpha, 
     return critical_curve_point(a, theta_o, rp, alpha, beta_plus) ? 1 : 0;
 }
 
+int so_approach_state(const so_scene* S, const so_frame* f, double x, double yv, double r1, double tol, int method,
+                      double* state, int* attempts) {
+    if (!S || !f || !state || !(r1 > 0.0) || !(tol > 0.0) || (method != 0 && method != 1)) return SO_ERR_ARG;
+    RayC c;
+    double y[6];
+    camera_photon(S->a, f->kp, f->ph, f->t, view_dir(*f, x, yv), f->beta, c, y);
+    int att = 0;
+    if (method == 0) {
+        if (!far_applies(c, y, r1)) return SO_ERR_ARG;
+        double psi = 0.0;
+        int nc = 0;
+        att = far_approach(c, y, r1, tol, 100000, &psi, &nc, false);
+        if (att < 0) return SO_ERR_STATE;
+    } else {
+        // Mino-time DP5(4) with the reference's controller; a step that would pass r1 is shortened
+        // (secant in r) until the ray stops within 1e-12 r1 above r1
+        if (!(y[0] > r1) || !(y[1] < 0.0)) return SO_ERR_ARG;
+        double k1[6], yn[6], k7[6];
+        rhs(c, y, k1);
+        double h = initial_step(y);
+        while (y[0] - r1 > 1e-12 * r1) {
+            if (++att > 10000000) return SO_ERR_STATE;
+            const double hc = h;
+            const double err = dp54(c, y, k1, hc, tol, yn, k7);
+            if (!(err <= 1.0)) {
+                h = reject_step(hc, err);
+                continue;
+            }
+            if (yn[0] < r1) {
+                h = hc * (y[0] - r1) / (y[0] - yn[0]) * (1.0 - 1e-13);
+                continue;
+            }
+            for (int i = 0; i < 6; ++i) {
+                y[i] = yn[i];
+                k1[i] = k7[i];
+            }
+            project_radial(c, y, k1);
+            if (y[1] >= 0.0) return SO_ERR_ARG;  // radial turning point above r1
+            h = accept_step(hc, err);
+        }
+    }
+    for (int i = 0; i < 6; ++i) state[i] = y[i];
+    if (attempts) *attempts = att;
+    return SO_OK;
+}
+
 // Torus turbulence modes (so_tracer.h): directions uniform on the sphere, |k| log-uniform in
 // [k_min, k_max], phases uniform, amplitude^2 proportional to |k|^(3 + spectral_index) -- the
 // variance per logarithmic k interval of a 3-D power spectrum P(k) ~ k^spectral_index -- scaled so

@@ -164,3 +164,28 @@ def test_init_fails_loudly_without_device_or_bad_args(so):
     assert lib.so_render(None, None, None, 0.5, None, None) == so.abi.SO_ERR_ARG
     assert lib.so_trace_rays(None, None, 1, None, None, None) == so.abi.SO_ERR_ARG
     assert lib.so_last_error(None)  # message of the last failed init
+
+
+def test_far_field_approach_matches_mino_time(so):
+    """The mixed path's far-field transport (DP5(4) in 1/r) lands on the state that the reference's
+    Mino-time DP5(4) reaches at tolerance 1e-13, from the synchrotron camera at r = 1e7 M down to
+    r = 100 M: u, u' within 1e-10, phi within 2e-8 rad (its tolerance is 4e-9 per step), the
+    coordinate time within 1e-5 M of 1e7 M, in a few dozen attempts where Mino time needs hundreds
+    even at tolerance 1e-8.  Rays it does not apply to are refused."""
+    sh = so.Shot("synchrotron_1024.ini", [])
+    f = sh.frame(0)
+    rng = np.random.default_rng(3)
+    for al, be in rng.uniform(-17.0, 17.0, size=(12, 2)):  # image-plane offsets in M
+        x, y = al / f.r, be / f.r  # tangent-plane units
+        ref, n_ref = so.approach_state(sh.scene, f, x, y, 100.0, 1e-13, 1)
+        far, n_far = so.approach_state(sh.scene, f, x, y, ref[0], 1e-9, 0)
+        loose, n_loose = so.approach_state(sh.scene, f, x, y, 100.0, 1e-8, 1)
+        assert far[0] == ref[0]
+        assert abs(far[1] - ref[1]) <= 1e-12 * abs(ref[1])
+        assert abs(far[2] - ref[2]) <= 1e-10 and abs(far[3] - ref[3]) <= 1e-10 * max(1.0, abs(ref[3]))
+        assert abs(far[4] - ref[4]) <= 2e-8
+        assert abs(far[5] - ref[5]) <= 1e-5
+        assert n_far <= 40 and n_loose >= 200, (n_far, n_loose)
+    # impact parameter beyond r1: a radial turning point above it, far transport refused
+    with pytest.raises(so.TracerError):
+        so.approach_state(sh.scene, f, 150.0 / f.r, 0.0, 100.0, 1e-9, 0)
