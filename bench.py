@@ -238,6 +238,17 @@ def run_ours(args, so, world, rank, local):
         roof = {"bound": "fp64", "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
                 "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel": "k_trace64", "kernel_ms": st.ms_kernel,
                 "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
+    elif st.ms_turb > 0:
+        # deferred turbulence: the batched mode sums dominate, one SFU cosine per Fourier mode per
+        # record slot (the FP32 tracer and the ordered transfer are listed beside it)
+        sfu_peak = so.probe_sfu_peak(local)
+        ops = st.turb_records * n_modes
+        roof = {"bound": "sfu", "achieved": round(ops / (st.ms_turb * 1e-3) / 1e9, 3), "peak": round(sfu_peak, 3),
+                "unit": "Gop/s", "kernel": "k_turb_records", "kernel_ms": st.ms_turb, "per_launch": ops,
+                "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
+                "fp32_tflops_peak": round(fp32_peak, 3), "tracer_k_trace32_ms": round(st.ms_fp32_trace, 3),
+                "transfer_k_flow_records_ms": round(st.ms_fp32 - st.ms_fp32_trace - st.ms_turb, 3),
+                "record_slots": st.turb_records}
     else:
         sfu_peak = so.probe_sfu_peak(local)
         ops = st.attempts_fp32 * SFU_ATTEMPT + st.flow_steps_fp32 * (SFU_FLOW + n_modes)
@@ -261,9 +272,9 @@ def run_ours(args, so, world, rank, local):
     e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
     e2e = world * npix / (e2e_step * 1e-3) / 1e6
     del host
-    # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, re-trace, gather,
-    # resolve (mixed); spp_max = spp, so no adaptive pass
-    gpu_launches = args.steps * (2 if path == "fp64" else 7)
+    # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, [turbulence sums,
+    # transfer,] re-trace, gather, resolve (mixed); spp_max = spp, so no adaptive pass
+    gpu_launches = args.steps * (2 if path == "fp64" else 9 if st.ms_turb > 0 else 7)
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",

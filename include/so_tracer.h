@@ -170,6 +170,10 @@ typedef struct so_stats {
     long long redo_turn;  /* mixed precision: FP32 rays re-traced for a radial turning point inside turn_r */
     long long redo_drift; /* mixed precision: FP32 rays re-traced for constraint drift above drift_tol */
     long long redo_limit; /* mixed precision: FP32 rays re-traced after reaching max_steps in FP32 */
+    double ms_fp32_trace; /* mixed precision, deferred turbulence: device time of the FP32 geodesic tracer */
+    double ms_turb;       /* ... of the batched turbulence sums (ms_fp32 covers tracer + sums + transfer) */
+    long long turb_records; /* ... record slots summed (segments in use x 16) */
+    long long redo_records; /* ... FP32 rays re-traced in FP64 because the record pool ran out */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -222,6 +226,11 @@ typedef struct so_mixed_opts {
                               * far field carries no emission, and the synchrotron frame's image moves
                               * by 2e-5 L1 and keeps every class for it, at 7 % less frame time) */
     int t32_blocks;          /* FP32 tracer: resident 128-thread CTAs per SM, 4, 5 or 6 (0 = 4) */
+    int turbulence;          /* torus turbulence of the FP32 rays: 0 = deferred (the tracer records its
+                              * emitting flow steps, one batched kernel sums the Fourier modes at all of
+                              * them, one kernel runs the ordered transfer per ray; the record pool takes
+                              * up to half of the free device memory), 1 = summed in the tracer
+                              * (warp-cooperative, interleaved with the geodesic work) */
     int approach;            /* FP64 approach integrator: 0 = DP5(4) in the inverse radius 1/r on ingoing
                               * legs without a radial turning point above r_switch (a few steps where
                               * Mino time takes hundreds from a distant camera; other rays as 1),

@@ -237,6 +237,7 @@ struct Ray32 {
     float h, trans, psi, pp0, pp1, pp2;
     float acc[4];
     int ncross, natt, nacc, nflow, it;
+    int seg, cnt, head, nrec;  // deferred turbulence: current record segment, slots used in it, first, total
     uint32_t sid;
 };
 
@@ -371,7 +372,12 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
 
 // FP32 tracer.  One loop iteration = one DP5(4) attempt for every active lane.  The loop body is
 // split in two around the warp-cooperative turbulence sum, so every lane reaches the shuffles.
-template <int VAR, int MINB>
+// DEFER (radio torus with Fourier modes): instead of the turbulence sum and the transfer, every
+// emitting flow step is recorded (r, u, advected azimuth, step) in the ray's chain of record
+// segments; k_turb_records and k_flow_records finish the emission.  The geodesic does not depend on
+// the emission; only the opacity cut (trans < 1e-5) does, and k_flow_records applies it at the
+// record where it happens, so the result is the one of the in-line form to FP32 rounding.
+template <int VAR, int MINB, bool DEFER>
 __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     extern __shared__ float4 sm4[];
     const so_scene& S = L.scenes[0];
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     tp.half_var = (float)L.half_var;
     float4* km = sm4;
     float* amp = reinterpret_cast<float*>(sm4 + tp.n_modes);
-    if (tp.n_modes > 0) {
+    if (!DEFER && tp.n_modes > 0) {
         for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
             so_mode m = L.modes[i];
             // phase folded into (-pi, pi]: its FP32 rounding then stays small
@@ -450,6 +456,9 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                     c.Q3 = fmaf(c.lam, c.lam, c.eta);
                     R.trans = 1.f;
                     R.acc[0] = R.acc[1] = R.acc[2] = R.acc[3] = 0.f;
+                    R.seg = R.head = -1;
+                    R.cnt = REC_SEG;
+                    R.nrec = 0;
                     rhs32(c, R.rh + R.rl, R.prh + R.prl, R.uh + R.ul, R.puh + R.pul, R.k1);
                     float u = R.uh + R.ul, sp = sqrtf(fmaxf((1.f - u) * (1.f + u), 0.f)), s4, c4;
                     __sincosf(R.phh + R.phl, &s4, &c4);
@@ -465,6 +474,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         bool accepted = false, want_flow = false, want_turb = false;
         float nrh = 0.f, nrl = 0.f, nprh = 0.f, nprl = 0.f, nuh = 0.f, nul = 0.f, npuh = 0.f, npul = 0.f;
         float n0 = 0.f, n1 = 0.f, n2 = 0.f, hc = 0.f, err = 0.f, TX = 0.f, TY = 0.f, TZ = 0.f;
+        float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         float k7[6], dy[6];
         if (active) {
             if (R.it >= S.max_steps) {
@@ -569,11 +579,17 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                             float Rk = fmaxf(Rc, risco);
                             float Omf = flow_kep * __frcp_rn(fmaf(Rk, sqrtf(Rk), c.a));
                             float phc = (ph_h + ph_l) - Omf * t_rel;
-                            float sp, cp;
-                            __sincosf(phc, &sp, &cp);
-                            TX = Rc * cp;
-                            TY = Rc * sp;
-                            TZ = n0 * n2;
+                            if (DEFER) {
+                                // order n = floor(psi / pi) (>= 3 as 3) in the sign bits of r and h
+                                const int nb = min((int)(R.psi * (float)(1.0 / PI)), 3);
+                                rec = make_float4((nb & 1) ? -n0 : n0, n2, phc, (nb & 2) ? -hc : hc);
+                            } else {
+                                float sp, cp;
+                                __sincosf(phc, &sp, &cp);
+                                TX = Rc * cp;
+                                TY = Rc * sp;
+                                TZ = n0 * n2;
+                            }
                             want_turb = true;
                         }
                     }
@@ -582,7 +598,36 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         }
         // ---- all lanes: turbulence sums of the lanes that need one ------------------------------
         float delta = 0.f;
-        if (VAR == VAR_RADIO && tp.n_modes > 0) delta = warp_turbulence(km, amp, tp.n_modes, want_turb, TX, TY, TZ);
+        if (DEFER) {
+            // record slot: lanes whose segment is full take the next ones (one atomic per warp)
+            const bool need_seg = want_turb && R.cnt == REC_SEG;
+            const unsigned ms = __ballot_sync(FULL, need_seg);
+            if (ms) {
+                const int leader = __ffs(ms) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(&L.nlists[5], (unsigned long long)__popc(ms));
+                base = __shfl_sync(FULL, base, leader);
+                if (need_seg) {
+                    const unsigned long long idx = base + __popc(ms & ((1u << lane) - 1u));
+                    if (idx >= (unsigned long long)L.seg_cap) {
+                        fate = 5;  // out of record segments: the FP64 tracer takes the ray
+                        want_turb = false;
+                    } else {
+                        if (R.seg >= 0) L.seg_next[R.seg] = (uint32_t)idx;
+                        else R.head = (int)idx;
+                        R.seg = (int)idx;
+                        R.cnt = 0;
+                    }
+                }
+            }
+            if (want_turb) {
+                L.rec[(long long)R.seg * REC_SEG + R.cnt] = rec;
+                ++R.cnt;
+                ++R.nrec;
+            }
+        } else if (VAR == VAR_RADIO && tp.n_modes > 0) {
+            delta = warp_turbulence(km, amp, tp.n_modes, want_turb, TX, TY, TZ);
+        }
         // ---- part 2 (active lanes): emission, commit, termination ------------------------------
         if (!active) continue;
         if (accepted) {
@@ -613,7 +658,8 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                     if (R.trans < 1e-4f) fate = -1;
                 }
             }
-            if (want_flow) {
+            if (DEFER && want_flow) ++R.nflow;
+            if (!DEFER && want_flow) {
                 float dI, dtau;
                 flow_step32(S, tp, delta, n0, n2, c.lam, c.E, hc, &dI, &dtau);
                 ++R.nflow;
@@ -678,8 +724,15 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         n_turn += fate == 3 ? 1 : 0;
         n_drift += fate == 4 ? 1 : 0;
         n_lim += fate == 0 ? 1 : 0;
+        if (fate == 5) atomicAdd(&L.nlists[6], 1ull);
         if (!redo) {
-            L.sample_out[R.sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
+            if (DEFER && R.nrec > 0) {
+                // emission by k_flow_records (which may still end the ray on its opacity)
+                L.ray_meta[R.sid] = make_int2(R.head, R.nrec);
+                L.acc_list[atomicAdd(&L.nlists[4], 1ull)] = R.sid;
+            } else {
+                L.sample_out[R.sid] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
+            }
             if (L.sample_fate) L.sample_fate[R.sid] = (int8_t)fate;
         }
         active = false;
@@ -704,7 +757,164 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     }
 }
 
+// ---- deferred turbulence: batched mode sums, ordered transfer ------------------------------------
+// Torus parameters of the launch in FP32 (as the tracer sets them up).
+__device__ __forceinline__ Torus32 torus32_of(const TraceLaunch& L) {
+    Torus32 tp;
+    tp.on = L.torus;
+    tp.n_modes = L.torus ? L.n_modes : 0;
+    tp.ne_index = (float)L.ne_index;
+    tp.te_index = (float)L.te_index;
+    tp.h_sph = (float)L.h_sph;
+    tp.theta_e0 = (float)L.theta_e0;
+    tp.half_var = (float)L.half_var;
+    return tp;
+}
+
+// Turbulence sum at every record slot in use: the records' positions (the tracer's in-line form:
+// R = r sqrt(max((1-u)(1+u), 1e-12)), x = R cos phi_c, y = R sin phi_c, z = r u), TURB_P positions
+// per thread spread over the slots, the modes broadcast from shared memory, so every lane does the
+// same work and the SFU cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine
+// and one FMA per mode and position).  Slots of a segment past its ray's last record hold stale
+// data; their sums are never read.
+constexpr int TURB_P = 4;
+__global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
+    extern __shared__ float4 sm4[];
+    const int nm = L.n_modes;
+    float4* km = sm4;
+    float* amp = reinterpret_cast<float*>(sm4 + nm);
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) {
+        so_mode m = L.modes[i];
+        double ph = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
+        km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)ph);
+        amp[i] = (float)m.amp;
+    }
+    __syncthreads();
+    unsigned long long used = L.nlists[5];
+    if (used > (unsigned long long)L.seg_cap) used = (unsigned long long)L.seg_cap;
+    const long long nslots = (long long)used * REC_SEG;
+    const long long span = (nslots + TURB_P - 1) / TURB_P;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < span; i += (long long)gridDim.x * blockDim.x) {
+        float x[TURB_P], y[TURB_P], z[TURB_P], acc[TURB_P];
+#pragma unroll
+        for (int q = 0; q < TURB_P; ++q) {
+            const long long j = min(i + q * span, nslots - 1);
+            const float4 v = L.rec[j];
+            const float r = fabsf(v.x), u = v.y;
+            const float s2 = fmaxf((1.f - u) * (1.f + u), 1e-12f), Rc = r * sqrtf(s2);
+            float sp, cp;
+            __sincosf(v.z, &sp, &cp);
+            x[q] = Rc * cp;
+            y[q] = Rc * sp;
+            z[q] = r * u;
+            acc[q] = 0.f;
+        }
+#pragma unroll 2
+        for (int m = 0; m < nm; ++m) {
+            const float4 k = km[m];
+            const float am = amp[m];
+#pragma unroll
+            for (int q = 0; q < TURB_P; ++q)
+                acc[q] = fmaf(am, __cosf(fmaf(k.z, z[q], fmaf(k.y, y[q], fmaf(k.x, x[q], k.w)))), acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < TURB_P; ++q)
+            if (i + q * span < nslots) L.rec_delta[i + q * span] = acc[q];
+    }
+}
+
+// Ordered transfer per ray (trace.cuh:130-143 in the tracer's FP32 form), one warp per ray: the
+// warp takes 32 records (two segments) at a time, each lane runs flow_step32 on one with its
+// turbulence sum, an inclusive warp scan of dtau gives every record the transmittance in front of
+// it, T exp(-sum of the dtau before it) (the in-line form multiplies the factors one by one: the
+// same to FP32 rounding), and the ray ends (class captured) after the first record behind which
+// the transmittance is below 1e-5, that record's light included.  Sums by photon-ring order.
+__global__ void __launch_bounds__(256) k_flow_records(const TraceLaunch L) {
+    const so_scene& S = L.scenes[0];
+    const Torus32 tp = torus32_of(L);
+    const long long n = (long long)L.nlists[4];
+    const long long ns = L.nsamples;
+    const int lane = threadIdx.x & 31;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = w0; i < n; i += nw) {
+        const uint32_t sid = L.acc_list[i];
+        const int2 meta = L.ray_meta[sid];
+        const float4 p3 = L.state[3 * ns + sid];
+        const float lam = p3.x, E = p3.z;
+        const int nrec = meta.y;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, T = 1.f;
+        bool opaque = false;
+        long long sa = meta.x;
+        for (int k0 = 0; k0 < nrec && !opaque; k0 += 32) {
+            const long long sb = k0 + 16 < nrec ? (long long)L.seg_next[sa] : sa;
+            const int k = k0 + lane;
+            float dI = 0.f, dtau = 0.f;
+            int nb = 0;
+            if (k < nrec) {
+                const long long j = (lane < 16 ? sa : sb) * REC_SEG + (lane & 15);
+                const float4 v = L.rec[j];
+                const float delta = L.rec_delta[j];
+                nb = (int)(__float_as_uint(v.x) >> 31) | (int)((__float_as_uint(v.w) >> 31) << 1);
+                flow_step32(S, tp, delta, fabsf(v.x), v.y, lam, E, fabsf(v.w), &dI, &dtau);
+            }
+            float incl = dtau;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const float Tb = T * __expf(-(incl - dtau)), Ta = T * __expf(-incl);
+            const unsigned cut = __ballot_sync(FULL, k < nrec && Ta < 1e-5f);
+            bool use = k < nrec;
+            if (cut) {
+                use = use && lane <= __ffs(cut) - 1;
+                opaque = true;
+            }
+            const float cc = use ? Tb * dI : 0.f;
+            a0 += cc;
+            a1 += nb == 1 ? cc : 0.f;
+            a2 += nb == 2 ? cc : 0.f;
+            a3 += nb == 3 ? cc : 0.f;
+            T = __shfl_sync(FULL, Ta, 31);
+            if (k0 + 32 < nrec) sa = (long long)L.seg_next[sb];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(FULL, a0, o);
+            a1 += __shfl_xor_sync(FULL, a1, o);
+            a2 += __shfl_xor_sync(FULL, a2, o);
+            a3 += __shfl_xor_sync(FULL, a3, o);
+        }
+        if (lane == 0) {
+            L.sample_out[sid] = make_float4(a0, a1, a2, a3);
+            if (opaque && L.sample_fate) L.sample_fate[sid] = -1;
+        }
+    }
+}
+
 // ---- launchers -----------------------------------------------------------------------------------
+cudaError_t launch_turb_records(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    const size_t smem = (size_t)L.n_modes * (sizeof(float4) + sizeof(float));
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_turb_records, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_turb_records, 256, smem);
+    if (e != cudaSuccess) return e;
+    k_turb_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, smem, st>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_records, 256, 0);
+    if (e != cudaSuccess) return e;
+    k_flow_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st) {
     long long blocks = (L.nsamples + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
@@ -725,7 +935,8 @@ cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cu
 
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st) {
     const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;
-    size_t smem = torus ? (size_t)L.n_modes * (sizeof(float4) + sizeof(float)) : 0;
+    const bool defer = torus && L.defer;
+    size_t smem = torus && !defer ? (size_t)L.n_modes * (sizeof(float4) + sizeof(float)) : 0;
     int per_sm = 1;
     cudaError_t e;
     auto go = [&](auto kern) -> cudaError_t {
@@ -744,11 +955,15 @@ cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int n
     // register budget: 4 CTAs of 128 per SM (128 registers, no spills) or 5 / 6 (96 / 80 registers,
     // a few spills to L1); chosen by the caller or the autotuner
     switch (variant) {
-        case VAR_VACUUM: e = go(k_trace32<VAR_VACUUM, 4>); break;
-        case VAR_DISK: e = go(k_trace32<VAR_DISK, 4>); break;
+        case VAR_VACUUM: e = go(k_trace32<VAR_VACUUM, 4, false>); break;
+        case VAR_DISK: e = go(k_trace32<VAR_DISK, 4, false>); break;
         default:
-            e = L.t32_min_blocks >= 6 ? go(k_trace32<VAR_RADIO, 6>)
-                : L.t32_min_blocks == 5 ? go(k_trace32<VAR_RADIO, 5>) : go(k_trace32<VAR_RADIO, 4>);
+            if (defer)
+                e = L.t32_min_blocks >= 6 ? go(k_trace32<VAR_RADIO, 6, true>)
+                    : L.t32_min_blocks == 5 ? go(k_trace32<VAR_RADIO, 5, true>) : go(k_trace32<VAR_RADIO, 4, true>);
+            else
+                e = L.t32_min_blocks >= 6 ? go(k_trace32<VAR_RADIO, 6, false>)
+                    : L.t32_min_blocks == 5 ? go(k_trace32<VAR_RADIO, 5, false>) : go(k_trace32<VAR_RADIO, 4, false>);
             break;
     }
     return e;

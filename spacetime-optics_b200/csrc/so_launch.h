@@ -24,6 +24,9 @@ enum Variant : int {
 };
 
 // Device counters of one launch (zeroed before the launch).
+constexpr int REC_SEG = 16;  // flow-step record slots per segment (256 bytes)
+constexpr int NLISTS = 8;
+
 struct Counters {
     unsigned long long next;          // ray-queue head
     unsigned long long step_limited;  // samples that hit max_steps
@@ -100,13 +103,26 @@ struct TraceLaunch {
     uint32_t* list64;         // FP64 work list (band rays), filled by the router
     uint32_t* redo;           // FP64 re-trace list (drift check / radial turning point near the hole)
     uint32_t* parked;         // rays parked at r_switch by the FP64 approach (the FP32 work list)
-    unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked counts
+    // deferred torus turbulence (FP32 tracer, radio torus with Fourier modes): the tracer records
+    // every emitting flow step, one batched kernel sums the modes at all records, one kernel runs
+    // the ordered transfer per ray
+    int defer;                // 1 = record flow steps instead of evaluating them in the tracer
+    float4* rec;              // flow-step records (|r| sign bit = order bit 0, |h| sign = bit 1, u, phi_c)
+    float* rec_delta;         // turbulence sum per record slot
+    uint32_t* seg_next;       // per segment of REC_SEG record slots: the ray's next segment
+    int2* ray_meta;           // per sample id: (first segment, record count)
+    uint32_t* acc_list;       // rays with records, for the transfer kernel
+    long long seg_cap;        // record segments available
+    unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked, [4] acc_list counts,
+                                // [5] record segments used, [6] rays re-traced for want of segments
 };
 
 // Mixed-path kernels (k_trace_mixed.cu).
 cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st);
 cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st);
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
+cudaError_t launch_turb_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
+cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);
 
 }  // namespace so

@@ -77,7 +77,20 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0};
+    // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
+    float4* d_rec = nullptr;
+    float* d_rec_delta = nullptr;
+    uint32_t* d_seg_next = nullptr;
+    int2* d_ray_meta = nullptr;
+    uint32_t* d_acc_list = nullptr;
+    long long seg_cap = 0, meta_cap = 0;
+    double rec_per_ray = 320.0;             // pool size per FP32 ray (records), doubled after a shortage
+    unsigned long long* h_seg = nullptr;    // pinned: [0] segments requested, [1] rays short of segments
+    cudaEvent_t ev_seg = nullptr;           // after the copy into h_seg
+    bool seg_pending = false;
+    bool last_defer = false;                // the last mixed frame deferred its turbulence
+    cudaEvent_t ev_turb[2] = {nullptr, nullptr};  // tracer end, sums end
     // attempts of the reference's Mino-time approach of the central ray, for the key below
     int approach_it = 0;
     double approach_key[6] = {-1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -134,7 +147,8 @@ void free_all(so_renderer* r) {
     for (void* p : ps)
         if (p) cudaFree(p);
     void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked,
-                  r->d_nlists, r->d_cnt3, r->d_band};
+                  r->d_nlists, r->d_cnt3, r->d_band, r->d_rec, r->d_rec_delta, r->d_seg_next, r->d_ray_meta,
+                  r->d_acc_list};
     for (void* p : pm)
         if (p) cudaFree(p);
     for (int k = 1; k < r->lev.n; ++k)
@@ -142,6 +156,10 @@ void free_all(so_renderer* r) {
     if (r->d_tmp) cudaFree(r->d_tmp);
     for (cudaEvent_t e : r->ev32)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : r->ev_turb)
+        if (e) cudaEventDestroy(e);
+    if (r->ev_seg) cudaEventDestroy(r->ev_seg);
+    if (r->h_seg) cudaFreeHost(r->h_seg);
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
     if (r->st2) cudaStreamDestroy(r->st2);
@@ -293,6 +311,57 @@ int mino_approach_attempts(const so_scene& S, const so_frame& F, double r_sw) {
     return it;
 }
 
+// Record pool of the deferred turbulence for ns FP32 rays: rec_per_ray records per ray on average
+// plus one partly filled segment per ray, within half of the free device memory.  A frame that ran
+// short (its rays re-traced in FP64, so still correct) doubles rec_per_ray for the next frames; the
+// shortage is read from the previous frame's counters once they have arrived (no wait here).
+int ensure_records(so_renderer* r, long long ns) {
+    if (!r->h_seg) {
+        SO_CK(r, cudaMallocHost((void**)&r->h_seg, 2 * sizeof(unsigned long long)));
+        r->h_seg[0] = r->h_seg[1] = 0;
+        SO_CK(r, cudaEventCreateWithFlags(&r->ev_seg, cudaEventDisableTiming));
+        for (cudaEvent_t& e : r->ev_turb) SO_CK(r, cudaEventCreate(&e));
+    }
+    if (r->seg_pending && cudaEventQuery(r->ev_seg) == cudaSuccess) {
+        r->seg_pending = false;
+        if (r->h_seg[1] > 0) r->rec_per_ray *= 2.0;
+    }
+    cudaGetLastError();  // a pending event reports cudaErrorNotReady
+    const long long want = std::min<long long>((long long)std::ceil((double)ns * r->rec_per_ray / REC_SEG) + ns,
+                                               0x7fffffffll);
+    if (want > r->seg_cap) {
+        SO_CK(r, cudaStreamSynchronize(r->st));
+        if (r->d_rec) cudaFree(r->d_rec);
+        if (r->d_rec_delta) cudaFree(r->d_rec_delta);
+        if (r->d_seg_next) cudaFree(r->d_seg_next);
+        r->d_rec = nullptr;
+        r->d_rec_delta = nullptr;
+        r->d_seg_next = nullptr;
+        r->seg_cap = 0;
+        size_t fr = 0, tot = 0;
+        SO_CK(r, cudaMemGetInfo(&fr, &tot));
+        const double per_seg = REC_SEG * (sizeof(float4) + sizeof(float)) + sizeof(uint32_t);
+        const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
+        if (cap < 1) return fail(r, SO_ERR_ALLOC, "record pool: no device memory");
+        if (dalloc(&r->d_rec, (size_t)cap * REC_SEG) != cudaSuccess ||
+            dalloc(&r->d_rec_delta, (size_t)cap * REC_SEG) != cudaSuccess ||
+            dalloc(&r->d_seg_next, (size_t)cap) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "record pool: device allocation");
+        r->seg_cap = cap;
+    }
+    if (ns > r->meta_cap) {
+        if (r->d_ray_meta) cudaFree(r->d_ray_meta);
+        if (r->d_acc_list) cudaFree(r->d_acc_list);
+        r->d_ray_meta = nullptr;
+        r->d_acc_list = nullptr;
+        r->meta_cap = 0;
+        if (dalloc(&r->d_ray_meta, (size_t)ns) != cudaSuccess || dalloc(&r->d_acc_list, (size_t)ns) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "record lists: device allocation");
+        r->meta_cap = ns;
+    }
+    return SO_OK;
+}
+
 int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     const long long ns = (long long)f.W * f.H * f.spp;
     r->last_mixed_ns = 0;
@@ -313,7 +382,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         r->mixed_cap = ns;
     }
     if (!r->d_nlists) {
-        if (dalloc(&r->d_nlists, 4) != cudaSuccess || (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess))
+        if (dalloc(&r->d_nlists, NLISTS) != cudaSuccess || (!r->d_band && dalloc(&r->d_band, BAND_N) != cudaSuccess))
             return fail(r, SO_ERR_ALLOC, "mixed path: device allocation");
         if (int rc = ensure_side_queue(r)) return rc;
         SO_CK(r, cudaEventCreate(&r->ev32[0]));
@@ -358,7 +427,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     L.redo = r->d_redo;
     L.parked = r->d_parked;
     L.nlists = r->d_nlists;
-    SO_CK(r, cudaMemsetAsync(r->d_nlists, 0, 4 * sizeof(unsigned long long), r->st));
+    SO_CK(r, cudaMemsetAsync(r->d_nlists, 0, NLISTS * sizeof(unsigned long long), r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt3, 0, 2 * sizeof(Counters), r->st));
     // The reference's sheared fBm turbulence (flow or disk) is evaluated at a noise generation
     // k = floor(t / P) of the raw coordinate time t ~ -r_cam: a relative change eps of the radius moves
@@ -380,9 +449,32 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
     SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
+    const bool defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0 && r->mixed.turbulence == 0;
+    L.defer = defer ? 1 : 0;
+    if (defer) {
+        rc = ensure_records(r, ns);
+        if (rc) return rc;
+        L.rec = r->d_rec;
+        L.rec_delta = r->d_rec_delta;
+        L.seg_next = r->d_seg_next;
+        L.ray_meta = r->d_ray_meta;
+        L.acc_list = r->d_acc_list;
+        L.seg_cap = r->seg_cap;
+    }
     SO_CK(r, launch_approach64(L, ns, r->num_sms, r->st));
     SO_CK(r, cudaEventRecord(r->ev32[0], r->st));
     SO_CK(r, launch_trace32(L, ns, variant_of(r->S), r->num_sms, r->st));
+    if (defer) {
+        SO_CK(r, cudaEventRecord(r->ev_turb[0], r->st));
+        SO_CK(r, launch_turb_records(L, r->num_sms, r->st));
+        SO_CK(r, cudaEventRecord(r->ev_turb[1], r->st));
+        SO_CK(r, launch_flow_records(L, r->num_sms, r->st));
+        SO_CK(r, cudaMemcpyAsync(r->h_seg, &r->d_nlists[5], 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 r->st));
+        SO_CK(r, cudaEventRecord(r->ev_seg, r->st));
+        r->seg_pending = true;
+    }
+    r->last_defer = defer;
     SO_CK(r, cudaEventRecord(r->ev32[1], r->st));
     // FP64 re-trace of the rays the FP32 tracer handed back
     TraceLaunch Lr = Lb;
@@ -506,8 +598,21 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
                 c.step_limited += x.step_limited;
                 c.flow_steps += x.flow_steps;
             }
-            unsigned long long nl[4];
+            unsigned long long nl[NLISTS];
             SO_CK(r, cudaMemcpy(nl, r->d_nlists, sizeof nl, cudaMemcpyDeviceToHost));
+            stats->ms_fp32_trace = ms32;
+            stats->ms_turb = 0.0;
+            stats->turb_records = 0;
+            stats->redo_records = (long long)nl[6];
+            if (r->last_defer) {
+                float a = 0.f, b = 0.f;
+                cudaEventElapsedTime(&a, r->ev32[0], r->ev_turb[0]);
+                cudaEventElapsedTime(&b, r->ev_turb[0], r->ev_turb[1]);
+                stats->ms_fp32_trace = a;
+                stats->ms_turb = b;
+                stats->turb_records =
+                    (long long)std::min<unsigned long long>(nl[5], (unsigned long long)r->seg_cap) * REC_SEG;
+            }
             // c.attempts now holds FP32 attempts (k_trace32) + band + re-trace FP64 attempts;
             // the FP64 approach's attempts are in pad[0]
             stats->attempts_fp32 = (long long)(c.attempts - c3[0].attempts - c3[1].attempts);
@@ -520,6 +625,8 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->flow_steps_fp32 = 0;
             stats->ms_fp32 = 0.0;
             stats->redo_turn = stats->redo_drift = stats->redo_limit = 0;
+            stats->ms_fp32_trace = stats->ms_turb = 0.0;
+            stats->turb_records = stats->redo_records = 0;
             c.fp64_rays = 0;
         }
         float ms1 = 0.f, ms2 = 0.f;
@@ -945,6 +1052,8 @@ int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
     if (!r) return SO_ERR_ARG;
     if (precision != SO_PREC_FP64 && precision != SO_PREC_MIXED) return fail(r, SO_ERR_ARG, "bad precision");
     if (opts && opts->approach != 0 && opts->approach != 1) return fail(r, SO_ERR_ARG, "so_mixed_opts.approach: 0 or 1");
+    if (opts && opts->turbulence != 0 && opts->turbulence != 1)
+        return fail(r, SO_ERR_ARG, "so_mixed_opts.turbulence: 0 or 1");
     r->precision = precision;
     if (opts) r->mixed = *opts;
     return SO_OK;
