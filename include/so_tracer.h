@@ -235,6 +235,9 @@ typedef struct so_mixed_opts {
                               * legs without a radial turning point above r_switch (a few steps where
                               * Mino time takes hundreds from a distant camera; other rays as 1),
                               * 1 = the reference's Mino-time DP5(4) for every ray */
+    double records_per_ray;  /* deferred turbulence: record pool per FP32 ray at the renderer's first
+                              * mixed frame (0 = 320; doubled after a frame that ran short, whose rays
+                              * without a record slot are re-traced in FP64) */
 } so_mixed_opts;
 
 /* ---- renderer lifecycle ---------------------------------------------------------------------- */

@@ -77,7 +77,7 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0};
     // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
     float4* d_rec = nullptr;
     float* d_rec_delta = nullptr;
@@ -1054,6 +1054,9 @@ int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
     if (opts && opts->approach != 0 && opts->approach != 1) return fail(r, SO_ERR_ARG, "so_mixed_opts.approach: 0 or 1");
     if (opts && opts->turbulence != 0 && opts->turbulence != 1)
         return fail(r, SO_ERR_ARG, "so_mixed_opts.turbulence: 0 or 1");
+    if (opts && !(opts->records_per_ray >= 0.0 && opts->records_per_ray <= 1e6))
+        return fail(r, SO_ERR_ARG, "so_mixed_opts.records_per_ray: 0 .. 1e6");
+    if (opts && opts->records_per_ray > 0.0) r->rec_per_ray = opts->records_per_ray;
     r->precision = precision;
     if (opts) r->mixed = *opts;
     return SO_OK;

@@ -151,3 +151,63 @@ def test_mixed_classes_exact_outside_band(so):
     assert set(np.unique(f64)) >= {-1, 1}
     assert np.array_equal(fm[out], f64[out]), int((fm[out] != f64[out]).sum())
     r.close()
+
+
+def _mixed_fates(so, r, f, n, **mixed):
+    r.set_precision(so.abi.SO_PREC_MIXED, **mixed)
+    img, _, st = r.render(f)
+    fm, band = r.last_fates(n)
+    return img, st, fm
+
+
+def test_deferred_turbulence_matches_in_tracer_sums(so):
+    """The deferred form (flow-step records, batched mode sums, warp-per-ray transfer) gives the
+    image of the in-tracer sums within 1e-5 relative L1 (FP32 summation order and the scanned
+    transmittance) and the same termination class for every sample, also at a density 1000 times
+    the normalised one, where the transfer ends many rays on their opacity."""
+    W = 128
+    thin = None
+    for n0, opaque in ((N0, False), ("flow.n0=1594262800.0", True)):
+        sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", n0])
+        r = so.Renderer(sh.scene, sh.tables, sh.settings)
+        r.set_plasma(sh.plasma())
+        f = sh.frame(0)
+        n = W * W * sh.settings.spp
+        a, sa, fa = _mixed_fates(so, r, f, n, turbulence=1)
+        b, sb, fb = _mixed_fates(so, r, f, n, turbulence=0)
+        assert sa.turb_records == 0 and sb.turb_records >= sb.flow_steps_fp32 > 0
+        assert sb.redo_records == 0
+        l1, flux = _errors(a, b)
+        assert l1 <= 1e-5 and flux <= 1e-5, (l1, flux)
+        assert np.array_equal(fa, fb), int((fa != fb).sum())
+        if opaque:
+            # ended on opacity: captured where the normal-density frame escapes
+            assert ((fb == -1) & (thin == 1)).sum() > 100
+        thin = fb
+        r.close()
+
+
+def test_deferred_turbulence_record_pool_shortage(so):
+    """A record pool far too small for the frame: the rays that find no record slot are re-traced
+    in FP64, so the image stays within the mixed path's bar of the FP64 frame, and the next frame's
+    pool is larger."""
+    W = 96
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", N0])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED, records_per_ray=1.0)
+    img1, _, st1 = r.render(f)
+    assert st1.redo_records > 0
+    l1, flux = _errors(img64, img1)
+    assert l1 <= 1e-3 and flux <= 1e-3, (l1, flux)
+    redo = [st1.redo_records]
+    for _ in range(8):
+        _, _, st = r.render(f)
+        redo.append(st.redo_records)
+    assert redo[-1] < redo[0], redo
+    with pytest.raises(so.TracerError):
+        r.set_precision(so.abi.SO_PREC_MIXED, turbulence=2)
+    r.close()
