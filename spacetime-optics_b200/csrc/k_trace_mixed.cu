@@ -477,8 +477,8 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         float k7[6], dy[6];
         if (active) {
-            if (R.it >= S.max_steps) {
-                fate = 0;
+            if (R.it >= S.max_steps || R.natt >= L.t32_max_att) {
+                fate = 0;  // the FP64 re-trace decides (step limit, or an FP32 controller that stalls)
             } else {
                 ++R.it;
                 ++R.natt;
@@ -773,11 +773,13 @@ __device__ __forceinline__ Torus32 torus32_of(const TraceLaunch& L) {
 
 // Turbulence sum at every record slot in use: the records' positions (the tracer's in-line form:
 // R = r sqrt(max((1-u)(1+u), 1e-12)), x = R cos phi_c, y = R sin phi_c, z = r u), TURB_P positions
-// per thread spread over the slots, the modes broadcast from shared memory, so every lane does the
-// same work and the SFU cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine
-// and one FMA per mode and position).  Slots of a segment past its ray's last record hold stale
-// data; their sums are never read.
+// per thread, the modes broadcast from shared memory, so every lane does the same work and the SFU
+// cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine and one FMA per mode
+// and position).  Blocks take chunks of TURB_P x 256 slots from a work counter, so SMs that also
+// host the FP64 re-trace (on the other stream) do less of it instead of finishing last.  Slots of
+// a segment past its ray's last record hold stale data; their sums are never read.
 constexpr int TURB_P = 4;
+constexpr int TURB_CHUNK = TURB_P * 256;
 __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
     extern __shared__ float4 sm4[];
     const int nm = L.n_modes;
@@ -789,16 +791,21 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
         km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)ph);
         amp[i] = (float)m.amp;
     }
-    __syncthreads();
+    __shared__ long long chunk;
     unsigned long long used = L.nlists[5];
     if (used > (unsigned long long)L.seg_cap) used = (unsigned long long)L.seg_cap;
     const long long nslots = (long long)used * REC_SEG;
-    const long long span = (nslots + TURB_P - 1) / TURB_P;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < span; i += (long long)gridDim.x * blockDim.x) {
+    for (;;) {
+        __syncthreads();  // modes loaded; the previous chunk index read by every thread
+        if (threadIdx.x == 0) chunk = (long long)atomicAdd(&L.nlists[7], 1ull) * TURB_CHUNK;
+        __syncthreads();
+        const long long c0 = chunk;
+        if (c0 >= nslots) break;
+        const long long i = c0 + threadIdx.x;  // slots i, i + 256, i + 512, i + 768
         float x[TURB_P], y[TURB_P], z[TURB_P], acc[TURB_P];
 #pragma unroll
         for (int q = 0; q < TURB_P; ++q) {
-            const long long j = min(i + q * span, nslots - 1);
+            const long long j = min(i + q * 256, nslots - 1);
             const float4 v = L.rec[j];
             const float r = fabsf(v.x), u = v.y;
             const float s2 = fmaxf((1.f - u) * (1.f + u), 1e-12f), Rc = r * sqrtf(s2);
@@ -819,7 +826,7 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
         }
 #pragma unroll
         for (int q = 0; q < TURB_P; ++q)
-            if (i + q * span < nslots) L.rec_delta[i + q * span] = acc[q];
+            if (i + q * 256 < nslots) L.rec_delta[i + q * 256] = acc[q];
     }
 }
 
@@ -828,16 +835,19 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
 // turbulence sum, an inclusive warp scan of dtau gives every record the transmittance in front of
 // it, T exp(-sum of the dtau before it) (the in-line form multiplies the factors one by one: the
 // same to FP32 rounding), and the ray ends (class captured) after the first record behind which
-// the transmittance is below 1e-5, that record's light included.  Sums by photon-ring order.
+// the transmittance is below 1e-5, that record's light included.  Sums by photon-ring order.  Warps
+// take rays from a work counter (record counts per ray range from one to thousands).
 __global__ void __launch_bounds__(256) k_flow_records(const TraceLaunch L) {
     const so_scene& S = L.scenes[0];
     const Torus32 tp = torus32_of(L);
     const long long n = (long long)L.nlists[4];
     const long long ns = L.nsamples;
     const int lane = threadIdx.x & 31;
-    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long i = w0; i < n; i += nw) {
+    for (;;) {
+        unsigned long long ii = 0;
+        if (lane == 0) ii = atomicAdd(&L.nlists[8], 1ull);
+        const long long i = (long long)__shfl_sync(FULL, ii, 0);
+        if (i >= n) break;
         const uint32_t sid = L.acc_list[i];
         const int2 meta = L.ray_meta[sid];
         const float4 p3 = L.state[3 * ns + sid];

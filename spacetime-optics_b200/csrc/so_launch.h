@@ -25,7 +25,7 @@ enum Variant : int {
 
 // Device counters of one launch (zeroed before the launch).
 constexpr int REC_SEG = 16;  // flow-step record slots per segment (256 bytes)
-constexpr int NLISTS = 8;
+constexpr int NLISTS = 10;
 
 struct Counters {
     unsigned long long next;          // ray-queue head
@@ -90,6 +90,7 @@ struct TraceLaunch {
                               // (the reference's Mino-time count there, for the max_steps limit)
     double r_emit;            // FP32 tracer: outgoing beyond this radius = escaped (0 = off)
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
+    int t32_max_att;          // FP32 attempts after which a ray goes to the FP64 re-trace
     // batched frames (RAYS_PIXELS over nframes)
     int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
     int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
@@ -114,7 +115,8 @@ struct TraceLaunch {
     uint32_t* acc_list;       // rays with records, for the transfer kernel
     long long seg_cap;        // record segments available
     unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked, [4] acc_list counts,
-                                // [5] record segments used, [6] rays re-traced for want of segments
+                                // [5] record segments used, [6] rays re-traced for want of segments,
+                                // [7] / [8] work heads of k_turb_records / k_flow_records
 };
 
 // Mixed-path kernels (k_trace_mixed.cu).

@@ -77,7 +77,7 @@ struct so_renderer {
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0};
     // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
     float4* d_rec = nullptr;
     float* d_rec_delta = nullptr;
@@ -276,10 +276,6 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
     return SO_OK;
 }
 
-// Pass 1 of the mixed path into d_accum / d_ystat (see k_trace_mixed.cu):
-//   route (band / FP32 lists) -> FP64 approach to r_switch -> FP32 tracer, with the band list traced
-//   by the FP64 tracer on a second stream meanwhile, then the FP64 re-trace list, then the
-//   per-pixel gather of the samples.  Counts stay on the device: nothing waits on the host.
 // Attempts the reference's Mino-time integrator (trace.cuh:80-96, with its disk step cap) takes for
 // the frame's central ray from the camera down to r_sw.  Rays that far_approach brings to r_sw are
 // credited with this count, so that the max_steps limit of the FP32 tracer counts about the
@@ -362,6 +358,11 @@ int ensure_records(so_renderer* r, long long ns) {
     return SO_OK;
 }
 
+// Pass 1 of the mixed path into d_accum / d_ystat (see k_trace_mixed.cu):
+//   route (band / FP32 lists) -> FP64 approach to r_switch -> FP32 tracer [-> turbulence sums ->
+//   ordered transfer], with the band list traced by the FP64 tracer on a second stream meanwhile and
+//   the FP64 re-trace list after it on that stream once the FP32 tracer has made the list, then the
+//   per-pixel gather of the samples.  Counts stay on the device: nothing waits on the host.
 int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     const long long ns = (long long)f.W * f.H * f.spp;
     r->last_mixed_ns = 0;
@@ -411,6 +412,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     }
     L.approach_it = r->approach_it;
     L.t32_min_blocks = r->mixed.t32_blocks > 0 ? r->mixed.t32_blocks : 4;
+    L.t32_max_att = r->mixed.fp32_max_attempts > 0 ? r->mixed.fp32_max_attempts : 2000;
     // outgoing rays beyond every emitter cannot come back: the FP32 tracer ends them as escaped
     double r_emit = 0.0;
     if (r->S.mode == SO_MODE_RADIO && r->S.flow_on) r_emit = std::max(r_emit, r->S.r_flow_max);
@@ -448,7 +450,6 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     Lb.emit32 = 1;  // FP64 geometry in the band; the emission needs no more than FP32
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
-    SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
     const bool defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0 && r->mixed.turbulence == 0;
     L.defer = defer ? 1 : 0;
     if (defer) {
@@ -464,6 +465,16 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     SO_CK(r, launch_approach64(L, ns, r->num_sms, r->st));
     SO_CK(r, cudaEventRecord(r->ev32[0], r->st));
     SO_CK(r, launch_trace32(L, ns, variant_of(r->S), r->num_sms, r->st));
+    // FP64 re-trace of the rays the FP32 tracer handed back, on the second stream (after the band)
+    SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
+    SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
+    TraceLaunch Lr = Lb;
+    Lr.list = r->d_redo;
+    Lr.nrays_dev = &r->d_nlists[2];
+    Lr.counters = &r->d_cnt3[1];
+    rc = run_tracer(r, Lr, r->st2);
+    if (rc) return rc;
+    SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
     if (defer) {
         SO_CK(r, cudaEventRecord(r->ev_turb[0], r->st));
         SO_CK(r, launch_turb_records(L, r->num_sms, r->st));
@@ -476,13 +487,6 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     }
     r->last_defer = defer;
     SO_CK(r, cudaEventRecord(r->ev32[1], r->st));
-    // FP64 re-trace of the rays the FP32 tracer handed back
-    TraceLaunch Lr = Lb;
-    Lr.list = r->d_redo;
-    Lr.nrays_dev = &r->d_nlists[2];
-    Lr.counters = &r->d_cnt3[1];
-    rc = run_tracer(r, Lr, r->st);
-    if (rc) return rc;
     SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
     SO_CK(r, launch_gather_samples(L, r->st));
     r->last_mixed_ns = ns;
