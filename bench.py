@@ -249,6 +249,12 @@ def run_ours(args, so, world, rank, local):
                 "fp32_tflops_peak": round(fp32_peak, 3), "tracer_k_trace32_ms": round(st.ms_fp32_trace, 3),
                 "transfer_k_flow_records_ms": round(st.ms_fp32 - st.ms_fp32_trace - st.ms_turb, 3),
                 "record_slots": st.turb_records}
+        # DRAM bytes per record slot of k_turb_records from its ncu capture on the 512^2 frame
+        # (profiles/k_turb_records_synchrotron512.md: 1.349 GB for 68.16 M slots), scaled by this
+        # frame's slots; the algorithmic figure is 20 bytes per slot
+        roof["traffic"] = round(19.79 * st.turb_records)
+        roof["traffic_source"] = "ncu dram bytes per slot at 512^2 x this frame's record slots"
+        roof["algorithmic_bytes"] = 20 * st.turb_records
     else:
         sfu_peak = so.probe_sfu_peak(local)
         ops = st.attempts_fp32 * SFU_ATTEMPT + st.flow_steps_fp32 * (SFU_FLOW + n_modes)
@@ -257,7 +263,7 @@ def run_ours(args, so, world, rank, local):
                 "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
                 "fp32_tflops_peak": round(fp32_peak, 3)}
     roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
-    roof["traffic"] = None
+    roof.setdefault("traffic", None)
     # e2e: host buffers through so_render (frame H2D, image D2H inside the timed region)
     host = np.empty((W, W, 4), np.float32)
     host_pinned = torch.empty((W, W, 4), dtype=torch.float32).pin_memory().numpy()

@@ -778,7 +778,7 @@ __device__ __forceinline__ Torus32 torus32_of(const TraceLaunch& L) {
 // and position).  Blocks take chunks of TURB_P x 256 slots from a work counter, so SMs that also
 // host the FP64 re-trace (on the other stream) do less of it instead of finishing last.  Slots of
 // a segment past its ray's last record hold stale data; their sums are never read.
-constexpr int TURB_P = 4;
+constexpr int TURB_P = 8;
 constexpr int TURB_CHUNK = TURB_P * 256;
 __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
     extern __shared__ float4 sm4[];
@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
         __syncthreads();
         const long long c0 = chunk;
         if (c0 >= nslots) break;
-        const long long i = c0 + threadIdx.x;  // slots i, i + 256, i + 512, i + 768
+        const long long i = c0 + threadIdx.x;  // slots i + 256 q, q < TURB_P
         float x[TURB_P], y[TURB_P], z[TURB_P], acc[TURB_P];
 #pragma unroll
         for (int q = 0; q < TURB_P; ++q) {
