@@ -288,6 +288,18 @@ int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_frame, int 
 /* Same as so_trace_rays with x, y and the outputs already in device memory (device pointers). */
 int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
                          const so_rays_out* d_out);
+/* Flow turbulence of the reference plasma model (radio mode, flow.turbulence > 0).
+ * SO_FLOW_NOISE_BAKED (so_init's choice, as Renderer::init's, render.cu:594-620): before every
+ * trace of a frame its turbulence is baked into 24 retarded-time slices of 512 x 192 x 48 density
+ * factors on (phi, ln R, z/R) (453 MB of device memory, render.cu:449-460, 679-682) and each flow
+ * step interpolates them trilinearly and in time (emission.cuh:112-124; here in FP32 arithmetic from
+ * plain device memory where the reference fetches through the texture unit, whose weights have 8
+ * fractional bits).  SO_FLOW_NOISE_INLINE evaluates the sheared fBm noise at every flow step (the
+ * reference's turb_nt = 0 path) and frees the slices.  No effect on other plasma models.  The
+ * batched frames (so_batch_*) and so_radio_flux_noalloc always evaluate the noise in place. */
+enum { SO_FLOW_NOISE_BAKED = 0, SO_FLOW_NOISE_INLINE = 1 };
+int so_set_flow_noise(so_renderer* r, int mode);
+
 /* Precision and plasma extensions (no reference counterpart: the reference has one FP64 path and
  * the scene.hpp flow model). */
 int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts);

@@ -394,6 +394,55 @@ typedef struct {
 } Ctx;
 
 /* flow_step, emission.cuh:264-340, with the torus model as an alternative density/temperature. */
+/* Baked flow turbulence (render.cu:447-460 bake, 594-620 set-up, emission.cuh:112-124 sampling).
+ * Texel values are computed on demand with the bake's formula at the texel centre (the same values
+ * as a full bake of the slice); the interpolation is the library kernels' FP32 trilinear (x, then
+ * y, then z, each an fmaf), which the reference does in the texture unit with 8-bit weights. */
+enum { TNPHI = 512, TNLR = 192, TNZ = 48, TNT = 24 };
+void orc_turb_setup(so_scene* S) { /* render.cu:614-619 */
+    S->turb_nt = TNT;
+    S->turb_lr0 = (float)log(0.8 * S->rh);
+    S->turb_lr1 = (float)log(S->r_flow_max * 1.05);
+    S->turb_zmax = (float)fmin(2.0, 5.0 * S->h_r);
+    S->turb_d0 = -250.f;
+    S->turb_dd = 260.f / (TNT - 1);
+}
+static float turb_texel(const Ctx* X, int k, int l, int j, int i) { /* render.cu:449-460 */
+    const so_scene* S = X->S;
+    const so_frame* F = X->F;
+    const float delta = S->turb_d0 + k * S->turb_dd;
+    const double phi = (i + 0.5) / TNPHI * 2.0 * PI_D;
+    const double R = exp(S->turb_lr0 + (j + 0.5) / TNLR * (S->turb_lr1 - S->turb_lr0));
+    const double z = (-1.0 + 2.0 * (l + 0.5) / TNZ) * S->turb_zmax * R;
+    const double r = sqrt(fma(R, R, z * z));
+    const double t = (F->t - (F->r - r + 2.0 * log(F->r / r))) + delta;
+    const float n = sheared_noise(S, R, phi, z, t, S->flow_turb_scale, S->flow_tcorr, S->seed ^ 0x51f15eedu);
+    const float a = S->flow_turb_amp;
+    return expf(a * n - 0.5f * a * a);
+}
+static float turb_fetch(const Ctx* X, int k, float x, float y, float z) {
+    const float xb = (x - floorf(x)) * (float)TNPHI - 0.5f;
+    const float yb = fminf(fmaxf(y * (float)TNLR - 0.5f, -1.f), (float)TNLR);
+    const float zb = fminf(fmaxf(z * (float)TNZ - 0.5f, -1.f), (float)TNZ);
+    const float fi = floorf(xb), fj = floorf(yb), fl = floorf(zb);
+    const float a = xb - fi, b = yb - fj, c = zb - fl;
+    const int i = (int)fi, j = (int)fj, l = (int)fl;
+    const int i0 = i < 0 ? i + TNPHI : i, i1 = i + 1 >= TNPHI ? i + 1 - TNPHI : i + 1;
+    const int j0 = j < 0 ? 0 : j > TNLR - 1 ? TNLR - 1 : j, j1 = j + 1 < 0 ? 0 : j + 1 > TNLR - 1 ? TNLR - 1 : j + 1;
+    const int l0 = l < 0 ? 0 : l > TNZ - 1 ? TNZ - 1 : l, l1 = l + 1 < 0 ? 0 : l + 1 > TNZ - 1 ? TNZ - 1 : l + 1;
+    float p, q;
+    p = turb_texel(X, k, l0, j0, i0); q = turb_texel(X, k, l0, j0, i1);
+    const float v00 = fmaf(a, q - p, p);
+    p = turb_texel(X, k, l0, j1, i0); q = turb_texel(X, k, l0, j1, i1);
+    const float v01 = fmaf(a, q - p, p);
+    p = turb_texel(X, k, l1, j0, i0); q = turb_texel(X, k, l1, j0, i1);
+    const float v10 = fmaf(a, q - p, p);
+    p = turb_texel(X, k, l1, j1, i0); q = turb_texel(X, k, l1, j1, i1);
+    const float v11 = fmaf(a, q - p, p);
+    const float w0 = fmaf(b, v01 - v00, v00), w1 = fmaf(b, v11 - v10, v10);
+    return fmaf(c, w1 - w0, w0);
+}
+
 static void flow_step(const Ctx* X, double r, double u, double phi, double t, double lam, double Ecam, double h,
                       double* dI, double* dtau) {
     const so_scene* S = X->S;
@@ -423,7 +472,19 @@ static void flow_step(const Ctx* X, double r, double u, double phi, double t, do
         double vert = exp(-0.5 * zh * zh);
         if (vert < 1e-7) return;
         ne = S->n0 * exp(-S->n_index * log(r)) * vert;
-        if (S->flow_turb_amp > 0.f) {
+        if (S->flow_turb_amp > 0.f && S->turb_nt > 0) {
+            /* emission.cuh:112-124 */
+            const double tref = X->F->t - (X->F->r - r + 2.0 * log(X->F->r / r));
+            const float y = (float)((log(R) - S->turb_lr0) / (S->turb_lr1 - S->turb_lr0));
+            const float x = (float)(phi * (0.5 / PI_D));
+            const float w = (float)(0.5 + 0.5 * (z / R) / S->turb_zmax);
+            float sl = (float)((t - tref) - S->turb_d0) / S->turb_dd;
+            sl = fminf(fmaxf(sl, 0.f), (float)(TNT - 1) - 1e-4f);
+            const int k = (int)sl;
+            const float f = sl - (float)k;
+            const float A = turb_fetch(X, k, x, y, w), B = turb_fetch(X, k + 1, x, y, w);
+            ne *= fmaf(B - A, f, A);
+        } else if (S->flow_turb_amp > 0.f) {
             float n = sheared_noise(S, R, phi, z, t, S->flow_turb_scale, S->flow_tcorr, S->seed ^ 0x51f15eedu);
             ne *= exp((double)(S->flow_turb_amp * n - 0.5f * S->flow_turb_amp * S->flow_turb_amp));
         }

@@ -56,6 +56,7 @@ def lib():
         L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
         L.so_set_precision.argtypes = [vp, C.c_int, P(MixedOpts)]
         L.so_set_plasma.argtypes = [vp, P(Plasma), P(Mode)]
+        L.so_set_flow_noise.argtypes = [vp, C.c_int]
         L.so_stream.argtypes = [vp]
         L.so_stream.restype = vp
         L.so_last_error.argtypes = [vp]
@@ -229,6 +230,10 @@ class Renderer:
     def update_scene(self, scene):
         self.scene = scene
         _check(lib().so_update_scene(self.h, C.byref(scene)), self.h)
+
+    def set_flow_noise(self, mode):
+        """Reference flow turbulence: abi.SO_FLOW_NOISE_BAKED (default) or abi.SO_FLOW_NOISE_INLINE."""
+        _check(lib().so_set_flow_noise(self.h, mode), self.h)
 
     def set_plasma(self, plasma, modes=None):
         if plasma is None:

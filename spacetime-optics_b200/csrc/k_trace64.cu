@@ -155,12 +155,13 @@ __device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, double* 
 // Second half (trace.cuh:130-163): hot-flow transfer with the turbulence sum delta, commit,
 // projection, controller, termination.  Returns 1 when the ray is finished.
 template <int VAR>
-__device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const TorusParams& tp, double delta,
+__device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const so_frame& F, const float* field,
+                                          const TorusParams& tp, double delta,
                                           const double* yn, const double* k7, double hc, double err, int* fate,
                                           double* th, double* ph) {
     if (VAR == VAR_RADIO && S.flow_on && yn[0] < S.r_flow_max) {
         double dI, dtau;
-        flow_step(S, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+        flow_step(S, F, field, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
         ++R.nflow;
         float cc = (float)(R.trans * dI);
         int n = (int)(R.psi * (1.0 / PI));
@@ -406,7 +407,9 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
         // ---- second half: emission and commit (active lanes) ----------------------------------
         if (!active || stage == ST_REJECTED) continue;
         double th = 0.0, ph = 0.0;
-        if (stage == ST_ACCEPTED && !ray_commit<VAR>(R, *S, tp, delta, yn, k7, hc, err, &fate, &th, &ph)) continue;
+        if (stage == ST_ACCEPTED &&
+            !ray_commit<VAR>(R, *S, *F, L.turb_field, tp, delta, yn, k7, hc, err, &fate, &th, &ph))
+            continue;
         // sample finished
         n_att += (unsigned long long)R.natt;
         n_acc += (unsigned long long)R.nacc;
@@ -470,6 +473,34 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
 
 // Host launcher: grid = SMs x resident CTAs per SM (persistent; capped by L.ctas_per_sm), dynamic
 // shared memory for the mode table.  Returns the CUDA error of the launch.
+// Bake of the flow turbulence for the frame in d_frame (k_bake_turb, render.cu:449-460): slice k
+// holds exp(a n - a^2 / 2) of the sheared noise n at the retarded time t_ref(r) + delta_k, on cell
+// centres phi = 2 pi (i + 1/2) / 512, ln R uniform over [lr0, lr1] (192 cells), z / R uniform over
+// [-zmax, zmax] (48 cells).  One thread per cell, phi fastest (coalesced stores).
+__global__ void __launch_bounds__(256) k_bake_turb(const so_scene* __restrict__ Sp, const so_frame* __restrict__ Fp,
+                                                   const TurbBake b, float* __restrict__ field) {
+    const so_scene& S = *Sp;
+    const so_frame& F = *Fp;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z % TURB_NZ, k = blockIdx.z / TURB_NZ;
+    if (i >= TURB_NPHI || j >= TURB_NLR) return;
+    const double phi = (i + 0.5) / TURB_NPHI * 2.0 * PI;
+    const double R = exp(S.turb_lr0 + (j + 0.5) / TURB_NLR * (S.turb_lr1 - S.turb_lr0));
+    const double z = (-1.0 + 2.0 * (l + 0.5) / TURB_NZ) * S.turb_zmax * R;
+    const double r = sqrt(fma(R, R, z * z));
+    const double t = (F.t - (F.r - r + 2.0 * log(F.r / r))) + b.delta[k];
+    const float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);
+    const float a = S.flow_turb_amp;
+    field[(((size_t)k * TURB_NZ + l) * TURB_NLR + j) * TURB_NPHI + i] = __expf(a * n - 0.5f * a * a);
+}
+
+cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,
+                             cudaStream_t st) {
+    const dim3 block(32, 8), grid(TURB_NPHI / 32, TURB_NLR / 8, TURB_NZ * TURB_NT);
+    k_bake_turb<<<grid, block, 0, st>>>(d_scene, d_frame, b, field);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaStream_t st) {
     const int tpb = 128;
     const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;

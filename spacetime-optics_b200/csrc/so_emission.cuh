@@ -10,6 +10,7 @@
 // same operations.
 #pragma once
 #include "so_kerr.cuh"
+#include "so_launch.h"
 
 namespace so {
 
@@ -231,9 +232,40 @@ __device__ __forceinline__ bool torus_position(const so_scene& S, const TorusPar
     return true;
 }
 
+// Trilinear sample of one baked turbulence slice at normalised coordinates (x = phi / 2 pi, wrapped;
+// y = ln R, z = z / R, clamped to the edge texels), texel centres at (i + 1/2) / N as for linear
+// texture filtering with normalised coordinates.  The reference fetches through the texture unit
+// (emission.cuh:121-122), whose weights have 8 fractional bits; here the weights are FP32 and the
+// three interpolations are explicit fmaf in a fixed order (x, then y, then z), which the CPU oracle
+// repeats.
+__device__ __forceinline__ float turb_fetch(const float* __restrict__ slice, float x, float y, float z) {
+    const float xb = (x - floorf(x)) * (float)TURB_NPHI - 0.5f;
+    const float yb = fminf(fmaxf(y * (float)TURB_NLR - 0.5f, -1.f), (float)TURB_NLR);
+    const float zb = fminf(fmaxf(z * (float)TURB_NZ - 0.5f, -1.f), (float)TURB_NZ);
+    const float fi = floorf(xb), fj = floorf(yb), fl = floorf(zb);
+    const float a = xb - fi, b = yb - fj, c = zb - fl;
+    const int i = (int)fi, j = (int)fj, l = (int)fl;
+    const int i0 = i < 0 ? i + TURB_NPHI : i, i1 = i + 1 >= TURB_NPHI ? i + 1 - TURB_NPHI : i + 1;
+    const int j0 = min(max(j, 0), TURB_NLR - 1), j1 = min(max(j + 1, 0), TURB_NLR - 1);
+    const int l0 = min(max(l, 0), TURB_NZ - 1), l1 = min(max(l + 1, 0), TURB_NZ - 1);
+    const float* p00 = slice + ((size_t)l0 * TURB_NLR + j0) * TURB_NPHI;
+    const float* p01 = slice + ((size_t)l0 * TURB_NLR + j1) * TURB_NPHI;
+    const float* p10 = slice + ((size_t)l1 * TURB_NLR + j0) * TURB_NPHI;
+    const float* p11 = slice + ((size_t)l1 * TURB_NLR + j1) * TURB_NPHI;
+    const float v00 = fmaf(a, __ldg(p00 + i1) - __ldg(p00 + i0), __ldg(p00 + i0));
+    const float v01 = fmaf(a, __ldg(p01 + i1) - __ldg(p01 + i0), __ldg(p01 + i0));
+    const float v10 = fmaf(a, __ldg(p10 + i1) - __ldg(p10 + i0), __ldg(p10 + i0));
+    const float v11 = fmaf(a, __ldg(p11 + i1) - __ldg(p11 + i0), __ldg(p11 + i0));
+    const float w0 = fmaf(b, v01 - v00, v00), w1 = fmaf(b, v11 - v10, v10);
+    return fmaf(c, w1 - w0, w0);
+}
+
 // flow_step with the torus turbulence sum `delta` at this point already evaluated (torus_position).
-static __device__ void flow_step(const so_scene& S, const TorusParams& tp, double delta, double r, double u,
-                                 double phi, double t, double lam, double Ecam, double h, double* dI, double* dtau) {
+// With `field` (the frame's baked slices) the reference model's turbulence is sampled as
+// emission.cuh:112-124 does, else its sheared noise is evaluated in place (the turb_nt = 0 path).
+static __device__ void flow_step(const so_scene& S, const so_frame& F, const float* field, const TorusParams& tp,
+                                 double delta, double r, double u, double phi, double t, double lam, double Ecam,
+                                 double h, double* dI, double* dtau) {
     *dI = 0.0;
     *dtau = 0.0;
     const double a = S.a;
@@ -255,8 +287,24 @@ static __device__ void flow_step(const so_scene& S, const TorusParams& tp, doubl
         if (vert < 1e-7) return;
         ne = S.n0 * exp(-S.n_index * log(r)) * vert;
         if (S.flow_turb_amp > 0.f) {
-            float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);
-            ne *= exp((double)(S.flow_turb_amp * n - 0.5f * S.flow_turb_amp * S.flow_turb_amp));
+            if (field) {
+                // two slices around the retarded time t - t_ref(r), interpolated (emission.cuh:112-124)
+                const double tref = F.t - (F.r - r + 2.0 * log(F.r / r));
+                const float y = (float)((log(R) - S.turb_lr0) / (S.turb_lr1 - S.turb_lr0));
+                const float x = (float)(phi * (0.5 / PI));
+                const float w = (float)(0.5 + 0.5 * (z / R) / S.turb_zmax);
+                float sl = (float)((t - tref) - S.turb_d0) / S.turb_dd;
+                sl = fminf(fmaxf(sl, 0.f), (float)(TURB_NT - 1) - 1e-4f);
+                const int k = (int)sl;
+                const float f = sl - (float)k;
+                const size_t slice = (size_t)TURB_NPHI * TURB_NLR * TURB_NZ;
+                const float A = turb_fetch(field + (size_t)k * slice, x, y, w);
+                const float B = turb_fetch(field + (size_t)(k + 1) * slice, x, y, w);
+                ne *= fmaf(B - A, f, A);
+            } else {
+                float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);
+                ne *= exp((double)(S.flow_turb_amp * n - 0.5f * S.flow_turb_amp * S.flow_turb_amp));
+            }
         }
         Th = 0.0;
     }

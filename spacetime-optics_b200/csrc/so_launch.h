@@ -25,6 +25,13 @@ enum Variant : int {
 
 // Device counters of one launch (zeroed before the launch).
 constexpr int REC_SEG = 16;  // flow-step record slots per segment (256 bytes)
+
+// Baked flow turbulence (render.cu:447-460, 594-620): per frame, TURB_NT retarded-time slices of
+// TURB_NPHI x TURB_NLR x TURB_NZ density factors on (phi, ln R, z/R), phi fastest, in HBM.
+constexpr int TURB_NPHI = 512, TURB_NLR = 192, TURB_NZ = 48, TURB_NT = 24;
+struct TurbBake {
+    float delta[TURB_NT];  // retarded-time offset of each slice, d0 + k dd (host float, as render.cu:681)
+};
 constexpr int NLISTS = 10;
 
 struct Counters {
@@ -91,6 +98,7 @@ struct TraceLaunch {
     double r_emit;            // FP32 tracer: outgoing beyond this radius = escaped (0 = off)
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
     int t32_max_att;          // FP32 attempts after which a ray goes to the FP64 re-trace
+    const float* turb_field;  // baked flow turbulence of this frame (NULL: inline sheared noise)
     // batched frames (RAYS_PIXELS over nframes)
     int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
     int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
@@ -123,6 +131,8 @@ struct TraceLaunch {
 cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st);
 cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st);
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
+cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,
+                             cudaStream_t st);
 cudaError_t launch_turb_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);

@@ -93,6 +93,10 @@ struct so_renderer {
     cudaEvent_t ev_turb[2] = {nullptr, nullptr};  // tracer end, sums end
     // attempts of the reference's Mino-time approach of the central ray, for the key below
     int approach_it = 0;
+    // baked flow turbulence (reference flow model with turbulence, radio mode): the frame's slices
+    float* d_turb = nullptr;
+    int flow_noise = SO_FLOW_NOISE_BAKED;
+    TurbBake tb{};
     double approach_key[6] = {-1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     // mixed-path buffers (grown on demand) and the critical-curve table of the current frame
     long long mixed_cap = 0;
@@ -148,7 +152,7 @@ void free_all(so_renderer* r) {
         if (p) cudaFree(p);
     void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked,
                   r->d_nlists, r->d_cnt3, r->d_band, r->d_rec, r->d_rec_delta, r->d_seg_next, r->d_ray_meta,
-                  r->d_acc_list};
+                  r->d_acc_list, r->d_turb};
     for (void* p : pm)
         if (p) cudaFree(p);
     for (int k = 1; k < r->lev.n; ++k)
@@ -209,6 +213,43 @@ int upload_scene(so_renderer* r) {
     r->S.k2_lntab = r->d_k2;
     r->S.bb_xyz = r->d_bb;
     SO_CK(r, cudaMemcpyAsync(r->d_scene, &r->S, sizeof(so_scene), cudaMemcpyHostToDevice, r->st));
+    return SO_OK;
+}
+
+// Baked flow turbulence as Renderer::init sets it up (render.cu:594-620): for a radio scene with
+// the hot flow and its turbulence, TURB_NT slices over ln R in [ln(0.8 r+), ln(1.05 r_flow_max)],
+// z / R within +-min(2, 5 h_r), retarded-time offsets -250 + 260 k / (TURB_NT - 1).  Otherwise (or
+// with SO_FLOW_NOISE_INLINE) turb_nt = 0 and the kernels evaluate the sheared noise in place.  The
+// texture handles of so_scene stay zero: the slices are plain device memory here.
+int turb_setup(so_renderer* r) {
+    so_scene& S = r->S;
+    for (int k = 0; k < 24; ++k) S.turb_tex[k] = 0;
+    const bool bake = S.flow_on && S.mode == SO_MODE_RADIO && S.flow_turb_amp > 0.f &&
+                      r->flow_noise == SO_FLOW_NOISE_BAKED;
+    if (!bake) {
+        S.turb_nt = 0;
+        if (r->d_turb) cudaFree(r->d_turb);
+        r->d_turb = nullptr;
+        return SO_OK;
+    }
+    if (!r->d_turb && dalloc(&r->d_turb, (size_t)TURB_NT * TURB_NPHI * TURB_NLR * TURB_NZ) != cudaSuccess)
+        return fail(r, SO_ERR_ALLOC, "baked turbulence: device allocation");
+    S.turb_nt = TURB_NT;
+    S.turb_lr0 = (float)std::log(0.8 * S.rh);
+    S.turb_lr1 = (float)std::log(S.r_flow_max * 1.05);
+    S.turb_zmax = (float)std::min(2.0, 5.0 * S.h_r);
+    S.turb_d0 = -250.f;
+    S.turb_dd = 260.f / (TURB_NT - 1);
+    for (int k = 0; k < TURB_NT; ++k) r->tb.delta[k] = S.turb_d0 + k * S.turb_dd;
+    return SO_OK;
+}
+
+// Re-bake of the turbulence for the frame just uploaded to d_frame (render.cu:679-682), queued on
+// the renderer's stream, and the slices given to the tracer launch L.
+int bake_turbulence(so_renderer* r, TraceLaunch& L) {
+    if (r->S.turb_nt <= 0 || !r->d_turb) return SO_OK;
+    SO_CK(r, launch_bake_turb(r->d_scene, r->d_frame, r->tb, r->d_turb, r->st));
+    L.turb_field = r->d_turb;
     return SO_OK;
 }
 
@@ -527,6 +568,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
     L.sample0 = 0;
     L.accum = (float*)r->d_accum;
     L.ystat = (float*)r->d_ystat;
+    if (int brc = bake_turbulence(r, L)) return brc;
     if (stats) cudaEventRecord(ev[0], r->st);
     const bool mixed = r->precision == SO_PREC_MIXED;
     int rc = mixed ? trace_pass1_mixed(r, f, L) : run_tracer(r, L);
@@ -837,7 +879,8 @@ int so_init(so_renderer** out, int device, const so_scene* scene, const so_table
         r->S.k2_n = tables->k2_n;
         r->S.bb_n = tables->bb_n;
         r->rs = *rs;
-        rc = upload_scene(r);
+        rc = turb_setup(r);
+        if (!rc) rc = upload_scene(r);
     }
     if (!rc) rc = alloc_frame_buffers(r, rs->W, rs->H);
     if (!rc && cudaStreamSynchronize(r->st) != cudaSuccess) rc = SO_ERR_CUDA;
@@ -854,11 +897,19 @@ int so_init(so_renderer** out, int device, const so_scene* scene, const so_table
 int so_update_scene(so_renderer* r, const so_scene* scene) {
     if (!r || !scene) return fail(r, SO_ERR_ARG, "so_update_scene: NULL argument");
     if (scene->sky_on) return fail(r, SO_ERR_UNSUPPORTED, "sky texture lookups are not supported");
-    int dn = r->S.disk_n, kn = r->S.k2_n, bn = r->S.bb_n;
+    // tables and the baked-turbulence set-up stay as so_init made them (render.cu:658-675)
+    const so_scene keep = r->S;
     r->S = *scene;
-    r->S.disk_n = dn;
-    r->S.k2_n = kn;
-    r->S.bb_n = bn;
+    r->S.disk_n = keep.disk_n;
+    r->S.k2_n = keep.k2_n;
+    r->S.bb_n = keep.bb_n;
+    for (int k = 0; k < 24; ++k) r->S.turb_tex[k] = keep.turb_tex[k];
+    r->S.turb_nt = keep.turb_nt;
+    r->S.turb_lr0 = keep.turb_lr0;
+    r->S.turb_lr1 = keep.turb_lr1;
+    r->S.turb_zmax = keep.turb_zmax;
+    r->S.turb_d0 = keep.turb_d0;
+    r->S.turb_dd = keep.turb_dd;
     return upload_scene(r);
 }
 
@@ -962,6 +1013,7 @@ static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const doubl
     SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
     TraceLaunch L;
     launch_common(r, L);
+    if (int brc = bake_turbulence(r, L)) return brc;
     L.kind = RAYS_LIST;
     L.nrays = n;
     L.x = d_x;
@@ -1085,6 +1137,17 @@ int so_set_plasma(so_renderer* r, const so_plasma* p, const so_mode* modes) {
         SO_CK(r, cudaMemcpy(r->d_modes, modes, (size_t)p->n_modes * sizeof(so_mode), cudaMemcpyHostToDevice));
     }
     return SO_OK;
+}
+
+int so_set_flow_noise(so_renderer* r, int mode) {
+    if (!r) return SO_ERR_ARG;
+    if (mode != SO_FLOW_NOISE_BAKED && mode != SO_FLOW_NOISE_INLINE)
+        return fail(r, SO_ERR_ARG, "so_set_flow_noise: SO_FLOW_NOISE_BAKED or SO_FLOW_NOISE_INLINE");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    r->flow_noise = mode;
+    if (int rc = turb_setup(r)) return rc;
+    return upload_scene(r);
 }
 
 void* so_stream(so_renderer* r) { return r ? (void*)r->st : nullptr; }

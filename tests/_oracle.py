@@ -41,6 +41,8 @@ def oracle():
         L.orc_kerr_point.restype = None
         L.orc_radial_drift.argtypes = [C.c_double, C.c_double, C.c_double, Vec3, C.c_double, C.c_int, P(C.c_int)]
         L.orc_radial_drift.restype = C.c_double
+        L.orc_turb_setup.argtypes = [P(Scene)]
+        L.orc_turb_setup.restype = None
         L.so_rpow5.argtypes = [C.c_double]
         L.so_rpow5.restype = C.c_double
         _orc = L
@@ -83,6 +85,13 @@ def ref():
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def baked(scene):
+    """Copy of scene with the baked flow turbulence set up as the renderer does (orc_turb_setup)."""
+    sc = Scene.from_buffer_copy(scene)
+    oracle().orc_turb_setup(C.byref(sc))
+    return sc
 
 
 def orc_trace(scene, frame, x, y, plasma=None, modes=None, threads=8, cross=False):
