@@ -294,8 +294,10 @@ __device__ __forceinline__ float warp_turbulence(const float4* __restrict__ km, 
 
 // flow_step (emission.cuh:264-340) in FP32, given the turbulence sum delta at this point (torus
 // model).  The reference plasma enters only without its fBm turbulence (see the router).
+// bfac: the reference model's baked turbulence factor at this point (1 without turbulence).
 __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp, float delta, float r, float u,
-                                            float lam, float Ecam, float h, float* dI, float* dtau) {
+                                            float lam, float Ecam, float h, float* dI, float* dtau,
+                                            float bfac = 1.f) {
     *dI = 0.f;
     *dtau = 0.f;
     const float a = (float)S.a;
@@ -316,7 +318,7 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
         float zh = __fdividef(z, (float)S.h_r * R);
         float vert = __expf(-0.5f * zh * zh);
         if (vert < 1e-7f) return;
-        ne = (float)S.n0 * __expf(-(float)S.n_index * __logf(r)) * vert;
+        ne = (float)S.n0 * __expf(-(float)S.n_index * __logf(r)) * vert * bfac;
         Th = (float)S.theta0 * __expf(-(float)S.theta_index * __logf(r));
     }
     float dr = r - rh;
@@ -411,6 +413,8 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     const float step_frac = (float)S.step_frac;
     const float rcam_hi = (float)F.r, rcam_lo = (float)(F.r - (double)(float)F.r);
     const float risco = (float)S.r_isco, flow_kep = (float)S.flow_kep;
+    const float tcam = (float)F.t;
+    const bool baked = VAR == VAR_RADIO && !tp.on && L.turb_field != nullptr && S.flow_turb_amp > 0.f;
     const float r_out = (float)L.r_emit;
     const bool radio = VAR == VAR_RADIO;
     C32 c;
@@ -475,6 +479,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         float nrh = 0.f, nrl = 0.f, nprh = 0.f, nprl = 0.f, nuh = 0.f, nul = 0.f, npuh = 0.f, npul = 0.f;
         float n0 = 0.f, n1 = 0.f, n2 = 0.f, hc = 0.f, err = 0.f, TX = 0.f, TY = 0.f, TZ = 0.f;
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+        float bfac = 1.f;
         float k7[6], dy[6];
         if (active) {
             if (R.it >= S.max_steps || R.natt >= L.t32_max_att) {
@@ -593,6 +598,29 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                             want_turb = true;
                         }
                     }
+                    if (!DEFER && want_flow && baked) {
+                        // the reference flow's baked turbulence (emission.cuh:112-124) at the end of
+                        // the step, its retarded time t - t_ref(r) from the two-float t
+                        float s2 = fmaxf((1.f - n2) * (1.f + n2), 1e-12f);
+                        float Rc = n0 * sqrtf(s2);
+                        if (Rc >= 1e-3f) {
+                            float ph_h = R.phh, ph_l = R.phl, t_h = R.th, t_l = R.tl;
+                            acc2(ph_h, ph_l, dy[4]);
+                            acc2(t_h, t_l, dy[5]);
+                            float tr = (((t_h + rcam_hi) + (t_l + rcam_lo)) - n0 + 2.f * __logf(__fdividef(rcam_hi, n0))) - tcam;
+                            float y = __fdividef(__logf(Rc) - S.turb_lr0, S.turb_lr1 - S.turb_lr0);
+                            float x = (ph_h + ph_l) * (float)(0.5 / PI);
+                            float w = 0.5f + 0.5f * __fdividef(__fdividef(n0 * n2, Rc), S.turb_zmax);
+                            float sl = __fdividef(tr - S.turb_d0, S.turb_dd);
+                            sl = fminf(fmaxf(sl, 0.f), (float)(TURB_NT - 1) - 1e-4f);
+                            const int k = (int)sl;
+                            const float f = sl - (float)k;
+                            const size_t slice = (size_t)TURB_NPHI * TURB_NLR * TURB_NZ;
+                            const float A = turb_fetch(L.turb_field + (size_t)k * slice, x, y, w);
+                            const float B = turb_fetch(L.turb_field + (size_t)(k + 1) * slice, x, y, w);
+                            bfac = fmaf(B - A, f, A);
+                        }
+                    }
                 }
             }
         }
@@ -661,7 +689,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
             if (DEFER && want_flow) ++R.nflow;
             if (!DEFER && want_flow) {
                 float dI, dtau;
-                flow_step32(S, tp, delta, n0, n2, c.lam, c.E, hc, &dI, &dtau);
+                flow_step32(S, tp, delta, n0, n2, c.lam, c.E, hc, &dI, &dtau, bfac);
                 ++R.nflow;
                 float cc = R.trans * dI;
                 int nb = (int)(R.psi * (float)(1.0 / PI));

@@ -472,11 +472,14 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     L.nlists = r->d_nlists;
     SO_CK(r, cudaMemsetAsync(r->d_nlists, 0, NLISTS * sizeof(unsigned long long), r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt3, 0, 2 * sizeof(Counters), r->st));
-    // The reference's sheared fBm turbulence (flow or disk) is evaluated at a noise generation
+    // The reference's sheared fBm turbulence (flow or disk) evaluated in place uses a noise generation
     // k = floor(t / P) of the raw coordinate time t ~ -r_cam: a relative change eps of the radius moves
     // its phase by ~ (t / P) eps, so any integrator that is not the FP64 one decorrelates it.  Such
-    // scenes, and radio scenes with a disk (not in the FP32 tracer), go to FP64 entirely.
-    const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f) ||
+    // scenes, and radio scenes with a disk (not in the FP32 tracer), go to FP64 entirely.  A baked
+    // flow field (L.turb_field) is sampled at the position and at t - t_ref(r), both well conditioned,
+    // so the FP32 tracer takes those scenes.
+    const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f &&
+                        !L.turb_field) ||
                        (r->S.disk_on && r->S.disk_turb_amp > 0.f) || (r->S.mode == SO_MODE_RADIO && r->S.disk_on);
     SO_CK(r, launch_route(L, all64 ? 1 : 0, r->st));
     // band rays: plain FP64 tracer on the second stream, concurrently with the FP32 work

@@ -58,13 +58,34 @@ def test_mixed_turning_point_retrace(so):
 
 
 def test_mixed_reference_fbm_is_all_fp64(so):
-    """The reference's fBm turbulence is ill-conditioned in the coordinate time, so the mixed path
-    traces such scenes entirely in FP64: the image equals the FP64 one bit for bit."""
-    img64, img32, _, st32 = _render_pair(so, "m87_reference_flow.ini", ["camera.width=48", "camera.height=48",
-                                                                         "render.spp=1", "render.spp_max=1"],
-                                         plasma=False)
+    """The reference's fBm turbulence evaluated in place is ill-conditioned in the coordinate time, so
+    the mixed path traces such scenes entirely in FP64: the image equals the FP64 one bit for bit."""
+    sh = so.Shot("m87_reference_flow.ini", ["camera.width=48", "camera.height=48", "render.spp=1",
+                                            "render.spp_max=1"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    img32, _, st32 = r.render(f)
     assert st32.band_rays == 48 * 48 and st32.attempts_fp32 == 0
     assert np.array_equal(img64, img32)
+    r.close()
+
+
+def test_mixed_reference_flow_baked_turbulence(so):
+    """The same flow with its turbulence baked per frame (the renderer's default): sampled at the
+    position and the retarded time, it is well conditioned, and the FP32 tracer takes the rays off
+    the band.  Emission quadrature converged (step fraction 0.01) as for the flow without
+    turbulence: L1 <= 2e-3, flux <= 1e-3 against the FP64 frame with the same baked field."""
+    img64, img32, _, st32 = _render_pair(so, "m87_reference_flow.ini", ["camera.width=96", "camera.height=96",
+                                                                         "render.spp=1", "render.spp_max=1",
+                                                                         "render.step_fraction=0.01"], plasma=False)
+    assert st32.attempts_fp32 > 0 and st32.band_rays < 96 * 96 // 4
+    l1, flux = _errors(img64, img32)
+    assert img64[..., 0].max() > 0
+    assert l1 <= 2e-3 and flux <= 1e-3, (l1, flux)
 
 
 def test_mixed_reference_flow_without_turbulence(so):
