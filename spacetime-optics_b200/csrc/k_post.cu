@@ -113,4 +113,119 @@ cudaError_t post_radio_blur(const PostLevels& L, float4* tmp, double sigma, cuda
     return cudaGetLastError();
 }
 
+// ---- luminance statistics (render.cu:771-790) -----------------------------------------------------
+namespace {
+
+// Y per pixel with the host expression's roundings (float in radio mode, double in visible mode;
+// explicit _rn operations so that no multiply-add is fused), and the block maxima of Y > 0.
+__global__ void __launch_bounds__(256) k_lum(const float4* __restrict__ img, long long n, int radio, float hide,
+                                             float* __restrict__ lum, double* __restrict__ part) {
+    __shared__ double sm[256];
+    double m = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float4 c = img[i];
+        double Y;
+        if (radio) {
+            const float d = fmaxf(__fsub_rn(__fsub_rn(__fsub_rn(c.x, c.y), c.z), c.w), 0.f);
+            Y = (double)__fsub_rn(c.x, __fmul_rn(hide, d));
+        } else {
+            Y = __dadd_rn(__dadd_rn(__dmul_rn(0.2126, (double)c.x), __dmul_rn(0.7152, (double)c.y)),
+                          __dmul_rn(0.0722, (double)c.z));
+        }
+        lum[i] = Y > 0.0 ? (float)Y : -1.f;
+        if (Y > 0.0) m = fmax(m, Y);
+    }
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+
+__global__ void __launch_bounds__(256) k_lum_max(const double* __restrict__ part, int nb, LumStat* st) {
+    __shared__ double sm[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmax(m, part[i]);
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        st->mx = sm[0];
+        st->pv = 0.f;
+        st->nsig = 0;
+        st->k = 0;
+        st->prefix = 0;
+    }
+}
+
+// Radix pass over the significant values (v > mx 1e-5, v as double): pass 0 bins bits 30..19 of the
+// float pattern, pass 1 bits 18..8 of those whose bits 30..19 are the selected prefix, pass 2 bits
+// 7..0 of those whose bits 30..8 are.  (Positive floats order as their bit patterns.)
+__global__ void __launch_bounds__(256) k_lum_hist(const float* __restrict__ lum, long long n, const LumStat* st,
+                                                  int pass, unsigned* __restrict__ hist) {
+    __shared__ unsigned sh[LUM_HIST];
+    for (int b = threadIdx.x; b < LUM_HIST; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+    const double thr = __dmul_rn(st->mx, 1e-5);
+    const unsigned prefix = st->prefix;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float v = lum[i];
+        if (!(v > 0.f) || !((double)v > thr)) continue;
+        const unsigned u = __float_as_uint(v);
+        if (pass == 0) atomicAdd(&sh[(u >> 19) & 4095u], 1u);
+        else if (pass == 1 && (u >> 19) == prefix) atomicAdd(&sh[(u >> 8) & 2047u], 1u);
+        else if (pass == 2 && (u >> 8) == prefix) atomicAdd(&sh[u & 255u], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < LUM_HIST; b += blockDim.x)
+        if (sh[b]) atomicAdd(&hist[b], sh[b]);
+}
+
+// The bin holding rank k (one thread: at most 4096 bins), then the rank inside it.  After pass 0
+// the rank is min(n - 1, (size_t)(percentile (n - 1))) of the n significant values, as the host's.
+__global__ void k_lum_pick(const unsigned* __restrict__ hist, int pass, double percentile, LumStat* st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nb = pass == 0 ? 4096 : pass == 1 ? 2048 : 256;
+    unsigned long long k = st->k;
+    if (pass == 0) {
+        unsigned long long n = 0;
+        for (int b = 0; b < nb; ++b) n += hist[b];
+        st->nsig = n;
+        if (n == 0) return;
+        k = (unsigned long long)(percentile * (double)(n - 1));
+        if (k > n - 1) k = n - 1;
+    }
+    if (st->nsig == 0) return;
+    unsigned long long cum = 0;
+    int b = 0;
+    for (; b < nb - 1; ++b) {
+        if (cum + hist[b] > k) break;
+        cum += hist[b];
+    }
+    st->k = k - cum;
+    if (pass == 0) st->prefix = (unsigned)b;
+    else if (pass == 1) st->prefix = (st->prefix << 11) | (unsigned)b;
+    else st->pv = __uint_as_float((st->prefix << 8) | (unsigned)b);
+}
+
+}  // namespace
+
+cudaError_t post_luminance(const float4* img, long long n, int radio, float hide, double percentile,
+                           const LumScratch& s, cudaStream_t st) {
+    k_lum<<<LUM_BLOCKS, 256, 0, st>>>(img, n, radio, hide, s.lum, s.part);
+    k_lum_max<<<1, 256, 0, st>>>(s.part, LUM_BLOCKS, s.stat);
+    for (int pass = 0; pass < 3; ++pass) {
+        cudaError_t e = cudaMemsetAsync(s.hist, 0, LUM_HIST * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+        k_lum_hist<<<LUM_BLOCKS, 256, 0, st>>>(s.lum, n, s.stat, pass, s.hist);
+        k_lum_pick<<<1, 32, 0, st>>>(s.hist, pass, percentile, s.stat);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace so

@@ -57,6 +57,29 @@ struct PostLevels {
 cudaError_t post_bloom(const PostLevels& L, float strength, cudaStream_t st);
 cudaError_t post_radio_blur(const PostLevels& L, float4* tmp, double sigma, cudaStream_t st);
 
+// Luminance statistics of the HDR frame (render.cu:771-790) on the device: the maximum of Y over
+// the pixels with Y > 0 and the given percentile of the values above 1e-5 of that maximum (an exact
+// order statistic, by radix selection on the float bit patterns).
+struct LumStat {
+    double mx;                // maximum luminance (0 if none positive)
+    float pv;                 // percentile value (0 if no significant pixel)
+    float pad_;
+    unsigned long long nsig;  // significant pixels
+    unsigned long long k;     // rank still to find inside the selected prefix
+    unsigned prefix;          // selected high bits so far
+    unsigned pad2_;
+};
+constexpr int LUM_BLOCKS = 1184;   // grid of the luminance pass (8 x 148)
+constexpr int LUM_HIST = 4096;     // radix bins of the first pass
+struct LumScratch {
+    float* lum;               // per pixel: Y as float, or -1 if Y <= 0
+    double* part;             // LUM_BLOCKS partial maxima
+    unsigned* hist;           // LUM_HIST bins
+    LumStat* stat;
+};
+cudaError_t post_luminance(const float4* img, long long n, int radio, float hide, double percentile,
+                           const LumScratch& s, cudaStream_t st);
+
 struct TraceLaunch {
     const so_scene* scenes;   // device array, indexed by frame_scene[f]
     const so_frame* frames;   // device array

@@ -114,6 +114,9 @@ struct so_renderer {
     // post filters: pyramid levels 1.. of d_img and a scratch frame (allocated on first use)
     PostLevels lev{};
     float4* d_tmp = nullptr;
+    // luminance statistics of so_render (device buffers and the pinned result)
+    LumScratch lum{};
+    LumStat* h_lum = nullptr;
     std::string err;
 };
 
@@ -164,6 +167,10 @@ void free_all(so_renderer* r) {
         if (e) cudaEventDestroy(e);
     if (r->ev_seg) cudaEventDestroy(r->ev_seg);
     if (r->h_seg) cudaFreeHost(r->h_seg);
+    void* pl[] = {r->lum.lum, r->lum.part, r->lum.hist, r->lum.stat};
+    for (void* p : pl)
+        if (p) cudaFree(p);
+    if (r->h_lum) cudaFreeHost(r->h_lum);
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
     if (r->st2) cudaStreamDestroy(r->st2);
@@ -274,6 +281,16 @@ void launch_common(so_renderer* r, TraceLaunch& L) {
     L.tol32 = r->mixed.tol32;
     L.turn_r = r->mixed.turn_r;
     L.drift_tol = r->mixed.drift_tol;
+}
+
+// Buffers of the device luminance statistics (allocated on the first so_render).
+int ensure_lum(so_renderer* r) {
+    if (r->lum.lum) return SO_OK;
+    if (dalloc(&r->lum.lum, (size_t)r->npix) != cudaSuccess || dalloc(&r->lum.part, LUM_BLOCKS) != cudaSuccess ||
+        dalloc(&r->lum.hist, LUM_HIST) != cudaSuccess || dalloc(&r->lum.stat, 1) != cudaSuccess)
+        return fail(r, SO_ERR_ALLOC, "luminance statistics: device allocation");
+    SO_CK(r, cudaMallocHost((void**)&r->h_lum, sizeof(LumStat)));
+    return SO_OK;
 }
 
 // Pyramid of the frame for the post filters, level sizes as the reference's (render.cu:638-647).
@@ -921,6 +938,7 @@ int so_render(so_renderer* r, const so_frame* f_in, const so_post* post, double 
     if (!r || !f_in || !out || !out->px) return fail(r, SO_ERR_ARG, "so_render: NULL argument");
     if (post && (!(post->bloom >= 0.f && post->bloom <= 1.f) || !(post->blur_sigma_px >= 0.0)))
         return fail(r, SO_ERR_ARG, "so_render: bloom must be in [0, 1] and blur_sigma_px >= 0");
+    if (!(percentile >= 0.0 && percentile <= 1.0)) return fail(r, SO_ERR_ARG, "so_render: percentile must be in [0, 1]");
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
     so_frame f = *f_in;
     f.W = r->rs.W;
@@ -940,33 +958,18 @@ int so_render(so_renderer* r, const so_frame* f_in, const so_post* post, double 
     }
     out->W = f.W;
     out->H = f.H;
-    SO_CK(r, cudaMemcpyAsync(out->px, r->d_img, (size_t)r->npix * sizeof(float4), cudaMemcpyDeviceToHost, r->st));
-    SO_CK(r, cudaStreamSynchronize(r->st));
-    // Luminance percentile over significant pixels (render.cu:771-790)
+    // Luminance percentile over significant pixels (render.cu:771-790), on the device: Y per pixel
+    // (radio: I minus hide_direct times the direct light, visible: Rec. 709 luma), its maximum, and
+    // the percentile of the values above 1e-5 of the maximum (the same order statistic as the
+    // reference's nth_element), read back with the frame
     const float hide = post ? post->hide_direct : 0.f;
-    std::vector<float> lum;
-    lum.reserve((size_t)r->npix);
-    double mx = 0;
-    for (long long i = 0; i < r->npix; ++i) {
-        const float* c = &out->px[4 * i];
-        double Y = r->S.mode == SO_MODE_RADIO ? c[0] - hide * std::max(c[0] - c[1] - c[2] - c[3], 0.f)
-                                              : 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2];
-        if (Y > 0) {
-            lum.push_back((float)Y);
-            mx = std::max(mx, Y);
-        }
-    }
-    std::vector<float> sig;
-    for (float v : lum)
-        if (v > mx * 1e-5) sig.push_back(v);
-    double pv = 0;
-    if (!sig.empty()) {
-        size_t idx = std::min(sig.size() - 1, (size_t)(percentile * (sig.size() - 1)));
-        std::nth_element(sig.begin(), sig.begin() + idx, sig.end());
-        pv = sig[idx];
-    }
-    out->lum_percentile = pv;
-    out->lum_max = mx;
+    if (int lrc = ensure_lum(r)) return lrc;
+    SO_CK(r, post_luminance(r->d_img, r->npix, r->S.mode == SO_MODE_RADIO, hide, percentile, r->lum, r->st));
+    SO_CK(r, cudaMemcpyAsync(out->px, r->d_img, (size_t)r->npix * sizeof(float4), cudaMemcpyDeviceToHost, r->st));
+    SO_CK(r, cudaMemcpyAsync(r->h_lum, r->lum.stat, sizeof(LumStat), cudaMemcpyDeviceToHost, r->st));
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    out->lum_percentile = r->h_lum->nsig ? (double)r->h_lum->pv : 0.0;
+    out->lum_max = r->h_lum->mx;
     if (stats) {
         stats->ms_trace = t1 - t0;
         stats->ms_post = now_ms() - t1;

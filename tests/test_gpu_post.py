@@ -36,3 +36,43 @@ def test_visible_glare_matches_oracle(so, orc):
     assert err <= 1e-5, err
     assert np.array_equal(out[..., 3], img[..., 3])  # the order channel is untouched
     r.close()
+
+
+def _lum_stats(img, radio, hide, p):
+    """The reference's host luminance statistics (render.cu:771-790) in numpy, same roundings."""
+    c = img.reshape(-1, 4).astype(np.float32)
+    if radio:
+        d = np.maximum(((c[:, 0] - c[:, 1]) - c[:, 2]) - c[:, 3], np.float32(0))
+        Y = (c[:, 0] - np.float32(hide) * d).astype(np.float64)
+    else:
+        Y = (0.2126 * c[:, 0].astype(np.float64) + 0.7152 * c[:, 1].astype(np.float64)) + \
+            0.0722 * c[:, 2].astype(np.float64)
+    pos = Y > 0
+    mx = float(Y[pos].max()) if pos.any() else 0.0
+    lum = Y[pos].astype(np.float32)
+    sig = lum[lum.astype(np.float64) > mx * 1e-5]
+    if sig.size == 0:
+        return 0.0, mx
+    idx = min(sig.size - 1, int(p * (sig.size - 1)))
+    return float(np.partition(sig, idx)[idx]), mx
+
+
+@pytest.mark.parametrize("shot, radio, hide, pct", [
+    ("m87_reference_flow.ini", True, 0.0, 0.995),
+    ("m87_reference_flow.ini", True, 0.6, 0.5),
+    ("thin_disk_4096.ini", False, 0.0, 0.9),
+    ("thin_disk_4096.ini", False, 0.0, 1.0),
+])
+def test_luminance_statistics_exact(so, shot, radio, hide, pct):
+    """so_render's luminance maximum and percentile (computed on the device by radix selection) are
+    exactly the reference's host statistics of the returned frame."""
+    sh = so.Shot(shot, ["camera.width=80", "camera.height=60", "render.spp=1", "render.spp_max=1"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    img, hdr, _ = r.render(sh.frame(0), percentile=pct, hide_direct=hide)
+    pv, mx = _lum_stats(img, radio, hide, pct)
+    assert mx > 0
+    assert hdr.lum_max == mx, (hdr.lum_max, mx)
+    assert hdr.lum_percentile == pv, (hdr.lum_percentile, pv)
+    with pytest.raises(so.TracerError):
+        r.render(sh.frame(0), percentile=1.5)
+    r.close()
