@@ -801,24 +801,17 @@ __device__ __forceinline__ Torus32 torus32_of(const TraceLaunch& L) {
 
 // Turbulence sum at every record slot in use: the records' positions (the tracer's in-line form:
 // R = r sqrt(max((1-u)(1+u), 1e-12)), x = R cos phi_c, y = R sin phi_c, z = r u), TURB_P positions
-// per thread, the modes broadcast from shared memory, so every lane does the same work and the SFU
+// per thread, the modes read from constant memory (the kernel parameter M, the same address for the
+// whole warp: no shared-memory loads in the MIO queue that feeds the SFU), so every lane does the
+// same work and the SFU
 // cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine and one FMA per mode
 // and position).  Blocks take chunks of TURB_P x 256 slots from a work counter, so SMs that also
 // host the FP64 re-trace (on the other stream) do less of it instead of finishing last.  Slots of
 // a segment past its ray's last record hold stale data; their sums are never read.
 constexpr int TURB_P = 8;
 constexpr int TURB_CHUNK = TURB_P * 256;
-__global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
-    extern __shared__ float4 sm4[];
-    const int nm = L.n_modes;
-    float4* km = sm4;
-    float* amp = reinterpret_cast<float*>(sm4 + nm);
-    for (int i = threadIdx.x; i < nm; i += blockDim.x) {
-        so_mode m = L.modes[i];
-        double ph = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
-        km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)ph);
-        amp[i] = (float)m.amp;
-    }
+__global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L, const __grid_constant__ TurbModes M) {
+    const int nm = M.n;
     __shared__ long long chunk;
     unsigned long long used = L.nlists[5];
     if (used > (unsigned long long)L.seg_cap) used = (unsigned long long)L.seg_cap;
@@ -846,8 +839,8 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L) {
         }
 #pragma unroll 2
         for (int m = 0; m < nm; ++m) {
-            const float4 k = km[m];
-            const float am = amp[m];
+            const float4 k = M.k[m];
+            const float am = M.a[m];
 #pragma unroll
             for (int q = 0; q < TURB_P; ++q)
                 acc[q] = fmaf(am, __cosf(fmaf(k.z, z[q], fmaf(k.y, y[q], fmaf(k.x, x[q], k.w)))), acc[q]);
@@ -932,16 +925,21 @@ __global__ void __launch_bounds__(256) k_flow_records(const TraceLaunch L) {
 }
 
 // ---- launchers -----------------------------------------------------------------------------------
-cudaError_t launch_turb_records(const TraceLaunch& L, int num_sms, cudaStream_t st) {
-    const size_t smem = (size_t)L.n_modes * (sizeof(float4) + sizeof(float));
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_turb_records, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+void turb_modes_fold(const so_mode* modes, int n, TurbModes* out) {
+    out->n = n;
+    for (int i = 0; i < n; ++i) {
+        const so_mode& m = modes[i];
+        const double ph = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
+        out->k[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)ph);
+        out->a[i] = (float)m.amp;
     }
+}
+
+cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st) {
     int per_sm = 1;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_turb_records, 256, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_turb_records, 256, 0);
     if (e != cudaSuccess) return e;
-    k_turb_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, smem, st>>>(L);
+    k_turb_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, st>>>(L, M);
     return cudaGetLastError();
 }
 

@@ -156,7 +156,15 @@ cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cu
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
 cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,
                              cudaStream_t st);
-cudaError_t launch_turb_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
+// Fourier modes of the torus turbulence in FP32 (phase folded into (-pi, pi]), passed to the batched
+// sums as a kernel parameter (constant memory; up to SO_MAX_MODES = 1024, 20 KB).
+struct TurbModes {
+    float4 k[SO_MAX_MODES];  // kx, ky, kz, phase
+    float a[SO_MAX_MODES];   // amplitude
+    int n;
+};
+void turb_modes_fold(const so_mode* modes, int n, TurbModes* out);
+cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
 cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);
 

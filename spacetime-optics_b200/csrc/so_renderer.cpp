@@ -76,6 +76,7 @@ struct so_renderer {
     // plasma / precision
     so_plasma plasma{};
     so_mode* d_modes = nullptr;
+    TurbModes* turb_modes = nullptr;  // the modes folded to FP32 for the batched turbulence sums
     int precision = SO_PREC_FP64;
     so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0};
     // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
@@ -171,6 +172,7 @@ void free_all(so_renderer* r) {
     for (void* p : pl)
         if (p) cudaFree(p);
     if (r->h_lum) cudaFreeHost(r->h_lum);
+    delete r->turb_modes;
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
     if (r->st2) cudaStreamDestroy(r->st2);
@@ -538,7 +540,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
     if (defer) {
         SO_CK(r, cudaEventRecord(r->ev_turb[0], r->st));
-        SO_CK(r, launch_turb_records(L, r->num_sms, r->st));
+        SO_CK(r, launch_turb_records(L, *r->turb_modes, r->num_sms, r->st));
         SO_CK(r, cudaEventRecord(r->ev_turb[1], r->st));
         SO_CK(r, launch_flow_records(L, r->num_sms, r->st));
         SO_CK(r, cudaMemcpyAsync(r->h_seg, &r->d_nlists[5], 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -1141,6 +1143,8 @@ int so_set_plasma(so_renderer* r, const so_plasma* p, const so_mode* modes) {
     if (p->model == SO_PLASMA_TORUS && p->n_modes > 0) {
         if (dalloc(&r->d_modes, (size_t)p->n_modes) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "modes alloc");
         SO_CK(r, cudaMemcpy(r->d_modes, modes, (size_t)p->n_modes * sizeof(so_mode), cudaMemcpyHostToDevice));
+        if (!r->turb_modes) r->turb_modes = new TurbModes;
+        turb_modes_fold(modes, p->n_modes, r->turb_modes);
     }
     return SO_OK;
 }
