@@ -49,7 +49,7 @@ enum {
     SO_ERR_STATE = 6,      /* call not valid in the renderer's current state */
     SO_ERR_WATCHDOG = 7,   /* a device-side bounded wait gave up (persistent queue) */
     SO_ERR_SIZE = 8,       /* request larger than a fixed capacity */
-    SO_ERR_UNSUPPORTED = 9 /* option outside the implemented path (e.g. sky texture lookups) */
+    SO_ERR_UNSUPPORTED = 9 /* option outside the implemented path (e.g. the star map in batched frames) */
 };
 
 /* ---- enums shared with the reference (scene.hpp:16) ------------------------------------------ */
@@ -248,7 +248,8 @@ typedef struct so_mixed_opts {
 typedef struct so_renderer so_renderer;
 
 /* Renderer::init (render.cu:531-656).  Creates the CUDA stream, uploads the tables and allocates
- * the frame buffers for rs->W x rs->H.  The sky texture is not supported (scene->sky_on must be 0).
+ * the frame buffers for rs->W x rs->H.  The star map (Renderer::init's SkyTexture) is given
+ * afterwards by so_set_sky.
  * On failure *out is NULL and the status says why (no process abort). */
 int so_init(so_renderer** out, int device, const so_scene* scene, const so_tables* tables,
             const so_settings* rs);
@@ -288,6 +289,22 @@ int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_frame, int 
 /* Same as so_trace_rays with x, y and the outputs already in device memory (device pointers). */
 int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
                          const so_rays_out* d_out);
+/* The star map of Renderer::init's SkyTexture (renderer.hpp:14-17, render.cu:550-593): w x h texels
+ * of half2 (brightness s, s T / 1e4) as 16-bit halves, row-major.  Made a mipmapped texture (box-
+ * filtered levels down to 1 x 1) sampled as the reference samples it (bilinear and between levels,
+ * anisotropy up to 16, u wrapped, v clamped).  Used when the scene given to so_init asked for the sky
+ * (sky_on) and the mode is visible: every frame then traces the (W + 1) x (H + 1) pixel corners first
+ * (k_corners) for the pixel footprints, and each escaping sample adds the star map's blackbody
+ * radiance through its footprint (trace.cuh:149-161).  Without so_set_sky no sky is drawn, as the
+ * reference without a texture.  Frames with the sky run in FP64 on the mixed path too. */
+int so_set_sky(so_renderer* r, int w, int h, const uint16_t* data);
+/* load_sky (scene_build.cpp:61-81): a .bhsk star map (uint32 magic "BHSK", width, height, float
+ * brightness scale, then width x height half2 texels).  With data NULL only the header is read
+ * (w, h, scale); else data receives w * h * 2 halves.  The reference multiplies sky.brightness
+ * (so_scene.sky_scale) by the file's scale (main.cpp:461-467).  SO_ERR_CONFIG for a missing or bad
+ * file. */
+int so_sky_file(const char* path, int* w, int* h, float* scale, uint16_t* data);
+
 /* Flow turbulence of the reference plasma model (radio mode, flow.turbulence > 0).
  * SO_FLOW_NOISE_BAKED (so_init's choice, as Renderer::init's, render.cu:594-620): before every
  * trace of a frame its turbulence is baked into 24 retarded-time slices of 512 x 192 x 48 density

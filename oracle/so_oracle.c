@@ -559,6 +559,30 @@ typedef struct {
 } RayOut;
 
 /* trace_ray, trace.cuh:62-165 (sky lookups excluded: the sky texture is outside this path). */
+/* Sky of the visible mode (trace.cuh:24-43, 149-161) for an analytic star map: brightness
+ * s(u, v) = c0 + cu u + cv v at a fixed temperature T (the texture unit's filtering of a sampled map
+ * has no CPU form; a constant map, which every filter returns unchanged, checks the rest exactly). */
+static double g_sky[4] = {0.0, 0.0, 0.0, 0.0}; /* c0, cu, cv, T; c0 = cu = cv = 0: no sky */
+void orc_set_sky(double c0, double cu, double cv, double T) {
+    g_sky[0] = c0;
+    g_sky[1] = cu;
+    g_sky[2] = cv;
+    g_sky[3] = T;
+}
+static void sky_uv(const so_scene* S, double th, double ph, float* u, float* v) { /* trace.cuh:24-33 */
+    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+    const double dx = st * cp, dy = st * sp, dz = ct;
+    const so_mat3* m = &S->sky_rot;
+    const double gx = fma(m->r0.z, dz, fma(m->r0.y, dy, m->r0.x * dx));
+    const double gy = fma(m->r1.z, dz, fma(m->r1.y, dy, m->r1.x * dx));
+    const double gz = fma(m->r2.z, dz, fma(m->r2.y, dy, m->r2.x * dx));
+    const double l = atan2(gy, gx), b = asin(fmax(-1.0, fmin(1.0, gz)));
+    float uu = (float)(0.5 - l * (0.5 / PI_D));
+    uu -= floorf(uu);
+    *u = uu;
+    *v = (float)(0.5 - b / PI_D);
+}
+
 static void trace_ray(const Ctx* X, double x, double yv, RayOut* o) {
     const so_scene* S = X->S;
     const so_frame* F = X->F;
@@ -671,6 +695,21 @@ static void trace_ray(const Ctx* X, double x, double yv, RayOut* o) {
         if (y[0] > S->r_escape && y[1] > 0.0) {
             o->fate = 1;
             escape_angles(y, k1, &o->th, &o->ph);
+            if (!radio && S->sky_on && (g_sky[0] != 0.0 || g_sky[1] != 0.0 || g_sky[2] != 0.0)) {
+                float u, v;
+                sky_uv(S, o->th, o->ph, &u, &v);
+                const float s = (float)(g_sky[0] + g_sky[1] * u + g_sky[2] * v);
+                if (s > 0.f) {
+                    const float T = (float)g_sky[3];
+                    const float g = (float)(1.0 / c.E);
+                    float xyz[3];
+                    blackbody_xyz(S, g * T, xyz);
+                    const float sc = s * S->sky_scale, tf = (float)trans;
+                    o->acc[0] += tf * (xyz[0] * sc);
+                    o->acc[1] += tf * (xyz[1] * sc);
+                    o->acc[2] += tf * (xyz[2] * sc);
+                }
+            }
             break;
         }
     }

@@ -57,6 +57,8 @@ def lib():
         L.so_set_precision.argtypes = [vp, C.c_int, P(MixedOpts)]
         L.so_set_plasma.argtypes = [vp, P(Plasma), P(Mode)]
         L.so_set_flow_noise.argtypes = [vp, C.c_int]
+        L.so_set_sky.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.so_sky_file.argtypes = [C.c_char_p, P(C.c_int), P(C.c_int), P(C.c_float), vp]
         L.so_stream.argtypes = [vp]
         L.so_stream.restype = vp
         L.so_last_error.argtypes = [vp]
@@ -184,6 +186,15 @@ class Shot:
         return p
 
 
+def sky_file(path):
+    """so_sky_file: (texels uint16 [h, w, 2], scale) of a .bhsk star map."""
+    w, h, sc = C.c_int(), C.c_int(), C.c_float()
+    _check(lib().so_sky_file(path.encode(), C.byref(w), C.byref(h), C.byref(sc), None))
+    t = np.empty((h.value, w.value, 2), np.uint16)
+    _check(lib().so_sky_file(path.encode(), C.byref(w), C.byref(h), C.byref(sc), t.ctypes.data_as(C.c_void_p)))
+    return t, sc.value
+
+
 def approach_state(scene, frame, x, y, r1, tol, method):
     """so_approach_state: (state [r, r', u, u', phi, t], attempts) of the backward ray through image
     point (x, y) at radius r1; method 0 = far-field transport in 1/r, 1 = Mino-time DP5(4)."""
@@ -230,6 +241,13 @@ class Renderer:
     def update_scene(self, scene):
         self.scene = scene
         _check(lib().so_update_scene(self.h, C.byref(scene)), self.h)
+
+    def set_sky(self, texels):
+        """Star map (so_set_sky): uint16 array [h, w, 2] of half2 texels (s, s T / 1e4)."""
+        t = np.ascontiguousarray(texels, np.uint16)
+        if t.ndim != 3 or t.shape[2] != 2:
+            raise ValueError("texels must be [h, w, 2] uint16")
+        _check(lib().so_set_sky(self.h, t.shape[1], t.shape[0], t.ctypes.data_as(C.c_void_p)), self.h)
 
     def set_flow_noise(self, mode):
         """Reference flow turbulence: abi.SO_FLOW_NOISE_BAKED (default) or abi.SO_FLOW_NOISE_INLINE."""

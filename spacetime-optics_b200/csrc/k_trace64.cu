@@ -21,6 +21,7 @@
 // than FP32.
 //
 // Compiled with -fmad=false: every fusion is an explicit fma() (so_kerr.cuh), matching the oracle.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "so_emission.cuh"
@@ -415,6 +416,17 @@ __global__ void __launch_bounds__(128) k_trace64(const TraceLaunch L) {
         n_acc += (unsigned long long)R.nacc;
         n_flow += (unsigned long long)R.nflow;
         if (fate == 0) ++n_lim;
+        if (VAR != VAR_RADIO && fate == 1 && L.sky_uv && L.kind != RAYS_LIST) {
+            // escaped in visible mode: the star map through the pixel's footprint (trace.cuh:149-161)
+            const int px = (int)(pix % L.W), py = (int)(pix / L.W);
+            const SkyGrad g = pixel_grad(L.sky_uv, L.W, px, py, L.sky_grad_scale);
+            float xyz[3];
+            sky_radiance(*S, sky_uv(*S, th, ph), g, R.c.E, xyz);
+            const float tf = (float)R.trans;
+            R.acc[0] += tf * xyz[0];
+            R.acc[1] += tf * xyz[1];
+            R.acc[2] += tf * xyz[2];
+        }
         if (L.kind == RAYS_LIST) {
             const so_rays_out& o = L.out;
             if (o.fate) o.fate[job] = (int8_t)fate;
@@ -492,6 +504,59 @@ __global__ void __launch_bounds__(256) k_bake_turb(const so_scene* __restrict__ 
     const float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);
     const float a = S.flow_turb_amp;
     field[(((size_t)k * TURB_NZ + l) * TURB_NLR + j) * TURB_NPHI + i] = __expf(a * n - 0.5f * a * a);
+}
+
+// Pixel corners (k_corners, render.cu:40-52): corner (x, y) of a W x H frame at tangent-plane point
+// ((x - W/2) pix, (H/2 - y) pix), x in [0, W], y in [0, H].
+__global__ void k_corner_points(const so_frame* __restrict__ Fp, int W, int H, double* __restrict__ xs,
+                                double* __restrict__ ys) {
+    const long long n = (long long)(W + 1) * (H + 1);
+    const double pix = Fp->pix;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % (W + 1)), y = (int)(i / (W + 1));
+        xs[i] = (x - 0.5 * W) * pix;
+        ys[i] = (0.5 * H - y) * pix;
+    }
+}
+
+__global__ void k_corner_uv(const so_scene* __restrict__ Sp, long long n, const int8_t* __restrict__ fate,
+                            const double* __restrict__ th, const double* __restrict__ ph, float2* __restrict__ uv) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        uv[i] = fate[i] == 1 ? sky_uv(*Sp, th[i], ph[i]) : make_float2(-1.f, -1.f);
+}
+
+// One mip level of the star map (k_mip_half2, render.cu:462-475): mean of the 2 x 2 texels below
+// (indices clamped to the level above), rounded to half.
+__global__ void k_mip_half2(cudaSurfaceObject_t src, int sw, int sh, cudaSurfaceObject_t dst, int dw, int dh) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= dw || y >= dh) return;
+    float a = 0.f, b = 0.f;
+    for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+            ushort2 v;
+            surf2Dread(&v, src, min(2 * x + i, sw - 1) * 4, min(2 * y + j, sh - 1));
+            a += __half2float(__ushort_as_half(v.x));
+            b += __half2float(__ushort_as_half(v.y));
+        }
+    surf2Dwrite(make_ushort2(__half_as_ushort(__float2half(0.25f * a)), __half_as_ushort(__float2half(0.25f * b))), dst,
+                x * 4, y);
+}
+
+cudaError_t launch_corner_points(const so_frame* d_frame, int W, int H, double* x, double* y, cudaStream_t st) {
+    k_corner_points<<<592, 256, 0, st>>>(d_frame, W, H, x, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corner_uv(const so_scene* d_scene, long long n, const int8_t* fate, const double* th,
+                             const double* ph, float2* uv, cudaStream_t st) {
+    k_corner_uv<<<592, 256, 0, st>>>(d_scene, n, fate, th, ph, uv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mip_half2(cudaSurfaceObject_t src, int sw, int sh, cudaSurfaceObject_t dst, int dw, int dh,
+                             cudaStream_t st) {
+    k_mip_half2<<<dim3((dw + 15) / 16, (dh + 15) / 16), dim3(16, 16), 0, st>>>(src, sw, sh, dst, dw, dh);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,

@@ -359,4 +359,60 @@ __device__ __forceinline__ void escape_angles(const double* y, const double* k, 
     *ph = fma(y[0], dphdr, y[4]);
 }
 
+// sky_uv (trace.cuh:24-33): galactic texture coordinates of an escape direction, u wrapped into [0, 1).
+__device__ __forceinline__ float2 sky_uv(const so_scene& S, double th, double ph) {
+    double st, ct, sp, cp;
+    sincos(th, &st, &ct);
+    sincos(ph, &sp, &cp);
+    const double dx = st * cp, dy = st * sp, dz = ct;
+    const so_mat3& m = S.sky_rot;
+    const double gx = fma(m.r0.z, dz, fma(m.r0.y, dy, m.r0.x * dx));
+    const double gy = fma(m.r1.z, dz, fma(m.r1.y, dy, m.r1.x * dx));
+    const double gz = fma(m.r2.z, dz, fma(m.r2.y, dy, m.r2.x * dx));
+    const double l = atan2(gy, gx), b = asin(fmax(-1.0, fmin(1.0, gz)));
+    float u = (float)(0.5 - l * (0.5 / PI));
+    u -= floorf(u);
+    return make_float2(u, (float)(0.5 - b / PI));
+}
+
+// pixel_grad (render.cu:56-72): the pixel's footprint on the sky from the escape coordinates of its
+// four corners (uv grid of (W + 1) x (H + 1), (-1, -1) where a corner ray did not escape), u
+// differences wrapped; a footprint that touches a non-escaping corner gets a fixed 0.02 box.
+struct SkyGrad {
+    float2 dx, dy;
+};
+__device__ __forceinline__ float wrapd(float d) { return d > 0.5f ? d - 1.f : (d < -0.5f ? d + 1.f : d); }
+__device__ __forceinline__ SkyGrad pixel_grad(const float2* __restrict__ uv, int W, int px, int py, float scale) {
+    const int W1 = W + 1;
+    const float2 a = uv[(long long)py * W1 + px], b = uv[(long long)py * W1 + px + 1];
+    const float2 c = uv[(long long)(py + 1) * W1 + px], d = uv[(long long)(py + 1) * W1 + px + 1];
+    SkyGrad g;
+    if (a.x < 0.f || b.x < 0.f || c.x < 0.f || d.x < 0.f) {
+        g.dx = make_float2(0.02f, 0.f);
+        g.dy = make_float2(0.f, 0.02f);
+        return g;
+    }
+    const float dux = 0.5f * (wrapd(b.x - a.x) + wrapd(d.x - c.x)), dvx = 0.5f * ((b.y - a.y) + (d.y - c.y));
+    const float duy = 0.5f * (wrapd(c.x - a.x) + wrapd(d.x - b.x)), dvy = 0.5f * ((c.y - a.y) + (d.y - b.y));
+    g.dx = make_float2(dux * scale, dvx * scale);
+    g.dy = make_float2(duy * scale, dvy * scale);
+    return g;
+}
+
+// sky_radiance (trace.cuh:35-43): star-map texel (s, s T / 1e4) by the texture unit's anisotropic
+// mip filtering over the pixel footprint, shifted by the photon's energy at the camera.
+__device__ __forceinline__ void sky_radiance(const so_scene& S, float2 uv, const SkyGrad& gr, double Ecam,
+                                             float* xyz) {
+    const float2 v = tex2DGrad<float2>((cudaTextureObject_t)S.sky_tex, uv.x, uv.y, gr.dx, gr.dy);
+    xyz[0] = xyz[1] = xyz[2] = 0.f;
+    if (v.x <= 0.f) return;
+    const float T = 1e4f * v.y / v.x;
+    const float g = (float)(1.0 / Ecam);
+    blackbody_xyz(S, g * T, xyz);
+    const float s = v.x * S.sky_scale;
+    xyz[0] *= s;
+    xyz[1] *= s;
+    xyz[2] *= s;
+}
+
 }  // namespace so

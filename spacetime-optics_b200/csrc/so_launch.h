@@ -122,6 +122,9 @@ struct TraceLaunch {
     int t32_min_blocks;       // FP32 tracer register budget: resident CTAs per SM (4, 5 or 6)
     int t32_max_att;          // FP32 attempts after which a ray goes to the FP64 re-trace
     const float* turb_field;  // baked flow turbulence of this frame (NULL: inline sheared noise)
+    const float2* sky_uv;     // visible mode with the star map: escape (u, v) of the pixel corners,
+                              // (W + 1) x (H + 1), for the footprint of each pixel (NULL: no sky)
+    float sky_grad_scale;     // footprint scale: 0.7 in pass 1, 0.5 in pass 2 (render.cu:102, 214)
     // batched frames (RAYS_PIXELS over nframes)
     int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
     int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
@@ -155,6 +158,13 @@ cudaError_t launch_route(const TraceLaunch& L, int all64, cudaStream_t st);
 cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cudaStream_t st);
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
 cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,
+                             cudaStream_t st);
+// Sky: tangent-plane points of the (W + 1) x (H + 1) pixel corners of the frame in d_frame, the
+// corners' escape (u, v) from the tracer's outputs, and one box-filtered half2 mip level.
+cudaError_t launch_corner_points(const so_frame* d_frame, int W, int H, double* x, double* y, cudaStream_t st);
+cudaError_t launch_corner_uv(const so_scene* d_scene, long long n, const int8_t* fate, const double* th,
+                             const double* ph, float2* uv, cudaStream_t st);
+cudaError_t launch_mip_half2(cudaSurfaceObject_t src, int sw, int sh, cudaSurfaceObject_t dst, int dw, int dh,
                              cudaStream_t st);
 // Fourier modes of the torus turbulence in FP32 (phase folded into (-pi, pi]), passed to the batched
 // sums as a kernel parameter (constant memory; up to SO_MAX_MODES = 1024, 20 KB).

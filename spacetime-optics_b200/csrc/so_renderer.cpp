@@ -115,6 +115,15 @@ struct so_renderer {
     // post filters: pyramid levels 1.. of d_img and a scratch frame (allocated on first use)
     PostLevels lev{};
     float4* d_tmp = nullptr;
+    // star map (visible mode): mipmapped half2 texture and the pixel-corner escape coordinates
+    int sky_requested = 0;  // the scene asked for the sky (sky_on at so_init)
+    cudaMipmappedArray_t sky_mip = nullptr;
+    cudaTextureObject_t sky_tex = 0;
+    double *d_cx = nullptr, *d_cy = nullptr, *d_cth = nullptr, *d_cph = nullptr;
+    int8_t* d_cfate = nullptr;
+    float2* d_uvgrid = nullptr;
+    long long corner_cap = 0;
+    Counters* d_cnt_corner = nullptr;
     // luminance statistics of so_render (device buffers and the pinned result)
     LumScratch lum{};
     LumStat* h_lum = nullptr;
@@ -172,6 +181,11 @@ void free_all(so_renderer* r) {
     for (void* p : pl)
         if (p) cudaFree(p);
     if (r->h_lum) cudaFreeHost(r->h_lum);
+    void* pc[] = {r->d_cx, r->d_cy, r->d_cth, r->d_cph, r->d_cfate, r->d_uvgrid, r->d_cnt_corner};
+    for (void* p : pc)
+        if (p) cudaFree(p);
+    if (r->sky_tex) cudaDestroyTextureObject(r->sky_tex);
+    if (r->sky_mip) cudaFreeMipmappedArray(r->sky_mip);
     delete r->turb_modes;
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
@@ -333,6 +347,45 @@ int ensure_side_queue(so_renderer* r) {
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
     cudaError_t e = launch_trace64(L, variant_of(r->S), r->num_sms, st ? st : r->st);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
+    return SO_OK;
+}
+
+// Escape (u, v) of the (W + 1) x (H + 1) pixel corners of the frame in d_frame (k_corners,
+// render.cu:40-52, 686-691): the corner rays through the tracer's ray list (own counters), then
+// sky_uv of those that escape.  Gives the pixel footprints for the star-map filtering.
+int trace_corners(so_renderer* r, int W, int H) {
+    const long long n = (long long)(W + 1) * (H + 1);
+    if (n > r->corner_cap) {
+        void* pc[] = {r->d_cx, r->d_cy, r->d_cth, r->d_cph, r->d_cfate, r->d_uvgrid};
+        for (void* p : pc)
+            if (p) cudaFree(p);
+        r->d_cx = r->d_cy = r->d_cth = r->d_cph = nullptr;
+        r->d_cfate = nullptr;
+        r->d_uvgrid = nullptr;
+        r->corner_cap = 0;
+        if (dalloc(&r->d_cx, (size_t)n) != cudaSuccess || dalloc(&r->d_cy, (size_t)n) != cudaSuccess ||
+            dalloc(&r->d_cth, (size_t)n) != cudaSuccess || dalloc(&r->d_cph, (size_t)n) != cudaSuccess ||
+            dalloc(&r->d_cfate, (size_t)n) != cudaSuccess || dalloc(&r->d_uvgrid, (size_t)n) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "sky corners: device allocation");
+        r->corner_cap = n;
+    }
+    if (!r->d_cnt_corner && dalloc(&r->d_cnt_corner, 1) != cudaSuccess)
+        return fail(r, SO_ERR_ALLOC, "sky corners: device allocation");
+    SO_CK(r, cudaMemsetAsync(r->d_cnt_corner, 0, sizeof(Counters), r->st));
+    SO_CK(r, launch_corner_points(r->d_frame, W, H, r->d_cx, r->d_cy, r->st));
+    TraceLaunch L;
+    launch_common(r, L);
+    L.counters = r->d_cnt_corner;
+    L.kind = RAYS_LIST;
+    L.nrays = n;
+    L.x = r->d_cx;
+    L.y = r->d_cy;
+    L.out.fate = r->d_cfate;
+    L.out.theta = r->d_cth;
+    L.out.phi = r->d_cph;
+    int rc = run_tracer(r, L);
+    if (rc) return rc;
+    SO_CK(r, launch_corner_uv(r->d_scene, n, r->d_cfate, r->d_cth, r->d_cph, r->d_uvgrid, r->st));
     return SO_OK;
 }
 
@@ -499,6 +552,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     // so the FP32 tracer takes those scenes.
     const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f &&
                         !L.turb_field) ||
+                       (L.sky_uv != nullptr) ||  // the star map needs escape directions (FP64 only)
                        (r->S.disk_on && r->S.disk_turb_amp > 0.f) || (r->S.mode == SO_MODE_RADIO && r->S.disk_on);
     SO_CK(r, launch_route(L, all64 ? 1 : 0, r->st));
     // band rays: plain FP64 tracer on the second stream, concurrently with the FP32 work
@@ -593,6 +647,12 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
     if (int brc = bake_turbulence(r, L)) return brc;
     if (stats) cudaEventRecord(ev[0], r->st);
     const bool mixed = r->precision == SO_PREC_MIXED;
+    if (r->S.sky_on && r->S.mode == SO_MODE_VISIBLE) {
+        int crc = trace_corners(r, f.W, f.H);
+        if (crc) return crc;
+        L.sky_uv = r->d_uvgrid;
+        L.sky_grad_scale = 0.7f;
+    }
     int rc = mixed ? trace_pass1_mixed(r, f, L) : run_tracer(r, L);
     if (rc) return rc;
     if (stats) cudaEventRecord(ev[1], r->st);
@@ -633,6 +693,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             L2.chunk_acc = (float*)r->d_chunk_acc;
             L2.chunk = CHUNK;
             L2.ystat = nullptr;
+            L2.sky_grad_scale = 0.5f;
             // the queue head restarts for pass 2; the sample counters keep accumulating
             SO_CK(r, cudaMemsetAsync(&r->d_cnt->next, 0, sizeof(unsigned long long), r->st));
             if (stats) cudaEventRecord(ev[2], r->st);
@@ -868,7 +929,6 @@ int so_init(so_renderer** out, int device, const so_scene* scene, const so_table
     *out = nullptr;
     if (!scene || !tables || !rs) return fail(nullptr, SO_ERR_ARG, "so_init: NULL argument");
     if (rs->W <= 0 || rs->H <= 0 || rs->spp <= 0) return fail(nullptr, SO_ERR_ARG, "so_init: bad render settings");
-    if (scene->sky_on) return fail(nullptr, SO_ERR_UNSUPPORTED, "so_init: sky texture lookups are not supported");
     if (!tables->k2_ln || tables->k2_n < 2 || !tables->bb_xyz || tables->bb_n < 2 || !tables->disk_lnT ||
         tables->disk_n < 2)
         return fail(nullptr, SO_ERR_ARG, "so_init: missing tables");
@@ -901,6 +961,10 @@ int so_init(so_renderer** out, int device, const so_scene* scene, const so_table
         r->S.k2_n = tables->k2_n;
         r->S.bb_n = tables->bb_n;
         r->rs = *rs;
+        // the star map comes with so_set_sky; until then no sky (render.cu:550, 590-592)
+        r->sky_requested = scene->sky_on ? 1 : 0;
+        r->S.sky_on = 0;
+        r->S.sky_tex = 0;
         rc = turb_setup(r);
         if (!rc) rc = upload_scene(r);
     }
@@ -918,13 +982,14 @@ int so_init(so_renderer** out, int device, const so_scene* scene, const so_table
 
 int so_update_scene(so_renderer* r, const so_scene* scene) {
     if (!r || !scene) return fail(r, SO_ERR_ARG, "so_update_scene: NULL argument");
-    if (scene->sky_on) return fail(r, SO_ERR_UNSUPPORTED, "sky texture lookups are not supported");
     // tables and the baked-turbulence set-up stay as so_init made them (render.cu:658-675)
     const so_scene keep = r->S;
     r->S = *scene;
     r->S.disk_n = keep.disk_n;
     r->S.k2_n = keep.k2_n;
     r->S.bb_n = keep.bb_n;
+    r->S.sky_tex = keep.sky_tex;
+    r->S.sky_on = keep.sky_on;
     for (int k = 0; k < 24; ++k) r->S.turb_tex[k] = keep.turb_tex[k];
     r->S.turb_nt = keep.turb_nt;
     r->S.turb_lr0 = keep.turb_lr0;
@@ -1147,6 +1212,66 @@ int so_set_plasma(so_renderer* r, const so_plasma* p, const so_mode* modes) {
         turb_modes_fold(modes, p->n_modes, r->turb_modes);
     }
     return SO_OK;
+}
+
+int so_set_sky(so_renderer* r, int w, int h, const uint16_t* data) {
+    if (!r) return SO_ERR_ARG;
+    if (w <= 0 || h <= 0 || !data || (long long)w * h > (1ll << 28))
+        return fail(r, SO_ERR_ARG, "so_set_sky: w, h > 0 and a w x h half2 texel array");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    SO_CK(r, cudaStreamSynchronize(r->st));
+    if (r->sky_tex) cudaDestroyTextureObject(r->sky_tex);
+    if (r->sky_mip) cudaFreeMipmappedArray(r->sky_mip);
+    r->sky_tex = 0;
+    r->sky_mip = nullptr;
+    r->S.sky_tex = 0;
+    r->S.sky_on = 0;
+    // mip chain down to 1 x 1, level l box-filtered from level l - 1 (render.cu:551-575)
+    int levels = 1;
+    while ((w >> levels) > 0 || (h >> levels) > 0) ++levels;
+    cudaChannelFormatDesc fd = cudaCreateChannelDescHalf2();
+    SO_CK(r, cudaMallocMipmappedArray(&r->sky_mip, &fd, make_cudaExtent(w, h, 0), levels, cudaArraySurfaceLoadStore));
+    cudaArray_t l0;
+    SO_CK(r, cudaGetMipmappedArrayLevel(&l0, r->sky_mip, 0));
+    SO_CK(r, cudaMemcpy2DToArray(l0, 0, 0, data, (size_t)w * 4, (size_t)w * 4, h, cudaMemcpyHostToDevice));
+    for (int l = 1; l < levels; ++l) {
+        cudaArray_t a, b;
+        SO_CK(r, cudaGetMipmappedArrayLevel(&a, r->sky_mip, l - 1));
+        SO_CK(r, cudaGetMipmappedArrayLevel(&b, r->sky_mip, l));
+        cudaResourceDesc ra = {}, rb = {};
+        ra.resType = rb.resType = cudaResourceTypeArray;
+        ra.res.array.array = a;
+        rb.res.array.array = b;
+        cudaSurfaceObject_t sa = 0, sb = 0;
+        SO_CK(r, cudaCreateSurfaceObject(&sa, &ra));
+        cudaError_t e = cudaCreateSurfaceObject(&sb, &rb);
+        if (e == cudaSuccess) {
+            const int sw = std::max(w >> (l - 1), 1), sh = std::max(h >> (l - 1), 1);
+            const int dw = std::max(w >> l, 1), dh = std::max(h >> l, 1);
+            e = launch_mip_half2(sa, sw, sh, sb, dw, dh, r->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(r->st);
+            cudaDestroySurfaceObject(sb);
+        }
+        cudaDestroySurfaceObject(sa);
+        if (e != cudaSuccess) return cuda_fail(r, e, "so_set_sky: mip level");
+    }
+    // the reference's sampler: bilinear + linear between mips, anisotropy up to 16, u wrapped
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeMipmappedArray;
+    rd.res.mipmap.mipmap = r->sky_mip;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    td.mipmapFilterMode = cudaFilterModeLinear;
+    td.maxMipmapLevelClamp = (float)(levels - 1);
+    td.maxAnisotropy = 16;
+    SO_CK(r, cudaCreateTextureObject(&r->sky_tex, &rd, &td, nullptr));
+    r->S.sky_tex = (unsigned long long)r->sky_tex;
+    r->S.sky_on = r->sky_requested;
+    return upload_scene(r);
 }
 
 int so_set_flow_noise(so_renderer* r, int mode) {

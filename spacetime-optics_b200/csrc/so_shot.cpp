@@ -627,6 +627,29 @@ int so_critical_curve_point(double a, double theta_o, double rp, double* alpha, 
     return critical_curve_point(a, theta_o, rp, alpha, beta_plus) ? 1 : 0;
 }
 
+int so_sky_file(const char* path, int* w, int* h, float* scale, uint16_t* data) {
+    if (!path || !w || !h || !scale) return SO_ERR_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SO_ERR_CONFIG;
+    uint32_t hdr[3];
+    float sc = 0.f;
+    if (std::fread(hdr, 4, 3, f) != 3 || hdr[0] != 0x4b534842u || std::fread(&sc, 4, 1, f) != 1 || hdr[1] == 0 ||
+        hdr[2] == 0 || (uint64_t)hdr[1] * hdr[2] > (1ull << 28)) {
+        std::fclose(f);
+        return SO_ERR_CONFIG;
+    }
+    *w = (int)hdr[1];
+    *h = (int)hdr[2];
+    *scale = sc;
+    int rc = SO_OK;
+    if (data) {
+        const size_t n = (size_t)hdr[1] * hdr[2] * 2;
+        if (std::fread(data, 2, n, f) != n) rc = SO_ERR_CONFIG;
+    }
+    std::fclose(f);
+    return rc;
+}
+
 int so_approach_state(const so_scene* S, const so_frame* f, double x, double yv, double r1, double tol, int method,
                       double* state, int* attempts) {
     if (!S || !f || !state || !(r1 > 0.0) || !(tol > 0.0) || (method != 0 && method != 1)) return SO_ERR_ARG;

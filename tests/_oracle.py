@@ -41,6 +41,8 @@ def oracle():
         L.orc_kerr_point.restype = None
         L.orc_radial_drift.argtypes = [C.c_double, C.c_double, C.c_double, Vec3, C.c_double, C.c_int, P(C.c_int)]
         L.orc_radial_drift.restype = C.c_double
+        L.orc_set_sky.argtypes = [C.c_double] * 4
+        L.orc_set_sky.restype = None
         L.orc_turb_setup.argtypes = [P(Scene)]
         L.orc_turb_setup.restype = None
         L.so_rpow5.argtypes = [C.c_double]

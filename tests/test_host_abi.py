@@ -189,3 +189,22 @@ def test_far_field_approach_matches_mino_time(so):
     # impact parameter beyond r1: a radial turning point above it, far transport refused
     with pytest.raises(so.TracerError):
         so.approach_state(sh.scene, f, 150.0 / f.r, 0.0, 100.0, 1e-9, 0)
+
+
+def test_sky_file_roundtrip(so, tmp_path):
+    """so_sky_file reads the reference's .bhsk layout (scene_build.cpp:61-81) and rejects others."""
+    u = (np.arange(8) + 0.5) / 8
+    v = (np.arange(4) + 0.5) / 4
+    sv = 1.0 + u[None, :] + v[:, None]
+    t = np.stack([sv.astype(np.float16).view(np.uint16), (0.7 * sv).astype(np.float16).view(np.uint16)], -1)
+    p = tmp_path / "sky.bhsk"
+    with open(p, "wb") as fh:
+        fh.write(np.array([0x4b534842, 8, 4], np.uint32).tobytes())
+        fh.write(np.array([1.75], np.float32).tobytes())
+        fh.write(t.tobytes())
+    data, sc = so.sky_file(str(p))
+    assert sc == np.float32(1.75) and np.array_equal(data, t)
+    bad = tmp_path / "bad.bhsk"
+    bad.write_bytes(b"nope")
+    with pytest.raises(so.TracerError):
+        so.sky_file(str(bad))
