@@ -488,9 +488,23 @@ def run_wavefront(args, so, world, rank, local):
     value = job_rate(world, nrays, ms_step) / 1e6
     fp64_peak, _ = so.probe_fma_peak(local)
     n_modes = shots[0].plasma().n_modes
-    flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
-             st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
-    achieved = flops / (ms_step * 1e-3) / 1e12
+    if prec == so.abi.SO_PREC_FP64:
+        # FP64 geometry and FP64 turbulence sums: FP64 pipe
+        flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
+                 st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
+        achieved = flops / (ms_step * 1e-3) / 1e12
+        roof = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / fp64_peak, 4), "traffic": None, "kernel": "k_trace64",
+                "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
+    else:
+        # FP64 geometry, FP32 turbulence sums: the SFU cosines (one per mode per flow step) dominate
+        sfu_peak = so.probe_sfu_peak(local)
+        ops = st.flow_steps * n_modes
+        achieved = ops / (ms_step * 1e-3) / 1e9
+        roof = {"bound": "sfu", "achieved": round(achieved, 3), "peak": round(sfu_peak, 3), "unit": "Gop/s",
+                "frac": round(achieved / sfu_peak, 4), "traffic": None, "kernel": "k_trace64 (FP32 sums)",
+                "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
+                "fp64_geometry_flops": st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT}
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
@@ -502,9 +516,7 @@ def run_wavefront(args, so, world, rank, local):
                    "frames_per_s": round(world * len(frames) / (ms_step * 1e-3), 4),
                    "attempts_per_ray": st.attempts / nrays, "flow_steps_per_ray": st.flow_steps / nrays,
                    "l2": "inputs (mode table, frame descriptors) are small; no flush (one step is seconds long)"},
-        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
-                     "frac": round(achieved / fp64_peak, 4), "traffic": None, "kernel": "k_trace64",
-                     "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"},
+        "roofline": roof,
         "e2e": None,
         "gpu_launches": args.steps * 3,
         "clocks": clk.summary(),
