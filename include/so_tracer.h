@@ -238,6 +238,10 @@ typedef struct so_mixed_opts {
     double records_per_ray;  /* deferred turbulence: record pool per FP32 ray at the renderer's first
                               * mixed frame (0 = 320; doubled after a frame that ran short, whose rays
                               * without a record slot are re-traced in FP64) */
+    int sky_fp32;            /* visible frames with the star map: 0 = traced in FP64 (default, the plain
+                              * image), 1 = FP32 rays off the band, their escape carried to r_escape in
+                              * FP64 (~1.9x faster; escape directions within ~1e-6 rad, which shows
+                              * where a magnified map is steep: L1 5e-3 on a point-star test map) */
     int fp32_max_attempts;   /* FP32 attempts after which a ray is handed to the FP64 re-trace (0 = 2000:
                               * the FP32 controller stalls on a few rays far from the critical curve,
                               * which the FP64 tracer finishes normally; at 2048^2 the synchrotron

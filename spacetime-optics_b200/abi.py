@@ -111,7 +111,7 @@ class MixedOpts(C.Structure):
     _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_r", C.c_double), ("drift_tol", C.c_double),
                 ("r_switch", C.c_double), ("tol_approach", C.c_double), ("t32_blocks", C.c_int),
                 ("turbulence", C.c_int), ("approach", C.c_int), ("records_per_ray", C.c_double),
-                ("fp32_max_attempts", C.c_int)]
+                ("sky_fp32", C.c_int), ("fp32_max_attempts", C.c_int)]
 
 
 class Tune(C.Structure):

@@ -174,6 +174,17 @@ __global__ void __launch_bounds__(128) k_approach64(const TraceLaunch L) {
             if (done) {
                 L.sample_out[sid] = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (L.sample_fate) L.sample_fate[sid] = (int8_t)fate;
+                if (fate == 1 && L.esc_list) {
+                    // escaped in the far field of a star-map frame: the sky is added by k_sky_escape
+                    float2 r = split(y[0]), pr = split(y[1]), u = split(y[2]), pu = split(y[3]), ph = split(y[4]),
+                           t = split(y[5]);
+                    L.state[0 * ns + sid] = make_float4(r.x, r.y, pr.x, pr.y);
+                    L.state[1 * ns + sid] = make_float4(u.x, u.y, pu.x, pu.y);
+                    L.state[2 * ns + sid] = make_float4(ph.x, ph.y, t.x, t.y);
+                    L.state[3 * ns + sid] = make_float4((float)c.lam, (float)c.eta, (float)c.E, (float)h);
+                    L.state[4 * ns + sid] = make_float4(1.f, 0.f, 0.f, 0.f);
+                    L.esc_list[atomicAdd(&L.nlists[9], 1ull)] = sid;
+                }
             } else {
                 park = true;
                 float2 r = split(y[0]), pr = split(y[1]), u = split(y[2]), pu = split(y[3]), ph = split(y[4]),
@@ -753,6 +764,15 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         n_drift += fate == 4 ? 1 : 0;
         n_lim += fate == 0 ? 1 : 0;
         if (fate == 5) atomicAdd(&L.nlists[6], 1ull);
+        if (!redo && fate == 1 && L.esc_list) {
+            // star-map frame: park the end state for the FP64 transport to the escape radius
+            L.state[0 * ns + R.sid] = make_float4(R.rh, R.rl, R.prh, R.prl);
+            L.state[1 * ns + R.sid] = make_float4(R.uh, R.ul, R.puh, R.pul);
+            L.state[2 * ns + R.sid] = make_float4(R.phh, R.phl, R.th, R.tl);
+            L.state[3 * ns + R.sid] = make_float4(c.lam, c.eta, c.E, R.h);
+            L.state[4 * ns + R.sid] = make_float4(R.trans, 0.f, 0.f, 0.f);
+            L.esc_list[atomicAdd(&L.nlists[9], 1ull)] = R.sid;
+        }
         if (!redo) {
             if (DEFER && R.nrec > 0) {
                 // emission by k_flow_records (which may still end the ray on its opacity)
@@ -924,7 +944,73 @@ __global__ void __launch_bounds__(256) k_flow_records(const TraceLaunch L) {
     }
 }
 
+// ---- star map behind FP32 rays -----------------------------------------------------------------
+// An FP32 ray of a star-map frame that escaped (beyond every emitter and radial turning point, or
+// past r_escape) is carried to r_escape in FP64 by the inverse-radius transport (a few DP5 steps
+// where Mino time takes hundreds; the Mino-time DP5(4) where that does not apply), its escape
+// direction is taken there as the reference takes it
+// (escape_angles, trace.cuh:45-55), and the star map's radiance through the pixel's footprint,
+// weighted by the transmittance in front, is added to the sample (trace.cuh:149-161).
+__global__ void __launch_bounds__(128) k_sky_escape(const TraceLaunch L) {
+    const so_scene& S = L.scenes[0];
+    const long long n = (long long)L.nlists[9];
+    const long long ns = L.nsamples;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t sid = L.esc_list[i];
+        const float4 p0 = L.state[0 * ns + sid], p1 = L.state[1 * ns + sid], p2 = L.state[2 * ns + sid];
+        const float4 p3 = L.state[3 * ns + sid], p4 = L.state[4 * ns + sid];
+        double y[6] = {(double)p0.x + p0.y, (double)p0.z + p0.w, (double)p1.x + p1.y,
+                       (double)p1.z + p1.w, (double)p2.x + p2.y, (double)p2.z + p2.w};
+        RayC c;
+        ray_consts(c, S.a, (double)p3.x, (double)p3.y, (double)p3.z);
+        double psi = 0.0;
+        int nc = 0;
+        double k[6];
+        bool there = !(y[0] < S.r_escape);
+        if (!there && far_applies(c, y, S.r_escape))
+            there = far_approach(c, y, S.r_escape, S.tol, 256, &psi, &nc, false) >= 0;
+        rhs(c, y, k);
+        if (!there) {
+            // the reference's Mino-time DP5(4) out to r_escape (trace.cuh:80-96, 150)
+            double yn[6], k7[6];
+            double h = initial_step(y);
+            for (int it = 0; it < S.max_steps && !(y[0] > S.r_escape && y[1] > 0.0); ++it) {
+                const double hc = h;
+                const double err = dp54(c, y, k, hc, S.tol, yn, k7);
+                if (!(err <= 1.0)) {
+                    h = reject_step(hc, err);
+                    continue;
+                }
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    y[q] = yn[q];
+                    k[q] = k7[q];
+                }
+                project_radial(c, y, k);
+                h = accept_step(hc, err);
+            }
+        }
+        double th, ph;
+        escape_angles(y, k, &th, &ph);
+        const long long pix = sid / L.spp;
+        const SkyGrad g = pixel_grad(L.sky_uv, L.W, (int)(pix % L.W), (int)(pix / L.W), L.sky_grad_scale);
+        float xyz[3];
+        sky_radiance(S, sky_uv(S, th, ph), g, c.E, xyz);
+        const float tf = p4.x;
+        float4 o = L.sample_out[sid];
+        o.x += tf * xyz[0];
+        o.y += tf * xyz[1];
+        o.z += tf * xyz[2];
+        L.sample_out[sid] = o;
+    }
+}
+
 // ---- launchers -----------------------------------------------------------------------------------
+cudaError_t launch_sky_escape(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    k_sky_escape<<<num_sms * 4, 128, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
 void turb_modes_fold(const so_mode* modes, int n, TurbModes* out) {
     out->n = n;
     for (int i = 0; i < n; ++i) {

@@ -308,14 +308,16 @@ SO_HD bool critical_curve_point(double a, double theta_o, double rp, double* alp
 //   d tau / dx = -(q + v N/D) - w a (lam - a s^2),   w = 1/sqrt(Rt) = 1 + x^2 v,
 //   N/D = (1 + a^2 x^2)(1 + CP x^2) / D = 1 + 2x + x^2 q,   q = (CP + 4 - 2 a^2 x + a^2 CP x^2) / D,
 //   v = (D K - 2 CP - CP^2 x^2) / (sqrt(Rt) (1 + sqrt(Rt))),
-// all free of cancellation at x -> 0.  z = (u, u', phi, tau), u' = du/dlambda as in rhs().
-SO_HD void far_rhs(const RayC& c, double x, const double* z, double* d) {
+// all free of cancellation at x -> 0.  z = (u, u', phi, tau), u' = du/dlambda as in rhs().  An
+// outgoing leg (sg = -1, x decreasing) has d lambda / dx = -1/sqrt(Rt) and the pole terms with the
+// opposite sign: t(x) = t0 - (1/x - 1/x0) + 2 ln(x / x0) + tau, d tau / dx = (q + v N/D) - w a (...).
+SO_HD void far_rhs(const RayC& c, double x, const double* z, double* d, double sg = 1.0) {
     double x2 = x * x;
     double D = fma(x, fma(c.A2, x, -2.0), 1.0);
     double cpx = fma(c.CP, x2, 1.0);
     double Rt = fma(cpx, cpx, -(x2 * D * c.K));
     double sR = sqrt(Rt);
-    double w = 1.0 / sR;
+    double w = sg / sR;
     double u = z[0], u2 = u * u;
     double s2 = fmax(1.0 - u2, 1e-300);
     double iD = 1.0 / D;
@@ -325,22 +327,26 @@ SO_HD void far_rhs(const RayC& c, double x, const double* z, double* d) {
     double q = fma(x, fma(c.A2 * c.CP, x, -2.0 * c.A2), c.CP + 4.0) * iD;
     double v = fma(-(c.CP * c.CP), x2, fma(D, c.K, -2.0 * c.CP)) / (sR * (1.0 + sR));
     double nd = fma(c.A2, x2, 1.0) * cpx * iD;
-    d[3] = -fma(v, nd, q) - w * c.a * fma(-c.a, s2, c.lam);
+    d[3] = -sg * fma(v, nd, q) - w * c.a * fma(-c.a, s2, c.lam);
 }
 
-// Whether far_approach() applies from radius r0 (state y0) to r1: an ingoing ray whose radial
-// potential keeps Rt >= 1/2 on [1/r0, 1/r1] (K x^2 <= 1/4 bounds the only decreasing term).
+// Whether far_approach() applies from radius r0 (state y0) to r1: an ingoing ray towards a smaller
+// r1, or an outgoing one towards a larger r1, whose radial potential keeps Rt >= 1/2 between them
+// (K x^2 <= 1/4 at the inner end bounds the only decreasing term).
 SO_HD bool far_applies(const RayC& c, const double* y0, double r1) {
-    if (!(y0[0] > r1) || !(y0[1] < 0.0)) return false;
-    double x1 = 1.0 / r1, x2 = x1 * x1;
-    if (!(c.K * x2 <= 0.25)) return false;
+    const bool in = y0[0] > r1 && y0[1] < 0.0, out = y0[0] < r1 && y0[1] > 0.0;
+    if (!in && !out) return false;
+    double x1 = 1.0 / (in ? r1 : y0[0]), x2 = x1 * x1;
+    // outwards the ray is already past its last turning point: only keep clear of its neighbourhood
+    if (!(c.K * x2 <= (in ? 0.25 : 0.5))) return false;
     double cpx = fma(c.CP, x2, 1.0);
     double D = fma(x1, fma(c.A2, x1, -2.0), 1.0);
-    return fma(cpx, cpx, -(x2 * D * c.K)) >= 0.5;
+    return fma(cpx, cpx, -(x2 * D * c.K)) >= (in ? 0.5 : 0.25);
 }
 
-// DP5(4) in x from the camera state y (r, r', u, u', phi, t) at r = y[0] to r1, in place: on return
-// y is the state at r1 with r' = -sqrt(R(r1)) from the radial constraint.  Error norm as dp54's for
+// DP5(4) in x from the state y (r, r', u, u', phi, t) at r = y[0] to r1, in place, inwards (from the
+// camera) or outwards (to the escape radius) as far_applies() decided: on return y is the state at
+// r1 with r' = -sqrt(R(r1)) inwards, +sqrt(R(r1)) outwards, from the radial constraint.  Error norm as dp54's for
 // u, u', phi (tol, tol max(1,|u'|), 4 tol) plus tol max(1, |tau|) for tau.  psi and ncross are
 // accumulated per accepted step as the reference's driver does (trace.cuh:97-106).  Returns the
 // number of attempts, or -1 (y, psi, ncross untouched) if max_att attempts did not reach r1.
@@ -349,40 +355,41 @@ SO_HD int far_approach(const RayC& c, double* y, double r1, double tol, int max_
     double psi = *psi_io;
     int ncross = *ncross_io;
     const double r0 = y[0], x0 = 1.0 / r0, x1 = 1.0 / r1;
+    const double sg = x1 > x0 ? 1.0 : -1.0;  // +1 inwards (x increasing), -1 outwards
     double z[4] = {y[2], y[3], y[4], 0.0}, k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], t[4], zn[4];
-    far_rhs(c, x0, z, k1);
+    far_rhs(c, x0, z, k1, sg);
     double x = x0;
-    double h = fmin(x1 - x0, 0.1 / sqrt(c.K + 1.0));
+    double h = sg * fmin(sg * (x1 - x0), 0.1 / sqrt(c.K + 1.0));
     double sp = sqrt(fmax(fma(-z[0], z[0], 1.0), 0.0));
     double pp0 = sp * cos(z[2]), pp1 = sp * sin(z[2]), pp2 = z[0];
     int att = 0;
-    while (x < x1) {
+    while (sg * (x1 - x) > 0.0) {
         if (att >= max_att) return -1;
         ++att;
-        const bool last = x + h >= x1;
+        const bool last = sg * (x + h - x1) >= 0.0;
         const double hc = last ? x1 - x : h;
 #pragma unroll
         for (int i = 0; i < 4; ++i) t[i] = fma(hc, A21 * k1[i], z[i]);
-        far_rhs(c, fma(0.2, hc, x), t, k2);
+        far_rhs(c, fma(0.2, hc, x), t, k2, sg);
 #pragma unroll
         for (int i = 0; i < 4; ++i) t[i] = fma(hc, fma(A32, k2[i], A31 * k1[i]), z[i]);
-        far_rhs(c, fma(0.3, hc, x), t, k3);
+        far_rhs(c, fma(0.3, hc, x), t, k3, sg);
 #pragma unroll
         for (int i = 0; i < 4; ++i) t[i] = fma(hc, fma(A43, k3[i], fma(A42, k2[i], A41 * k1[i])), z[i]);
-        far_rhs(c, fma(0.8, hc, x), t, k4);
+        far_rhs(c, fma(0.8, hc, x), t, k4, sg);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             t[i] = fma(hc, fma(A54, k4[i], fma(A53, k3[i], fma(A52, k2[i], A51 * k1[i]))), z[i]);
-        far_rhs(c, fma(8.0 / 9.0, hc, x), t, k5);
+        far_rhs(c, fma(8.0 / 9.0, hc, x), t, k5, sg);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             t[i] = fma(hc, fma(A65, k5[i], fma(A64, k4[i], fma(A63, k3[i], fma(A62, k2[i], A61 * k1[i])))), z[i]);
         const double xn = last ? x1 : x + hc;
-        far_rhs(c, xn, t, k6);
+        far_rhs(c, xn, t, k6, sg);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
             zn[i] = fma(hc, fma(B6, k6[i], fma(B5, k5[i], fma(B4, k4[i], fma(B3, k3[i], B1 * k1[i])))), z[i]);
-        far_rhs(c, xn, zn, k7);
+        far_rhs(c, xn, zn, k7, sg);
         double sc[4];
         sc[0] = tol;
         sc[1] = tol * fmax(1.0, fmax(fabs(z[1]), fabs(zn[1])));
@@ -416,9 +423,9 @@ SO_HD int far_approach(const RayC& c, double* y, double r1, double tol, int max_
         x = xn;
         if (!last) h = accept_step(hc, err);
     }
-    y[5] = y[5] + (r1 - r0) - 2.0 * log(r0 / r1) + z[3];
+    y[5] = y[5] + sg * (r1 - r0) - sg * 2.0 * log(r0 / r1) + z[3];
     y[0] = r1;
-    y[1] = -sqrt(fmax(radial_pot(c, r1), 0.0));
+    y[1] = -sg * sqrt(fmax(radial_pot(c, r1), 0.0));
     y[2] = z[0];
     y[3] = z[1];
     y[4] = z[2];

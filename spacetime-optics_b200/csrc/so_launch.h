@@ -147,6 +147,8 @@ struct TraceLaunch {
     uint32_t* seg_next;       // per segment of REC_SEG record slots: the ray's next segment
     int2* ray_meta;           // per sample id: (first segment, record count)
     uint32_t* acc_list;       // rays with records, for the transfer kernel
+    uint32_t* esc_list;       // star-map frames: FP32 rays that escaped, their end state parked in
+                              // state (P4.x = transmittance), for k_sky_escape (count nlists[9])
     long long seg_cap;        // record segments available
     unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked, [4] acc_list counts,
                                 // [5] record segments used, [6] rays re-traced for want of segments,
@@ -175,6 +177,7 @@ struct TurbModes {
 };
 void turb_modes_fold(const so_mode* modes, int n, TurbModes* out);
 cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
+cudaError_t launch_sky_escape(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);
 

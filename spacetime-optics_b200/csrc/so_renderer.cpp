@@ -78,7 +78,7 @@ struct so_renderer {
     so_mode* d_modes = nullptr;
     TurbModes* turb_modes = nullptr;  // the modes folded to FP32 for the batched turbulence sums
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0, 0};
     // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
     float4* d_rec = nullptr;
     float* d_rec_delta = nullptr;
@@ -94,6 +94,8 @@ struct so_renderer {
     cudaEvent_t ev_turb[2] = {nullptr, nullptr};  // tracer end, sums end
     // attempts of the reference's Mino-time approach of the central ray, for the key below
     int approach_it = 0;
+    uint32_t* d_esc_list = nullptr;  // star-map frames on the mixed path: escaped FP32 rays
+    long long esc_cap = 0;
     // baked flow turbulence (reference flow model with turbulence, radio mode): the frame's slices
     float* d_turb = nullptr;
     int flow_noise = SO_FLOW_NOISE_BAKED;
@@ -165,7 +167,7 @@ void free_all(so_renderer* r) {
         if (p) cudaFree(p);
     void* pm[] = {r->d_state, r->d_sample_out, r->d_sample_fate, r->d_list32, r->d_list64, r->d_redo, r->d_parked,
                   r->d_nlists, r->d_cnt3, r->d_band, r->d_rec, r->d_rec_delta, r->d_seg_next, r->d_ray_meta,
-                  r->d_acc_list, r->d_turb};
+                  r->d_acc_list, r->d_turb, r->d_esc_list};
     for (void* p : pm)
         if (p) cudaFree(p);
     for (int k = 1; k < r->lev.n; ++k)
@@ -530,7 +532,20 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     double r_emit = 0.0;
     if (r->S.mode == SO_MODE_RADIO && r->S.flow_on) r_emit = std::max(r_emit, r->S.r_flow_max);
     if (r->S.disk_on) r_emit = std::max(r_emit, r->S.disk_rout);
+    // star-map frames: escaping FP32 rays stop there and k_sky_escape carries them on in FP64
+    const bool sky = L.sky_uv != nullptr && r->mixed.sky_fp32 != 0;
+    if (sky) r_emit = std::max(r_emit, 10.0);
     L.r_emit = r_emit > 0.0 ? std::max(r_emit, 10.0) : 0.0;
+    if (sky) {
+        if (!r->d_esc_list || r->esc_cap < ns) {
+            if (r->d_esc_list) cudaFree(r->d_esc_list);
+            r->d_esc_list = nullptr;
+            r->esc_cap = 0;
+            if (dalloc(&r->d_esc_list, (size_t)ns) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "sky escape list");
+            r->esc_cap = ns;
+        }
+        L.esc_list = r->d_esc_list;
+    }
     L.band_rho = r->d_band;
     L.band_n = BAND_N;
     L.nsamples = ns;
@@ -552,7 +567,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     // so the FP32 tracer takes those scenes.
     const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f &&
                         !L.turb_field) ||
-                       (L.sky_uv != nullptr) ||  // the star map needs escape directions (FP64 only)
+                       (L.sky_uv != nullptr && r->mixed.sky_fp32 == 0) ||  // star map: FP64 unless asked
                        (r->S.disk_on && r->S.disk_turb_amp > 0.f) || (r->S.mode == SO_MODE_RADIO && r->S.disk_on);
     SO_CK(r, launch_route(L, all64 ? 1 : 0, r->st));
     // band rays: plain FP64 tracer on the second stream, concurrently with the FP32 work
@@ -603,6 +618,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         r->seg_pending = true;
     }
     r->last_defer = defer;
+    if (sky) SO_CK(r, launch_sky_escape(L, r->num_sms, r->st));
     SO_CK(r, cudaEventRecord(r->ev32[1], r->st));
     SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
     SO_CK(r, launch_gather_samples(L, r->st));
@@ -1181,6 +1197,7 @@ int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
     if (!r) return SO_ERR_ARG;
     if (precision != SO_PREC_FP64 && precision != SO_PREC_MIXED) return fail(r, SO_ERR_ARG, "bad precision");
     if (opts && opts->approach != 0 && opts->approach != 1) return fail(r, SO_ERR_ARG, "so_mixed_opts.approach: 0 or 1");
+    if (opts && opts->sky_fp32 != 0 && opts->sky_fp32 != 1) return fail(r, SO_ERR_ARG, "so_mixed_opts.sky_fp32: 0 or 1");
     if (opts && opts->turbulence != 0 && opts->turbulence != 1)
         return fail(r, SO_ERR_ARG, "so_mixed_opts.turbulence: 0 or 1");
     if (opts && !(opts->records_per_ray >= 0.0 && opts->records_per_ray <= 1e6))

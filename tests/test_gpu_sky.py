@@ -5,7 +5,10 @@ The texture unit's anisotropic mip filtering of a sampled map has no CPU form, s
     against the oracle: escape direction, galactic (u, v), blackbody at the camera-shifted
     temperature, brightness scale and the disk's transmittance in front (1e-5 of the maximum);
   * a map that varies linearly in latitude checks the (u, v) mapping, the rotation and the pixel
-    footprints against the oracle's analytic map, within the texels' half precision (1 per cent).
+    footprints against the oracle's analytic map, within the texels' half precision (1 per cent);
+  * the mixed path traces star-map frames in FP64 by default (bit for bit the plain image); with
+    sky_fp32 (FP32 rays whose escape is carried to r_escape in FP64) both smooth maps stay within
+    the mixed path's image bar of the FP64 frame (L1 <= 1e-3).
 """
 import numpy as np
 import pytest
@@ -66,10 +69,18 @@ def test_constant_sky_vs_oracle(so, orc):
     assert _close(img, ref, 1e-5) <= 1e-5, _close(img, ref, 1e-5)
     sky_px = ((dark[..., 1] == 0) & (img[..., 1] > 0)).sum()  # no disk in front, sky behind
     assert sky_px > W * H // 4, sky_px
-    # the mixed path traces sky frames in FP64 (its FP32 rays have no escape direction)
+    # mixed path: star-map frames in FP64 by default (the plain image bit for bit) ...
     r.set_precision(so.abi.SO_PREC_MIXED)
+    img64m, _, st64m = r.render(f)
+    assert np.array_equal(img64m, img) and st64m.attempts_fp32 == 0
+    # ... or, with sky_fp32, FP32 rays off the band whose escape is carried to r_escape in FP64
+    r.set_precision(so.abi.SO_PREC_MIXED, sky_fp32=1)
     img32, _, st32 = r.render(f)
-    assert np.array_equal(img32, img) and st32.attempts_fp32 == 0
+    assert st32.attempts_fp32 > 0
+    a, b = img[..., 1].astype(np.float64), img32[..., 1].astype(np.float64)
+    assert np.abs(a - b).sum() / np.abs(a).sum() <= 1e-3
+    sky_only = (dark[..., 1] == 0) & (img[..., 1] > 0)
+    assert np.abs(a[sky_only] - b[sky_only]).max() <= 1e-4 * a[sky_only].max()
     r.close()
 
 
@@ -94,4 +105,10 @@ def test_latitude_gradient_sky_vs_oracle(so, orc):
     assert abs(y1.sum() / y0.sum() - 1.0) < 5e-3
     # the map's latitude gradient is visible across the frame
     assert y0[lit].max() / y0[lit].min() > 1.05
+    # mixed path with sky_fp32 (FP32 rays, FP64 transport to r_escape) against the FP64 frame
+    r.set_precision(so.abi.SO_PREC_MIXED, sky_fp32=1)
+    img32, _, st32 = r.render(f)
+    assert st32.attempts_fp32 > 0
+    y2 = img32[..., 1].astype(np.float64)
+    assert np.abs(y2 - y1).sum() / np.abs(y1).sum() <= 1e-3, np.abs(y2 - y1).sum() / np.abs(y1).sum()
     r.close()
