@@ -174,6 +174,7 @@ typedef struct so_stats {
     double ms_turb;       /* ... of the batched turbulence sums (ms_fp32 covers tracer + sums + transfer) */
     long long turb_records; /* ... record slots summed (segments in use x 16) */
     long long redo_records; /* ... FP32 rays re-traced in FP64 because the record pool ran out */
+    long long record_waves; /* ... waves the FP32 rays were traced in (the pool holds one wave's records) */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -242,6 +243,9 @@ typedef struct so_mixed_opts {
                               * image), 1 = FP32 rays off the band, their escape carried to r_escape in
                               * FP64 (~1.9x faster; escape directions within ~1e-6 rad, which shows
                               * where a magnified map is steep: L1 5e-3 on a point-star test map) */
+    double pool_mb;          /* deferred turbulence: record pool size limit in MiB (0 = half of the free
+                              * device memory); a frame whose records exceed it is traced in waves of
+                              * FP32 rays that each fit (the image does not depend on the split) */
     int fp32_max_attempts;   /* FP32 attempts after which a ray is handed to the FP64 re-trace (0 = 2000:
                               * the FP32 controller stalls on a few rays far from the critical curve,
                               * which the FP64 tracer finishes normally; at 2048^2 the synchrotron

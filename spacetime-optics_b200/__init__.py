@@ -264,9 +264,9 @@ class Renderer:
 
     def set_precision(self, precision, band_m=0.05, tol32=3e-6, turn_r=0.0, drift_tol=1e-4, r_switch=0.0,
                       tol_approach=0.0, t32_blocks=0, turbulence=0, approach=0, records_per_ray=0.0,
-                      fp32_max_attempts=0, sky_fp32=0):
+                      fp32_max_attempts=0, sky_fp32=0, pool_mb=0.0):
         o = MixedOpts(band_m, tol32, turn_r, drift_tol, r_switch, tol_approach, t32_blocks, turbulence, approach,
-                      records_per_ray, sky_fp32, fp32_max_attempts)
+                      records_per_ray, sky_fp32, pool_mb, fp32_max_attempts)
         _check(lib().so_set_precision(self.h, precision, C.byref(o)), self.h)
 
     def render(self, frame, percentile=0.995, hide_direct=0.0, out=None, bloom=0.0, blur_sigma_px=0.0):

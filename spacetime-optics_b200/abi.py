@@ -87,7 +87,7 @@ class Stats(C.Structure):
                 ("attempts_fp32", C.c_longlong), ("band_rays", C.c_longlong), ("flow_steps_fp32", C.c_longlong),
                 ("ms_fp32", C.c_double), ("redo_turn", C.c_longlong), ("redo_drift", C.c_longlong),
                 ("redo_limit", C.c_longlong), ("ms_fp32_trace", C.c_double), ("ms_turb", C.c_double),
-                ("turb_records", C.c_longlong), ("redo_records", C.c_longlong)]
+                ("turb_records", C.c_longlong), ("redo_records", C.c_longlong), ("record_waves", C.c_longlong)]
 
 
 class RaysOut(C.Structure):
@@ -111,7 +111,7 @@ class MixedOpts(C.Structure):
     _fields_ = [("band_m", C.c_double), ("tol32", C.c_double), ("turn_r", C.c_double), ("drift_tol", C.c_double),
                 ("r_switch", C.c_double), ("tol_approach", C.c_double), ("t32_blocks", C.c_int),
                 ("turbulence", C.c_int), ("approach", C.c_int), ("records_per_ray", C.c_double),
-                ("sky_fp32", C.c_int), ("fp32_max_attempts", C.c_int)]
+                ("sky_fp32", C.c_int), ("pool_mb", C.c_double), ("fp32_max_attempts", C.c_int)]
 
 
 class Tune(C.Structure):

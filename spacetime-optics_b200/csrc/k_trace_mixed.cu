@@ -416,7 +416,9 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         __syncthreads();
     }
     const long long ns = L.nsamples;
-    const long long total = (long long)L.nlists[3];
+    const long long parked = (long long)L.nlists[3];
+    const long long lo = L.wave_end > 0 ? min(L.wave_begin, parked) : 0;
+    const long long total = L.wave_end > 0 ? min(L.wave_end, parked) : parked;
     const uint32_t* work = L.parked;
     const int lane = threadIdx.x & 31;
     const float tol = (float)L.tol32;
@@ -443,7 +445,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
             if (lane == leader) base = atomicAdd(&L.counters->next, (unsigned long long)__popc(m));
             base = __shfl_sync(FULL, base, leader);
             if (need) {
-                const unsigned long long j = base + __popc(m & ((1u << lane) - 1u));
+                const unsigned long long j = (unsigned long long)lo + base + __popc(m & ((1u << lane) - 1u));
                 if (j >= (unsigned long long)total) {
                     exhausted = true;
                 } else {
@@ -836,6 +838,7 @@ __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L, const
     unsigned long long used = L.nlists[5];
     if (used > (unsigned long long)L.seg_cap) used = (unsigned long long)L.seg_cap;
     const long long nslots = (long long)used * REC_SEG;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.nlists[10], used);
     for (;;) {
         __syncthreads();  // modes loaded; the previous chunk index read by every thread
         if (threadIdx.x == 0) chunk = (long long)atomicAdd(&L.nlists[7], 1ull) * TURB_CHUNK;

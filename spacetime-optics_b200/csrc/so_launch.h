@@ -32,7 +32,7 @@ constexpr int TURB_NPHI = 512, TURB_NLR = 192, TURB_NZ = 48, TURB_NT = 24;
 struct TurbBake {
     float delta[TURB_NT];  // retarded-time offset of each slice, d0 + k dd (host float, as render.cu:681)
 };
-constexpr int NLISTS = 10;
+constexpr int NLISTS = 12;
 
 struct Counters {
     unsigned long long next;          // ray-queue head
@@ -150,9 +150,12 @@ struct TraceLaunch {
     uint32_t* esc_list;       // star-map frames: FP32 rays that escaped, their end state parked in
                               // state (P4.x = transmittance), for k_sky_escape (count nlists[9])
     long long seg_cap;        // record segments available
+    long long wave_begin, wave_end;  // deferred turbulence in waves: the FP32 tracer takes the parked
+                                     // rays [wave_begin, wave_end) (wave_end <= 0: all of them)
     unsigned long long* nlists; // [0] list32, [1] list64, [2] redo, [3] parked, [4] acc_list counts,
                                 // [5] record segments used, [6] rays re-traced for want of segments,
-                                // [7] / [8] work heads of k_turb_records / k_flow_records
+                                // [7] / [8] work heads of k_turb_records / k_flow_records,
+                                // [9] sky escape list, [10] record segments summed over the waves
 };
 
 // Mixed-path kernels (k_trace_mixed.cu).

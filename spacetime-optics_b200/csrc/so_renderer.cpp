@@ -78,7 +78,7 @@ struct so_renderer {
     so_mode* d_modes = nullptr;
     TurbModes* turb_modes = nullptr;  // the modes folded to FP32 for the batched turbulence sums
     int precision = SO_PREC_FP64;
-    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0, 0};
+    so_mixed_opts mixed{0.05, 3e-6, 0.0, 1e-4, 0.0, 0.0, 0, 0, 0, 0.0, 0, 0.0, 0};
     // deferred turbulence: record pool (segments of REC_SEG slots), grown when a frame runs out
     float4* d_rec = nullptr;
     float* d_rec_delta = nullptr;
@@ -91,7 +91,11 @@ struct so_renderer {
     cudaEvent_t ev_seg = nullptr;           // after the copy into h_seg
     bool seg_pending = false;
     bool last_defer = false;                // the last mixed frame deferred its turbulence
-    cudaEvent_t ev_turb[2] = {nullptr, nullptr};  // tracer end, sums end
+    long long pool_target = -1;             // pool size (segments) last asked for
+    int waves = 1;                          // FP32 ray waves per frame (the pool holds one wave)
+    long long wave_rays = 0;                // parked-list entries per wave
+    int last_waves = 0;
+    std::vector<cudaEvent_t> ev_wave;       // per wave: tracer end, sums end, transfer end
     // attempts of the reference's Mino-time approach of the central ray, for the key below
     int approach_it = 0;
     uint32_t* d_esc_list = nullptr;  // star-map frames on the mixed path: escaped FP32 rays
@@ -175,7 +179,7 @@ void free_all(so_renderer* r) {
     if (r->d_tmp) cudaFree(r->d_tmp);
     for (cudaEvent_t e : r->ev32)
         if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : r->ev_turb)
+    for (cudaEvent_t e : r->ev_wave)
         if (e) cudaEventDestroy(e);
     if (r->ev_seg) cudaEventDestroy(r->ev_seg);
     if (r->h_seg) cudaFreeHost(r->h_seg);
@@ -431,16 +435,19 @@ int ensure_records(so_renderer* r, long long ns) {
         SO_CK(r, cudaMallocHost((void**)&r->h_seg, 2 * sizeof(unsigned long long)));
         r->h_seg[0] = r->h_seg[1] = 0;
         SO_CK(r, cudaEventCreateWithFlags(&r->ev_seg, cudaEventDisableTiming));
-        for (cudaEvent_t& e : r->ev_turb) SO_CK(r, cudaEventCreate(&e));
     }
     if (r->seg_pending && cudaEventQuery(r->ev_seg) == cudaSuccess) {
         r->seg_pending = false;
         if (r->h_seg[1] > 0) r->rec_per_ray *= 2.0;
     }
     cudaGetLastError();  // a pending event reports cudaErrorNotReady
-    const long long want = std::min<long long>((long long)std::ceil((double)ns * r->rec_per_ray / REC_SEG) + ns,
-                                               0x7fffffffll);
-    if (want > r->seg_cap) {
+    const double per_seg = REC_SEG * (sizeof(float4) + sizeof(float)) + sizeof(uint32_t);
+    const double seg_per_ray = r->rec_per_ray / REC_SEG + 1.0;  // with the partly filled last segment
+    long long want = std::min<long long>((long long)std::ceil((double)ns * seg_per_ray), 0x7fffffffll);
+    if (r->mixed.pool_mb > 0.0)
+        want = std::min<long long>(want, std::max<long long>(1, (long long)(r->mixed.pool_mb * 1048576.0 / per_seg)));
+    // grow to a larger estimate; shrink only to a lowered cap
+    if (want > r->pool_target || (r->mixed.pool_mb > 0.0 && want < r->seg_cap)) {
         SO_CK(r, cudaStreamSynchronize(r->st));
         if (r->d_rec) cudaFree(r->d_rec);
         if (r->d_rec_delta) cudaFree(r->d_rec_delta);
@@ -451,7 +458,6 @@ int ensure_records(so_renderer* r, long long ns) {
         r->seg_cap = 0;
         size_t fr = 0, tot = 0;
         SO_CK(r, cudaMemGetInfo(&fr, &tot));
-        const double per_seg = REC_SEG * (sizeof(float4) + sizeof(float)) + sizeof(uint32_t);
         const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
         if (cap < 1) return fail(r, SO_ERR_ALLOC, "record pool: no device memory");
         if (dalloc(&r->d_rec, (size_t)cap * REC_SEG) != cudaSuccess ||
@@ -459,6 +465,16 @@ int ensure_records(so_renderer* r, long long ns) {
             dalloc(&r->d_seg_next, (size_t)cap) != cudaSuccess)
             return fail(r, SO_ERR_ALLOC, "record pool: device allocation");
         r->seg_cap = cap;
+        r->pool_target = want;
+    }
+    // waves of FP32 rays whose expected records fit the pool (at most 64)
+    const long long per_wave = std::max<long long>(1, (long long)((double)r->seg_cap / seg_per_ray));
+    r->waves = (int)std::min<long long>(64, (ns + per_wave - 1) / per_wave);
+    r->wave_rays = (ns + r->waves - 1) / r->waves;
+    while ((int)r->ev_wave.size() < 3 * r->waves) {
+        cudaEvent_t e;
+        SO_CK(r, cudaEventCreate(&e));
+        r->ev_wave.push_back(e);
     }
     if (ns > r->meta_cap) {
         if (r->d_ray_meta) cudaFree(r->d_ray_meta);
@@ -596,28 +612,52 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     }
     SO_CK(r, launch_approach64(L, ns, r->num_sms, r->st));
     SO_CK(r, cudaEventRecord(r->ev32[0], r->st));
-    SO_CK(r, launch_trace32(L, ns, variant_of(r->S), r->num_sms, r->st));
-    // FP64 re-trace of the rays the FP32 tracer handed back, on the second stream (after the band)
-    SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
-    SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
-    TraceLaunch Lr = Lb;
-    Lr.list = r->d_redo;
-    Lr.nrays_dev = &r->d_nlists[2];
-    Lr.counters = &r->d_cnt3[1];
-    rc = run_tracer(r, Lr, r->st2);
-    if (rc) return rc;
-    SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
+    // Deferred turbulence with a pool that holds only part of the frame's records: the parked FP32
+    // rays are traced in waves (slices of the parked list), each wave's records summed and
+    // transferred before the next wave reuses the pool.  Every ray's result depends on the ray alone,
+    // so the image does not depend on the split.
+    const int waves = defer ? r->waves : 1;
+    for (int w = 0; w < waves; ++w) {
+        TraceLaunch Lw = L;
+        if (waves > 1) {
+            Lw.wave_begin = (long long)w * r->wave_rays;
+            Lw.wave_end = (long long)(w + 1) * r->wave_rays;
+        }
+        if (w > 0) {
+            // tracer work counter; pool segments, accepted-ray list and the sums' work counters
+            SO_CK(r, cudaMemsetAsync(&r->d_cnt->next, 0, sizeof(unsigned long long), r->st));
+            SO_CK(r, cudaMemsetAsync(&r->d_nlists[4], 0, 2 * sizeof(unsigned long long), r->st));
+            SO_CK(r, cudaMemsetAsync(&r->d_nlists[7], 0, 2 * sizeof(unsigned long long), r->st));
+        }
+        if (defer) SO_CK(r, cudaEventRecord(r->ev_wave[3 * w], r->st));
+        SO_CK(r, launch_trace32(Lw, ns, variant_of(r->S), r->num_sms, r->st));
+        if (w == waves - 1) {
+            // FP64 re-trace of the rays the FP32 tracer handed back, on the second stream (after the band)
+            SO_CK(r, cudaEventRecord(r->ev_fork, r->st));
+            SO_CK(r, cudaStreamWaitEvent(r->st2, r->ev_fork, 0));
+            TraceLaunch Lr = Lb;
+            Lr.list = r->d_redo;
+            Lr.nrays_dev = &r->d_nlists[2];
+            Lr.counters = &r->d_cnt3[1];
+            rc = run_tracer(r, Lr, r->st2);
+            if (rc) return rc;
+            SO_CK(r, cudaEventRecord(r->ev_join, r->st2));
+        }
+        if (defer) {
+            SO_CK(r, cudaEventRecord(r->ev_wave[3 * w + 1], r->st));
+            SO_CK(r, launch_turb_records(Lw, *r->turb_modes, r->num_sms, r->st));
+            SO_CK(r, cudaEventRecord(r->ev_wave[3 * w + 2], r->st));
+            SO_CK(r, launch_flow_records(Lw, r->num_sms, r->st));
+        }
+    }
     if (defer) {
-        SO_CK(r, cudaEventRecord(r->ev_turb[0], r->st));
-        SO_CK(r, launch_turb_records(L, *r->turb_modes, r->num_sms, r->st));
-        SO_CK(r, cudaEventRecord(r->ev_turb[1], r->st));
-        SO_CK(r, launch_flow_records(L, r->num_sms, r->st));
         SO_CK(r, cudaMemcpyAsync(r->h_seg, &r->d_nlists[5], 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                  r->st));
         SO_CK(r, cudaEventRecord(r->ev_seg, r->st));
         r->seg_pending = true;
     }
     r->last_defer = defer;
+    r->last_waves = waves;
     if (sky) SO_CK(r, launch_sky_escape(L, r->num_sms, r->st));
     SO_CK(r, cudaEventRecord(r->ev32[1], r->st));
     SO_CK(r, cudaStreamWaitEvent(r->st, r->ev_join, 0));
@@ -749,14 +789,20 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->ms_turb = 0.0;
             stats->turb_records = 0;
             stats->redo_records = (long long)nl[6];
+            stats->record_waves = 0;
             if (r->last_defer) {
-                float a = 0.f, b = 0.f;
-                cudaEventElapsedTime(&a, r->ev32[0], r->ev_turb[0]);
-                cudaEventElapsedTime(&b, r->ev_turb[0], r->ev_turb[1]);
-                stats->ms_fp32_trace = a;
-                stats->ms_turb = b;
-                stats->turb_records =
-                    (long long)std::min<unsigned long long>(nl[5], (unsigned long long)r->seg_cap) * REC_SEG;
+                double ta = 0.0, tb = 0.0;
+                for (int w = 0; w < r->last_waves; ++w) {
+                    float a = 0.f, b = 0.f;
+                    cudaEventElapsedTime(&a, r->ev_wave[3 * w], r->ev_wave[3 * w + 1]);
+                    cudaEventElapsedTime(&b, r->ev_wave[3 * w + 1], r->ev_wave[3 * w + 2]);
+                    ta += a;
+                    tb += b;
+                }
+                stats->ms_fp32_trace = ta;
+                stats->ms_turb = tb;
+                stats->turb_records = (long long)nl[10] * REC_SEG;  // segments summed, all waves
+                stats->record_waves = r->last_waves;
             }
             // c.attempts now holds FP32 attempts (k_trace32) + band + re-trace FP64 attempts;
             // the FP64 approach's attempts are in pad[0]
@@ -772,6 +818,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->redo_turn = stats->redo_drift = stats->redo_limit = 0;
             stats->ms_fp32_trace = stats->ms_turb = 0.0;
             stats->turb_records = stats->redo_records = 0;
+            stats->record_waves = 0;
             c.fp64_rays = 0;
         }
         float ms1 = 0.f, ms2 = 0.f;
@@ -1202,6 +1249,8 @@ int so_set_precision(so_renderer* r, int precision, const so_mixed_opts* opts) {
         return fail(r, SO_ERR_ARG, "so_mixed_opts.turbulence: 0 or 1");
     if (opts && !(opts->records_per_ray >= 0.0 && opts->records_per_ray <= 1e6))
         return fail(r, SO_ERR_ARG, "so_mixed_opts.records_per_ray: 0 .. 1e6");
+    if (opts && !(opts->pool_mb >= 0.0 && opts->pool_mb <= 1e7))
+        return fail(r, SO_ERR_ARG, "so_mixed_opts.pool_mb: 0 .. 1e7");
     if (opts && opts->records_per_ray > 0.0) r->rec_per_ray = opts->records_per_ray;
     r->precision = precision;
     if (opts) r->mixed = *opts;

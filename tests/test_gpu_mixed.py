@@ -232,3 +232,28 @@ def test_deferred_turbulence_record_pool_shortage(so):
     with pytest.raises(so.TracerError):
         r.set_precision(so.abi.SO_PREC_MIXED, turbulence=2)
     r.close()
+
+
+def test_deferred_turbulence_record_waves(so):
+    """A record pool capped below the frame's records: the FP32 rays are traced in waves that each
+    fit the pool, and once no ray runs short of records the image is bit-identical to the frame
+    traced in one wave (every ray's result depends on the ray alone)."""
+    W = 128
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", N0])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    one, _, st1 = r.render(f)
+    assert st1.record_waves == 1 and st1.redo_records == 0
+    r.set_precision(so.abi.SO_PREC_MIXED, pool_mb=2.0)
+    for _ in range(6):  # a wave short of records doubles the estimate for the next frame
+        img, _, st = r.render(f)
+        if st.redo_records == 0:
+            break
+    assert st.redo_records == 0 and st.record_waves > 1, (st.redo_records, st.record_waves)
+    assert st.turb_records == st1.turb_records
+    assert np.array_equal(img, one)
+    with pytest.raises(so.TracerError):
+        r.set_precision(so.abi.SO_PREC_MIXED, pool_mb=-1.0)
+    r.close()
