@@ -306,6 +306,103 @@ def run_ours(args, so, world, rank, local):
     return line
 
 
+def run_shadow(args, so, world, rank, local):
+    """The vacuum shadow scene (a = 0.94, i = 17 deg, observer at 1000 M, pixel centres over +-8 M,
+    DP5(4) tolerance 1e-10, no emission) at 2048^2 through the mixed path, against the plain FP64
+    tracer on the same frame.  The per-image figure is the termination class of every sample (the
+    image itself is empty without a sky or disk)."""
+    import torch
+    torch.cuda.set_device(local)
+    W = args.size or 2048
+    sh = so.Shot("shadow_selftest_256.ini", [f"camera.width={W}", f"camera.height={W}"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = rank_frame(sh, rank)
+    npix = W * W
+    d_img = torch.empty((W, W, 4), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(r.stream())
+    r.set_precision(so.abi.SO_PREC_FP64)
+    st64 = r.render_device(f, d_img.data_ptr(), stats=True)
+    path = "fp64" if args.path == "fp64" else "mixed"
+    if path == "mixed":
+        r.set_precision(so.abi.SO_PREC_MIXED)
+    for _ in range(args.warmup):
+        r.render_device(f, d_img.data_ptr())
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
+            r.render_device(f, d_img.data_ptr())
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    barrier(world)
+    ms_step = allreduce_max(ms_step, world)
+    value = job_rate(world, npix, ms_step) / 1e6
+    st = r.render_device(f, d_img.data_ptr(), stats=True)
+    classes = None
+    if path == "mixed":
+        fm, band = r.last_fates(npix)
+        r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+        r.render_device(f, d_img.data_ptr())
+        f64, _ = r.last_fates(npix)
+        r.set_precision(so.abi.SO_PREC_MIXED)
+        out = ~band
+        classes = {"samples_outside_band": int(out.sum()),
+                   "class_mismatch_outside_band": int((fm[out] != f64[out]).sum()),
+                   "class_mismatch_in_band": int((fm[band] != f64[band]).sum())}
+    fp64_peak, fp32_peak = so.probe_fma_peak(local)
+    if path == "fp64":
+        flops = st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT
+        roof = {"bound": "fp64", "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
+                "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel": "k_trace64", "kernel_ms": st.ms_kernel,
+                "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
+    else:
+        # FP32 tracer: the DP5(4) attempt's algorithmic flops in FP32 (the two-sum compensation and
+        # the FP32 reciprocals not counted) against the measured FP32 FMA rate
+        flops = st.attempts_fp32 * FLOPS_ATTEMPT
+        roof = {"bound": "fp32", "achieved": round(flops / (st.ms_fp32 * 1e-3) / 1e12, 3),
+                "peak": round(fp32_peak, 3), "unit": "TFLOP/s", "kernel": "k_trace32", "kernel_ms": st.ms_fp32,
+                "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP32 FMA chains on this GPU)"}
+    roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
+    roof["traffic"] = None
+    host_pinned = torch.empty((W, W, 4), dtype=torch.float32).pin_memory().numpy()
+    for _ in range(2):
+        r.render(f, out=host_pinned)
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        r.render(f, out=host_pinned)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = allreduce_max(float(np.mean(e2e_ms)), world)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if path == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"vacuum shadow scene {W}x{W}, a=0.94, i=17 deg, observer 1000 M, pixel centres "
+                               f"over +-8 M, DP5(4) tolerance 1e-10", "path": path,
+                   "band_rays": st.band_rays if path == "mixed" else None,
+                   "fp64_rays": st.fp64_rays if path == "mixed" else None,
+                   "plain_fp64_mrays_s": round(npix / (st64.ms_kernel * 1e-3) / 1e6, 4),
+                   "attempts_per_ray": st.attempts / npix, "termination_class": classes,
+                   "l2": "256 MiB buffer written between timed steps"},
+        "roofline": roof,
+        "e2e": {"value": round(world * npix / (e2e_step * 1e-3) / 1e6, 4), "unit": "Mrays/s",
+                "h2d_bytes_per_step": C.sizeof(so.abi.Frame), "d2h_bytes_per_step": W * W * 16},
+        "gpu_launches": args.steps * (2 if path == "fp64" else 7),
+        "clocks": clk.summary(),
+    }
+    r.close()
+    return line
+
+
 # surrogate network: forward FLOPs per ray (FMA = 2; the head is 16 wide on the tensor cores)
 SUR_FLOPS_RAY = 2 * (128 * 256 + 3 * 256 * 256 + 256 * 16)
 SUR_SIGMA = 0.35           # std of the random Fourier frequencies per unit of the scaled inputs
@@ -605,7 +702,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="synchrotron", choices=["synchrotron", "surrogate", "wavefront"])
+    ap.add_argument("--workload", default="synchrotron",
+                    choices=["synchrotron", "surrogate", "wavefront", "shadow"])
     ap.add_argument("--size", type=int, default=0, help="frame width (default 2048 / 4096 / 512 per workload)")
     ap.add_argument("--band", type=float, default=0.1, help="surrogate: critical band half-width (M)")
     ap.add_argument("--train-rays", type=int, default=1 << 24)
@@ -627,6 +725,8 @@ def main():
         line = run_surrogate(args, so, world, rank, local)
     elif args.workload == "wavefront":
         line = run_wavefront(args, so, world, rank, local)
+    elif args.workload == "shadow":
+        line = run_shadow(args, so, world, rank, local)
     else:
         args.size = args.size or 2048
         line = run_ours(args, so, world, rank, local)

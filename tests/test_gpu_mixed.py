@@ -257,3 +257,30 @@ def test_deferred_turbulence_record_waves(so):
     with pytest.raises(so.TracerError):
         r.set_precision(so.abi.SO_PREC_MIXED, pool_mb=-1.0)
     r.close()
+
+
+def test_mixed_shadow_scene_classes(so):
+    """The vacuum shadow self-test scene (a = 0.94, i = 17 deg, observer at 1000 M, pixel centres over
+    +-8 M, tolerance 1e-10) through the mixed path: FP32 geometry outside the critical band, the
+    scene's FP64 tolerance inside it.  Every sample outside the band ends with the termination class
+    of the plain FP64 tracer, and the band holds the shadow edge."""
+    W = 256
+    sh = so.Shot("shadow_selftest_256.ini", [])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    n = W * W
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    _, _, st = r.render(f)
+    fm, band = r.last_fates(n)
+    assert 0 < st.band_rays == int(band.sum()) < n // 4
+    assert st.attempts_fp32 > 0
+    r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+    r.render(f)
+    f64, allband = r.last_fates(n)
+    assert allband.all()
+    out = ~band
+    assert set(np.unique(f64[out])) == {-1, 1}
+    assert np.array_equal(fm[out], f64[out]), int((fm[out] != f64[out]).sum())
+    # the band straddles the shadow edge: both classes inside it
+    assert (f64[band] == -1).any() and (f64[band] == 1).any()
+    r.close()
