@@ -284,3 +284,47 @@ def test_mixed_shadow_scene_classes(so):
     # the band straddles the shadow edge: both classes inside it
     assert (f64[band] == -1).any() and (f64[band] == 1).any()
     r.close()
+
+
+@pytest.mark.parametrize("W,H", [(37, 23), (5, 3), (1, 1)])
+def test_mixed_ragged_and_tiny_frames(so, W, H):
+    """Frames of odd, non-square and sub-warp sizes through the mixed path (deferred turbulence on):
+    every sample outside the band ends with the FP64 termination class, the image is finite and, at
+    37 x 23, within the mixed path's bar of the FP64 frame."""
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={H}", N0])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    n = W * H * sh.settings.spp
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    img, _, st = r.render(f)
+    assert img.shape == (H, W, 4) and np.isfinite(img).all()
+    fm, band = r.last_fates(n)
+    r.set_precision(so.abi.SO_PREC_MIXED, band_m=1e6)
+    r.render(f)
+    f64, _ = r.last_fates(n)
+    assert np.array_equal(fm[~band], f64[~band])
+    if W * H > 100:
+        assert st.turb_records > 0
+        l1, flux = _errors(img64, img)
+        assert l1 <= 1e-3 and flux <= 1e-3, (l1, flux)
+    r.close()
+
+
+def test_trace_rays_empty_list(so):
+    """An empty ray list is a no-op through both the host and the device entry points."""
+    sh = so.Shot("shadow_selftest_256.ini", ["camera.width=8", "camera.height=8"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    k = r.trace_rays(f, np.zeros(0), np.zeros(0))
+    assert all(v.size == 0 for v in k.values() if isinstance(v, np.ndarray))
+    import ctypes as C
+    out = so.abi.RaysOut()
+    assert so.lib().so_trace_rays_device(r.h, C.byref(f), 0, None, None, C.byref(out)) == so.abi.SO_OK
+    assert so.lib().so_trace_rays(r.h, C.byref(f), -1, None, None, C.byref(out)) == so.abi.SO_ERR_ARG
+    # still usable afterwards
+    k = r.trace_rays(f, np.array([0.0, 0.01]), np.array([0.0, 0.0]))
+    assert k["fate"][0] == -1 and k["fate"][1] == 1
+    r.close()
