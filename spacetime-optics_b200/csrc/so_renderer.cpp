@@ -446,8 +446,8 @@ int ensure_records(so_renderer* r, long long ns) {
     long long want = std::min<long long>((long long)std::ceil((double)ns * seg_per_ray), 0x7fffffffll);
     if (r->mixed.pool_mb > 0.0)
         want = std::min<long long>(want, std::max<long long>(1, (long long)(r->mixed.pool_mb * 1048576.0 / per_seg)));
-    // grow to a larger estimate; shrink only to a lowered cap
-    if (want > r->pool_target || (r->mixed.pool_mb > 0.0 && want < r->seg_cap)) {
+    // grow to a larger estimate; shrink only to a lowered cap; retry after a failed allocation
+    if (r->seg_cap <= 0 || want > r->pool_target || (r->mixed.pool_mb > 0.0 && want < r->seg_cap)) {
         SO_CK(r, cudaStreamSynchronize(r->st));
         if (r->d_rec) cudaFree(r->d_rec);
         if (r->d_rec_delta) cudaFree(r->d_rec_delta);
@@ -456,6 +456,7 @@ int ensure_records(so_renderer* r, long long ns) {
         r->d_rec_delta = nullptr;
         r->d_seg_next = nullptr;
         r->seg_cap = 0;
+        r->pool_target = -1;
         size_t fr = 0, tot = 0;
         SO_CK(r, cudaMemGetInfo(&fr, &tot));
         const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
