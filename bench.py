@@ -250,9 +250,9 @@ def run_ours(args, so, world, rank, local):
                 "transfer_k_flow_records_ms": round(st.ms_fp32 - st.ms_fp32_trace - st.ms_turb, 3),
                 "record_slots": st.turb_records}
         # DRAM bytes per record slot of k_turb_records from its ncu capture on the 512^2 frame
-        # (profiles/k_turb_records_synchrotron512.md: 1.349 GB for 68.16 M slots), scaled by this
+        # (profiles/k_turb_records_synchrotron512.md: 1.347 GB for 68.16 M slots), scaled by this
         # frame's slots; the algorithmic figure is 20 bytes per slot
-        roof["traffic"] = round(19.79 * st.turb_records)
+        roof["traffic"] = round(19.77 * st.turb_records)
         roof["traffic_source"] = "ncu dram bytes per slot at 512^2 x this frame's record slots"
         roof["algorithmic_bytes"] = 20 * st.turb_records
     else:
