@@ -145,8 +145,13 @@ def barrier(world):
         dist.barrier()
 
 
-def build_scene(so, W, flux_norm=True):
-    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}"])
+# reference flow workload: the shot's baked fBm turbulence at a converged emission quadrature
+FLOW_SHOT = "m87_reference_flow.ini"
+FLOW_OVERRIDES = ["render.spp=1", "render.spp_max=1", "render.step_fraction=0.01"]
+
+
+def build_scene(so, W, flux_norm=True, shot="synchrotron_1024.ini", extra=()):
+    sh = so.Shot(shot, [f"camera.width={W}", f"camera.height={W}", *extra])
     r = so.Renderer(sh.scene, sh.tables, sh.settings)
     p = sh.plasma()
     r.set_plasma(p)
@@ -167,7 +172,11 @@ def run_ours(args, so, world, rank, local):
     import torch
     torch.cuda.set_device(local)
     W = args.size
-    sh, r, norm = build_scene(so, W)
+    flow = args.workload == "flow"
+    if flow:
+        sh, r, norm = build_scene(so, W, shot=FLOW_SHOT, extra=FLOW_OVERRIDES)
+    else:
+        sh, r, norm = build_scene(so, W)
     path = args.path
     if path == "auto":
         path = "mixed"
@@ -231,7 +240,8 @@ def run_ours(args, so, world, rank, local):
     # roofline of the dominant kernel: the FP64 tracer (plain path, FP64 pipe) or the FP32 tracer
     # (mixed path, SFU-bound: one cosine per Fourier mode per flow step)
     fp64_peak, fp32_peak = so.probe_fma_peak(local)
-    n_modes = sh.plasma().n_modes
+    pl = sh.plasma()
+    n_modes = pl.n_modes if pl is not None else 0  # reference flow model: no Fourier modes
     if path == "fp64":
         flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT +
                  st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
@@ -280,13 +290,19 @@ def run_ours(args, so, world, rank, local):
     del host
     # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, [turbulence sums,
     # transfer,] re-trace, gather, resolve (mixed); spp_max = spp, so no adaptive pass
-    gpu_launches = args.steps * (2 if path == "fp64" else 9 if st.ms_turb > 0 else 7)
+    gpu_launches = args.steps * ((2 if path == "fp64" else 9 if st.ms_turb > 0 else 7) + (1 if flow else 0))
+    if flow:
+        workload = (f"reference flow {W}x{W} (n ~ r^-1.1, fBm turbulence baked per frame into 24 slices of "
+                    f"512x192x48), a=0.94, i=163 deg, fov 30 M, 230 GHz, step fraction 0.01, 1 R2-jittered "
+                    f"sample/pixel (k_pass1 sampling)")
+    else:
+        workload = (f"synchrotron torus frame {W}x{W}, a=0.94, i=163 deg, fov +-12 M, 230 GHz, "
+                    f"512 Fourier modes, 1 R2-jittered sample/pixel (k_pass1 sampling)")
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if path == "fp64" else "f32+f64", "data": "synthetic",
-        "config": {"workload": f"synchrotron torus frame {W}x{W}, a=0.94, i=163 deg, fov +-12 M, 230 GHz, "
-                               f"512 Fourier modes, 1 R2-jittered sample/pixel (k_pass1 sampling)", "path": path,
+        "config": {"workload": workload, "path": path,
                    "band_rays": st.band_rays if path == "mixed" else None,
                    "fp64_rays": st.fp64_rays if path == "mixed" else None,
                    "plain_fp64_mrays_s": round(fp64_mrays, 4), "image_rel_l1_vs_fp64": err_l1,
@@ -300,7 +316,7 @@ def run_ours(args, so, world, rank, local):
         "gpu_launches": gpu_launches,
         "clocks": clk.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not flow:
         line["cpu_baseline"] = cpu_baseline(so, sh, f, W, budget_s=args.cpu_seconds)
     r.close()
     return line
@@ -703,8 +719,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="synchrotron",
-                    choices=["synchrotron", "surrogate", "wavefront", "shadow"])
-    ap.add_argument("--size", type=int, default=0, help="frame width (default 2048 / 4096 / 512 per workload)")
+                    choices=["synchrotron", "surrogate", "wavefront", "shadow", "flow"])
+    ap.add_argument("--size", type=int, default=0, help="frame width (default: synchrotron and shadow 2048, surrogate 4096, wavefront 512, flow 1024)")
     ap.add_argument("--band", type=float, default=0.1, help="surrogate: critical band half-width (M)")
     ap.add_argument("--train-rays", type=int, default=1 << 24)
     ap.add_argument("--train-steps", type=int, default=40000)
@@ -727,6 +743,9 @@ def main():
         line = run_wavefront(args, so, world, rank, local)
     elif args.workload == "shadow":
         line = run_shadow(args, so, world, rank, local)
+    elif args.workload == "flow":
+        args.size = args.size or 1024
+        line = run_ours(args, so, world, rank, local)
     else:
         args.size = args.size or 2048
         line = run_ours(args, so, world, rank, local)

@@ -55,13 +55,16 @@ __device__ __forceinline__ void sample_point(int W, int H, int jitter, const so_
     *yv = (0.5 * H - (py + jy)) * F.pix;
 }
 
+// The twelve edge gradients of grad3's switch (device_util.cuh:32-41), selected without a branch (a 12-way
+// switch on a hash diverges in every warp): case g < 8 takes fx first, else fy; g < 4 takes fy
+// second, else fz; bit 0 of g negates the first term, bit 1 the second.  Same sums, bit for bit
+// (a - b is a + (-b) in IEEE arithmetic).
 __device__ __forceinline__ float grad3(int ix, int iy, int iz, uint32_t seed, float fx, float fy, float fz) {
     uint32_t h = pcg((uint32_t)ix * 73856093u ^ pcg((uint32_t)iy * 19349663u ^ pcg((uint32_t)iz * 83492791u ^ seed)));
-    switch (h % 12u) {
-        case 0: return fx + fy;   case 1: return -fx + fy;  case 2: return fx - fy;   case 3: return -fx - fy;
-        case 4: return fx + fz;   case 5: return -fx + fz;  case 6: return fx - fz;   case 7: return -fx - fz;
-        case 8: return fy + fz;   case 9: return -fy + fz;  case 10: return fy - fz;  default: return -fy - fz;
-    }
+    const uint32_t g = h % 12u;
+    const float u = g < 8u ? fx : fy;
+    const float v = g < 4u ? fy : fz;
+    return ((g & 1u) ? -u : u) + ((g & 2u) ? -v : v);
 }
 static __device__ float gnoise(float x, float y, float z, uint32_t seed) {
     float fx = floorf(x), fy = floorf(y), fz = floorf(z);
