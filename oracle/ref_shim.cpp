@@ -187,6 +187,18 @@ double ref_radial_drift(int* steps_out) {
     return worst;
 }
 
+// The reference's noise at n points, for function-level pins of the oracle's noise (whole rays
+// through turbulence are ill-conditioned in the noise phase): fbm3 (device_util.cuh:61-72) and
+// sheared_noise (emission.cuh:34-51, which reads the scene's spin and ISCO radius).
+void ref_fbm3(int n, const float* x, const float* y, const float* z, int oct, uint32_t seed, float* out) {
+    for (int i = 0; i < n; ++i) out[i] = fbm3(x[i], y[i], z[i], oct, seed);
+}
+void ref_sheared_noise(const void* scene, int n, const double* R, const double* phi, const double* z, const double* t,
+                       float scale, float tcorr, uint32_t seed, float* out) {
+    std::memcpy(&c_S, scene, sizeof(SceneGPU));
+    for (int i = 0; i < n; ++i) out[i] = sheared_noise(R[i], phi[i], z[i], t[i], scale, tcorr, seed);
+}
+
 // trace_ray (trace.cuh:62) for n tangent-plane points, nthreads host threads.  Outputs: fate (int8),
 // theta/phi from escape_angles (recomputed from the uv path is not possible, so the shim exposes
 // the reference's own escape_angles through a copy of the final state: see ref_trace_state).

@@ -748,6 +748,16 @@ static void* job_run(void* p) {
     return NULL;
 }
 
+/* The oracle's noise at n points (fbm3, device_util.cuh:61-72; sheared_noise, emission.cuh:34-51),
+   for the function-level pins against the reference's own code. */
+void orc_fbm3(int n, const float* x, const float* y, const float* z, int oct, uint32_t seed, float* out) {
+    for (int i = 0; i < n; ++i) out[i] = fbm3(x[i], y[i], z[i], oct, seed);
+}
+void orc_sheared_noise(const so_scene* S, int n, const double* R, const double* phi, const double* z, const double* t,
+                       float scale, float tcorr, uint32_t seed, float* out) {
+    for (int i = 0; i < n; ++i) out[i] = sheared_noise(S, R[i], phi[i], z[i], t[i], scale, tcorr, seed);
+}
+
 /* trace_ray over n explicit tangent-plane points (x[i], y[i]) with nthreads host threads. */
 int orc_trace_rays(const so_scene* S, const so_plasma* pl, const so_mode* modes, const so_frame* F, int n,
                    const double* x, const double* y, const so_rays_out* out, int nthreads) {

@@ -45,6 +45,10 @@ def oracle():
         L.orc_set_sky.restype = None
         L.orc_turb_setup.argtypes = [P(Scene)]
         L.orc_turb_setup.restype = None
+        L.orc_fbm3.argtypes = [C.c_int, vp, vp, vp, C.c_int, C.c_uint32, vp]
+        L.orc_fbm3.restype = None
+        L.orc_sheared_noise.argtypes = [P(Scene), C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
+        L.orc_sheared_noise.restype = None
         L.so_rpow5.argtypes = [C.c_double]
         L.so_rpow5.restype = C.c_double
         _orc = L
@@ -81,6 +85,10 @@ def ref():
         L.ref_trace_rays.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, C.c_int]
         L.ref_trace_vacuum.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int]
         L.ref_render_pass1.argtypes = [vp, vp, vp, P(C.c_longlong), C.c_int]
+        L.ref_fbm3.argtypes = [C.c_int, vp, vp, vp, C.c_int, C.c_uint32, vp]
+        L.ref_fbm3.restype = None
+        L.ref_sheared_noise.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
+        L.ref_sheared_noise.restype = None
         _ref = L
     return _ref
 
@@ -191,6 +199,24 @@ def ref_pass1(scene, frame, threads=8):
     lim = C.c_longlong()
     ref().ref_render_pass1(C.byref(scene), C.byref(frame), _p(acc), C.byref(lim), threads)
     return acc, lim.value
+
+
+def noise(lib, kind, x, y, z, seed, scene=None, scale=None, tcorr=None, t=None, oct=4):
+    """fbm3 (kind "fbm3": float x, y, z) or sheared_noise (kind "sheared": double R, phi, z, t with the
+    scene's spin / ISCO) at n points, from the oracle (lib "orc") or the reference (lib "ref")."""
+    n = len(x)
+    out = np.zeros(n, np.float32)
+    if kind == "fbm3":
+        a = [np.ascontiguousarray(v, np.float32) for v in (x, y, z)]
+        f = oracle().orc_fbm3 if lib == "orc" else ref().ref_fbm3
+        f(n, _p(a[0]), _p(a[1]), _p(a[2]), oct, seed, _p(out))
+    else:
+        a = [np.ascontiguousarray(v, np.float64) for v in (x, y, z, t)]
+        if lib == "orc":
+            oracle().orc_sheared_noise(C.byref(scene), n, *(_p(v) for v in a), scale, tcorr, seed, _p(out))
+        else:
+            ref().ref_sheared_noise(C.byref(scene), n, *(_p(v) for v in a), scale, tcorr, seed, _p(out))
+    return out
 
 
 def _module(name, fname):

@@ -107,7 +107,34 @@ def main():
         kp.append([a, r, th] + [getattr(k, n) for n, _ in O.KerrPoint._fields_])
     np.savez_compressed(os.path.join(HERE, "selftest.npz"), edges=np.array(rows), drift=np.float64(drift),
                         drift_steps=np.int64(steps.value), ccp=np.array(ccp), kerr_point=np.array(kp))
+    noise_fixture()
     print("golden fixtures written to", HERE)
+
+
+def noise_fixture():
+    """7. The reference's noise, function by function (whole rays through turbulence are
+    ill-conditioned in the noise phase): fbm3 at random float points for three seeds, and
+    sheared_noise with the reference flow's and the thin disk's turbulence parameters at random
+    (R, phi, z) and times up to 1e5 M and up to 1e7 M (the camera's coordinate time)."""
+    rng = np.random.default_rng(20261203)
+    n = 2048
+    x, y, z = (rng.uniform(-40, 40, n).astype(np.float32) for _ in range(3))
+    seeds = np.array([1, 0x51f15eed ^ 7, 123456789], np.uint32)
+    fbm = np.stack([O.noise("ref", "fbm3", x, y, z, int(sd)) for sd in seeds])
+    out = dict(fx=x, fy=y, fz=z, fseeds=seeds, fbm3=fbm)
+    for tag, shot, disk in (("flow", "m87_reference_flow", False), ("disk", "thin_disk_4096", True)):
+        S = O.RefShot(os.path.join(SHOTS, shot + ".ini")).scene
+        scale, tcorr = (S.disk_turb_scale, S.disk_tcorr) if disk else (S.flow_turb_scale, S.flow_tcorr)
+        seed = S.seed if disk else S.seed ^ 0x51f15eed
+        R = rng.uniform(1.5, 60, n)
+        phi = rng.uniform(0, 2 * np.pi, n)
+        zz = np.zeros(n) if disk else rng.uniform(-0.4, 0.4, n) * R
+        t = np.concatenate([rng.uniform(-1e5, 1e5, n // 2), rng.uniform(-1e7, 1e7, n - n // 2)])
+        out.update({f"{tag}_scene": scene_bytes(S), f"{tag}_R": R, f"{tag}_phi": phi, f"{tag}_z": zz, f"{tag}_t": t,
+                    f"{tag}_param": np.array([scale, tcorr], np.float32), f"{tag}_seed": np.uint32(seed),
+                    f"{tag}_noise": O.noise("ref", "sheared", R, phi, zz, seed, scene=S, scale=scale, tcorr=tcorr,
+                                             t=t)})
+    np.savez_compressed(os.path.join(HERE, "noise.npz"), **out)
 
 
 if __name__ == "__main__":

@@ -178,3 +178,25 @@ def test_planted_mistake_is_caught(orc, mismatch):
         s.r_stop = s.r_stop + 0.5  # a wrong capture radius changes fates near the shadow
         o = orc.orc_trace(s, f, g["x"], g["y"])
         assert not np.array_equal(o["n_accepted"], g["n_accepted"])
+
+
+def test_noise_vs_reference(orc):
+    """The oracle's noise against the reference's own fbm3 and sheared_noise (golden/noise.npz, made
+    by make_golden.py from the reference compiled for the host).  fbm3 is float arithmetic in the
+    same order: bit-exact.  sheared_noise is bit-exact up to |t| = 1e5 M; at the camera's coordinate
+    time (|t| up to 1e7 M) the oracle's fused R sqrt(R) + a in the Keplerian rate (the device build's
+    form) may move the float noise by a few ulps.  Only the scene's spin and ISCO radius are read."""
+    g = np.load(os.path.join(GOLD, "noise.npz"))
+    for sd, want in zip(g["fseeds"], g["fbm3"]):
+        got = orc.noise("orc", "fbm3", g["fx"], g["fy"], g["fz"], int(sd))
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    for tag in ("flow", "disk"):
+        S = scene_from_bytes(orc, g[f"{tag}_scene"])
+        scale, tcorr = (float(v) for v in g[f"{tag}_param"])
+        got = orc.noise("orc", "sheared", g[f"{tag}_R"], g[f"{tag}_phi"], g[f"{tag}_z"], int(g[f"{tag}_seed"]),
+                        scene=S, scale=scale, tcorr=tcorr, t=g[f"{tag}_t"])
+        want = g[f"{tag}_noise"]
+        near = np.abs(g[f"{tag}_t"]) <= 1e5
+        assert near.sum() >= 1000 and np.array_equal(got[near], want[near])
+        assert np.abs(got - want).max() <= 4e-6 and np.mean(got == want) >= 0.999
+        assert want.std() > 0.5  # a unit-variance field, not a constant
