@@ -13,8 +13,8 @@ Multi-GPU: frames are independent, so N ranks each render their own frame (weak 
 collective on the data path); the max over ranks of the device time gives the job time.
 
 --impl reference times the reference's own CPU tracer (oracle/_ref, built from the reference
-sources) on the host cores over a bounded sample of the same pixels; see DESIGN.md for how its
-plasma maps onto this workload.
+sources) on the host cores over a bounded sample of the same pixels.  The torus plasma is not part
+of the reference, so that arm runs the reference's own flow model with the torus's indices.
 """
 import argparse
 import ctypes as C
@@ -34,7 +34,7 @@ PKG_DIR = os.path.join(ROOT, "spacetime-optics_b200")
 METRIC = "Mrays/s at ≤1e-3 image error: surrogate/mixed vs plain FP64 kernel, 1 B200"
 
 # Algorithmic FP64 flops (FMA = 2, divide = 1, sqrt = 1; comparisons, fabs and fmin/fmax not counted),
-# counted from spacetime-optics_b200/csrc/so_kerr.cuh and so_emission.cuh (see DESIGN.md):
+# counted from spacetime-optics_b200/csrc/so_kerr.cuh and so_emission.cuh:
 FLOPS_ATTEMPT = 469        # one DP5(4) attempt: 6 RHS (31 each) + stage sums + 5th-order sum + error norm
 FLOPS_ACCEPT = 49          # controller err^-1/5 (34) + projection (11) + psi bookkeeping excluded (radio)
 FLOPS_FLOW = 160           # flow_step without the turbulence sum (transcendentals counted as 20 each)

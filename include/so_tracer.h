@@ -441,7 +441,7 @@ int so_sur_dataset(so_renderer* r, const so_frame* f, long long n, int groups, u
  * curve goes to the FP64 integrator; of the others a random audit_frac sample (seeded) goes to the
  * integrator as well, and the surrogate shades the rest from its predicted crossing radii (the
  * redshift is the exact one of that radius and the ray's constants of motion).  The integrator
- * judges the surrogate on the audit rays.  Renderer r holds a visible-mode disk scene (no disk
+ * checks the surrogate on the audit rays.  Renderer r holds a visible-mode disk scene (no disk
  * turbulence); d_px is W x H x 4 floats of device memory, the same quantity so_trace_rays reports
  * as I at the pixel centres. */
 typedef struct so_sur_frame_opts { double band_m, audit_frac; uint32_t audit_seed; } so_sur_frame_opts;

@@ -56,8 +56,10 @@ def main():
                             info=np.array(Rs.info), settings=np.array(Rs.settings[:4], np.int64),
                             target_err=np.float32(Rs.settings[4]))
 
-    # 4. Hot flow, the reference's model without turbulence (its fBm time phase is ill-conditioned,
-    #    see DESIGN.md), 32 x 32 pixel centres, and pass 1 with R2 jitter at spp = 2
+    # 4. Hot flow, the reference's model without turbulence (its fBm time phase is ill-conditioned:
+    #    the noise generation and advection use the raw coordinate time t ~ -r_cam, so 1e-10 of
+    #    position moves the noise by ~1e-4), 32 x 32 pixel centres, and pass 1 with R2 jitter at
+    #    spp = 2
     Rf = O.RefShot(os.path.join(SHOTS, "m87_reference_flow.ini"), ["flow.turbulence=0", "camera.width=32",
                                                                     "camera.height=32"])
     ff = Rf.frame(0)

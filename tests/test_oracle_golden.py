@@ -1,6 +1,6 @@
 """The CPU oracle (oracle/so_oracle.c) against golden vectors produced by the reference's own code.
 
-These pin the oracle before it is used to judge the CUDA kernels.  The fixtures come from
+These pin the oracle before it is used to check the CUDA kernels.  The fixtures come from
 tests/golden/make_golden.py, which runs the reference's trace_ray / kerr.hpp / scene_build.cpp /
 shot.cpp compiled for the host.
 """
