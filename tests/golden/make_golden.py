@@ -139,5 +139,36 @@ def noise_fixture():
     np.savez_compressed(os.path.join(HERE, "noise.npz"), **out)
 
 
+# Vacuum scenes beyond the shadow self-test: spins and inclinations that reach the builder's spin
+# clamp (build_scene keeps a in [1e-6, 0.9999]), the near-extremal horizon, an edge-on camera, a
+# camera 0.5 deg off the pole, one below the plane, and a camera ON the pole (sin(theta) = 0: every
+# ray's phi derivative is infinite, the error estimate NaN, so each ray only shrinks its step until
+# max_steps and ends step-limited -- the reference's behaviour, reproduced, not fixed).
+SWEEP = ((0.0, 60.0), (-0.7, 75.0), (0.5, 90.0), (0.998, 45.0), (0.94, 0.5), (0.3, 163.0), (1.0, 30.0),
+         (0.94, 0.0))
+
+
+def sweep_fixture():
+    """8. Spin / inclination sweep on the shadow self-test shot: 256 rays (every 257th pixel centre
+    of the 256^2 grid) per scene, 16 for the pole camera, traced by the reference's trace_ray."""
+    out = dict(cases=np.array(SWEEP))
+    for c, (spin, incl) in enumerate(SWEEP):
+        ov = [f"bh.spin={spin}", f"camera.incl={incl}"]
+        R = O.RefShot(os.path.join(SHOTS, "shadow_selftest_256.ini"), ov)
+        f = R.frame(0)
+        X, Y = so.pixel_centres(f, 256, 256)
+        idx = np.arange(0, 256 * 256, 257 if incl > 0 else 4099)
+        v = O.ref_vacuum(R.scene, f, X[idx], Y[idx])
+        out.update({f"c{c}_x": X[idx], f"c{c}_y": Y[idx], f"c{c}_a": np.float64(R.scene.a),
+                    f"c{c}_scene": scene_bytes(R.scene), f"c{c}_frame": scene_bytes(f)})
+        out.update({f"c{c}_{k}": val for k, val in v.items()})
+    np.savez_compressed(os.path.join(HERE, "sweep_rays.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    # no argument: every fixture; otherwise only the named ones (noise, sweep)
+    if len(sys.argv) == 1:
+        main()
+        sweep_fixture()
+    for name in sys.argv[1:]:
+        {"noise": noise_fixture, "sweep": sweep_fixture}[name]()

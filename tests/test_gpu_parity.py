@@ -59,6 +59,34 @@ def test_shadow_vs_reference_golden(so, shadow):
         assert rel.max() < 1e-9, (key, rel.max())
 
 
+def test_spin_inclination_sweep(so, orc):
+    """golden/sweep_rays.npz: the shadow shot at eight other spins and inclinations (spin clamp at
+    both ends, a = 0.998 and 0.9999, edge-on, 0.5 deg off the pole, below the plane, on the pole).
+    The package's shot builder gives the reference's scene and frame for each; the kernel equals
+    the oracle on every ray (fate, winding order, step counts; escape direction 1e-13 relative) and
+    the reference's trace_ray in fate, winding order and escape direction (1e-9 relative)."""
+    g = np.load(os.path.join(GOLD, "sweep_rays.npz"))
+    for c, (spin, incl) in enumerate(g["cases"]):
+        sh = so.Shot("shadow_selftest_256.ini", [f"bh.spin={spin}", f"camera.incl={incl}"])
+        assert sh.scene.a == float(g[f"c{c}_a"])
+        f = sh.frame(0)
+        assert bytes(memoryview(f)) == g[f"c{c}_frame"].tobytes(), (spin, incl)
+        x, y = g[f"c{c}_x"], g[f"c{c}_y"]
+        r = so.Renderer(sh.scene, sh.tables, sh.settings)
+        try:
+            k = r.trace_rays(f, x, y)
+        finally:
+            r.close()
+        _cmp_geometry(orc.orc_trace(sh.scene, f, x, y), k)
+        assert np.array_equal(k["fate"], g[f"c{c}_fate"]), (spin, incl)
+        assert np.array_equal(k["ncross"], g[f"c{c}_ncross"]), (spin, incl)
+        esc = k["fate"] == 1
+        for key in ("theta", "phi"):
+            ref = g[f"c{c}_{key}"][esc]
+            rel = np.abs(k[key][esc] - ref) / np.maximum(np.abs(ref), 1e-300)
+            assert rel.max(initial=0.0) < 1e-9, (spin, incl, key, rel.max())
+
+
 def test_crossing_records_vs_oracle(so, orc, shadow):
     """First three equatorial crossings (radius, circular-emitter redshift) recorded per ray."""
     sh, r = shadow
