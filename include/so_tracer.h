@@ -336,7 +336,8 @@ int so_set_plasma(so_renderer* r, const so_plasma* plasma, const so_mode* modes)
 int so_last_fates(so_renderer* r, int8_t* fate, uint8_t* in_band, long long n);
 /* CUDA stream used by the renderer (cudaStream_t, as void*), for callers that order work on it. */
 void* so_stream(so_renderer* r);
-/* Message of the last failed call on r (or of the last failed so_init when r is NULL). */
+/* Message of the last failed call on r.  With r NULL: of the last failed call without a renderer
+ * (so_init, so_shot_load, so_radio_flux_noalloc, so_sur_gemm) made by the calling thread. */
 const char* so_last_error(const so_renderer* r);
 void so_destroy(so_renderer* r);
 

@@ -43,7 +43,10 @@ using namespace so;
 
 namespace {
 constexpr int CHUNK = 8;  // samples per pass-2 job (render.cu:30)
-std::string g_init_error;
+// Message of the last failed call that has no renderer to hold it (so_init, the shot builders,
+// so_radio_flux_noalloc, so_sur_gemm).  One per host thread, like errno: renderers on different
+// GPUs may be driven from different threads, and a shared string would be a data race.
+thread_local std::string g_init_error;
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();

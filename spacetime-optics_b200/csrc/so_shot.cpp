@@ -299,6 +299,8 @@ void scene_set_spin(so_scene* S, double a) {
     S->r_isco = isco_radius(a);
     S->r_stop = S->rh + margin;
 }
+
+void set_global_error(const std::string& msg);  // so_renderer.cpp: so_last_error(NULL)
 }  // namespace so
 
 using namespace so;
@@ -538,13 +540,17 @@ double find_critical(const so_shot* sh, const ShotFrame& f, double a, double psi
 extern "C" {
 
 int so_shot_load(const char* ini_path, const char* const* overrides, int n_overrides, so_shot** out) {
-    if (!out) return SO_ERR_ARG;
+    if (!out || !ini_path || n_overrides < 0 || (n_overrides > 0 && !overrides)) {
+        so::set_global_error("so_shot_load: NULL path / output or bad override list");
+        if (out) *out = nullptr;
+        return SO_ERR_ARG;
+    }
     *out = nullptr;
-    if (!ini_path || n_overrides < 0 || (n_overrides > 0 && !overrides)) return SO_ERR_ARG;
     so_shot* sh = new so_shot;
     std::string err;
     if (!sh->cfg.load(ini_path, &err)) {
         std::fprintf(stderr, "so_shot_load: %s\n", err.c_str());
+        so::set_global_error("so_shot_load: " + err);
         delete sh;
         return SO_ERR_CONFIG;
     }
@@ -552,6 +558,7 @@ int so_shot_load(const char* ini_path, const char* const* overrides, int n_overr
         std::string kv = overrides[i] ? overrides[i] : "";
         size_t eq = kv.find('=');
         if (eq == std::string::npos) {
+            so::set_global_error("so_shot_load: override '" + kv + "' is not key=value");
             delete sh;
             return SO_ERR_ARG;
         }

@@ -166,6 +166,42 @@ def test_init_fails_loudly_without_device_or_bad_args(so):
     assert lib.so_last_error(None)  # message of the last failed init
 
 
+def test_handleless_errors_are_per_thread(so, tmp_path):
+    """so_last_error(NULL) reports the calling thread's last failed handle-less call: the shot loader
+    says which file or override it refused, and threads failing at the same time each read their
+    own message (the string is thread-local, as errno is)."""
+    import threading
+    lib = so.lib()
+    h = C.c_void_p()
+    arr = (C.c_char_p * 1)(b"camera.width")
+    good = os.path.join(ROOT, "spacetime-optics_b200", "shots", "shadow_selftest_256.ini").encode()
+    assert lib.so_shot_load(good, arr, 1, C.byref(h)) == so.abi.SO_ERR_ARG and not h.value
+    assert b"camera.width" in lib.so_last_error(None)
+    assert lib.so_shot_load(None, None, 0, C.byref(h)) == so.abi.SO_ERR_ARG
+    assert b"NULL" in lib.so_last_error(None)
+
+    seen, start = {}, threading.Barrier(4)
+
+    def worker(i):
+        path = str(tmp_path / f"missing_{i}.ini").encode()
+        start.wait()
+        out = []
+        for _ in range(200):
+            hh = C.c_void_p()
+            rc = lib.so_shot_load(path, None, 0, C.byref(hh))
+            out.append((rc, lib.so_last_error(None)))
+        seen[i] = (path, out)
+
+    ts = [threading.Thread(target=worker, args=(i,)) for i in range(4)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    for i, (path, out) in seen.items():
+        for rc, msg in out:
+            assert rc == so.abi.SO_ERR_CONFIG and path in msg, (i, msg)
+
+
 def test_far_field_approach_matches_mino_time(so):
     """The mixed path's far-field transport (DP5(4) in 1/r) lands on the state that the reference's
     Mino-time DP5(4) reaches at tolerance 1e-13, from the synchrotron camera at r = 1e7 M down to
