@@ -165,10 +165,38 @@ def sweep_fixture():
     np.savez_compressed(os.path.join(HERE, "sweep_rays.npz"), **out)
 
 
+# Emission at other spins and inclinations: the thin disk (its Novikov-Thorne table follows the
+# spin's ISCO) and the reference hot flow without turbulence (the noise phase is ill-conditioned).
+EMISSION = (("thin_disk_4096", 0.5, 30.0), ("thin_disk_4096", 0.998, 85.0),
+            ("m87_reference_flow", 0.3, 40.0), ("m87_reference_flow", 1.0, 100.0))
+
+
+def emission_fixture():
+    """9. 24 x 24 pixel centres per case, traced by the reference's trace_ray with its own scene
+    and tables for that spin (stored with the rays)."""
+    out = dict(cases=np.array([(0 if sh.startswith("thin") else 1, a, i) for sh, a, i in EMISSION]))
+    k2 = bb = None
+    for c, (shot, spin, incl) in enumerate(EMISSION):
+        ov = [f"bh.spin={spin}", f"camera.incl={incl}", "camera.width=24", "camera.height=24"]
+        if shot.startswith("m87"):
+            ov.append("flow.turbulence=0")
+        R = O.RefShot(os.path.join(SHOTS, shot + ".ini"), ov)
+        f = R.frame(0)
+        X, Y = so.pixel_centres(f, 24, 24)
+        t = O.ref_trace(R.scene, f, X, Y)
+        out.update({f"c{c}_x": X, f"c{c}_y": Y, f"c{c}_fate": t["fate"], f"c{c}_I": t["I"],
+                    f"c{c}_scene": scene_bytes(R.scene), f"c{c}_frame": scene_bytes(f), f"c{c}_disk": R.disk})
+        # the K2 and blackbody tables do not depend on the spin: stored once
+        assert k2 is None or (np.array_equal(k2, R.k2) and np.array_equal(bb, R.bb))
+        k2, bb = R.k2, R.bb
+    np.savez_compressed(os.path.join(HERE, "emission_rays.npz"), k2=k2, bb=bb, **out)
+
+
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
+        emission_fixture()
     for name in sys.argv[1:]:
-        {"noise": noise_fixture, "sweep": sweep_fixture}[name]()
+        {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture}[name]()

@@ -243,3 +243,25 @@ def test_spin_inclination_sweep_vs_reference(orc):
             assert esc.any() and (g["fate"] == -1).any()
         n += 1
     assert n == 8
+
+
+def test_emission_at_other_spins_vs_reference(orc):
+    """golden/emission_rays.npz: the thin disk at (a, i) = (0.5, 30 deg) and (0.998, 85 deg), and
+    the reference hot flow (turbulence off) at (0.3, 40 deg) and (0.9999, 100 deg), 24 x 24 pixel
+    centres each, traced by the reference's trace_ray with its own scene and tables for that spin.
+    Fates exact; the float colour / intensity stages within 1e-5 of the case's maximum per channel
+    group, as for the shipped shots; the flow's total flux within 1e-7."""
+    g = np.load(os.path.join(GOLD, "emission_rays.npz"))
+    for c, (kind, spin, incl) in enumerate(g["cases"]):
+        tabs = dict(disk=g[f"c{c}_disk"], k2=g["k2"], bb=g["bb"])
+        s, keep = with_tables(orc, scene_from_bytes(orc, g[f"c{c}_scene"]), tabs)
+        f = frame_from_bytes(orc, g[f"c{c}_frame"])
+        o = orc.orc_trace(s, f, g[f"c{c}_x"], g[f"c{c}_y"])
+        assert np.array_equal(o["fate"], g[f"c{c}_fate"]), (spin, incl)
+        I0, I1 = o["I"].astype(np.float64), g[f"c{c}_I"].astype(np.float64)
+        assert I1[:, 0].max() > 0, (spin, incl)
+        if kind == 0:
+            assert np.abs(I0 - I1).max() <= 1e-5 * np.abs(I1).max(), (spin, incl)
+        else:
+            assert np.abs(I0 - I1).max() <= 1e-5 * np.abs(I1[:, 0]).max(), (spin, incl)
+            assert abs(I0[:, 0].sum() - I1[:, 0].sum()) <= 1e-7 * I1[:, 0].sum(), (spin, incl)
