@@ -318,4 +318,40 @@ int ref_render_pass1(const void* scene, const void* frame, float* accum, long lo
     return 0;
 }
 
+// k_pass2's per-chunk work (render.cu:196-224) on the host: entry e is `count` samples s0[e] ..
+// s0[e] + count - 1 of pixel pix[e] through sample_pixel's jitter, summed in float in sample order
+// (the reference then adds each chunk sum to its pixel with float atomics).
+int ref_render_chunks(const void* scene, const void* frame, long long n, const long long* pix, const int* s0,
+                      int count, float* out, int nthreads) {
+    std::memcpy(&c_S, scene, sizeof(SceneGPU));
+    std::memcpy(&c_F, frame, sizeof(FrameGPU));
+    const int W = c_F.W;
+    if (nthreads < 1) nthreads = 1;
+    auto work = [&](int t0) {
+        for (long long e = t0; e < n; e += nthreads) {
+            int p = (int)pix[e], px = p % W, py = p / W;
+            uint32_t h;
+            float r0, r1;
+            pixel_seed_h(p, &h, &r0, &r1);
+            SkyGrad g = {make_float2(0, 0), make_float2(0, 0)};
+            float4 a = make_float4(0, 0, 0, 0);
+            for (int i = 0; i < count; ++i) {
+                float jx, jy;
+                r2_sample((uint32_t)(s0[e] + i), r0, r1, &jx, &jy);
+                double tx = (px + jx - 0.5 * c_F.W) * c_F.pix;
+                double ty = (0.5 * c_F.H - (py + jy)) * c_F.pix;
+                int fate;
+                float4 v = trace_ray(tx, ty, g, true, &fate, nullptr);
+                a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
+            }
+            out[4 * e] = a.x; out[4 * e + 1] = a.y; out[4 * e + 2] = a.z; out[4 * e + 3] = a.w;
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nthreads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& t : th) t.join();
+    return 0;
+}
+
 }  // extern "C"

@@ -853,6 +853,75 @@ int orc_render_pass1(const so_scene* S, const so_plasma* pl, const so_mode* mode
     return SO_OK;
 }
 
+/* Pass-2 chunks (render.cu:196-224): entry e is `count` consecutive R2-jittered samples s0[e] ..
+ * s0[e] + count - 1 of pixel pix[e], summed in float in sample order into out[4 e .. 4 e + 3].  The
+ * reference adds such chunk sums to their pixels with float atomics; the CUDA path adds them in
+ * chunk order, which the caller repeats. */
+typedef struct {
+    const Ctx* X;
+    long long n;
+    const long long* pix;
+    const int* s0;
+    int count;
+    float* out;
+    long long* lim;
+    int t0, stride;
+} ChunkJob;
+
+static void* chunk_run(void* p) {
+    ChunkJob* j = (ChunkJob*)p;
+    const so_frame* F = j->X->F;
+    long long lim = 0;
+    for (long long e = j->t0; e < j->n; e += j->stride) {
+        const int pix = (int)j->pix[e];
+        const int px = pix % F->W, py = pix / F->W;
+        uint32_t hs = pcg((uint32_t)pix * 0x9E3779B9u ^ F->seed);
+        float r0 = rnd(&hs), r1 = rnd(&hs);
+        float a[4] = {0, 0, 0, 0};
+        for (int i = 0; i < j->count; ++i) {
+            float jx, jy;
+            r2_sample((uint32_t)(j->s0[e] + i), r0, r1, &jx, &jy);
+            double tx = (px + jx - 0.5 * F->W) * F->pix;
+            double ty = (0.5 * F->H - (py + jy)) * F->pix;
+            RayOut o;
+            trace_ray(j->X, tx, ty, &o);
+            if (o.fate == 0) ++lim;
+            for (int c = 0; c < 4; ++c) a[c] += o.acc[c];
+        }
+        memcpy(j->out + 4 * (size_t)e, a, 16);
+    }
+    j->lim[0] = lim;
+    return NULL;
+}
+
+int orc_render_chunks(const so_scene* S, const so_plasma* pl, const so_mode* modes, const so_frame* F, long long n,
+                      const long long* pix, const int* s0, int count, float* out, long long* step_limited,
+                      int nthreads) {
+    if (!S || !F || n < 0 || (n > 0 && (!pix || !s0 || !out)) || count <= 0 || F->W <= 0 || F->H <= 0)
+        return SO_ERR_ARG;
+    for (long long e = 0; e < n; ++e)
+        if (pix[e] < 0 || pix[e] >= (long long)F->W * F->H || s0[e] < 0) return SO_ERR_ARG;
+    Ctx X = {S, F, pl, modes};
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    ChunkJob jobs[256];
+    long long lim[256];
+    for (int t = 0; t < nthreads; ++t) {
+        ChunkJob j = {&X, n, pix, s0, count, out, &lim[t], t, nthreads};
+        jobs[t] = j;
+    }
+    for (int t = 1; t < nthreads; ++t) pthread_create(&th[t], NULL, chunk_run, &jobs[t]);
+    chunk_run(&jobs[0]);
+    long long L = lim[0];
+    for (int t = 1; t < nthreads; ++t) {
+        pthread_join(th[t], NULL);
+        L += lim[t];
+    }
+    if (step_limited) *step_limited = L;
+    return SO_OK;
+}
+
 /* vacuum_fate, kerr.hpp:234-253 (the controller with so_rpow5, the same fma placement as above). */
 int orc_vacuum_fate(double a, const so_frame* F, so_vec3 d, double tol, double r_escape, int max_steps) {
     RayC c;

@@ -49,6 +49,8 @@ def oracle():
         L.orc_fbm3.restype = None
         L.orc_sheared_noise.argtypes = [P(Scene), C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
         L.orc_sheared_noise.restype = None
+        L.orc_render_chunks.argtypes = [P(Scene), vp, vp, P(Frame), C.c_longlong, vp, vp, C.c_int, vp,
+                                        P(C.c_longlong), C.c_int]
         L.so_rpow5.argtypes = [C.c_double]
         L.so_rpow5.restype = C.c_double
         _orc = L
@@ -85,6 +87,7 @@ def ref():
         L.ref_trace_rays.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, C.c_int]
         L.ref_trace_vacuum.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int]
         L.ref_render_pass1.argtypes = [vp, vp, vp, P(C.c_longlong), C.c_int]
+        L.ref_render_chunks.argtypes = [vp, vp, C.c_longlong, vp, vp, C.c_int, vp, C.c_int]
         L.ref_fbm3.argtypes = [C.c_int, vp, vp, vp, C.c_int, C.c_uint32, vp]
         L.ref_fbm3.restype = None
         L.ref_sheared_noise.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
@@ -134,6 +137,38 @@ def orc_pass1(scene, frame, plasma=None, modes=None, jitter=1, threads=8):
                                    C.byref(att), threads)
     assert rc == 0
     return acc, ys, lim.value, att.value
+
+
+def orc_chunks(scene, frame, pix, s0, count, plasma=None, modes=None, threads=8):
+    """Sums of samples s0 .. s0 + count - 1 of pixels pix (pass-2 chunks), the C oracle's tracer."""
+    pix = np.ascontiguousarray(pix, np.int64)
+    s0 = np.ascontiguousarray(s0, np.int32)
+    out = np.zeros((pix.size, 4), np.float32)
+    lim = C.c_longlong()
+    pl = C.byref(plasma) if plasma is not None else None
+    rc = oracle().orc_render_chunks(C.byref(scene), pl, modes, C.byref(frame), pix.size, _p(pix), _p(s0), count,
+                                    _p(out), C.byref(lim), threads)
+    assert rc == 0
+    return out
+
+
+def orc_render_adaptive(scene, frame, spp_max, target, plasma=None, modes=None, threads=8):
+    """The whole adaptive frame (pass 1, k_adapt, k_dilate, scan, pass 2, resolve) on the oracle:
+    (image [H, W, 4], nsamp [H, W], chunks [H, W])."""
+    acc, ys, _, _ = orc_pass1(scene, frame, plasma, modes, 1, threads)
+    fr = frame_driver()
+    return fr.render_adaptive(acc, ys, frame.spp, spp_max, target,
+                              lambda p, s, c: orc_chunks(scene, frame, p, s, c, plasma, modes, threads),
+                              visible=scene.mode == abi.SO_MODE_VISIBLE)
+
+
+def ref_chunks(scene, frame, pix, s0, count, threads=8):
+    """The same chunk sums through the reference's own sample_pixel / trace_ray (ref_shim.cpp)."""
+    pix = np.ascontiguousarray(pix, np.int64)
+    s0 = np.ascontiguousarray(s0, np.int32)
+    out = np.zeros((pix.size, 4), np.float32)
+    ref().ref_render_chunks(C.byref(scene), C.byref(frame), pix.size, _p(pix), _p(s0), count, _p(out), threads)
+    return out
 
 
 class RefShot:
@@ -232,6 +267,11 @@ def _module(name, fname):
 def mlp():
     """oracle/so_mlp.py: the float64 restatement of the ray surrogate network."""
     return _module("so_mlp_oracle", "so_mlp.py")
+
+
+def frame_driver():
+    """oracle/so_frame.py: adaptive resampling and resolve around the tracer."""
+    return _module("so_frame_oracle", "so_frame.py")
 
 
 def post():

@@ -192,11 +192,28 @@ def emission_fixture():
     np.savez_compressed(os.path.join(HERE, "emission_rays.npz"), k2=k2, bb=bb, **out)
 
 
+def chunks_fixture():
+    """10. Pass-2 chunk sums (k_pass2, render.cu:196-224) through the reference's own sample_pixel
+    jitter and trace_ray: the reference hot flow (turbulence off) at 48 x 32, spp 2; the first
+    chunk (samples 2 .. 9) of every pixel and the fourth chunk (samples 26 .. 33) of every 7th."""
+    ov = ["camera.width=48", "camera.height=32", "render.spp=2", "render.spp_max=34", "flow.turbulence=0"]
+    R = O.RefShot(os.path.join(SHOTS, "m87_reference_flow.ini"), ov)
+    f = R.frame(0)
+    n = 48 * 32
+    pix = np.concatenate([np.arange(n), np.arange(0, n, 7)]).astype(np.int64)
+    s0 = np.concatenate([np.full(n, 2), np.full(len(range(0, n, 7)), 2 + 3 * 8)]).astype(np.int32)
+    sums = O.ref_chunks(R.scene, f, pix, s0, 8)
+    np.savez_compressed(os.path.join(HERE, "chunk_rays.npz"), scene=scene_bytes(R.scene), frame=scene_bytes(f),
+                        pix=pix, s0=s0, count=np.int32(8), sums=sums)
+
+
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
         emission_fixture()
+        chunks_fixture()
     for name in sys.argv[1:]:
-        {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture}[name]()
+        {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture,
+         "chunks": chunks_fixture}[name]()

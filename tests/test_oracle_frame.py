@@ -1,0 +1,107 @@
+"""The oracle of the frame driver (oracle/so_frame.py with the C oracle's chunk sampler) on CPU.
+
+Pass 2 draws its samples through the same pixel seed and R2 sequence as pass 1, continued at sample
+index spp + 8 k for chunk k (render.cu:196-224).  The chunk sums are pinned against the reference's
+own sample_pixel / trace_ray (golden/chunk_rays.npz); the per-pixel arithmetic of k_adapt,
+k_dilate, the scan and k_resolve is checked against its definition in FP64 and by its invariants.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FLOW = ["camera.width=48", "camera.height=32", "render.spp=2", "render.spp_max=34", "render.target_error=0.02",
+        "flow.turbulence=0"]
+
+
+def _shot(so, over=FLOW):
+    sh = so.Shot("m87_reference_flow.ini", over)
+    return sh, sh.frame(0)
+
+
+def test_pass2_chunks_vs_reference(orc):
+    """Chunk sums of samples 2 .. 9 of every pixel and 26 .. 33 of every 7th pixel of the reference
+    hot flow (turbulence off): the oracle against the reference's own sampler and tracer, within
+    1e-5 of the maximum (float accumulation of FP64 stages; the flow bar of the shipped shots)."""
+    g = np.load(os.path.join(GOLD, "chunk_rays.npz"))
+    s, f = orc.Scene(), orc.Frame()
+    C.memmove(C.byref(s), g["scene"].tobytes(), C.sizeof(s))
+    C.memmove(C.byref(f), g["frame"].tobytes(), C.sizeof(f))
+    tabs = np.load(os.path.join(GOLD, "build_m87_reference_flow.npz"))
+    keep = [np.ascontiguousarray(tabs[k], np.float32) for k in ("disk", "k2", "bb")]
+    P = C.POINTER(C.c_float)
+    s.disk_lnT, s.k2_lntab, s.bb_xyz = (k.ctypes.data_as(P) for k in keep)
+    o = orc.orc_chunks(s, f, g["pix"], g["s0"], int(g["count"]))
+    ref = g["sums"]
+    assert ref[:, 0].max() > 0 and (g["s0"] > 2).any()
+    assert np.abs(o - ref).max() <= 1e-5 * np.abs(ref[:, 0]).max()
+    assert (o == ref).all(axis=1).mean() > 0.85
+
+
+def test_chunk_sampler_continues_pass1(so, orc):
+    """Samples 0 .. spp - 1 through the chunk sampler are pass 1's samples, bit for bit."""
+    sh, f = _shot(so)
+    acc, ys, _, _ = orc.orc_pass1(sh.scene, f)
+    n = f.W * f.H
+    c = orc.orc_chunks(sh.scene, f, np.arange(n), np.zeros(n, np.int32), f.spp)
+    assert np.array_equal(c.reshape(acc.shape), acc)
+
+
+def test_adapt_and_dilate_definitions(so, orc):
+    """k_adapt against its formula in FP64 (the float result may sit one sample off where the want
+    is within float rounding of an integer), k_dilate as the 3x3 maximum in whole chunks."""
+    fr = orc.frame_driver()
+    sh, f = _shot(so)
+    _, ys, _, _ = orc.orc_pass1(sh.scene, f)
+    npix, spp, tgt, emax = f.W * f.H, f.spp, float(sh.settings.target_err), sh.settings.spp_max - f.spp
+    fsum = float(ys[..., 0].astype(np.float64).sum())
+    extra = fr.adapt(ys, spp, fsum, npix, tgt, emax)
+    yref = 0.03 * fsum / (npix * spp)
+    m = ys[..., 0].astype(np.float64) / spp
+    var = np.maximum(ys[..., 1].astype(np.float64) / spp - m * m, 0.0)
+    want = spp * (np.sqrt(var / spp) / (tgt * (m + yref))) ** 2
+    exact = np.clip(np.ceil(want) - spp, 0, emax)
+    assert np.abs(extra.astype(np.int64) - exact).max() <= 1
+    assert (extra.astype(np.int64) == exact).mean() > 0.99
+    assert 0 < extra.max() <= emax and (extra == 0).any()
+    ch = fr.dilate(extra, emax)
+    H, W = extra.shape
+    for y, x in [(0, 0), (H - 1, W - 1), (H // 2, W // 3), (5, W - 1)]:
+        nb = extra[max(y - 1, 0):y + 2, max(x - 1, 0):x + 2].max()
+        assert ch[y, x] == (min(nb, emax) + 7) // 8
+    assert (ch * 8 >= np.minimum(extra, emax)).all()
+
+
+def test_adaptive_frame_invariants(so, orc):
+    """The adaptive frame: samples per pixel = spp + 8 chunks, bounded by spp_max rounded up to a
+    chunk; pixels without chunks keep their pass-1 mean; the frame is deterministic; with
+    spp_max = spp there is no pass 2."""
+    fr = orc.frame_driver()
+    sh, f = _shot(so)
+    img, nsamp, chunks = orc.orc_render_adaptive(sh.scene, f, sh.settings.spp_max, sh.settings.target_err)
+    assert np.array_equal(nsamp, f.spp + 8 * chunks)
+    assert nsamp.max() <= f.spp + 8 * ((sh.settings.spp_max - f.spp + 7) // 8)
+    assert (chunks > 0).any() and (chunks == 0).any()
+    acc, _, _, _ = orc.orc_pass1(sh.scene, f)
+    still = chunks == 0
+    assert np.array_equal(img[still], fr.resolve(acc, np.full(chunks.shape, f.spp, np.uint32))[still])
+    img2, nsamp2, _ = orc.orc_render_adaptive(sh.scene, f, sh.settings.spp_max, sh.settings.target_err)
+    assert np.array_equal(img, img2) and np.array_equal(nsamp, nsamp2)
+    img1, nsamp1, ch1 = orc.orc_render_adaptive(sh.scene, f, f.spp, sh.settings.target_err)
+    assert (ch1 == 0).all() and np.array_equal(img1, fr.resolve(acc, nsamp1))
+    # the extra samples estimate the same pixel means: the frame's total moves by well under 10 %
+    tot1, tot = float(img1[..., 0].sum()), float(img[..., 0].sum())
+    assert abs(tot - tot1) < 0.1 * tot1
+
+
+def test_resolve_visible_matrix(orc):
+    """k_resolve in visible mode: XYZ mean -> linear sRGB (D65) x 683, order channel x 683."""
+    fr = orc.frame_driver()
+    acc = np.array([[[2.0, 4.0, 6.0, 8.0]]], np.float32)
+    out = fr.resolve(acc, np.array([[2]], np.uint32), visible=True)[0, 0].astype(np.float64)
+    X, Y, Z = 1.0, 2.0, 3.0
+    want = 683 * np.array([3.2404542 * X - 1.5371385 * Y - 0.4985314 * Z,
+                           -0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z,
+                           0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z, 4.0])
+    assert np.allclose(out, want, rtol=1e-6)
