@@ -92,6 +92,10 @@ def ref():
         L.ref_fbm3.restype = None
         L.ref_sheared_noise.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
         L.ref_sheared_noise.restype = None
+        L.ref_post_bloom.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float]
+        L.ref_post_bloom.restype = None
+        L.ref_post_radio_blur.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double]
+        L.ref_post_radio_blur.restype = None
         _ref = L
     return _ref
 
@@ -168,6 +172,20 @@ def ref_chunks(scene, frame, pix, s0, count, threads=8):
     s0 = np.ascontiguousarray(s0, np.int32)
     out = np.zeros((pix.size, 4), np.float32)
     ref().ref_render_chunks(C.byref(scene), C.byref(frame), pix.size, _p(pix), _p(s0), count, _p(out), threads)
+    return out
+
+
+def ref_post(img, bloom=None, sigma=None):
+    """The reference's own pyramid filters (render.cu:244-316, run host-side by
+    oracle/ref_post_shim.cpp) on a float32 frame [H, W, 4]: Impl::bloom with strength `bloom`, or
+    Impl::radio_blur with a beam of `sigma` pixels."""
+    img = np.ascontiguousarray(img, np.float32)
+    H, W = img.shape[:2]
+    out = np.zeros_like(img)
+    if bloom is not None:
+        ref().ref_post_bloom(_p(img), _p(out), W, H, bloom)
+    else:
+        ref().ref_post_radio_blur(_p(img), _p(out), W, H, sigma)
     return out
 
 

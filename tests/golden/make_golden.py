@@ -207,13 +207,35 @@ def chunks_fixture():
                         pix=pix, s0=s0, count=np.int32(8), sums=sums)
 
 
+def post_fixture():
+    """11. The post filters (render.cu:244-316 through Impl::bloom :732-740 and Impl::radio_blur
+    :742-753) run by the reference's own kernels, compiled for the host by oracle/ref_post_shim.cpp:
+    a 41 x 29 frame of peaky random values (bloom at strengths 0.35 and 1, beams of 0.8, 4 and 7.5
+    pixels: pyramid levels 0 and 1) and a 64 x 48 frame of a few bright points on a faint floor
+    (beams of 13 and 30 pixels: levels 2 and 3, then k_upsample)."""
+    rng = np.random.default_rng(11)
+    a = (rng.random((29, 41, 4)) ** 6).astype(np.float32)
+    b = np.full((48, 64, 4), 1e-3, np.float32)
+    for _ in range(6):
+        b[rng.integers(48), rng.integers(64)] += rng.random(4).astype(np.float32) * 50
+    out = {"a": a, "b": b}
+    for st in (0.35, 1.0):
+        out[f"a_bloom_{st}"] = O.ref_post(a, bloom=st)
+    for sg in (0.8, 4.0, 7.5):
+        out[f"a_blur_{sg}"] = O.ref_post(a, sigma=sg)
+    for sg in (13.0, 30.0):
+        out[f"b_blur_{sg}"] = O.ref_post(b, sigma=sg)
+    np.savez_compressed(os.path.join(HERE, "post_filters.npz"), **out)
+
+
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
         emission_fixture()
         chunks_fixture()
+        post_fixture()
     for name in sys.argv[1:]:
         {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture,
-         "chunks": chunks_fixture}[name]()
+         "chunks": chunks_fixture, "post": post_fixture}[name]()
