@@ -7,6 +7,9 @@
 //   __expf(x)  -> expf(x)                  (emission.cuh:55, 71)
 //   rsqrtf(x)  -> 1.0f / sqrtf(x)          (emission.cuh:50)
 //   tex3D / tex2DGrad -> zero stubs        (baked turbulence and sky: not used by the configs here)
+// render.cu's turbulence bake k_bake_turb (render.cu:448-461) is cut out by line range into
+// _ref/bake_kernel.inc by oracle/Makefile and compiled at the end of this file with its launch grid
+// walked on the host and surf3Dwrite writing one z layer into a host array.
 // The reference's own host builders (scene_build.cpp, shot.cpp, config.cpp, colour.cpp) are
 // compiled unchanged by oracle/Makefile and linked in.  sample_pixel / pixel_seed of render.cu:70-85
 // are restated here (render.cu itself needs the CUDA toolchain and the font atlas), calling the
@@ -355,3 +358,42 @@ int ref_render_chunks(const void* scene, const void* frame, long long n, const l
 }
 
 }  // extern "C"
+
+// k_bake_turb (render.cu:448-461) on the host.  The bake's surface is stood in for by a Layer: the
+// texel row x (bytes / 4), y of z layer l go to out[y * TURB_NPHI + x]; other layers are dropped.
+namespace refbake {
+struct Idx3 {
+    unsigned x, y, z;
+};
+thread_local Idx3 blockIdx, threadIdx, blockDim;
+struct Layer {
+    float* out;
+    int l;
+};
+inline void surf3Dwrite(float v, cudaSurfaceObject_t s, int xbytes, int y, int z) {
+    Layer* L = reinterpret_cast<Layer*>(s);
+    if (z == L->l) L->out[(size_t)y * 512 + xbytes / 4] = v;
+}
+#include "bake_kernel.inc"
+}  // namespace refbake
+
+extern "C" {
+// Layer l of the baked slice with time offset delta (render.cu:680: turb_d0 + k * turb_dd), through
+// the reference's launch shape (16 x 16 blocks, render.cu:679-680): out[j * 512 + i], 192 x 512.
+void ref_bake_turb_layer(const void* scene, const void* frame, float delta, int l, float* out) {
+    using namespace refbake;
+    std::memcpy(&c_S, scene, sizeof(SceneGPU));
+    std::memcpy(&c_F, frame, sizeof(FrameGPU));
+    static_assert(TURB_NPHI == 512, "layer row length");
+    Layer L = {out, l};
+    blockDim = {16u, 16u, 1u};
+    for (unsigned by = 0; by < (TURB_NLR + 15) / 16; ++by)
+        for (unsigned bx = 0; bx < (TURB_NPHI + 15) / 16; ++bx)
+            for (unsigned ty = 0; ty < 16; ++ty)
+                for (unsigned tx = 0; tx < 16; ++tx) {
+                    blockIdx = {bx, by, (unsigned)l};
+                    threadIdx = {tx, ty, 0u};
+                    k_bake_turb(reinterpret_cast<cudaSurfaceObject_t>(&L), delta);
+                }
+}
+}

@@ -420,6 +420,12 @@ static float turb_texel(const Ctx* X, int k, int l, int j, int i) { /* render.cu
     const float a = S->flow_turb_amp;
     return expf(a * n - 0.5f * a * a);
 }
+/* Layer l of baked slice k, texel (j, i) at out[j * 512 + i]: the bake's values, for the tests. */
+void orc_turb_layer(const so_scene* S, const so_frame* F, int k, int l, float* out) {
+    const Ctx X = {S, F, NULL, NULL};
+    for (int j = 0; j < TNLR; ++j)
+        for (int i = 0; i < TNPHI; ++i) out[j * TNPHI + i] = turb_texel(&X, k, l, j, i);
+}
 static float turb_fetch(const Ctx* X, int k, float x, float y, float z) {
     const float xb = (x - floorf(x)) * (float)TNPHI - 0.5f;
     const float yb = fminf(fmaxf(y * (float)TNLR - 0.5f, -1.f), (float)TNLR);

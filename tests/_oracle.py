@@ -51,6 +51,8 @@ def oracle():
         L.orc_sheared_noise.restype = None
         L.orc_render_chunks.argtypes = [P(Scene), vp, vp, P(Frame), C.c_longlong, vp, vp, C.c_int, vp,
                                         P(C.c_longlong), C.c_int]
+        L.orc_turb_layer.argtypes = [P(Scene), P(Frame), C.c_int, C.c_int, vp]
+        L.orc_turb_layer.restype = None
         L.so_rpow5.argtypes = [C.c_double]
         L.so_rpow5.restype = C.c_double
         _orc = L
@@ -92,6 +94,8 @@ def ref():
         L.ref_fbm3.restype = None
         L.ref_sheared_noise.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.c_float, C.c_float, C.c_uint32, vp]
         L.ref_sheared_noise.restype = None
+        L.ref_bake_turb_layer.argtypes = [vp, vp, C.c_float, C.c_int, vp]
+        L.ref_bake_turb_layer.restype = None
         L.ref_post_bloom.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float]
         L.ref_post_bloom.restype = None
         L.ref_post_radio_blur.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double]
@@ -172,6 +176,23 @@ def ref_chunks(scene, frame, pix, s0, count, threads=8):
     s0 = np.ascontiguousarray(s0, np.int32)
     out = np.zeros((pix.size, 4), np.float32)
     ref().ref_render_chunks(C.byref(scene), C.byref(frame), pix.size, _p(pix), _p(s0), count, _p(out), threads)
+    return out
+
+
+def orc_turb_layer(scene, frame, k, l):
+    """Layer l (0 .. 47) of the oracle's baked turbulence slice k (0 .. 23): [192, 512] float32,
+    rows ln R, columns phi.  scene must carry the bake's set-up (baked())."""
+    out = np.zeros((192, 512), np.float32)
+    oracle().orc_turb_layer(C.byref(scene), C.byref(frame), k, l, _p(out))
+    return out
+
+
+def ref_bake_layer(scene, frame, k, l):
+    """The same layer from the reference's own k_bake_turb (render.cu:448-461, run on the host by
+    oracle/ref_shim.cpp) with the slice's time offset turb_d0 + k * turb_dd (render.cu:680)."""
+    delta = np.float32(np.float32(scene.turb_d0) + np.float32(k) * np.float32(scene.turb_dd))
+    out = np.zeros((192, 512), np.float32)
+    ref().ref_bake_turb_layer(C.byref(scene), C.byref(frame), float(delta), l, _p(out))
     return out
 
 

@@ -207,6 +207,19 @@ def chunks_fixture():
                         pix=pix, s0=s0, count=np.int32(8), sums=sums)
 
 
+def turb_fixture():
+    """12. Baked flow turbulence texels (k_bake_turb, render.cu:448-461) from the reference's own
+    kernel run on the host: the reference hot flow's scene with the bake set-up of render.cu:614-619,
+    three (time slice, height layer) pairs, every 4th texel in ln R and in phi."""
+    R = O.RefShot(os.path.join(SHOTS, "m87_reference_flow.ini"), [])
+    f = R.frame(0)
+    sc = O.baked(R.scene)
+    kl = np.array([[0, 24], [23, 3], [11, 47]], np.int32)
+    tex = np.stack([O.ref_bake_layer(sc, f, int(k), int(l))[::4, ::4] for k, l in kl])
+    np.savez_compressed(os.path.join(HERE, "turb_bake.npz"), scene=scene_bytes(sc), frame=scene_bytes(f), kl=kl,
+                        texels=tex)
+
+
 def post_fixture():
     """11. The post filters (render.cu:244-316 through Impl::bloom :732-740 and Impl::radio_blur
     :742-753) run by the reference's own kernels, compiled for the host by oracle/ref_post_shim.cpp:
@@ -229,13 +242,15 @@ def post_fixture():
 
 
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post, turb)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
         emission_fixture()
         chunks_fixture()
         post_fixture()
+        turb_fixture()
     for name in sys.argv[1:]:
         {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture,
-         "chunks": chunks_fixture, "post": post_fixture}[name]()
+         "chunks": chunks_fixture, "post": post_fixture,
+         "turb": turb_fixture}[name]()

@@ -265,3 +265,19 @@ def test_emission_at_other_spins_vs_reference(orc):
         else:
             assert np.abs(I0 - I1).max() <= 1e-5 * np.abs(I1[:, 0]).max(), (spin, incl)
             assert abs(I0[:, 0].sum() - I1[:, 0].sum()) <= 1e-7 * I1[:, 0].sum(), (spin, incl)
+
+
+def test_turbulence_bake_vs_reference(orc):
+    """Baked turbulence texels (render.cu:448-461): the oracle's on-demand texels against the
+    reference's own k_bake_turb at three (time slice, height layer) pairs, every 4th texel.  The
+    reference sums R^2 + z^2 unfused where the oracle fuses it, which moves a float noise value by an
+    ulp now and then: at least 99 % of the texels are bit-identical, all within 1e-5 of the maximum."""
+    g = np.load(os.path.join(GOLD, "turb_bake.npz"))
+    s = scene_from_bytes(orc, g["scene"])
+    f = frame_from_bytes(orc, g["frame"])
+    assert s.turb_nt == 24
+    for (k, l), ref in zip(g["kl"], g["texels"]):
+        o = orc.orc_turb_layer(s, f, int(k), int(l))[::4, ::4]
+        assert ref.min() > 0
+        assert (o == ref).mean() > 0.99
+        assert np.abs(o - ref).max() <= 1e-5 * np.abs(ref).max()
