@@ -1,5 +1,5 @@
-// ref_post_shim.cpp -- host build of the REFERENCE's own pyramid-filter kernels.  TEST INFRASTRUCTURE
-// ONLY.
+// ref_post_shim.cpp -- host build of the REFERENCE's own pyramid-filter kernels and of its k_adapt /
+// k_dilate.  TEST INFRASTRUCTURE ONLY.
 //
 // render.cu as a whole needs nvcc and the font atlas, but its post filters (render.cu:244-316:
 // k_down, bilinear, LevelPtrs, k_bloom, k_gauss, k_upsample) are plain per-pixel code.  oracle/Makefile
@@ -13,11 +13,16 @@
 // The launch sequences are Impl::bloom (render.cu:732-740) and Impl::radio_blur (:742-753) on the
 // pyramid that Renderer::init sizes (:638-647), restated in bloom() / radio_blur() below.
 //
-// Output: linked into oracle/_ref/libbhref.so; tests/test_oracle_post.py pins oracle/so_post.py on it.
+// k_adapt / k_dilate (render.cu:130-150) come the same way from _ref/adapt_kernels.inc.  Host
+// caveat: g++ (no -mfma, no contraction) evaluates k_adapt's s.y / n - mean * mean in two roundings
+// where nvcc fuses it, so a pixel whose estimate sits on an integer may differ by one sample.
+//
+// Output: linked into oracle/_ref/libbhref.so; tests/golden/make_golden.py writes fixtures from it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -33,7 +38,9 @@ struct Idx3 {
 thread_local Idx3 blockIdx, threadIdx, blockDim;
 
 constexpr int MAX_LEVELS = 9;  // render.cu:32
+constexpr int CHUNK = 8;       // render.cu:30
 
+#include "adapt_kernels.inc"
 #include "post_kernels.inc"
 
 // grid2(w, h) with 16 x 16 blocks (render.cu's launch shape for every filter kernel): every thread
@@ -91,6 +98,18 @@ void bloom(const float* img, float* out, int W, int H, float strength) {
     std::memcpy(out, d, sizeof(float4) * (size_t)W * H);
 }
 
+// A 1-D launch of 256-thread blocks over n items (render.cu:703).
+template <class K>
+void launch1(int n, K kernel) {
+    blockDim = {256u, 1u, 1u};
+    for (int b = 0; b < (n + 255) / 256; ++b)
+        for (int t = 0; t < 256; ++t) {
+            blockIdx = {(unsigned)b, 0u, 0u};
+            threadIdx = {(unsigned)t, 0u, 0u};
+            kernel();
+        }
+}
+
 void radio_blur(const float* img, float* out, int W, int H, double sigma) {
     Pyramid P(img, W, H);
     int k = 0;
@@ -115,6 +134,16 @@ extern "C" {
 // Impl::bloom on a W x H float4 frame (row-major, 4 floats per pixel); in and out may not overlap.
 void ref_post_bloom(const float* img, float* out, int W, int H, float strength) {
     refpost::bloom(img, out, W, H, strength);
+}
+// k_adapt then k_dilate on a W x H frame (render.cu:702-704): ystat is W*H float2, nsamp W*H
+// counts; extra and chunks receive W*H counts each.
+void ref_adapt_dilate(const float* ystat, const uint32_t* nsamp, int W, int H, float yref, float target, int extra_max,
+                      uint32_t* extra, uint32_t* chunks) {
+    using namespace refpost;
+    const float2* ys = reinterpret_cast<const float2*>(ystat);
+    const int n = W * H;
+    launch1(n, [&] { k_adapt(ys, nsamp, n, yref, target, extra_max, extra); });
+    launch2(W, H, [&] { k_dilate(extra, chunks, W, H, extra_max); });
 }
 // Impl::radio_blur with a beam of sigma pixels.
 void ref_post_radio_blur(const float* img, float* out, int W, int H, double sigma) {

@@ -96,6 +96,8 @@ def ref():
         L.ref_sheared_noise.restype = None
         L.ref_bake_turb_layer.argtypes = [vp, vp, C.c_float, C.c_int, vp]
         L.ref_bake_turb_layer.restype = None
+        L.ref_adapt_dilate.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, vp, vp]
+        L.ref_adapt_dilate.restype = None
         L.ref_post_bloom.argtypes = [vp, vp, C.c_int, C.c_int, C.c_float]
         L.ref_post_bloom.restype = None
         L.ref_post_radio_blur.argtypes = [vp, vp, C.c_int, C.c_int, C.c_double]
@@ -194,6 +196,18 @@ def ref_bake_layer(scene, frame, k, l):
     out = np.zeros((192, 512), np.float32)
     ref().ref_bake_turb_layer(C.byref(scene), C.byref(frame), float(delta), l, _p(out))
     return out
+
+
+def ref_adapt_dilate(ystat, nsamp, yref, target, extra_max):
+    """The reference's own k_adapt and k_dilate (render.cu:130-150, run on the host by
+    oracle/ref_post_shim.cpp) on ystat [H, W, 2] float32 and nsamp [H, W]: (extra, chunks)."""
+    ystat = np.ascontiguousarray(ystat, np.float32)
+    nsamp = np.ascontiguousarray(nsamp, np.uint32)
+    H, W = ystat.shape[:2]
+    extra = np.zeros((H, W), np.uint32)
+    chunks = np.zeros((H, W), np.uint32)
+    ref().ref_adapt_dilate(_p(ystat), _p(nsamp), W, H, yref, target, extra_max, _p(extra), _p(chunks))
+    return extra, chunks
 
 
 def ref_post(img, bloom=None, sigma=None):

@@ -220,6 +220,26 @@ def turb_fixture():
                         texels=tex)
 
 
+def adapt_fixture():
+    """13. k_adapt and k_dilate (render.cu:130-150) from the reference's own kernels run on the host,
+    on seeded luminance statistics of a 48 x 32 frame at spp 2 (log-normal samples whose spread grows
+    from 0 to 0.15 across the frame, so the extra counts run from 0 to the cap; a block of empty
+    pixels), yref as Impl::trace forms it (render.cu:702), target 0.02, extra_max 32."""
+    rng = np.random.default_rng(13)
+    H, W, spp = 32, 48, 2
+    yy, xx = np.mgrid[0:H, 0:W]
+    mu = np.sin(xx / 7.0) + 0.5 * np.cos(yy / 5.0)
+    sig = (0.15 * xx / (W - 1))[..., None]
+    Y = np.exp(mu[..., None] + sig * rng.normal(0.0, 1.0, (H, W, spp))).astype(np.float32)
+    Y[4:9, 30:40] = 0
+    ys = np.stack([Y.sum(-1, dtype=np.float32), (Y * Y).sum(-1, dtype=np.float32)], -1).astype(np.float32)
+    fsum = float(ys[..., 0].astype(np.float64).sum())
+    yref = np.float32(0.03 * fsum / (float(H * W) * spp) + 1e-37)
+    extra, chunks = O.ref_adapt_dilate(ys, np.full((H, W), spp, np.uint32), float(yref), 0.02, 32)
+    np.savez_compressed(os.path.join(HERE, "adapt.npz"), ystat=ys, spp=np.int32(spp), fsum=np.float64(fsum),
+                        target=np.float32(0.02), extra_max=np.int32(32), extra=extra, chunks=chunks)
+
+
 def post_fixture():
     """11. The post filters (render.cu:244-316 through Impl::bloom :732-740 and Impl::radio_blur
     :742-753) run by the reference's own kernels, compiled for the host by oracle/ref_post_shim.cpp:
@@ -242,7 +262,7 @@ def post_fixture():
 
 
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post, turb)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post, turb, adapt)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
@@ -250,7 +270,8 @@ if __name__ == "__main__":
         chunks_fixture()
         post_fixture()
         turb_fixture()
+        adapt_fixture()
     for name in sys.argv[1:]:
         {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture,
          "chunks": chunks_fixture, "post": post_fixture,
-         "turb": turb_fixture}[name]()
+         "turb": turb_fixture, "adapt": adapt_fixture}[name]()

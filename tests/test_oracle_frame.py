@@ -105,3 +105,23 @@ def test_resolve_visible_matrix(orc):
                            -0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z,
                            0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z, 4.0])
     assert np.allclose(out, want, rtol=1e-6)
+
+
+def test_adapt_dilate_vs_reference_kernels(orc):
+    """k_adapt and k_dilate against the reference's own kernels run on the host (golden fixture):
+    extra counts from 0 to the cap, chunk counts 0 .. 4.  The reference's host build rounds
+    s.y / n - mean * mean twice where the GPU fuses it, so an extra count may differ by one at a tie;
+    at least 99 % agree exactly and all within one.  k_dilate of the reference's extra counts is
+    bit-exact."""
+    fr = orc.frame_driver()
+    g = np.load(os.path.join(GOLD, "adapt.npz"))
+    ys = g["ystat"]
+    H, W = ys.shape[:2]
+    emax = int(g["extra_max"])
+    e = fr.adapt(ys, int(g["spp"]), float(g["fsum"]), H * W, float(g["target"]), emax)
+    ref = g["extra"].astype(np.int64)
+    assert ref.min() == 0 and ref.max() == emax
+    assert (e == ref).mean() >= 0.99
+    assert np.abs(e.astype(np.int64) - ref).max() <= 1
+    ch = fr.dilate(g["extra"], emax)
+    assert np.array_equal(ch, g["chunks"]) and set(np.unique(ch)) == {0, 1, 2, 3, 4}
