@@ -285,12 +285,16 @@ int so_render_device(so_renderer* r, const so_frame* f, float* d_px, so_stats* s
  * a radio scene whose table pointers are device pointers), d_frame (device so_frame built for width
  * n), plasma (host; NULL = the reference flow model) with its device modes d_modes, and d_jy (device
  * double that receives the flux density in Jy).  The n x n frame is traced at 2 samples per pixel,
- * as so_radio_flux does, asynchronously on `stream` (a cudaStream_t; NULL = default stream).
+ * with so_radio_flux's kernels in its order, asynchronously on `stream` (a cudaStream_t; NULL =
+ * default stream).  A turbulent reference-model flow (plasma NULL, flow turbulence on) evaluates the
+ * sheared noise at every flow step: the result equals so_radio_flux's on a renderer switched to
+ * SO_FLOW_NOISE_INLINE, and differs from its default baked slices (another draw of the turbulence).
  * Working memory is a fixed device array of the library, SO_NOALLOC_MAX_PIXELS float4 plus 5.4 KB,
  * held by every GPU that loads the library until the process exits: n*n above SO_NOALLOC_MAX_PIXELS
  * returns SO_ERR_SIZE (message in so_last_error(NULL)).  The first call on a device looks the array
- * up (cudaGetSymbolAddress) with that device current; make it before any stream capture.  All calls
- * share the array, so calls that overlap on the GPU race: order them on one stream. */
+ * up (cudaGetSymbolAddress) with that device current; make it before any stream capture, and do not
+ * reset the device (cudaDeviceReset) between calls.  All calls share the array, so calls that overlap
+ * on the GPU race: order them on one stream. */
 #define SO_NOALLOC_MAX_PIXELS 65536
 int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_frame, int n, double pix_sr,
                           const so_plasma* plasma, const so_mode* d_modes, double* d_jy, void* stream);

@@ -19,9 +19,11 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 }
 
-// img = accum / nsamp; visible mode converts XYZ to linear sRGB x 683 (render.cu:227-242).
-__global__ void k_resolve(float4* __restrict__ img, const float4* __restrict__ accum,
-                          const uint32_t* __restrict__ nsamp, uint32_t nconst, long long npix, int visible) {
+// img = accum / nsamp; visible mode converts XYZ to linear sRGB x 683 (render.cu:227-242).  img may be
+// accum itself (the batch and the fixed-scratch flux resolve in place), so that pair is not
+// __restrict__; each thread reads its pixel before it writes it.
+__global__ void k_resolve(float4* img, const float4* accum, const uint32_t* __restrict__ nsamp, uint32_t nconst,
+                          long long npix, int visible) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npix) return;
     float inv = 1.f / (float)(nsamp ? nsamp[p] : nconst);
@@ -246,11 +248,11 @@ cudaError_t launch_resolve(float4* img, const float4* accum, const uint32_t* nsa
     return cudaGetLastError();
 }
 
-// part must hold 592 doubles; result in *out.
+// part must hold SUM_MAX_PARTIALS doubles; result in *out.
 cudaError_t launch_sum_channel(const float* v, int stride, long long n, double* part, double* out, int num_sms,
                                cudaStream_t st) {
     int nb = num_sms * 4;
-    if (nb > 592) nb = 592;
+    if (nb > SUM_MAX_PARTIALS) nb = SUM_MAX_PARTIALS;
     long long need = (n + 255) / 256;
     if (need < nb) nb = (int)(need > 0 ? need : 1);
     k_sum_channel<<<nb, 256, 0, st>>>(v, stride, n, part);

@@ -33,6 +33,8 @@ struct TurbBake {
     float delta[TURB_NT];  // retarded-time offset of each slice, d0 + k dd (host float, as render.cu:681)
 };
 constexpr int NLISTS = 12;
+// Block partials of launch_sum_channel: at most this many doubles in its `part` buffer.
+constexpr int SUM_MAX_PARTIALS = 592;
 
 struct Counters {
     unsigned long long next;          // ray-queue head

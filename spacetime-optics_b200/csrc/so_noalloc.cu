@@ -8,6 +8,15 @@
 // modes and a device double for the result, all in memory it already owns, and the working memory
 // (per-pixel sums, reduction partials, ray-queue counters) comes from the fixed array below, which
 // exists from the moment the library is loaded on a GPU.
+//
+// A turbulent reference-model flow is traced with the sheared noise evaluated at every flow step (the
+// reference's turb_nt = 0 path): the renderer's default, 24 baked slices of 453 MB, cannot live in a
+// fixed array.  Its flux therefore equals so_radio_flux's once that renderer has been switched to
+// SO_FLOW_NOISE_INLINE; with the baked slices the two are different draws of the turbulence.
+//
+// The device address of the array is looked up once per device ordinal and kept for the life of the
+// process.  cudaDeviceReset (or anything else that unloads the library's module from a device)
+// between calls is not supported: the module may come back at another address.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -29,11 +38,14 @@ void set_global_error(const std::string& msg);
 namespace {
 
 // Layout of the scratch array: [0, 256) counters and the frame's scene index (cleared every call),
-// [256, 256 + 5120) reduction partials and the flux sum, then one float4 per pixel.
+// [256, 256 + 5120) the reduction partials (SUM_MAX_PARTIALS doubles) and the flux sum after them,
+// then one float4 per pixel.
 constexpr size_t OFF_COUNTERS = 0;
 constexpr size_t OFF_PARTIALS = 256;
+constexpr size_t OFF_SUM = OFF_PARTIALS + (size_t)so::SUM_MAX_PARTIALS * sizeof(double);
 constexpr size_t OFF_ACCUM = 256 + 5120;
 static_assert(sizeof(so::Counters) + sizeof(int) <= 256, "counters and scene index must fit the cleared header");
+static_assert(OFF_SUM + sizeof(double) <= OFF_ACCUM, "partials and the flux sum must fit before the pixels");
 constexpr size_t SCRATCH_BYTES = OFF_ACCUM + (size_t)SO_NOALLOC_MAX_PIXELS * 16;
 
 // Held by every GPU that loads the library, until the process exits.
@@ -99,7 +111,7 @@ extern "C" int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_
     Counters* cnt = reinterpret_cast<Counters*>(ds.base + OFF_COUNTERS);
     int* frame_scene = reinterpret_cast<int*>(ds.base + OFF_COUNTERS + sizeof(Counters));
     double* partials = reinterpret_cast<double*>(ds.base + OFF_PARTIALS);
-    double* sum = partials + 600;
+    double* sum = reinterpret_cast<double*>(ds.base + OFF_SUM);
     float4* accum = reinterpret_cast<float4*>(ds.base + OFF_ACCUM);
     // The array keeps the previous call's contents: clear the queue head, counters and scene index.
     cudaError_t e = cudaMemsetAsync(ds.base + OFF_COUNTERS, 0, 256, st);
@@ -130,7 +142,7 @@ extern "C" int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_
         }
         e = launch_trace64(L, VAR_RADIO, ds.num_sms, st);
     }
-    if (e == cudaSuccess) e = launch_resolve(accum, accum, nullptr, 2u, (long long)n * n, 0, st);
+    if (e == cudaSuccess) e = launch_resolve(accum, accum, nullptr, 2u, (long long)n * n, 0, st);  // in place
     if (e == cudaSuccess)
         e = launch_sum_channel(reinterpret_cast<const float*>(accum), 4, (long long)n * n, partials, sum, ds.num_sms, st);
     if (e == cudaSuccess) {
