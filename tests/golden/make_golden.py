@@ -220,6 +220,85 @@ def turb_fixture():
                         texels=tex)
 
 
+def shadow_grid_fixture():
+    """14. The whole 256^2 pixel-centre grid of the shadow self-test shot (a = 0.94, i = 17 deg,
+    r_obs = 1000 M, tolerance 1e-10): all 65,536 rays traced by the reference's trace_ray.  Escape
+    directions are stored for the escaping rays only (in grid order), the integers for every ray.
+    Near the critical curve a ray's escape direction amplifies any difference in its step sequence
+    by orders of magnitude.  Each escaping ray therefore also carries its sensitivity S (float32): the
+    relative change of the reference's escape direction per relative change of the ray's image-plane
+    position, by a finite difference of 1e-12 in x and in y (the largest over x, y and theta, phi)."""
+    R = O.RefShot(os.path.join(SHOTS, "shadow_selftest_256.ini"))
+    f = R.frame(0)
+    X, Y = so.pixel_centres(f, 256, 256)
+    v = O.ref_vacuum(R.scene, f, X, Y)
+    esc = v["fate"] == 1
+    eps = 1e-12
+    sens = np.zeros(int(esc.sum()))
+    for sx, sy in ((1, 0), (0, 1)):
+        p = O.ref_vacuum(R.scene, f, X[esc] * (1 + sx * eps), Y[esc] * (1 + sy * eps))
+        for k in ("theta", "phi"):
+            d = np.abs(p[k] - v[k][esc]) / np.abs(v[k][esc]) / eps
+            d[p["fate"] != 1] = np.inf
+            sens = np.maximum(sens, d)
+    np.savez_compressed(os.path.join(HERE, "shadow_grid_256.npz"), fate=v["fate"], ncross=v["ncross"],
+                        theta_esc=v["theta"][esc], phi_esc=v["phi"][esc], n_accepted=v["n_accepted"],
+                        n_attempts=v["n_attempts"], dir_sensitivity=sens.astype(np.float32))
+
+
+# An animated shot exercising every camera track the builders support: log-space tracks (r, zoom),
+# linear tracks (inclination, roll, yaw, pitch, zoom target, time), an orbiting camera with a boost,
+# offsets and the critical-curve zoom target at 40 deg, in visible mode at spin 0.7.
+ANIM_INI = """[shot]
+name = anim
+duration = 2
+fps = 3
+[bh]
+spin = 0.7
+[render]
+mode = visible
+[camera]
+r = 500
+incl = 35
+phi = 10
+roll = 20
+yaw = 1.5
+pitch = -2
+fov_m = 24
+width = 64
+height = 48
+motion = orbit
+target = 1
+offset_x_m = 0.3
+offset_y_m = -0.2
+target_psi_deg = 40
+[track]
+camera.r = 0:500, 1:80, 2:40
+camera.incl = 0:35, 0.7:60, 2:85
+camera.zoom = 0:1, 1:3, 2:50
+camera.roll = 0:20, 2:-40
+camera.yaw = 0:1.5, 1:-1, 2:0.5
+camera.pitch = 0:-2, 2:2
+camera.target = 0:0, 1.5:1
+time.t_m = 0:0, 2:100
+"""
+
+
+def anim_fixture():
+    """15. The animated shot ANIM_INI through the reference's build_scene / build_shot / make_frame:
+    the scene, its tables and info, and every frame (6) of the shot."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "anim.ini")
+        with open(path, "w") as fh:
+            fh.write(ANIM_INI)
+        R = O.RefShot(path)
+        frames = np.stack([scene_bytes(R.frame(i)) for i in range(6)])
+        np.savez_compressed(os.path.join(HERE, "build_anim.npz"), ini=np.array(ANIM_INI), scene=scene_bytes(R.scene),
+                            frames=frames, disk=R.disk, k2=R.k2, bb=R.bb, info=np.array(R.info),
+                            settings=np.array(R.settings[:4], np.int64))
+
+
 def adapt_fixture():
     """13. k_adapt and k_dilate (render.cu:130-150) from the reference's own kernels run on the host,
     on seeded luminance statistics of a 48 x 32 frame at spp 2 (log-normal samples whose spread grows
@@ -262,7 +341,8 @@ def post_fixture():
 
 
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post, turb, adapt)
+    # no argument: every fixture; otherwise only the named ones (noise, sweep, emission, chunks, post, turb, adapt,
+    # shadow_grid, anim)
     if len(sys.argv) == 1:
         main()
         sweep_fixture()
@@ -271,7 +351,10 @@ if __name__ == "__main__":
         post_fixture()
         turb_fixture()
         adapt_fixture()
+        shadow_grid_fixture()
+        anim_fixture()
     for name in sys.argv[1:]:
         {"noise": noise_fixture, "sweep": sweep_fixture, "emission": emission_fixture,
          "chunks": chunks_fixture, "post": post_fixture,
-         "turb": turb_fixture, "adapt": adapt_fixture}[name]()
+         "turb": turb_fixture, "adapt": adapt_fixture, "shadow_grid": shadow_grid_fixture,
+         "anim": anim_fixture}[name]()

@@ -79,6 +79,19 @@ def test_shadow_rays_vs_reference(orc):
     assert (g["fate"] == -1).any() and (g["fate"] == 1).any() and (g["ncross"] > 1).any()
 
 
+def test_shadow_full_grid_vs_reference(so, orc):
+    """Config shadow_selftest_256 on every pixel of the 256^2 grid (65,536 rays) against the
+    reference's own trace_ray: class and winding order identical on every ray, escape direction
+    within 1e-9 relative except where the reference's own integration error is larger (bar 1e-9 +
+    2 x that error; at most 0.1 % of the escaping rays)."""
+    import _parity
+    s, f, keep = load_build(orc, "shadow_selftest_256")
+    X, Y = so.pixel_centres(f, 256, 256)
+    o = orc.orc_trace(s, f, X, Y)
+    rep = _parity.shadow_grid_vs_reference(o)
+    assert rep["n_accepted_equal"] > 0.999 and rep["escaped"] > 40000 and rep["captured"] > 15000
+
+
 def test_flow_rays_vs_reference(orc):
     """Reference hot-flow model (turbulence off): per-ray I within float-accumulation precision."""
     g = np.load(os.path.join(GOLD, "flow_rays.npz"))
