@@ -69,6 +69,57 @@ def test_shot_builders_match_reference(so, name):
     assert np.array_equal(np.array(info), g["info"])
 
 
+def _assert_frame_equal(so, f, ref_bytes, tag):
+    """Every so_frame field but W, H, spp (which the caller sets) equals the reference frame's."""
+    ref_f = so.abi.Frame()
+    C.memmove(C.byref(ref_f), ref_bytes.tobytes(), C.sizeof(ref_f))
+    for fld, _ in so.abi.Frame._fields_:
+        if fld in ("W", "H", "spp"):
+            continue
+        a, b = getattr(f, fld), getattr(ref_f, fld)
+        assert (bytes(memoryview(a)) == bytes(memoryview(b)) if hasattr(a, "_fields_") else a == b), (tag, fld)
+
+
+def test_animated_shot_matches_reference(so, tmp_path):
+    """golden/build_anim.npz: a 6-frame shot with every camera track (log-space r and zoom, linear
+    inclination, roll, yaw, pitch, zoom target and time), an orbiting camera and the critical-curve
+    zoom target; scene, tables, info and every frame equal the reference's builders bit for bit."""
+    g = np.load(os.path.join(GOLD, "build_anim.npz"))
+    p = tmp_path / "anim.ini"
+    p.write_text(str(g["ini"]))
+    sh = so.Shot(str(p))
+    ref_scene = so.abi.Scene()
+    C.memmove(C.byref(ref_scene), g["scene"].tobytes(), C.sizeof(ref_scene))
+    assert _scene_bytes_no_ptrs(so, sh.scene) == _scene_bytes_no_ptrs(so, ref_scene)
+    n = sh.tables
+    assert np.array_equal(np.ctypeslib.as_array(n.disk_lnT, (n.disk_n,)), g["disk"])
+    assert np.array_equal(np.ctypeslib.as_array(n.k2_ln, (n.k2_n,)), g["k2"])
+    assert np.array_equal(np.ctypeslib.as_array(n.bb_xyz, (3 * n.bb_n,)), g["bb"])
+    assert np.array_equal(np.array([getattr(sh.info, k) for k, _ in so.abi.SceneInfo._fields_]), g["info"])
+    assert sh.nframes() == len(g["frames"]) == 6
+    for i in range(6):
+        _assert_frame_equal(so, sh.frame(i), g["frames"][i], i)
+
+
+def test_emission_scenes_match_reference(so):
+    """golden/emission_rays.npz holds the reference's scene and Novikov-Thorne temperature table for
+    the thin disk at a = 0.5 and 0.998 and the hot flow at a = 0.3 and 0.9999: the package's builders
+    give the same bytes for the same overrides."""
+    g = np.load(os.path.join(GOLD, "emission_rays.npz"))
+    for c, (kind, spin, incl) in enumerate(g["cases"]):
+        shot = "thin_disk_4096.ini" if kind == 0 else "m87_reference_flow.ini"
+        ov = [f"bh.spin={spin}", f"camera.incl={incl}", "camera.width=24", "camera.height=24"]
+        if kind == 1:
+            ov.append("flow.turbulence=0")
+        sh = so.Shot(shot, ov)
+        ref_scene = so.abi.Scene()
+        C.memmove(C.byref(ref_scene), g[f"c{c}_scene"].tobytes(), C.sizeof(ref_scene))
+        assert _scene_bytes_no_ptrs(so, sh.scene) == _scene_bytes_no_ptrs(so, ref_scene), (spin, incl)
+        n = sh.tables
+        assert np.array_equal(np.ctypeslib.as_array(n.disk_lnT, (n.disk_n,)), g[f"c{c}_disk"]), (spin, incl)
+        _assert_frame_equal(so, sh.frame(0), g[f"c{c}_frame"], (spin, incl))
+
+
 def test_overrides_and_tracks(so, tmp_path):
     p = tmp_path / "base.ini"
     p.write_text("[bh]\nspin = 0.5\n[camera]\nr = 100\nincl = 30\nfov_m = 20\nwidth = 8\nheight = 8\n"
