@@ -38,7 +38,8 @@ METRIC = "Mrays/s at ≤1e-3 image error: surrogate/mixed vs plain FP64 kernel, 
 FLOPS_ATTEMPT = 469        # one DP5(4) attempt: 6 RHS (31 each) + stage sums + 5th-order sum + error norm
 FLOPS_ACCEPT = 49          # controller err^-1/5 (34) + projection (11) + psi bookkeeping excluded (radio)
 FLOPS_FLOW = 160           # flow_step without the turbulence sum (transcendentals counted as 20 each)
-FLOPS_MODE = 8 + 20        # one Fourier mode: 3 fma (k.X + phase) + fma accumulate + cos (20)
+FLOPS_MODE = 8 + 22        # one Fourier mode: 3 fma (k.X + phase) + fma accumulate + cos_turns (10 fma, 1 add,
+                           # 1 multiply: 16 FP64 instructions per mode in all)
 # SFU operations of the FP32 tracer (k_trace32): per attempt 7 RHS x 2 reciprocals + 5 error
 # divides + err^-0.2 (2); per flow step ~20 (exp, log, sincos, rsqrt, divides) + one cosine per mode
 SFU_ATTEMPT = 21
@@ -188,32 +189,42 @@ def run_ours(args, so, world, rank, local):
     def set_prec(p):
         r.set_precision(so.abi.SO_PREC_MIXED if p == "mixed" else so.abi.SO_PREC_FP64)
 
-    # plain FP64 reference image (for the image error of the mixed path) and its timing
+    # larger-than-L2 buffer written between steps (the frame's inputs are tiny and stay cached;
+    # flushing keeps each step cold like a fresh frame)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed_frames(n):
+        """n frames, each after an L2 flush, timed by CUDA events on the renderer's stream, with the
+        clocks sampled meanwhile: (ms per frame, clock summary)."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        barrier(world)
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            for i in range(n):
+                with torch.cuda.stream(stream):
+                    flush.fill_(float(i))
+                    ev[i][0].record(stream)
+                r.render_device(f, d_img.data_ptr())
+                with torch.cuda.stream(stream):
+                    ev[i][1].record(stream)
+            torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in ev], clk.summary()
+
+    # The plain FP64 path under the same protocol as the measured path: warm-up, then >= 3 flushed,
+    # event-timed frames with their own clock record; its image is the reference of the image error
     set_prec("fp64")
+    for _ in range(min(max(args.warmup, 3), 5)):
+        r.render_device(f, d_img.data_ptr())
+    ms64, clk64 = timed_frames(max(3, min(args.steps, 5)))
+    ms64_frame = allreduce_max(float(np.mean(ms64)), world)
     st64 = r.render_device(f, d_img.data_ptr(), stats=True)
     img64 = d_img.cpu().numpy().copy()
-    results = {"fp64": {"ms_kernel": st64.ms_kernel, "attempts": st64.attempts, "flow_steps": st64.flow_steps,
-                        "accepted": st64.accepted}}
+    plain = plain_fp64_record(so, sh, st64, ms64, ms64_frame, clk64, npix, world, local)
     set_prec(path)
     for _ in range(args.warmup):
         r.render_device(f, d_img.data_ptr())
     torch.cuda.synchronize()
-    # larger-than-L2 buffer written between steps (the frame's inputs are tiny and stay cached;
-    # flushing keeps each step cold like a fresh frame)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(float(i))
-                ev[i][0].record(stream)
-            r.render_device(f, d_img.data_ptr())
-            with torch.cuda.stream(stream):
-                ev[i][1].record(stream)
-        torch.cuda.synchronize()
-    ms = [a.elapsed_time(b) for a, b in ev]
+    ms, clocks = timed_frames(args.steps)
     ms_step = float(np.mean(ms))
     barrier(world)
     ms_step = allreduce_max(ms_step, world)
@@ -236,7 +247,7 @@ def run_ours(args, so, world, rank, local):
                    "class_mismatch_in_band": int((fm[band] != f64[band]).sum())}
     err_l1 = float(np.abs(img[..., 0] - img64[..., 0]).sum() / max(np.abs(img64[..., 0]).sum(), 1e-300))
     flux_err = float(abs(img[..., 0].astype(np.float64).sum() / img64[..., 0].astype(np.float64).sum() - 1.0))
-    fp64_mrays = npix / (st64.ms_kernel * 1e-3) / 1e6
+    fp64_mrays = plain["mrays_s"]
     # roofline of the dominant kernel: the FP64 tracer (plain path, FP64 pipe) or the FP32 tracer
     # (mixed path, SFU-bound: one cosine per Fourier mode per flow step)
     fp64_peak, fp32_peak = so.probe_fma_peak(local)
@@ -290,7 +301,9 @@ def run_ours(args, so, world, rank, local):
     del host
     # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, [turbulence sums,
     # transfer,] re-trace, gather, resolve (mixed); spp_max = spp, so no adaptive pass
-    gpu_launches = args.steps * ((2 if path == "fp64" else 9 if st.ms_turb > 0 else 7) + (1 if flow else 0))
+    # (plain FP64 with deferred torus sums: recording pass, sums, replay pass, resolve)
+    gpu_launches = args.steps * (((4 if st.rec64_slots else 2) if path == "fp64" else 9 if st.ms_turb > 0 else 7) +
+                                 (1 if flow else 0))
     if flow:
         workload = (f"reference flow {W}x{W} (n ~ r^-1.1, fBm turbulence baked per frame into 24 slices of "
                     f"512x192x48), a=0.94, i=163 deg, fov 30 M, 230 GHz, step fraction 0.01, 1 R2-jittered "
@@ -305,7 +318,8 @@ def run_ours(args, so, world, rank, local):
         "config": {"workload": workload, "path": path,
                    "band_rays": st.band_rays if path == "mixed" else None,
                    "fp64_rays": st.fp64_rays if path == "mixed" else None,
-                   "plain_fp64_mrays_s": round(fp64_mrays, 4), "image_rel_l1_vs_fp64": err_l1,
+                   "plain_fp64_mrays_s": round(fp64_mrays, 4), "speedup_vs_plain_fp64": round(value / fp64_mrays, 3),
+                   "plain_fp64": plain, "image_rel_l1_vs_fp64": err_l1,
                    "total_flux_err_vs_fp64": flux_err, "frames_per_s": round(1e3 / ms_step * world, 4),
                    "l2": "256 MiB buffer written between timed steps", **norm,
                    "attempts_per_ray": st.attempts / npix, "flow_steps_per_ray": st.flow_steps / npix,
@@ -314,12 +328,95 @@ def run_ours(args, so, world, rank, local):
         "e2e": {"value": round(e2e, 4), "unit": "Mrays/s", "h2d_bytes_per_step": C.sizeof(so.abi.Frame),
                 "d2h_bytes_per_step": W * W * 16},
         "gpu_launches": gpu_launches,
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not flow:
         line["cpu_baseline"] = cpu_baseline(so, sh, f, W, budget_s=args.cpu_seconds)
     r.close()
+    if not flow and not args.no_same_scene:
+        line["config"]["same_scene"] = same_scene_record(args, so, world, rank, local)
     return line
+
+
+def plain_fp64_record(so, sh, st, ms, ms_frame, clocks, npix, world, local):
+    """The plain FP64 path's frames: rate, phase times and rooflines against the measured FP64 FMA
+    peak.  With the deferred torus turbulence the frame is recording pass + k_turb64_records +
+    replay pass; the sums kernel is the dominant one, its algorithmic FLOPs are the recorded
+    positions x modes x FLOPS_MODE."""
+    fp64_peak, _ = so.probe_fma_peak(local)
+    pl = sh.plasma()
+    n_modes = pl.n_modes if pl is not None else 0
+    flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT + st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
+    whole = {"kernels": "k_trace64 (recording + replay passes) + k_turb64_records" if st.rec64_slots else "k_trace64",
+             "ms": round(st.ms_kernel, 3), "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
+             "unit": "TFLOP/s", "per_launch": flops}
+    rec = {"bound": "fp64", "kernel": "k_trace64", "achieved": whole["achieved"], "peak": round(fp64_peak, 3),
+           "unit": "TFLOP/s", "kernel_ms": round(st.ms_kernel, 3), "per_launch": flops}
+    if st.rec64_slots:
+        sflops = st.rec64_records * n_modes * FLOPS_MODE
+        rec = {"bound": "fp64", "kernel": "k_turb64_records", "achieved": round(sflops / (st.ms_sum64 * 1e-3) / 1e12, 3),
+               "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel_ms": round(st.ms_sum64, 3), "per_launch": sflops,
+               "records": st.rec64_records, "slots_summed": st.rec64_slots, "jobs_summed_in_tracer": st.rec64_short,
+               "traffic": None, "algorithmic_bytes": 32 * st.rec64_records}
+    rec["frac"] = round(rec["achieved"] / rec["peak"], 4)
+    rec["peak_source"] = "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"
+    return {"mrays_s": round(world * npix / (ms_frame * 1e-3) / 1e6, 4), "ms_per_frame": round(ms_frame, 3),
+            "frames": len(ms), "ms_frames": [round(x, 3) for x in ms], "clocks": clocks,
+            "phases_ms": {"recording_pass": round(st.ms_rec64, 3), "turbulence_sums": round(st.ms_sum64, 3),
+                          "replay_pass": round(st.ms_replay64, 3)},
+            "roofline": rec, "whole_frame": whole}
+
+
+# The reference arm's scene (run_reference): the synchrotron geometry with the reference's own flow
+# model at the torus's indices, fBm turbulence evaluated in place, fixed density.
+REF_SCENE = ["flow.n_index=1.5", "flow.theta0=16.86", "flow.h_over_r=0.3", "flow.keplerian_fraction=0.8",
+             "flow.turbulence=0.3", "flow.n0=1e6"]
+
+
+def same_scene_record(args, so, world, rank, local):
+    """This library on exactly the reference arm's scene and pixels (pixel centres, one sample, fBm in
+    place), end to end through so_trace_rays with host arrays (the reference arm's per-ray call),
+    beside the reference's own trace_ray on the host cores over a bounded sample of those pixels."""
+    import torch
+    W = args.size
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", *REF_SCENE])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, W, W)
+    r.trace_rays(f, X[:65536], Y[:65536])  # warm-up
+    torch.cuda.synchronize()
+    t = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        out = r.trace_rays(f, X, Y)
+        t.append(time.perf_counter() - t0)
+    r.close()
+    ours = allreduce_max(float(np.mean(t)), world)
+    rec = {"workload": f"reference arm's scene: synchrotron geometry {W}x{W}, reference flow model (n ~ r^-1.5, "
+                       "Theta 16.86 r^-0.84, h/r 0.3, 0.8 Keplerian, fBm turbulence rms 0.3 in place, n0 1e6), "
+                       "every pixel centre, FP64",
+           "mrays_s_e2e": round(world * W * W / ours / 1e6, 4), "s_per_frame": round(ours, 3),
+           "api": "so_trace_rays, host arrays in and out", "escaped": int((out["fate"] == 1).sum())}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import _oracle
+        if _oracle.have_ref():
+            R = _oracle.RefShot(os.path.join(PKG_DIR, "shots", "synchrotron_1024.ini"),
+                                [f"camera.width={W}", f"camera.height={W}", *REF_SCENE])
+            threads = os.cpu_count() or 1
+            n = 65536
+            idx = np.linspace(0, W * W - 1, n).astype(np.int64)
+            fr = R.frame(0)
+            t0 = time.perf_counter()
+            _oracle.ref_trace(R.scene, fr, X[idx], Y[idx], threads=threads)
+            dt = time.perf_counter() - t0
+            v = n / dt / 1e6
+            rec["reference_cpu"] = {"mrays_s": round(v, 6), "cores": threads,
+                                    "sample": f"{n} evenly strided pixel centres, the reference's trace_ray "
+                                              f"(oracle/_ref), {dt:.1f} s"}
+            rec["speedup_vs_reference_cpu"] = round(rec["mrays_s_e2e"] / v, 1)
+    return rec
 
 
 def run_shadow(args, so, world, rank, local):
@@ -727,6 +824,7 @@ def main():
     ap.add_argument("--path", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-same-scene", action="store_true", help="skip the reference arm's scene on this library")
     args = ap.parse_args()
     so = load_package()
     if args.impl == "reference":

@@ -61,7 +61,7 @@ enum { SO_PREC_FP64 = 0, SO_PREC_MIXED = 1 };
 /* Hot-flow density / temperature model. */
 enum { SO_PLASMA_REFERENCE = 0, SO_PLASMA_TORUS = 1 };
 
-/* ---- geometry PODs (common.hpp:31-42, kerr.hpp:70-75) ---------------------------------------- */
+/* ---- geometry PODs (common.hpp:31-42, kerr.hpp:20-25) ---------------------------------------- */
 typedef struct so_vec3 { double x, y, z; } so_vec3;
 typedef struct so_mat3 { so_vec3 r0, r1, r2; } so_mat3; /* row-major */
 
@@ -175,6 +175,12 @@ typedef struct so_stats {
     long long turb_records; /* ... record slots summed (segments in use x 16) */
     long long redo_records; /* ... FP32 rays re-traced in FP64 because the record pool ran out */
     long long record_waves; /* ... waves the FP32 rays were traced in (the pool holds one wave's records) */
+    double ms_rec64;      /* plain FP64, deferred torus turbulence: device time of the recording pass */
+    double ms_sum64;      /* ... of the FP64 turbulence sums over all records (k_turb64_records) */
+    double ms_replay64;   /* ... of the replay pass (geodesic again, sums read back, emission) */
+    long long rec64_slots; /* ... record slots summed (segments taken x 16) */
+    long long rec64_short; /* ... jobs summed in the tracer because the record pool ran out */
+    long long rec64_records; /* ... records written (flow steps that needed a sum, up to each ray's end) */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -245,7 +251,10 @@ typedef struct so_mixed_opts {
                               * where a magnified map is steep: L1 5e-3 on a point-star test map) */
     double pool_mb;          /* deferred turbulence: record pool size limit in MiB (0 = half of the free
                               * device memory); a frame whose records exceed it is traced in waves of
-                              * FP32 rays that each fit (the image does not depend on the split) */
+                              * FP32 rays that each fit (the image does not depend on the split).  Also
+                              * caps the plain FP64 tracer's record pool (torus plasma, in either
+                              * precision), beyond which samples are summed in the tracer: the same
+                              * sums, bit for bit, at lower occupancy */
     int fp32_max_attempts;   /* FP32 attempts after which a ray is handed to the FP64 re-trace (0 = 2000:
                               * the FP32 controller stalls on a few rays far from the critical curve,
                               * which the FP64 tracer finishes normally; at 2048^2 the synchrotron
@@ -516,11 +525,15 @@ int so_probe_fma_peak(int device, double* fp64_tflops, double* fp32_tflops);
 /* Peak special-function-unit throughput (FP32 cosines, G ops/s) of `device`: the roofline of the
  * FP32 tracer, whose turbulence sum issues one SFU cosine per Fourier mode. */
 int so_probe_sfu_peak(int device, double* gops);
+/* The device's cos_turns (cos(2 pi t) of a phase in turns, used by the FP64 torus turbulence sums)
+ * at n phases d_t[i] into d_out[i] (device arrays, current device; synchronous): for checking it
+ * against the CPU oracle's restatement. */
+int so_probe_cos_turns(const double* d_t, double* d_out, long long n);
 
 /* ---- analytic helpers (kerr.hpp) --------------------------------------------------------------- */
-/* kerr_point (kerr.hpp:77-92). */
+/* kerr_point (kerr.hpp:27-42). */
 void so_kerr_point_at(double a, double r, double th, so_kerr_point* kp);
-/* critical_curve_point (kerr.hpp:260-270): Bardeen curve point for photon-orbit radius rp. */
+/* critical_curve_point (kerr.hpp:210-220): Bardeen curve point for photon-orbit radius rp. */
 int so_critical_curve_point(double a, double theta_o, double rp, double* alpha, double* beta_plus);
 
 #ifdef __cplusplus

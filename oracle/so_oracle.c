@@ -37,7 +37,7 @@
 #define CGS_QE 4.80320471e-10
 
 /* ------------------------------------------------------------------------------------------------
- * err^(-1/5), own implementation (replaces pow(err, -0.2) of trace.cuh:93/146, kerr.hpp:243/248).
+ * err^(-1/5), own implementation (replaces pow(err, -0.2) of trace.cuh:93/146, kerr.hpp:193/198).
  * x = m 2^e, m in [1,2), e = 5q + r:  x^(-1/5) = m^(-1/5) 2^(-r/5) 2^(-q).  m^(-1/5) from a quadratic
  * seed (rel. error 1.1e-3) and three Newton steps on m y^5 = 1 (error -> 3 eps^2 each).
  * Valid for positive normal x, +inf (returns 0) and NaN (returns NaN).
@@ -76,7 +76,7 @@ static so_vec3 cross3(so_vec3 a, so_vec3 b) {
     return c;
 }
 
-/* kerr_point, kerr.hpp:77-92 (host side of the frame set-up; plain libm, as the reference). */
+/* kerr_point, kerr.hpp:27-42 (host side of the frame set-up; plain libm, as the reference). */
 void orc_kerr_point(double a, double r, double th, so_kerr_point* k) {
     k->r = r;
     k->s = sin(th);
@@ -92,7 +92,7 @@ void orc_kerr_point(double a, double r, double th, so_kerr_point* k) {
     k->sqrtSigmaDelta = sqrt(k->Sigma * k->Delta);
 }
 
-double orc_horizon_radius(double a) { return 1.0 + sqrt(1.0 - a * a); } /* kerr.hpp:94 */
+double orc_horizon_radius(double a) { return 1.0 + sqrt(1.0 - a * a); } /* kerr.hpp:44 */
 
 /* ---- per-ray constants of motion and the geodesic right-hand side ---------------------------- */
 typedef struct {
@@ -112,7 +112,7 @@ static void ray_consts(RayC* c, double a, double lam, double eta, double E) {
     c->Q3 = fma(lam, lam, eta);
 }
 
-/* geodesic_rhs, kerr.hpp:153-166: backward Mino-time derivatives of (r, r', u, u', phi, t). */
+/* geodesic_rhs, kerr.hpp:103-116: backward Mino-time derivatives of (r, r', u, u', phi, t). */
 static void rhs(const RayC* c, const double* y, double* d) {
     double r = y[0], u = y[2];
     double r2 = r * r;
@@ -129,7 +129,7 @@ static void rhs(const RayC* c, const double* y, double* d) {
     d[5] = -fma((r2 + c->A2) * P, iD, c->a * fma(-c->a, s2, c->lam));
 }
 
-/* dp54_step, kerr.hpp:172-207: Dormand-Prince 5(4), FSAL, scaled max-norm error over (r, r', u, u',
+/* dp54_step, kerr.hpp:122-157: Dormand-Prince 5(4), FSAL, scaled max-norm error over (r, r', u, u',
  * phi).  Stage inputs are formed only for the four components the RHS reads (phi and t are
  * quadratures). */
 static const double A21 = 1.0 / 5, A31 = 3.0 / 40, A32 = 9.0 / 40, A41 = 44.0 / 45, A42 = -56.0 / 15,
@@ -175,7 +175,7 @@ static double dp54(const RayC* c, const double* y, const double* k1, double h, d
     return m;
 }
 
-/* project_radial, kerr.hpp:216-223 (radial_potential kerr.hpp:144-147). */
+/* project_radial, kerr.hpp:166-173 (radial_potential kerr.hpp:94-97). */
 static void project_radial(const RayC* c, double* y, double* k) {
     double r = y[0];
     double P = fma(r, r, c->CP);
@@ -189,12 +189,12 @@ static void project_radial(const RayC* c, double* y, double* k) {
     }
 }
 
-/* initial_step, kerr.hpp:225-228. */
+/* initial_step, kerr.hpp:175-178. */
 static double initial_step(const double* y) {
     return 0.02 * fmin(y[0] / (fabs(y[1]) + 1e-12), 1.0 / (fabs(y[3]) + 1e-3));
 }
 
-/* camera_photon, kerr.hpp:113-142.  y receives the backward state. */
+/* camera_photon, kerr.hpp:63-92.  y receives the backward state. */
 static void camera_photon(double a, const so_kerr_point* kp, double phi0, double t0, so_vec3 d, so_vec3 beta,
                           RayC* c, double* y) {
     double k0 = 1.0;
@@ -376,14 +376,55 @@ static double crossing_g(const so_scene* S, double r, double lam, double Ecam) {
     return 1.0 / (Ecam * kdotu);
 }
 
-/* Turbulence of the torus plasma: delta = sum amp cos(k.X + phase). */
+/* cos(2 pi t) of a phase in turns: the library's cos_turns (so_kerr.cuh), operation for operation.
+ * 2t is rounded to the nearest integer q by adding 1.5 * 2^52 (its parity is the low mantissa bit),
+ * g = t - q/2 is exact, and cos(2 pi g) comes from a polynomial of degree 8 in g^2 (a Chebyshev fit
+ * of cos(2 pi sqrt(z)) on [0, 1/16]). */
+static double cos_turns(double t) {
+    const double magic = 6755399441055744.0;
+    const double s = fma(t, 2.0, magic);
+    const double q = s - magic;
+    const double g = fma(q, -0.5, t);
+    const double z = g * g;
+    double p = 0x1.1678f9078a9b3p-2;
+    p = fma(p, z, -0x1.b6957b54dd389p+0);
+    p = fma(p, z, 0x1.f9d254582ac30p+2);
+    p = fma(p, z, -0x1.a6d1efc8c38bep+4);
+    p = fma(p, z, 0x1.e1f506813a321p+5);
+    p = fma(p, z, -0x1.55d3c7e3bfbf5p+6);
+    p = fma(p, z, 0x1.03c1f081b5992p+6);
+    p = fma(p, z, -0x1.3bd3cc9be45dbp+4);
+    p = fma(p, z, 1.0);
+    uint64_t bs, bp;
+    memcpy(&bs, &s, 8);
+    memcpy(&bp, &p, 8);
+    bp ^= (bs & 1ull) << 63;
+    memcpy(&p, &bp, 8);
+    return p;
+}
+double orc_cos_turns(double t) { return cos_turns(t); }
+
+/* Turbulence of the torus plasma: delta = sum amp cos(2 pi (k.X + p)) with the wave vector and phase
+ * in turns (k / 2 pi, phase / 2 pi, each a correctly rounded product with 1 / 2 pi), summed in the
+ * CUDA kernel's order: 32 partial sums, partial l over modes l, l + 32, l + 64, ... in turn, then a
+ * butterfly that adds partials l and l ^ o for o = 16, 8, 4, 2, 1. */
+#define INV_2PI 0x1.45f306dc9c883p-3
 static double torus_delta(const so_mode* md, int n, double X, double Y, double Z) {
-    double acc = 0.0;
-    for (int m = 0; m < n; ++m) {
-        double ph = fma(md[m].kz, Z, fma(md[m].ky, Y, fma(md[m].kx, X, md[m].phase)));
-        acc = fma(md[m].amp, cos(ph), acc);
+    double part[32], next[32];
+    for (int l = 0; l < 32; ++l) {
+        double acc = 0.0;
+        for (int m = l; m < n; m += 32) {
+            const double kx = md[m].kx * INV_2PI, ky = md[m].ky * INV_2PI, kz = md[m].kz * INV_2PI;
+            const double ph = md[m].phase * INV_2PI;
+            acc = fma(md[m].amp, cos_turns(fma(kz, Z, fma(ky, Y, fma(kx, X, ph)))), acc);
+        }
+        part[l] = acc;
     }
-    return acc;
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int l = 0; l < 32; ++l) next[l] = part[l] + part[l ^ o];
+        memcpy(part, next, sizeof part);
+    }
+    return part[0];
 }
 
 typedef struct {
@@ -393,7 +434,7 @@ typedef struct {
     const so_mode* modes;
 } Ctx;
 
-/* flow_step, emission.cuh:264-340, with the torus model as an alternative density/temperature. */
+/* flow_step, emission.cuh:99-175, with the torus model as an alternative density/temperature. */
 /* Baked flow turbulence (render.cu:447-460 bake, 594-620 set-up, emission.cuh:112-124 sampling).
  * Texel values are computed on demand with the bake's formula at the texel centre (the same values
  * as a full bake of the slice); the interpolation is the library kernels' FP32 trilinear (x, then
@@ -928,7 +969,7 @@ int orc_render_chunks(const so_scene* S, const so_plasma* pl, const so_mode* mod
     return SO_OK;
 }
 
-/* vacuum_fate, kerr.hpp:234-253 (the controller with so_rpow5, the same fma placement as above). */
+/* vacuum_fate, kerr.hpp:184-203 (the controller with so_rpow5, the same fma placement as above). */
 int orc_vacuum_fate(double a, const so_frame* F, so_vec3 d, double tol, double r_escape, int max_steps) {
     RayC c;
     double y[6], k1[6], yn[6], k7[6];
@@ -981,7 +1022,7 @@ double orc_find_critical_point(const so_frame* F, double a, double psi, double c
     return 0.5 * (lo + hi);
 }
 
-/* critical_curve_point, kerr.hpp:260-270 (Bardeen 1973). */
+/* critical_curve_point, kerr.hpp:210-220 (Bardeen 1973). */
 int orc_critical_curve_point(double a, double theta_o, double rp, double* alpha, double* beta_plus) {
     double D = rp * rp - 2.0 * rp + a * a;
     double lam = a + rp / a * (rp - 2.0 * D / (rp - 1.0));

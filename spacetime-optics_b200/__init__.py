@@ -43,6 +43,7 @@ def lib():
         L.so_render_device.argtypes = [vp, P(Frame), vp, P(Stats)]
         L.so_probe_fma_peak.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
         L.so_probe_sfu_peak.argtypes = [C.c_int, P(C.c_double)]
+        L.so_probe_cos_turns.argtypes = [vp, vp, C.c_longlong]
         L.so_radio_flux_noalloc.argtypes = [vp, vp, C.c_int, C.c_double, P(Plasma), vp, vp, vp]
         L.so_batch_create.argtypes = [vp, P(Scene), C.c_int, P(Frame), P(C.c_int), C.c_int, C.c_int, C.c_int,
                                       C.c_int, P(vp)]

@@ -87,7 +87,9 @@ class Stats(C.Structure):
                 ("attempts_fp32", C.c_longlong), ("band_rays", C.c_longlong), ("flow_steps_fp32", C.c_longlong),
                 ("ms_fp32", C.c_double), ("redo_turn", C.c_longlong), ("redo_drift", C.c_longlong),
                 ("redo_limit", C.c_longlong), ("ms_fp32_trace", C.c_double), ("ms_turb", C.c_double),
-                ("turb_records", C.c_longlong), ("redo_records", C.c_longlong), ("record_waves", C.c_longlong)]
+                ("turb_records", C.c_longlong), ("redo_records", C.c_longlong), ("record_waves", C.c_longlong),
+                ("ms_rec64", C.c_double), ("ms_sum64", C.c_double), ("ms_replay64", C.c_double),
+                ("rec64_slots", C.c_longlong), ("rec64_short", C.c_longlong), ("rec64_records", C.c_longlong)]
 
 
 class RaysOut(C.Structure):
@@ -182,7 +184,7 @@ LAYOUT_FIELDS = [
 # Every entry point include/so_tracer.h declares (checked against the built library's exports).
 EXPORTS = [
     "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
-    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak", "so_radio_flux_noalloc",
+    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak", "so_probe_cos_turns", "so_radio_flux_noalloc",
     "so_batch_create", "so_batch_render", "so_batch_autotune", "so_batch_set_tune", "so_batch_free",
     "so_set_precision", "so_set_plasma", "so_set_flow_noise", "so_set_sky", "so_sky_file", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",

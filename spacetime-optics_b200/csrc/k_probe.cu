@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/so_tracer.h"
+#include "so_kerr.cuh"
 
 namespace {
 template <typename T>
@@ -97,4 +98,18 @@ extern "C" int so_probe_fma_peak(int device, double* fp64_tflops, double* fp32_t
     int rc = probe<double>(nsm, 2000, fp64_tflops);
     if (!rc) rc = probe<float>(nsm, 4000, fp32_tflops);
     return rc;
+}
+
+namespace {
+__global__ void k_cos_turns(const double* __restrict__ t, double* __restrict__ out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = so::cos_turns(t[i]);
+}
+}  // namespace
+
+extern "C" int so_probe_cos_turns(const double* d_t, double* d_out, long long n) {
+    if (n < 0 || (n > 0 && (!d_t || !d_out))) return SO_ERR_ARG;
+    if (n == 0) return SO_OK;
+    k_cos_turns<<<592, 256>>>(d_t, d_out, n);
+    return cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess ? SO_OK : SO_ERR_CUDA;
 }

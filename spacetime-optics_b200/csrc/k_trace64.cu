@@ -71,10 +71,12 @@ enum Stage : int { ST_REJECTED = 0, ST_ACCEPTED = 1, ST_DONE = 2 };
 
 // First half of one loop iteration of trace_ray (trace.cuh:81-129): step cap, DP5(4) attempt,
 // controller on rejection, swept angle, equatorial crossing (with the disk).  On acceptance the new
-// state is in yn / k7 and the ray continues in ray_commit.
+// state is in yn / k7 and the ray continues in ray_commit.  Without `emit` (the recording pass of the
+// deferred turbulence) the disk is not shaded, so no ray ends on its opacity.
 template <int VAR>
-__device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, double* yn, double* k7, double* hc_out,
-                                           double* err_out, int* fate, double* cross_r, double* cross_g) {
+__device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, bool emit, double* yn, double* k7,
+                                           double* hc_out, double* err_out, int* fate, double* cross_r,
+                                           double* cross_g) {
     if (R.it >= S.max_steps) {
         *fate = 0;
         return ST_DONE;
@@ -115,7 +117,7 @@ __device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, double* 
     if ((R.y[2] > 0.0) != (yn[2] > 0.0)) {
         ++R.ncross;
         const bool rec = cross_r != nullptr && R.ncross <= 3;
-        const bool disk = VAR != VAR_VACUUM && S.disk_on;
+        const bool disk = VAR != VAR_VACUUM && S.disk_on && emit;
         if (disk || rec) {
             double lo = 0.0, hi = 1.0, u0 = R.y[2], u1 = yn[2], m0 = R.y[3] * hc, m1 = yn[3] * hc;
             for (int b = 0; b < 40; ++b) {
@@ -154,13 +156,15 @@ __device__ __forceinline__ int ray_attempt(Ray64& R, const so_scene& S, double* 
 }
 
 // Second half (trace.cuh:130-163): hot-flow transfer with the turbulence sum delta, commit,
-// projection, controller, termination.  Returns 1 when the ray is finished.
+// projection, controller, termination.  Returns 1 when the ray is finished.  Without `emit` only the
+// geometry advances (the ray's transmittance stays 1, so it ends only by capture, escape or the step
+// limit, never earlier than with emission).
 template <int VAR>
 __device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const so_frame& F, const float* field,
-                                          const TorusParams& tp, double delta,
+                                          const TorusParams& tp, double delta, bool emit,
                                           const double* yn, const double* k7, double hc, double err, int* fate,
                                           double* th, double* ph) {
-    if (VAR == VAR_RADIO && S.flow_on && yn[0] < S.r_flow_max) {
+    if (VAR == VAR_RADIO && emit && S.flow_on && yn[0] < S.r_flow_max) {
         double dI, dtau;
         flow_step(S, F, field, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
         ++R.nflow;
@@ -195,36 +199,73 @@ __device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const so_
     return 0;
 }
 
-// Turbulence sums of the lanes in `want`, each split over the warp (lane l takes modes l, l+32, ...)
-// and reduced with butterfly shuffles; two positions are served per pass so each mode read feeds two
-// cosines.  All 32 lanes must call this.  FP64: modes in shared memory as SoA doubles.
+// Turbulence sums delta = sum_m amp_m cos(2 pi (k_m . X + p_m)) (k and p in turns) at four positions
+// (px, py, pz)[j], split over the warp: lane l takes modes l, l + 32, l + 64, ... in that order into
+// one accumulator per position, then the 32 partial sums are added by butterfly shuffles (xor 16,
+// 8, 4, 2, 1), which leaves every lane with the same four sums.  The CPU oracle adds in exactly this
+// order.  Every mode read from shared memory feeds four independent branch-free cosines (cos_turns),
+// so the FP64 pipe has independent work while each chain waits on its previous operation.  All 32
+// lanes must call this.
+__device__ __forceinline__ void warp_sums4(const ModesSmem& md, int n, const double* px, const double* py,
+                                           const double* pz, double* acc) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[j] = 0.0;
+#pragma unroll 1
+    for (int i = lane; i < n; i += 32) {
+        const double kx = md.kx[i], ky = md.ky[i], kz = md.kz[i], p0 = md.ph[i], w = md.amp[i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            acc[j] = fma(w, cos_turns(fma(kz, pz[j], fma(ky, py[j], fma(kx, px[j], p0)))), acc[j]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[j] += __shfl_xor_sync(FULL, acc[j], o);
+    }
+}
+
+// The sums of the lanes in `want` (at their own X, Y, Z), four lanes' positions per warp_sums4 pass.
+// All 32 lanes must call this; it returns at once when no lane wants a sum.
 __device__ __forceinline__ double warp_turbulence64(const ModesSmem& md, int n, bool want, double X, double Y,
                                                     double Z) {
     const int lane = threadIdx.x & 31;
     unsigned m = __ballot_sync(FULL, want);
     double mine = 0.0;
     while (m) {
-        const int s0 = __ffs(m) - 1;
-        m &= m - 1;
-        const int s1 = m ? __ffs(m) - 1 : s0;
-        if (m) m &= m - 1;
-        const double x0 = __shfl_sync(FULL, X, s0), y0 = __shfl_sync(FULL, Y, s0), z0 = __shfl_sync(FULL, Z, s0);
-        const double x1 = __shfl_sync(FULL, X, s1), y1 = __shfl_sync(FULL, Y, s1), z1 = __shfl_sync(FULL, Z, s1);
-        double a = 0.0, b = 0.0;
-        for (int i = lane; i < n; i += 32) {
-            const double kx = md.kx[i], ky = md.ky[i], kz = md.kz[i], p0 = md.ph[i], w = md.amp[i];
-            a = fma(w, cos(fma(kz, z0, fma(ky, y0, fma(kx, x0, p0)))), a);
-            b = fma(w, cos(fma(kz, z1, fma(ky, y1, fma(kx, x1, p0)))), b);
-        }
+        int src[4];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_xor_sync(FULL, a, o);
-            b += __shfl_xor_sync(FULL, b, o);
+        for (int j = 0; j < 4; ++j) {
+            src[j] = m ? __ffs(m) - 1 : src[0];  // fewer than four left: repeat the first
+            if (m) m &= m - 1;
         }
-        if (lane == s0) mine = a;
-        if (lane == s1) mine = b;
+        double px[4], py[4], pz[4], acc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            px[j] = __shfl_sync(FULL, X, src[j]);
+            py[j] = __shfl_sync(FULL, Y, src[j]);
+            pz[j] = __shfl_sync(FULL, Z, src[j]);
+        }
+        warp_sums4(md, n, px, py, pz, acc);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (lane == src[j]) mine = acc[j];
     }
     return mine;
+}
+
+// The mode table in shared memory as SoA doubles, wave vector and phase in turns (k / 2 pi,
+// phase / 2 pi: each a correctly rounded product with 1 / 2 pi) for cos_turns.  Block-wide.
+__device__ __forceinline__ ModesSmem stage_modes64(double* smem, const so_mode* modes, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const so_mode m = modes[i];
+        smem[i] = m.kx * kInvTwoPi;
+        smem[n + i] = m.ky * kInvTwoPi;
+        smem[2 * n + i] = m.kz * kInvTwoPi;
+        smem[3 * n + i] = m.phase * kInvTwoPi;
+        smem[4 * n + i] = m.amp;
+    }
+    return ModesSmem{smem, smem + n, smem + 2 * n, smem + 3 * n, smem + 4 * n};
 }
 
 // Same with FP32 SFU cosines (modes as float4 (k, phase) and float amplitude in shared memory).
@@ -270,9 +311,13 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // Register budget: three 128-thread CTAs per SM (at most 170 registers).  Measured on the B200
 // against the compiler's free choice (194 registers, two CTAs): the plain FP64 synchrotron frame
 // runs 1.29x faster with a few spilled registers and 50 % more warps.
-template <int VAR, bool EMIT32>
-__global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
+// DEFER (deferred FP64 torus turbulence, radio torus only): 0 = sums in the tracer, 1 = recording pass
+// (geometry only: no emission code, so fewer registers and four CTAs per SM), 2 = replay pass.
+template <int VAR, bool EMIT32, int DEFER>
+__global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const TraceLaunch L) {
     extern __shared__ double smem[];
+    constexpr int defer = (VAR == VAR_RADIO && !EMIT32) ? DEFER : 0;
+    constexpr bool emit = defer != 1;
     TorusParams tp;
     tp.on = VAR == VAR_RADIO && L.torus;
     tp.n_modes = tp.on ? L.n_modes : 0;
@@ -281,24 +326,21 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
     tp.h_sph = L.h_sph;
     tp.theta_e0 = L.theta_e0;
     tp.half_var = L.half_var;
-    ModesSmem md = {smem, smem + tp.n_modes, smem + 2 * tp.n_modes, smem + 3 * tp.n_modes, smem + 4 * tp.n_modes};
+    ModesSmem md = {smem, smem, smem, smem, smem};
     float4* km = reinterpret_cast<float4*>(smem);
     float* kamp = reinterpret_cast<float*>(km + tp.n_modes);
-    if (tp.n_modes > 0) {
-        // Stage the mode table once per CTA; every lane then reads the modes of its share
-        for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
-            so_mode m = L.modes[i];
-            if (EMIT32) {
+    // The recording pass of the deferred turbulence sums nothing; the others stage the mode table
+    // once per CTA and every lane then reads the modes of its share
+    if (tp.n_modes > 0 && defer != 1) {
+        if (EMIT32) {
+            for (int i = threadIdx.x; i < tp.n_modes; i += blockDim.x) {
+                so_mode m = L.modes[i];
                 double p = m.phase - 2.0 * PI * floor(m.phase / (2.0 * PI) + 0.5);
                 km[i] = make_float4((float)m.kx, (float)m.ky, (float)m.kz, (float)p);
                 kamp[i] = (float)m.amp;
-            } else {
-                smem[i] = m.kx;
-                smem[tp.n_modes + i] = m.ky;
-                smem[2 * tp.n_modes + i] = m.kz;
-                smem[3 * tp.n_modes + i] = m.phase;
-                smem[4 * tp.n_modes + i] = m.amp;
             }
+        } else {
+            md = stage_modes64(smem, L.modes, tp.n_modes);
         }
         __syncthreads();
     }
@@ -312,18 +354,37 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
         const long long lanes = (long long)gridDim.x * blockDim.x;
         while (stride < 32 && total > 0 && (long long)(stride * 2) * total <= lanes) stride *= 2;
     }
-    long long job = 0, pix = 0;
-    int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
     bool active = false, exhausted = false;
     Ray64 R;
     float pa[4] = {0.f, 0.f, 0.f, 0.f};
     float ys = 0.f, yq = 0.f;
     double cr[3], cg[3];
-    unsigned long long n_att = 0, n_acc = 0, n_lim = 0, n_flow = 0;
+    unsigned long long n_att = 0, n_acc = 0, n_lim = 0, n_flow = 0, n_rec = 0;
     const so_scene* S = nullptr;
     const so_frame* F = nullptr;
     const bool radio_lum = VAR == VAR_RADIO;  // sample_lum, render.cu:87
     const bool rec = L.kind == RAYS_LIST && L.record_cross;
+    // deferred FP64 turbulence: the lane's place in its job's record chain (segment, slots used in it,
+    // first segment) and whether the job's sums are in place (pass 1: the pool ran out; pass 2: the
+    // job's records are incomplete)
+    int rseg = -1, rcnt = REC_SEG, rhead = -1;
+    bool rinline = false;
+    long long job = 0, pix = 0;
+    int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
+    // Each sample of a job has its own chain, head at job_head64[job * jobs_n + s]: the replay pass can
+    // end a sample on its opacity before the recording pass did, so the chains must not run on.
+    auto chain_start = [&](int s) {
+        if (defer == 1) {
+            rseg = rhead = -1;
+            rcnt = REC_SEG;  // the first record opens a segment
+            rinline = false;
+        } else {
+            rhead = L.job_head64[job * jobs_n + s];
+            rseg = rhead;
+            rcnt = 0;
+            rinline = rhead == -2;
+        }
+    };
 
     for (;;) {
         const bool need = !active && !exhausted && (lane & (stride - 1)) == 0;
@@ -384,6 +445,7 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
                     }
                     S = &L.scenes[L.frame_scene[fidx]];
                     F = &L.frames[fidx];
+                    if (defer) chain_start(0);
                     pa[0] = pa[1] = pa[2] = pa[3] = 0.f;
                     ys = yq = 0.f;
                     cr[0] = cr[1] = cr[2] = 0.0;
@@ -399,22 +461,84 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
         bool want = false;
         double TX = 0.0, TY = 0.0, TZ = 0.0;
         if (active) {
-            stage = ray_attempt<VAR>(R, *S, yn, k7, &hc, &err, &fate, rec ? cr : nullptr, cg);
+            stage = ray_attempt<VAR>(R, *S, emit, yn, k7, &hc, &err, &fate, rec ? cr : nullptr, cg);
             if (VAR == VAR_RADIO && stage == ST_ACCEPTED && S->flow_on && yn[0] < S->r_flow_max)
                 want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
         }
         // ---- all lanes: turbulence sums --------------------------------------------------------
         double delta = 0.0;
-        if (VAR == VAR_RADIO && tp.n_modes > 0)
-            delta = EMIT32 ? warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ)
-                           : warp_turbulence64(md, tp.n_modes, want, TX, TY, TZ);
+        if (VAR == VAR_RADIO && tp.n_modes > 0) {
+            if (EMIT32) {
+                delta = warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ);
+            } else if (defer == 1) {
+                // recording pass: append (X, Y, Z) to the job's chain; a lane whose segment is full
+                // takes the next one (one atomic per warp); a job the pool cannot hold is summed in
+                // place by the replay pass
+                const bool need_seg = want && !rinline && rcnt == REC_SEG;
+                const unsigned ms = __ballot_sync(FULL, need_seg);
+                if (ms) {
+                    const int leader = __ffs(ms) - 1;
+                    unsigned long long base = 0;
+                    if (lane == leader) base = atomicAdd(&L.rec64_ctl[0], (unsigned long long)__popc(ms));
+                    base = __shfl_sync(FULL, base, leader);
+                    if (need_seg) {
+                        const unsigned long long idx = base + __popc(ms & ((1u << lane) - 1u));
+                        if (idx >= (unsigned long long)L.seg_cap64) {
+                            rinline = true;
+                        } else {
+                            if (rseg >= 0) L.seg_next64[rseg] = (uint32_t)idx;
+                            else rhead = (int)idx;
+                            rseg = (int)idx;
+                            rcnt = 0;
+                        }
+                    }
+                }
+                if (want && !rinline) {
+                    double* slot = L.rec64 + 4 * ((long long)rseg * REC_SEG + rcnt);
+                    slot[0] = TX;
+                    slot[1] = TY;
+                    slot[2] = TZ;
+                    ++rcnt;
+                    ++n_rec;
+                }
+            } else {
+                // in the tracer (defer 0), or in place for the replay pass's incomplete jobs
+                delta = warp_turbulence64(md, tp.n_modes, want && (defer == 0 || rinline), TX, TY, TZ);
+                if (defer == 2 && want && !rinline) {
+                    if (rcnt == REC_SEG && rseg >= 0) {  // the job's next segment, in recording order
+                        const uint32_t nx = L.seg_next64[rseg];
+                        rseg = nx < (uint32_t)L.seg_cap64 ? (int)nx : -1;
+                        rcnt = 0;
+                    }
+                    // both passes take the same flow steps, so the chain always holds the record;
+                    // were it ever short, the sum would be NaN (visible), never a read out of bounds
+                    delta = rseg >= 0 ? L.rec64[4 * ((long long)rseg * REC_SEG + rcnt) + 3] : __longlong_as_double(-1ll);
+                    ++rcnt;
+                }
+            }
+        }
         // ---- second half: emission and commit (active lanes) ----------------------------------
         if (!active || stage == ST_REJECTED) continue;
         double th = 0.0, ph = 0.0;
         if (stage == ST_ACCEPTED &&
-            !ray_commit<VAR>(R, *S, *F, L.turb_field, tp, delta, yn, k7, hc, err, &fate, &th, &ph))
+            !ray_commit<VAR>(R, *S, *F, L.turb_field, tp, delta, emit, yn, k7, hc, err, &fate, &th, &ph))
             continue;
         // sample finished
+        if (defer == 1) {
+            // recording pass: no outputs; the sample's chain is closed and the job's next sample, if
+            // any, opens its own
+            L.job_head64[job * jobs_n + sample] = rinline ? -2 : rhead;
+            if (rinline) atomicAdd(&L.rec64_ctl[1], 1ull);
+            if ((L.kind == RAYS_PIXELS || L.kind == RAYS_CHUNKS) && ++sample < jobs_n) {
+                double x, yv;
+                pixel_point(L, *F, pix, sbase + sample, &x, &yv);
+                ray_init<VAR>(R, *S, *F, x, yv);
+                chain_start(sample);
+                continue;
+            }
+            active = false;
+            continue;
+        }
         n_att += (unsigned long long)R.natt;
         n_acc += (unsigned long long)R.nacc;
         n_flow += (unsigned long long)R.nflow;
@@ -463,6 +587,7 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
                 double x, yv;
                 pixel_point(L, *F, pix, sbase + sample, &x, &yv);
                 ray_init<VAR>(R, *S, *F, x, yv);
+                if (defer) chain_start(sample);
             } else if (L.kind == RAYS_PIXELS) {
                 const long long o = (long long)fidx * L.W * L.H + pix;
                 reinterpret_cast<float4*>(L.accum)[o] = make_float4(pa[0], pa[1], pa[2], pa[3]);
@@ -478,12 +603,64 @@ __global__ void __launch_bounds__(128, 3) k_trace64(const TraceLaunch L) {
     n_acc = warp_sum(n_acc);
     n_lim = warp_sum(n_lim);
     n_flow = warp_sum(n_flow);
+    if (defer == 1) {
+        n_rec = warp_sum(n_rec);
+        if (lane == 0) atomicAdd(&L.rec64_ctl[2], n_rec);
+    }
     if (lane == 0) {
         atomicAdd(&L.counters->attempts, n_att);
         atomicAdd(&L.counters->accepted, n_acc);
         atomicAdd(&L.counters->step_limited, n_lim);
         atomicAdd(&L.counters->flow_steps, n_flow);
     }
+}
+
+// Deferred FP64 turbulence: the sum at every record slot written by a recording pass of k_trace64,
+// by the same warp_sums4 arithmetic as the tracer's own sums (so the replay pass reads exactly the
+// value the tracer would have computed).  Each warp takes four consecutive slots at a time, the grid
+// strides over all slots of the segments taken; the slots past a chain's last record hold stale
+// positions whose sums nobody reads.  The whole SM runs this kernel, without the tracer's register
+// load, so many more warps hide the FP64 latency of the cosine chains.
+__global__ void __launch_bounds__(256) k_turb64_records(const TraceLaunch L) {
+    extern __shared__ double smem64[];
+    const int n = L.n_modes;
+    const ModesSmem md = stage_modes64(smem64, L.modes, n);
+    __syncthreads();
+    unsigned long long used = *(volatile unsigned long long*)&L.rec64_ctl[0];
+    if (used > (unsigned long long)L.seg_cap64) used = (unsigned long long)L.seg_cap64;
+    const long long nslots = (long long)used * REC_SEG;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long s0 = 4 * warp; s0 < nslots; s0 += 4 * nwarps) {
+        double px[4], py[4], pz[4], acc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double* rec = L.rec64 + 4 * min(s0 + j, nslots - 1);
+            px[j] = rec[0];
+            py[j] = rec[1];
+            pz[j] = rec[2];
+        }
+        warp_sums4(md, n, px, py, pz, acc);
+        double mine = acc[0];
+#pragma unroll
+        for (int j = 1; j < 4; ++j)
+            if (lane == j) mine = acc[j];
+        if (lane < 4 && s0 + lane < nslots) L.rec64[4 * (s0 + lane) + 3] = mine;
+    }
+}
+
+cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    const size_t smem = (size_t)L.n_modes * 5 * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_turb64_records, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_turb64_records, 256, smem);
+    if (e != cudaSuccess) return e;
+    k_turb64_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, smem, st>>>(L);
+    return cudaGetLastError();
 }
 
 // Host launcher: grid = SMs x resident CTAs per SM (persistent; capped by L.ctas_per_sm), dynamic
@@ -573,7 +750,8 @@ cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaS
     const int tpb = 128;
     const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;
     const bool emit32 = torus && L.emit32;
-    size_t smem = torus ? (size_t)L.n_modes * (emit32 ? sizeof(float4) + sizeof(float) : 5 * sizeof(double)) : 0;
+    size_t smem = torus && !(L.defer64 == 1 && !emit32)
+                      ? (size_t)L.n_modes * (emit32 ? sizeof(float4) + sizeof(float) : 5 * sizeof(double)) : 0;
     int per_sm = 1;
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e;
@@ -593,9 +771,13 @@ cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaS
         return cudaGetLastError();
     };
     switch (variant) {
-        case VAR_VACUUM: return go(k_trace64<VAR_VACUUM, false>);
-        case VAR_DISK: return go(k_trace64<VAR_DISK, false>);
-        default: return emit32 ? go(k_trace64<VAR_RADIO, true>) : go(k_trace64<VAR_RADIO, false>);
+        case VAR_VACUUM: return go(k_trace64<VAR_VACUUM, false, 0>);
+        case VAR_DISK: return go(k_trace64<VAR_DISK, false, 0>);
+        default:
+            if (emit32) return go(k_trace64<VAR_RADIO, true, 0>);
+            if (torus && L.defer64 == 1) return go(k_trace64<VAR_RADIO, false, 1>);
+            if (torus && L.defer64 == 2) return go(k_trace64<VAR_RADIO, false, 2>);
+            return go(k_trace64<VAR_RADIO, false, 0>);
     }
 }
 

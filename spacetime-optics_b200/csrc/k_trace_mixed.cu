@@ -3,7 +3,7 @@
 // Same physics as the plain FP64 tracer (trace_ray, blackholes/src/trace.cuh:62-165; flow_step,
 // emission.cuh:99-175), re-arranged for throughput:
 //   k_route       per sample: distance of its image point from the analytic critical curve
-//                 (critical_curve_point, kerr.hpp:260-270, tabulated per frame on the host).  Inside
+//                 (critical_curve_point, kerr.hpp:210-220, tabulated per frame on the host).  Inside
 //                 the band -> FP64 list; outside -> FP32 list.
 //   k_approach64  FP64 from the camera to r_switch (the far field, where the coordinate time and
 //                 radius are too large for FP32 increments): DP5(4) in the inverse radius
@@ -216,7 +216,7 @@ struct C32 {
     float a, lam, eta, E, A2, CP, K, Q3;
 };
 
-// geodesic_rhs in FP32 (kerr.hpp:153-166); s2 = (1-u)(1+u) keeps its relative precision at the poles.
+// geodesic_rhs in FP32 (kerr.hpp:103-116); s2 = (1-u)(1+u) keeps its relative precision at the poles.
 __device__ __forceinline__ void rhs32(const C32& c, float r, float pr, float u, float pu, float* d) {
     float Delta = fmaf(r, r - 2.f, c.A2);
     float P = fmaf(r, r, c.CP);
@@ -303,7 +303,7 @@ __device__ __forceinline__ float warp_turbulence(const float4* __restrict__ km, 
     return mine;
 }
 
-// flow_step (emission.cuh:264-340) in FP32, given the turbulence sum delta at this point (torus
+// flow_step (emission.cuh:99-175) in FP32, given the turbulence sum delta at this point (torus
 // model).  The reference plasma enters only without its fBm turbulence (see the router).
 // bfac: the reference model's baked turbulence factor at this point (1 without turbulence).
 __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp, float delta, float r, float u,
@@ -548,7 +548,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                 n2 = nuh + nul;
                 const float n3 = npuh + npul;
                 rhs32(c, n0, n1, n2, n3, k7);
-                // error norm of kerr.hpp:193-205 at tol32
+                // error norm of kerr.hpp:143-155 at tol32
                 float sc[5];
                 sc[0] = tol * (1e-6f + fmaxf(fabsf(y0), fabsf(n0)));
                 sc[1] = tol * (1e-6f + fmaxf(fmaxf(fabsf(y1), fabsf(n1)), y0 * y0));
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
             acc2(R.th, R.tl, dy[5]);
 #pragma unroll
             for (int i = 0; i < 6; ++i) R.k1[i] = k7[i];
-            // project_radial (kerr.hpp:216-223) in FP32
+            // project_radial (kerr.hpp:166-173) in FP32
             {
                 float r = n0, P = fmaf(r, r, c.CP), D = fmaf(r, r - 2.f, c.A2);
                 float Rr = fmaf(P, P, -(D * c.K)), r2 = r * r;

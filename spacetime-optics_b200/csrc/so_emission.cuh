@@ -198,7 +198,9 @@ struct TorusParams {
     double ne_index, te_index, h_sph, theta_e0, half_var;
 };
 
-// Fourier-mode turbulence delta(X) = sum amp cos(k.X + phase), modes in shared memory (SoA, double).
+// Fourier-mode turbulence delta(X) = sum amp cos(k.X + phase), modes in shared memory (SoA, double),
+// wave vector and phase stored in turns (multiplied by kInvTwoPi) for cos_turns.
+constexpr double kInvTwoPi = 0x1.45f306dc9c883p-3;  // 1 / (2 pi), correctly rounded
 struct ModesSmem {
     const double* kx;
     const double* ky;
@@ -207,7 +209,7 @@ struct ModesSmem {
     const double* amp;
 };
 
-// flow_step (emission.cuh:264-340): source term g^3 S (1 - e^-dtau) and optical depth of a Mino
+// flow_step (emission.cuh:99-175): source term g^3 S (1 - e^-dtau) and optical depth of a Mino
 // step h at (r, u, phi, t).  The torus model replaces the density / temperature / turbulence
 // lines; the rest of the physics is the reference's.  The torus pattern is advected by the flow to
 // the emission time counted from the radial light-travel time to the camera at rcam,

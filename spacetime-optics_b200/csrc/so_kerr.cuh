@@ -1,9 +1,9 @@
 // so_kerr.cuh -- Kerr null geodesics in Mino time and the Dormand-Prince 5(4) stepper, shared by the
 // CUDA kernels and the host-side shot set-up (critical-curve search).
 //
-// Follows the reference's blackholes/src/kerr.hpp: kerr_point (:77-92), camera_photon (:113-142),
-// geodesic_rhs (:153-166), dp54_step (:172-207), project_radial (:216-223), initial_step (:225-228),
-// vacuum_fate (:234-253), critical_curve_point (:260-270).
+// Follows the reference's blackholes/src/kerr.hpp: kerr_point (:27-42), camera_photon (:63-92),
+// geodesic_rhs (:103-116), dp54_step (:118-157), project_radial (:159-173), initial_step (:175-178),
+// vacuum_fate (:184-203), critical_curve_point (:210-220).
 //
 // Arithmetic contract: every multiply-add is an explicit fma() in a fixed order, device code is
 // compiled with -fmad=false and host code with -ffp-contract=off, so host and device evaluate the
@@ -71,11 +71,36 @@ SO_HD double rpow5(double x) {
     return y * bitsd((uint64_t)(1023 - q) << 52);
 }
 
+// cos(2 pi t) of a phase t given in turns, for |t| < 2^50, branch-free.  t = q/2 + g with the
+// nearest half-turn q/2 and |g| <= 1/4: q is read off 2t + 1.5 * 2^52 (rounding to the nearest
+// integer, parity in the low mantissa bit), g = t - q/2 is exact, and cos(2 pi t) = (-1)^q cos(2 pi g)
+// with cos(2 pi g) from a near-minimax polynomial of degree 8 in g^2 (Chebyshev fit of
+// cos(2 pi sqrt(z)) on z in [0, 1/16], coefficients by fit_cos_turns.py; abs error of the fit with
+// double coefficients 1e-16).  Sixteen FP64 operations and no branch, so a loop over independent
+// phases keeps the FP64 pipe fed; the CPU oracle repeats it operation for operation.
+SO_HD double cos_turns(double t) {
+    const double magic = 6755399441055744.0;  // 1.5 * 2^52
+    const double s = fma(t, 2.0, magic);      // magic + nearest integer to 2t (ties to even)
+    const double q = s - magic;                // exact
+    const double g = fma(q, -0.5, t);          // exact, |g| <= 1/4
+    const double z = g * g;
+    double p = 0x1.1678f9078a9b3p-2;
+    p = fma(p, z, -0x1.b6957b54dd389p+0);
+    p = fma(p, z, 0x1.f9d254582ac30p+2);
+    p = fma(p, z, -0x1.a6d1efc8c38bep+4);
+    p = fma(p, z, 0x1.e1f506813a321p+5);
+    p = fma(p, z, -0x1.55d3c7e3bfbf5p+6);
+    p = fma(p, z, 0x1.03c1f081b5992p+6);
+    p = fma(p, z, -0x1.3bd3cc9be45dbp+4);
+    p = fma(p, z, 1.0);
+    return bitsd(dbits(p) ^ ((dbits(s) & 1ull) << 63));  // (-1)^q
+}
+
 SO_HD double dot3(const so_vec3& a, const so_vec3& b) { return fma(a.z, b.z, fma(a.y, b.y, a.x * b.x)); }
 
 SO_HD double horizon_radius(double a) { return 1.0 + sqrt(1.0 - a * a); }
 
-// kerr_point (kerr.hpp:77-92): metric functions at (r, theta).  Host set-up, plain libm.
+// kerr_point (kerr.hpp:27-42): metric functions at (r, theta).  Host set-up, plain libm.
 inline void kerr_point(double a, double r, double th, so_kerr_point* k) {
     k->r = r;
     k->s = std::sin(th);
@@ -109,7 +134,7 @@ SO_HD void ray_consts(RayC& c, double a, double lam, double eta, double E) {
     c.Q3 = fma(lam, lam, eta);
 }
 
-// geodesic_rhs (kerr.hpp:153-166): backward Mino-time derivatives of y = (r, r', u, u', phi, t).
+// geodesic_rhs (kerr.hpp:103-116): backward Mino-time derivatives of y = (r, r', u, u', phi, t).
 SO_HD void rhs(const RayC& c, const double* y, double* d) {
     double r = y[0], u = y[2];
     double r2 = r * r;
@@ -126,7 +151,7 @@ SO_HD void rhs(const RayC& c, const double* y, double* d) {
     d[5] = -fma((r2 + c.A2) * P, iD, c.a * fma(-c.a, s2, c.lam));
 }
 
-// Dormand-Prince 5(4) tableau (kerr.hpp:174-179).
+// Dormand-Prince 5(4) tableau (kerr.hpp:124-129).
 constexpr double A21 = 1.0 / 5, A31 = 3.0 / 40, A32 = 9.0 / 40, A41 = 44.0 / 45, A42 = -56.0 / 15, A43 = 32.0 / 9;
 constexpr double A51 = 19372.0 / 6561, A52 = -25360.0 / 2187, A53 = 64448.0 / 6561, A54 = -212.0 / 729;
 constexpr double A61 = 9017.0 / 3168, A62 = -355.0 / 33, A63 = 46732.0 / 5247, A64 = 49.0 / 176,
@@ -135,7 +160,7 @@ constexpr double B1 = 35.0 / 384, B3 = 500.0 / 1113, B4 = 125.0 / 192, B5 = -218
 constexpr double E1 = 71.0 / 57600, E3 = -71.0 / 16695, E4 = 71.0 / 1920, E5 = -17253.0 / 339200,
                  E6 = 22.0 / 525, E7 = -1.0 / 40;
 
-// dp54_step (kerr.hpp:172-207).  One FSAL attempt from (y, k1) with step h; writes yo and k7 = f(yo)
+// dp54_step (kerr.hpp:122-157).  One FSAL attempt from (y, k1) with step h; writes yo and k7 = f(yo)
 // and returns the scaled max-norm error (<= 1 accepts).  Stage inputs are formed for the four
 // components the RHS reads; phi and t enter only through the 5th-order sum and the error.
 SO_HD double dp54(const RayC& c, const double* y, const double* k1, double h, double tol, double* yo,
@@ -179,14 +204,14 @@ SO_HD double dp54(const RayC& c, const double* y, const double* k1, double h, do
     return m;
 }
 
-// radial_potential (kerr.hpp:144-147) with this file's fma order.
+// radial_potential (kerr.hpp:94-97) with this file's fma order.
 SO_HD double radial_pot(const RayC& c, double r) {
     double P = fma(r, r, c.CP);
     double D = fma(r, r - 2.0, c.A2);
     return fma(P, P, -(D * c.K));
 }
 
-// project_radial (kerr.hpp:216-223).
+// project_radial (kerr.hpp:166-173).
 SO_HD void project_radial(const RayC& c, double* y, double* k) {
     double r = y[0];
     double R = radial_pot(c, r);
@@ -198,7 +223,7 @@ SO_HD void project_radial(const RayC& c, double* y, double* k) {
     }
 }
 
-// initial_step (kerr.hpp:225-228).
+// initial_step (kerr.hpp:175-178).
 SO_HD double initial_step(const double* y) {
     return 0.02 * fmin(y[0] / (fabs(y[1]) + 1e-12), 1.0 / (fabs(y[3]) + 1e-3));
 }
@@ -214,7 +239,7 @@ SO_HD so_vec3 view_dir(const so_frame& f, double x, double yv) {
     return d;
 }
 
-// camera_photon (kerr.hpp:113-142): constants of motion and backward initial state of the photon
+// camera_photon (kerr.hpp:63-92): constants of motion and backward initial state of the photon
 // reaching the camera along -d, with the optional Lorentz boost of the camera velocity beta.
 SO_HD void camera_photon(double a, const so_kerr_point& kp, double phi0, double t0, so_vec3 d, so_vec3 beta,
                          RayC& c, double* y) {
@@ -257,7 +282,7 @@ SO_HD double reject_step(double hc, double err) {
 }
 SO_HD double accept_step(double hc, double err) { return hc * fmin(5.0, fmax(0.2, 0.9 * rpow5(fmax(err, 1e-30)))); }
 
-// vacuum_fate (kerr.hpp:234-253): +1 escaped, -1 captured, 0 undecided.
+// vacuum_fate (kerr.hpp:184-203): +1 escaped, -1 captured, 0 undecided.
 SO_HD int vacuum_fate(double a, const so_frame& f, so_vec3 d, double tol, double r_escape, int max_steps) {
     RayC c;
     double y[6], k1[6], yn[6], k7[6];
@@ -283,7 +308,7 @@ SO_HD int vacuum_fate(double a, const so_frame& f, so_vec3 d, double tol, double
     return 0;
 }
 
-// critical_curve_point (kerr.hpp:260-270), Bardeen (1973).
+// critical_curve_point (kerr.hpp:210-220), Bardeen (1973).
 SO_HD bool critical_curve_point(double a, double theta_o, double rp, double* alpha, double* beta_plus) {
     double D = rp * rp - 2.0 * rp + a * a;
     double lam = a + rp / a * (rp - 2.0 * D / (rp - 1.0));

@@ -132,6 +132,17 @@ struct TraceLaunch {
     int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
     int ctas_per_sm;          // persistent grid: CTAs per SM (0 = as many as fit)
     int emit32;               // FP64 tracer: torus turbulence sums in FP32 (geometry stays FP64)
+    // deferred FP64 torus turbulence: pass 1 (defer64 = 1) integrates the geodesic only and records
+    // the position of every flow step that needs a sum in its job's chain of REC_SEG-slot segments;
+    // k_turb64_records sums the modes at every record; pass 2 (defer64 = 2) integrates again and reads
+    // each sum back in order.  0 = sums in the tracer.
+    int defer64;
+    double* rec64;            // record pool: slot s holds X, Y, Z, delta at doubles 4 s .. 4 s + 3
+    uint32_t* seg_next64;     // per segment: the job's next segment
+    int* job_head64;          // per sample of a job (job * samples per job + s): its chain's first segment,
+                              // -1 no records, -2 the pool ran out (the replay pass sums in place)
+    long long seg_cap64;      // segments in the pool
+    unsigned long long* rec64_ctl;  // [0] segments taken, [1] jobs that ran out of segments, [2] records
     const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi
     int band_n;
     float4* state;            // parked ray state, 5 float4 per sample id (SoA planes of nsamples)
@@ -182,6 +193,8 @@ struct TurbModes {
 };
 void turb_modes_fold(const so_mode* modes, int n, TurbModes* out);
 cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
+// FP64 sums at every record of a defer64 = 1 pass (modes from L.modes, L.n_modes of them).
+cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_sky_escape(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);

@@ -136,6 +136,20 @@ struct so_renderer {
     // luminance statistics of so_render (device buffers and the pinned result)
     LumScratch lum{};
     LumStat* h_lum = nullptr;
+    // deferred FP64 torus turbulence of the plain tracer: record pool (segments of REC_SEG slots of
+    // X, Y, Z, delta), per-job chain heads, the recording pass's counters, and the pool's use
+    double* d_rec64 = nullptr;
+    uint32_t* d_seg_next64 = nullptr;
+    int* d_job_head64 = nullptr;
+    unsigned long long* d_rec64_ctl = nullptr;  // [0] segments taken, [1] jobs that ran short, [2] records
+    Counters* d_cnt64 = nullptr;
+    long long seg_cap64 = 0, job_cap64 = 0, pool64_target = -1;
+    double rec_per_sample64 = 320.0;           // pool size per sample (records), doubled after a shortage
+    unsigned long long* h_rec64 = nullptr;     // pinned copy of d_rec64_ctl after the last deferred trace
+    cudaEvent_t ev_rec64 = nullptr;
+    bool rec64_pending = false;
+    cudaEvent_t ev64[4] = {nullptr, nullptr, nullptr, nullptr};  // recording pass, sums, replay pass
+    bool last_defer64 = false;
     std::string err;
 };
 
@@ -198,6 +212,13 @@ void free_all(so_renderer* r) {
     delete r->turb_modes;
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
+    void* p64[] = {r->d_rec64, r->d_seg_next64, r->d_job_head64, r->d_rec64_ctl, r->d_cnt64};
+    for (void* p : p64)
+        if (p) cudaFree(p);
+    if (r->h_rec64) cudaFreeHost(r->h_rec64);
+    if (r->ev_rec64) cudaEventDestroy(r->ev_rec64);
+    for (cudaEvent_t e : r->ev64)
+        if (e) cudaEventDestroy(e);
     if (r->st2) cudaStreamDestroy(r->st2);
     if (r->st) cudaStreamDestroy(r->st);
 }
@@ -205,7 +226,7 @@ void free_all(so_renderer* r) {
 constexpr int BAND_N = 2048;
 
 // Critical curve rho_c(psi) of a distant observer at inclination th (critical_curve_point,
-// kerr.hpp:260-270, both signs of beta), tabulated on BAND_N image angles psi in [-pi, pi).
+// kerr.hpp:210-220, both signs of beta), tabulated on BAND_N image angles psi in [-pi, pi).
 std::vector<float> band_table(double a, double th) {
     std::vector<float> out(BAND_N);
     if (a < 1e-4) {  // the 1/a parametrisation degenerates: Schwarzschild circle sqrt(27)
@@ -353,8 +374,108 @@ int ensure_side_queue(so_renderer* r) {
     return SO_OK;
 }
 
+// Record pool of the deferred FP64 turbulence for `jobs` tracer jobs of `per_job` samples:
+// rec_per_sample64 records per sample plus one partly filled segment per job, within half of the
+// free device memory and so_mixed_opts.pool_mb.  Jobs that do not fit are summed in place by the
+// replay pass (the same sums, slower); such a shortage doubles the estimate for the next traces.
+int ensure_records64(so_renderer* r, long long jobs, int per_job) {
+    if (!r->h_rec64) {
+        SO_CK(r, cudaMallocHost((void**)&r->h_rec64, 3 * sizeof(unsigned long long)));
+        r->h_rec64[0] = r->h_rec64[1] = r->h_rec64[2] = 0;
+        SO_CK(r, cudaEventCreateWithFlags(&r->ev_rec64, cudaEventDisableTiming));
+        for (cudaEvent_t& e : r->ev64) SO_CK(r, cudaEventCreate(&e));
+    }
+    if (!r->d_rec64_ctl && dalloc(&r->d_rec64_ctl, 3) != cudaSuccess)
+        return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
+    if (!r->d_cnt64 && dalloc(&r->d_cnt64, 1) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
+    if (r->rec64_pending && cudaEventQuery(r->ev_rec64) == cudaSuccess) {
+        r->rec64_pending = false;
+        if (r->h_rec64[1] > 0) r->rec_per_sample64 *= 2.0;
+    }
+    cudaGetLastError();  // a pending event reports cudaErrorNotReady
+    const double per_seg = REC_SEG * 4 * sizeof(double) + sizeof(uint32_t);
+    const double seg_per_job = (r->rec_per_sample64 / REC_SEG + 1.0) * per_job;  // a partly filled segment per sample
+    long long want = std::min<long long>((long long)std::ceil((double)jobs * seg_per_job), 0x7fffffffll);
+    if (r->mixed.pool_mb > 0.0)
+        want = std::min<long long>(want, std::max<long long>(1, (long long)(r->mixed.pool_mb * 1048576.0 / per_seg)));
+    if (r->seg_cap64 <= 0 || want > r->pool64_target || (r->mixed.pool_mb > 0.0 && want < r->seg_cap64)) {
+        SO_CK(r, cudaStreamSynchronize(r->st));
+        if (r->d_rec64) cudaFree(r->d_rec64);
+        if (r->d_seg_next64) cudaFree(r->d_seg_next64);
+        r->d_rec64 = nullptr;
+        r->d_seg_next64 = nullptr;
+        r->seg_cap64 = 0;
+        r->pool64_target = -1;
+        size_t fr = 0, tot = 0;
+        SO_CK(r, cudaMemGetInfo(&fr, &tot));
+        const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
+        if (cap < 1) return fail(r, SO_ERR_ALLOC, "FP64 record pool: no device memory");
+        if (dalloc(&r->d_rec64, (size_t)cap * REC_SEG * 4) != cudaSuccess ||
+            dalloc(&r->d_seg_next64, (size_t)cap) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "FP64 record pool: device allocation");
+        r->seg_cap64 = cap;
+        r->pool64_target = want;
+    }
+    const long long heads = jobs * per_job;  // one chain per sample
+    if (heads > r->job_cap64) {
+        if (r->d_job_head64) cudaFree(r->d_job_head64);
+        r->d_job_head64 = nullptr;
+        r->job_cap64 = 0;
+        if (dalloc(&r->d_job_head64, (size_t)heads) != cudaSuccess)
+            return fail(r, SO_ERR_ALLOC, "FP64 record pool: chain heads");
+        r->job_cap64 = heads;
+    }
+    return SO_OK;
+}
+
+// Launches of the FP64 tracer.  A torus-plasma launch with FP64 sums and at least kDeferMinJobs
+// host-counted jobs on the renderer's stream runs as recording pass -> k_turb64_records -> replay
+// pass (bit for bit the in-tracer result, with the sums at full occupancy); everything else, and any
+// launch whose pool cannot be had, sums in the tracer.
+constexpr long long kDeferMinJobs = 4096;
+
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
-    cudaError_t e = launch_trace64(L, variant_of(r->S), r->num_sms, st ? st : r->st);
+    const int var = variant_of(r->S);
+    const cudaStream_t s = st ? st : r->st;
+    const bool defer = var == VAR_RADIO && L.torus && L.n_modes > 0 && !L.emit32 && !L.nrays_dev &&
+                       L.nrays >= kDeferMinJobs && s == r->st;
+    r->last_defer64 = false;
+    if (defer) {
+        const int per_job = L.kind == RAYS_PIXELS ? L.spp : L.kind == RAYS_CHUNKS ? L.chunk : 1;
+        if (ensure_records64(r, L.nrays, per_job) == SO_OK) {
+            SO_CK(r, cudaMemsetAsync(r->d_rec64_ctl, 0, 3 * sizeof(unsigned long long), s));
+            SO_CK(r, cudaMemsetAsync(r->d_cnt64, 0, sizeof(Counters), s));
+            TraceLaunch L1 = L;
+            L1.defer64 = 1;
+            L1.counters = r->d_cnt64;
+            L1.rec64 = r->d_rec64;
+            L1.seg_next64 = r->d_seg_next64;
+            L1.job_head64 = r->d_job_head64;
+            L1.seg_cap64 = r->seg_cap64;
+            L1.rec64_ctl = r->d_rec64_ctl;
+            TraceLaunch L2 = L1;
+            L2.defer64 = 2;
+            L2.counters = L.counters;
+            cudaEventRecord(r->ev64[0], s);
+            cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
+            if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
+            cudaEventRecord(r->ev64[1], s);
+            e = launch_turb64_records(L1, r->num_sms, s);
+            if (e != cudaSuccess) return cuda_fail(r, e, "FP64 turbulence sums");
+            cudaEventRecord(r->ev64[2], s);
+            e = launch_trace64(L2, var, r->num_sms, s);
+            if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
+            cudaEventRecord(r->ev64[3], s);
+            SO_CK(r, cudaMemcpyAsync(r->h_rec64, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s));
+            SO_CK(r, cudaEventRecord(r->ev_rec64, s));
+            r->rec64_pending = true;
+            r->last_defer64 = true;
+            return SO_OK;
+        }
+        r->err.clear();  // no pool: sum in the tracer
+    }
+    cudaError_t e = launch_trace64(L, var, r->num_sms, s);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
     return SO_OK;
 }
@@ -824,6 +945,21 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->turb_records = stats->redo_records = 0;
             stats->record_waves = 0;
             c.fp64_rays = 0;
+        }
+        stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = 0.0;
+        stats->rec64_slots = stats->rec64_short = stats->rec64_records = 0;
+        if (r->last_defer64) {  // the last tracer launch deferred its FP64 sums (stream synchronised above)
+            float a = 0.f, b = 0.f, c2 = 0.f;
+            cudaEventElapsedTime(&a, r->ev64[0], r->ev64[1]);
+            cudaEventElapsedTime(&b, r->ev64[1], r->ev64[2]);
+            cudaEventElapsedTime(&c2, r->ev64[2], r->ev64[3]);
+            stats->ms_rec64 = a;
+            stats->ms_sum64 = b;
+            stats->ms_replay64 = c2;
+            const unsigned long long used = std::min<unsigned long long>(r->h_rec64[0], (unsigned long long)r->seg_cap64);
+            stats->rec64_slots = (long long)used * REC_SEG;
+            stats->rec64_short = (long long)r->h_rec64[1];
+            stats->rec64_records = (long long)r->h_rec64[2];
         }
         float ms1 = 0.f, ms2 = 0.f;
         cudaEventElapsedTime(&ms1, ev[0], ev[1]);

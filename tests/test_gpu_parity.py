@@ -122,7 +122,7 @@ def test_crossing_records_vs_oracle(so, orc, shadow):
 
 def test_analytic_shadow_edge(so, shadow):
     """bhrt --selftest on the GPU: the fate transition along the horizontal image axis of a distant
-    camera (r = 1e7) sits on the analytic Bardeen critical curve (kerr.hpp:260-270)."""
+    camera (r = 1e7) sits on the analytic Bardeen critical curve (kerr.hpp:210-220)."""
     import ctypes as C
     for a, incl in ((0.94, 17.0), (0.5, 90.0), (0.99, 90.0)):
         import tempfile
@@ -240,6 +240,21 @@ def _intensity_report(I0, I1, frac=1e-3):
             "rel_p99": float(np.percentile(rel, 99)), "bit_identical": float((I0 == I1).all(axis=1).mean())}
 
 
+def test_cos_turns_device_equals_oracle(so, orc):
+    """The device's cos_turns (FP64 torus turbulence) equals the oracle's restatement bit for bit."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(9)
+    t = np.concatenate([rng.uniform(-300, 300, 200000), rng.uniform(-1, 1, 50000), np.arange(-8, 8.001, 1 / 256)])
+    d_t = torch.tensor(t, dtype=torch.float64, device="cuda")
+    d_o = torch.empty_like(d_t)
+    assert so.lib().so_probe_cos_turns(C.c_void_p(d_t.data_ptr()), C.c_void_p(d_o.data_ptr()), t.size) == 0
+    f = orc.oracle().orc_cos_turns
+    f.argtypes, f.restype = [C.c_double], C.c_double
+    want = np.array([f(float(x)) for x in t])
+    assert np.array_equal(d_o.cpu().numpy().view(np.uint64), want.view(np.uint64))
+
+
 def test_torus_1024_strided_vs_oracle(so, orc):
     """Config synchrotron_1024 (a = 0.94, i = 163 deg, +-12 M, 230 GHz, 512-mode torus turbulence):
     every 61st pixel centre of the 1024^2 frame (17,190 rays) through the FP64 kernel against the
@@ -264,6 +279,35 @@ def test_torus_1024_strided_vs_oracle(so, orc):
     rep = _intensity_report(o["I"], k["I"])
     print("torus 1024 strided vs oracle:", rep)
     assert rep["rel_max"] <= 1e-5 and rep["above"] > 1500
+    r.close()
+
+
+def test_deferred_fp64_sums_multi_sample_frame(so, orc):
+    """The plain FP64 tracer on a torus frame of >= 4096 pixels defers its turbulence sums (recording
+    pass, k_turb64_records, replay pass), one record chain per sample.  A 64 x 64 frame at 2 samples
+    per pixel equals, bit for bit, the same frame with the record pool capped so that nearly every
+    sample is summed in the tracer instead, and matches the oracle's pass 1 within 1e-6 of the frame
+    maximum."""
+    n = 64
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={n}", f"camera.height={n}", "render.spp=2",
+                                          "render.spp_max=2", "flow.n0=1594262.8"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    p = sh.plasma()
+    modes = r.set_plasma(p)
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    a, _, sa = r.render(f)
+    assert sa.rec64_slots > 0 and sa.rec64_short == 0 and sa.rec64_records > 0
+    r.set_precision(so.abi.SO_PREC_FP64, pool_mb=0.001)  # two segments: the rest is summed in place
+    b, _, sb = r.render(f)
+    assert sb.rec64_short > 0.9 * n * n * 2
+    assert np.array_equal(a, b)
+    assert sa.attempts == sb.attempts and sa.flow_steps == sb.flow_steps
+    acc, ys, lim, att = orc.orc_pass1(sh.scene, f, plasma=p, modes=modes, threads=_threads())
+    ref = acc / 2.0
+    assert ref[..., 0].max() > 0
+    assert np.abs(a - ref).max() <= 1e-6 * ref[..., 0].max()
+    assert sa.attempts == att
     r.close()
 
 

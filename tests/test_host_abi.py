@@ -297,22 +297,31 @@ def test_sky_file_roundtrip(so, tmp_path):
         so.sky_file(str(bad))
 
 
-REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+def _reference_root():
+    """Where the reference's sources were when oracle/Makefile built the checkers (it records the
+    REF_ROOT it was given in oracle/_ref/REF_ROOT); REF_ROOT in the environment takes precedence."""
+    if os.environ.get("REF_ROOT"):
+        return os.environ["REF_ROOT"]
+    try:
+        with open(os.path.join(ROOT, "oracle", "_ref", "REF_ROOT")) as fh:
+            return fh.read().strip()
+    except OSError:
+        return ""
+
+
+REF_ROOT = _reference_root()
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF_ROOT, "blackholes", "src")),
                     reason="needs the reference's headers (renderer.hpp, scene.hpp)")
 def test_integration_binding_builds_against_reference_headers(so, tmp_path):
-    """The C++ Renderer binding printed in INTEGRATION.md compiles against the reference's own
+    """The C++ Renderer binding (spacetime-optics_b200/bindings/renderer_b200.cpp) compiles against the reference's own
     renderer.hpp / scene.hpp (its static_asserts check SceneGPU / FrameGPU against so_scene /
     so_frame), links with every so_* call resolved by libso_tracer.so, and, driven like main.cpp
     drives Renderer::init, reports a failed init through its error string instead of aborting."""
     import subprocess
     so.lib()
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    blocks = re.findall(r"```cpp\n(.*?)```", text, flags=re.S)
-    assert len(blocks) == 1
-    (tmp_path / "renderer_b200.cpp").write_text(blocks[0])
+    binding = os.path.join(ROOT, "spacetime-optics_b200", "bindings", "renderer_b200.cpp")
     (tmp_path / "drive.cpp").write_text(
         '#include "renderer.hpp"\n'
         "int main() {\n"
@@ -325,7 +334,7 @@ def test_integration_binding_builds_against_reference_headers(so, tmp_path):
     cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
     cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", f"-I{ROOT}/include", f"-I{cuda}/include",
            f"-I{REF_ROOT}/common", f"-I{REF_ROOT}/blackholes/src", "-o", str(tmp_path / "drive"),
-           str(tmp_path / "drive.cpp"), str(tmp_path / "renderer_b200.cpp"), f"-L{pkg}", "-lso_tracer",
+           str(tmp_path / "drive.cpp"), binding, f"-L{pkg}", "-lso_tracer",
            f"-Wl,-rpath,{pkg}", "-Wl,--no-undefined"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -79,6 +79,22 @@ def test_shadow_rays_vs_reference(orc):
     assert (g["fate"] == -1).any() and (g["fate"] == 1).any() and (g["ncross"] > 1).any()
 
 
+def test_cos_turns_accuracy(orc):
+    """cos(2 pi t) of the FP64 torus turbulence sums (the oracle's restatement of the library's
+    cos_turns): within 3e-16 absolute (about 1.4 ulp of 1) of the 40-digit value, for phases over
+    the range the torus modes reach (|t| < 300 turns), near 0, on the quadrant boundaries, and large."""
+    import mpmath as mp
+    orc.oracle().orc_cos_turns.argtypes = [C.c_double]
+    orc.oracle().orc_cos_turns.restype = C.c_double
+    mp.mp.dps = 40
+    rng = np.random.default_rng(5)
+    ts = np.concatenate([rng.uniform(-300, 300, 3000), rng.uniform(-1, 1, 3000), np.arange(-4, 4.001, 1 / 64),
+                         [1e6 + 0.1, -123456.789, 2.0 ** 40 + 0.3, 1e-300, -0.0]])
+    worst = max(float(abs(mp.mpf(orc.oracle().orc_cos_turns(float(t))) - mp.cos(2 * mp.pi * mp.mpf(float(t)))))
+                for t in ts)
+    assert worst <= 3e-16, worst
+
+
 def test_shadow_full_grid_vs_reference(so, orc):
     """Config shadow_selftest_256 on every pixel of the 256^2 grid (65,536 rays) against the
     reference's own trace_ray: class and winding order identical on every ray, escape direction
