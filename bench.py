@@ -592,6 +592,16 @@ def run_surrogate(args, so, world, rank, local):
     roof = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
             "frac": round(achieved / peaks["bf16_tflops"], 4), "traffic": None, "kernel": "k_mlp_fused",
             "kernel_ms": rep.ms_mlp, "per_launch": flops, "peak_source": src + ", dense bf16 burst"}
+    # Trade-off: the image error falls only as more pixels go to the integrator (the network's radius
+    # error is spread evenly over the disk, so no per-pixel score singles out the bad pixels); the
+    # seeded audit share is raised until the frame is at 1e-3 and the speed-up at each point recorded
+    tradeoff = []
+    for frac in (0.1, 0.3, 0.6, 0.8, 0.9, 0.95):
+        im, rp, mss = timed(args.band, frac, 2)
+        b = im.cpu().numpy().astype(np.float64)
+        e = float(np.abs(b[..., 1] - ref[..., 1]).sum() / max(np.abs(ref[..., 1]).sum(), 1e-300))
+        tradeoff.append({"integrator_share": round((rp.band_rays + rp.audit_rays) / rp.rays, 4), "image_rel_l1": e,
+                         "ms": round(float(np.mean(mss)), 3), "speedup_vs_fp64": round(fp64_ms / float(np.mean(mss)), 3)})
     # e2e: the frame into host memory (descriptor in, 4 floats per pixel out)
     host = torch.empty((W, W, 4), dtype=torch.float32).pin_memory()
     e2e_ms = []
@@ -621,7 +631,8 @@ def run_surrogate(args, so, world, rank, local):
                                 "dataset_s": round(t_data, 2), "train_s": round(t_train, 2),
                                 "last_loss": last.total, "heldout_loss": held.total,
                                 "heldout_class_accuracy": held.accuracy},
-                   "l2": "256 MiB buffer written between timed steps", "frames_per_s": round(1e3 / ms_step * world, 3)},
+                   "l2": "256 MiB buffer written between timed steps", "frames_per_s": round(1e3 / ms_step * world, 3),
+                   "tradeoff_integrator_share": tradeoff},
         "roofline": roof,
         "e2e": {"value": round(world * npix / (e2e_step * 1e-3) / 1e6, 4), "unit": "Mrays/s",
                 "h2d_bytes_per_step": C.sizeof(so.abi.Frame), "d2h_bytes_per_step": W * W * 16},
@@ -674,7 +685,7 @@ def run_wavefront(args, so, world, rank, local):
     tune = b.autotune(small.data_ptr())
     b.close()
     b, _, scenes, frames, fs = wf.photon_ring_batch(so, r, W)
-    b.set_tune(tune.ctas_per_sm, tune.interleave)
+    b.set_tune(tune.ctas_per_sm, tune.interleave, tune.tile, tune.queue_chunk)
     out = torch.zeros((len(frames), W, W, 4), dtype=torch.float32, device="cuda")
     stream = torch.cuda.ExternalStream(r.stream())
     for _ in range(args.warmup):
@@ -722,7 +733,8 @@ def run_wavefront(args, so, world, rank, local):
         "config": {"workload": f"photon-ring batch: {len(frames)} frames of {W}x{W} (spins 0/0.5/0.9/0.99, "
                                "incl 17/60 deg, 8 turbulence times, zoom 1e3-4e4 on the critical curve), torus "
                                "plasma with 512 modes, one persistent launch replayed from a CUDA graph",
-                   "tune": {"ctas_per_sm": tune.ctas_per_sm, "interleave": tune.interleave, "tuned_on": "128x128"},
+                   "tune": {"ctas_per_sm": tune.ctas_per_sm, "interleave": tune.interleave, "tile": tune.tile,
+                            "queue_chunk": tune.queue_chunk, "tuned_on": "128x128"},
                    "frames_per_s": round(world * len(frames) / (ms_step * 1e-3), 4),
                    "attempts_per_ray": st.attempts / nrays, "flow_steps_per_ray": st.flow_steps / nrays,
                    "l2": "inputs (mode table, frame descriptors) are small; no flush (one step is seconds long)"},

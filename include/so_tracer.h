@@ -363,9 +363,12 @@ void so_destroy(so_renderer* r);
  * spin, so disk scenes must share a spin).  The plasma is the renderer's (so_set_plasma).  The launch
  * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed. */
 typedef struct so_batch so_batch;
-/* Launch shape of the batch: resident CTAs per SM of the persistent grid (0 = as many as fit), and
- * the job order (0 = frame after frame, 1 = frames interleaved ray by ray). */
-typedef struct so_tune { int ctas_per_sm; int interleave; double ms; } so_tune;
+/* Launch shape of the batch: resident CTAs per SM of the persistent grid (0 = as many as fit); the
+ * job order (0 = frame after frame, 1 = frames interleaved in tiles of `tile` consecutive pixels,
+ * tile <= 1 meaning ray by ray; a tile that does not divide W * H is lowered to the largest power of
+ * two that does); and the queue chunk, the consecutive jobs a lane takes per grab from the shared
+ * queue (<= 1: one).  None of them changes any ray's result.  ms: the batch time the tuner measured. */
+typedef struct so_tune { int ctas_per_sm; int interleave; double ms; int tile; int queue_chunk; } so_tune;
 int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const so_frame* frames,
                     const int* frame_scene, int nframes, int W, int H, int spp, so_batch** out);
 /* Traces the batch into d_px (device memory, nframes * W * H * 4 floats, frame after frame) by

@@ -352,8 +352,8 @@ class Batch:
         _check(lib().so_batch_autotune(self.h, C.c_void_p(d_px), C.byref(t)), self.r.h)
         return t
 
-    def set_tune(self, ctas_per_sm, interleave):
-        t = abi.Tune(ctas_per_sm, interleave, 0.0)
+    def set_tune(self, ctas_per_sm, interleave, tile=1, queue_chunk=1):
+        t = abi.Tune(ctas_per_sm, interleave, 0.0, tile, queue_chunk)
         _check(lib().so_batch_set_tune(self.h, C.byref(t)), self.r.h)
 
     def close(self):

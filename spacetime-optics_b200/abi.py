@@ -117,7 +117,8 @@ class MixedOpts(C.Structure):
 
 
 class Tune(C.Structure):
-    _fields_ = [("ctas_per_sm", C.c_int), ("interleave", C.c_int), ("ms", C.c_double)]
+    _fields_ = [("ctas_per_sm", C.c_int), ("interleave", C.c_int), ("ms", C.c_double), ("tile", C.c_int),
+                ("queue_chunk", C.c_int)]
 
 
 class SurRay(C.Structure):

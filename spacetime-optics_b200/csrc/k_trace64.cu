@@ -386,16 +386,28 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
         }
     };
 
+    // Queue grabs: a lane takes `qchunk` consecutive jobs per grab (one atomic per warp for all its
+    // grabbing lanes) and works through them before grabbing again.
+    const int qchunk = L.queue_chunk > 1 ? L.queue_chunk : 1;
+    int chunk_left = 0;
     for (;;) {
         const bool need = !active && !exhausted && (lane & (stride - 1)) == 0;
-        const unsigned m = __ballot_sync(FULL, need);
+        const bool grab = need && chunk_left == 0;
+        const unsigned m = __ballot_sync(FULL, grab);
+        unsigned long long j = (unsigned long long)job + 1;  // the next job of the lane's grab
         if (m) {
             const int leader = __ffs(m) - 1;
             unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(&L.counters->next, (unsigned long long)__popc(m));
+            if (lane == leader) base = atomicAdd(&L.counters->next, (unsigned long long)qchunk * __popc(m));
             base = __shfl_sync(FULL, base, leader);
-            if (need) {
-                const unsigned long long j = base + __popc(m & ((1u << lane) - 1u));
+            if (grab) {
+                j = base + (unsigned long long)qchunk * __popc(m & ((1u << lane) - 1u));
+                chunk_left = qchunk;
+            }
+        }
+        if (need) {
+            --chunk_left;
+            {
                 if (j >= (unsigned long long)total) {
                     exhausted = true;
                 } else {
@@ -418,10 +430,13 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
                     } else if (L.kind == RAYS_PIXELS) {
                         const long long npix = (long long)L.W * L.H;
                         if (L.interleave && L.nframes > 1) {
-                            // consecutive jobs cycle through the frames: cheap and expensive frames
-                            // (different spins, zooms) mix in every warp instead of queueing up
-                            fidx = (int)(job % L.nframes);
-                            pix = job / L.nframes;
+                            // consecutive tiles of `tile` pixels cycle through the frames: cheap and
+                            // expensive frames (different spins, zooms) mix in every warp instead of
+                            // queueing up (the host keeps tile a divisor of W * H)
+                            const long long T = L.tile > 1 ? L.tile : 1;
+                            const long long t = job / T;
+                            fidx = (int)(t % L.nframes);
+                            pix = (t / L.nframes) * T + job % T;
                         } else {
                             fidx = (int)(job / npix);
                             pix = job % npix;

@@ -128,7 +128,9 @@ struct TraceLaunch {
                               // (W + 1) x (H + 1), for the footprint of each pixel (NULL: no sky)
     float sky_grad_scale;     // footprint scale: 0.7 in pass 1, 0.5 in pass 2 (render.cu:102, 214)
     // batched frames (RAYS_PIXELS over nframes)
-    int interleave;           // 0: job -> (frame = job / npix), 1: job -> (frame = job % nframes)
+    int interleave;           // 0: job -> (frame = job / npix), 1: tiles of `tile` pixels cycle through the frames
+    int tile;                 // interleave: consecutive pixels of one frame per tile (a divisor of W * H; <= 1: 1)
+    int queue_chunk;          // consecutive jobs a lane takes per queue grab (<= 1: 1)
     int list_frames;          // RAYS_LIST: > 0 = ray i belongs to frame i % list_frames (else frame 0)
     int ctas_per_sm;          // persistent grid: CTAs per SM (0 = as many as fit)
     int emit32;               // FP64 tracer: torus turbulence sums in FP32 (geometry stays FP64)

@@ -1545,11 +1545,11 @@ struct so_batch {
     so_frame* d_frames = nullptr;
     int* d_frame_scene = nullptr;
     Counters* d_cnt = nullptr;
-    so_tune tune{0, 1, 0.0};
+    so_tune tune{0, 1, 0.0, 1, 1};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     float* graph_px = nullptr;  // output buffer baked into the graph
-    so_tune graph_tune{-1, -1, 0.0};
+    so_tune graph_tune{-1, -1, 0.0, -1, -1};
 };
 
 namespace {
@@ -1560,6 +1560,23 @@ void batch_drop_graph(so_batch* b) {
     b->gexec = nullptr;
     b->graph = nullptr;
     b->graph_px = nullptr;
+}
+
+// Pixels per interleaved tile: the requested tile, lowered to the largest power of two that divides
+// W * H when it does not divide it itself (so no tile runs past a frame's end).
+int batch_tile(const so_batch* b) {
+    const long long npix = (long long)b->W * b->H;
+    long long t = std::max(1, b->tune.tile);
+    if (npix % t != 0) {
+        t = 1;
+        while (t * 2 <= std::max(1, b->tune.tile) && npix % (t * 2) == 0) t *= 2;
+    }
+    return (int)t;
+}
+
+bool same_tune(const so_tune& a, const so_tune& b) {
+    return a.ctas_per_sm == b.ctas_per_sm && a.interleave == b.interleave && a.tile == b.tile &&
+           a.queue_chunk == b.queue_chunk;
 }
 
 // The launch sequence of one batch: counter reset, persistent tracer over all frames, resolve.
@@ -1581,6 +1598,8 @@ int batch_enqueue(so_batch* b, float* d_px) {
     L.nrays = (long long)b->W * b->H * b->nframes;
     L.accum = d_px;
     L.interleave = b->tune.interleave;
+    L.tile = batch_tile(b);
+    L.queue_chunk = std::max(1, b->tune.queue_chunk);
     L.ctas_per_sm = b->tune.ctas_per_sm;
     // mixed precision on a batch: FP64 geometry everywhere (photon-ring windows lie in the critical
     // band), FP32 turbulence sums
@@ -1676,8 +1695,7 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
     if (!b || !d_px) return SO_ERR_ARG;
     so_renderer* r = b->r;
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
-    if (!b->gexec || b->graph_px != d_px || b->graph_tune.ctas_per_sm != b->tune.ctas_per_sm ||
-        b->graph_tune.interleave != b->tune.interleave) {
+    if (!b->gexec || b->graph_px != d_px || !same_tune(b->graph_tune, b->tune)) {
         int rc = batch_capture(b, d_px);
         if (rc) return rc;
     }
@@ -1716,9 +1734,13 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
 }
 
 int so_batch_set_tune(so_batch* b, const so_tune* t) {
-    if (!b || !t || t->ctas_per_sm < 0 || (t->interleave != 0 && t->interleave != 1)) return SO_ERR_ARG;
+    if (!b || !t || t->ctas_per_sm < 0 || (t->interleave != 0 && t->interleave != 1) || t->tile < 0 ||
+        t->queue_chunk < 0 || t->queue_chunk > 64)
+        return SO_ERR_ARG;
     b->tune.ctas_per_sm = t->ctas_per_sm;
     b->tune.interleave = t->interleave;
+    b->tune.tile = std::max(1, t->tile);
+    b->tune.queue_chunk = std::max(1, t->queue_chunk);
     return SO_OK;
 }
 
@@ -1735,18 +1757,37 @@ int so_batch_autotune(so_batch* b, float* d_px, so_tune* best) {
         if (rc) return rc;
         b->tune = keep;
     }
-    so_tune winner{0, 1, 1e300};
+    double ms = 0.0;
+    auto trial = [&](so_tune t, so_tune* win) -> int {
+        b->tune = t;
+        so_stats st;
+        int rc = so_batch_render(b, d_px, &st);
+        if (rc) return rc;
+        ms = t.ms = st.ms_kernel;
+        if (t.ms < win->ms) *win = t;
+        return SO_OK;
+    };
+    // 1. CTAs per SM x job order (ray by ray, one job per grab)
+    so_tune winner{0, 1, 1e300, 1, 1};
     for (int inter = 0; inter <= 1; ++inter) {
         for (int c = 1; c <= per_sm; ++c) {
-            so_tune t{c, inter, 0.0};
-            b->tune = t;
-            so_stats st;
-            int rc = so_batch_render(b, d_px, &st);
-            if (rc) return rc;
-            if (st.ms_kernel < winner.ms) winner = {c, inter, st.ms_kernel};
+            if (int rc = trial(so_tune{c, inter, 0.0, 1, 1}, &winner)) return rc;
             // a larger cap than the occupancy limit launches the same grid: stop early
-            if (c >= 2 && st.ms_kernel > 1.5 * winner.ms) break;
+            if (c >= 2 && ms > 1.5 * winner.ms) break;
         }
+    }
+    // 2. tile of the interleaved order, 3. queue chunk, each around the winner so far
+    if (winner.interleave) {
+        for (int tile : {32, 1024}) {
+            so_tune t = winner;
+            t.tile = tile;
+            if (int rc = trial(t, &winner)) return rc;
+        }
+    }
+    for (int chunk : {2, 4}) {
+        so_tune t = winner;
+        t.queue_chunk = chunk;
+        if (int rc = trial(t, &winner)) return rc;
     }
     b->tune = winner;
     if (best) *best = winner;

@@ -41,21 +41,23 @@ def test_batch_matches_single_frames(so):
     assert ref[..., 0].max() > 0
     b = so.Batch(r, scenes, frames, fs, W, W, 1)
     out = torch.zeros((len(frames), W, W, 4), dtype=torch.float32, device="cuda")
-    for inter in (0, 1):
-        for ctas in (0, 1):
-            b.set_tune(ctas, inter)
-            out.zero_()
-            st = b.render(out.data_ptr(), stats=True)
-            torch.cuda.synchronize()
-            assert np.array_equal(out.cpu().numpy(), ref), (inter, ctas)
-            assert st.samples == len(frames) * W * W and st.attempts > 0
+    # launch shapes, job orders, interleave tiles (1024 does not divide 24 x 24: lowered to 64) and
+    # queue chunks change which lane traces which ray, never a ray's result
+    for inter, ctas, tile, chunk in ((0, 0, 1, 1), (0, 1, 1, 1), (1, 0, 1, 1), (1, 1, 1, 1), (1, 0, 32, 1),
+                                     (1, 0, 1024, 3), (0, 2, 1, 4)):
+        b.set_tune(ctas, inter, tile, chunk)
+        out.zero_()
+        st = b.render(out.data_ptr(), stats=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), ref), (inter, ctas, tile, chunk)
+        assert st.samples == len(frames) * W * W and st.attempts > 0
     # graph replay without stats (asynchronous) gives the same again
     out.zero_()
     b.render(out.data_ptr())
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), ref)
     t = b.autotune(out.data_ptr())
-    assert t.ctas_per_sm >= 1 and t.interleave in (0, 1) and t.ms > 0
+    assert t.ctas_per_sm >= 1 and t.interleave in (0, 1) and t.ms > 0 and t.tile >= 1 and t.queue_chunk >= 1
     out.zero_()
     b.render(out.data_ptr())
     torch.cuda.synchronize()
