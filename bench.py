@@ -301,8 +301,10 @@ def run_ours(args, so, world, rank, local):
     del host
     # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, [turbulence sums,
     # transfer,] re-trace, gather, resolve (mixed); spp_max = spp, so no adaptive pass
-    # (plain FP64 with deferred torus sums: recording pass, sums, replay pass, resolve)
-    gpu_launches = args.steps * (((4 if st.rec64_slots else 2) if path == "fp64" else 9 if st.ms_turb > 0 else 7) +
+    # (plain FP64 with deferred torus sums: recording pass, sums, emission, ordered transfer, the
+    # replay pass that returns at once, resolve; or recording pass, sums, replay pass, resolve)
+    plain_launches = (6 if st.emit64 else 4) if st.rec64_slots else 2
+    gpu_launches = args.steps * ((plain_launches if path == "fp64" else 9 if st.ms_turb > 0 else 7) +
                                  (1 if flow else 0))
     if flow:
         workload = (f"reference flow {W}x{W} (n ~ r^-1.1, fBm turbulence baked per frame into 24 slices of "
@@ -341,13 +343,17 @@ def run_ours(args, so, world, rank, local):
 def plain_fp64_record(so, sh, st, ms, ms_frame, clocks, npix, world, local):
     """The plain FP64 path's frames: rate, phase times and rooflines against the measured FP64 FMA
     peak.  With the deferred torus turbulence the frame is recording pass + k_turb64_records +
-    replay pass; the sums kernel is the dominant one, its algorithmic FLOPs are the recorded
-    positions x modes x FLOPS_MODE."""
+    k_emit64_records + k_transfer64 (or a replay pass instead of the last two); the sums kernel is
+    the dominant one, its algorithmic FLOPs are the recorded positions x modes x FLOPS_MODE."""
     fp64_peak, _ = so.probe_fma_peak(local)
     pl = sh.plasma()
     n_modes = pl.n_modes if pl is not None else 0
     flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT + st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
-    whole = {"kernels": "k_trace64 (recording + replay passes) + k_turb64_records" if st.rec64_slots else "k_trace64",
+    kernels = "k_trace64"
+    if st.rec64_slots:
+        kernels = ("k_trace64 (recording pass) + k_turb64_records + k_emit64_records + k_transfer64" if st.emit64
+                   else "k_trace64 (recording + replay passes) + k_turb64_records")
+    whole = {"kernels": kernels,
              "ms": round(st.ms_kernel, 3), "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
              "unit": "TFLOP/s", "per_launch": flops}
     rec = {"bound": "fp64", "kernel": "k_trace64", "achieved": whole["achieved"], "peak": round(fp64_peak, 3),
@@ -356,14 +362,15 @@ def plain_fp64_record(so, sh, st, ms, ms_frame, clocks, npix, world, local):
         sflops = st.rec64_records * n_modes * FLOPS_MODE
         rec = {"bound": "fp64", "kernel": "k_turb64_records", "achieved": round(sflops / (st.ms_sum64 * 1e-3) / 1e12, 3),
                "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel_ms": round(st.ms_sum64, 3), "per_launch": sflops,
-               "records": st.rec64_records, "slots_summed": st.rec64_slots, "jobs_summed_in_tracer": st.rec64_short,
+               "records": st.rec64_records, "slots_summed": st.rec64_slots, "samples_summed_in_tracer": st.rec64_short,
                "traffic": None, "algorithmic_bytes": 32 * st.rec64_records}
     rec["frac"] = round(rec["achieved"] / rec["peak"], 4)
     rec["peak_source"] = "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"
     return {"mrays_s": round(world * npix / (ms_frame * 1e-3) / 1e6, 4), "ms_per_frame": round(ms_frame, 3),
             "frames": len(ms), "ms_frames": [round(x, 3) for x in ms], "clocks": clocks,
             "phases_ms": {"recording_pass": round(st.ms_rec64, 3), "turbulence_sums": round(st.ms_sum64, 3),
-                          "replay_pass": round(st.ms_replay64, 3)},
+                          "emission_and_transfer": round(st.ms_emit64, 3), "replay_pass": round(st.ms_replay64, 3)},
+            "deferred_emission": bool(st.emit64),
             "roofline": rec, "whole_frame": whole}
 
 

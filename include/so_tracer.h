@@ -177,10 +177,14 @@ typedef struct so_stats {
     long long record_waves; /* ... waves the FP32 rays were traced in (the pool holds one wave's records) */
     double ms_rec64;      /* plain FP64, deferred torus turbulence: device time of the recording pass */
     double ms_sum64;      /* ... of the FP64 turbulence sums over all records (k_turb64_records) */
-    double ms_replay64;   /* ... of the replay pass (geodesic again, sums read back, emission) */
+    double ms_replay64;   /* ... of the replay pass (geodesic again, sums read back, emission); with
+                             deferred emission it runs only when the record pool ran out */
     long long rec64_slots; /* ... record slots summed (segments taken x 16) */
-    long long rec64_short; /* ... jobs summed in the tracer because the record pool ran out */
+    long long rec64_short; /* ... samples summed in the tracer because the record pool ran out */
     long long rec64_records; /* ... records written (flow steps that needed a sum, up to each ray's end) */
+    double ms_emit64;     /* ... deferred emission: device time of the emission at every record and the
+                             ordered transfer (0 when the replay pass does the emission) */
+    int emit64;           /* ... 1 = the last trace deferred its emission too, 0 = replay pass */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */
@@ -329,13 +333,15 @@ int so_sky_file(const char* path, int* w, int* h, float* scale, uint16_t* data);
 /* Flow turbulence of the reference plasma model (radio mode, flow.turbulence > 0).
  * SO_FLOW_NOISE_BAKED (so_init's choice, as Renderer::init's, render.cu:594-620): before every
  * trace of a frame its turbulence is baked into 24 retarded-time slices of 512 x 192 x 48 density
- * factors on (phi, ln R, z/R) (453 MB of device memory, render.cu:449-460, 679-682) and each flow
- * step interpolates them trilinearly and in time (emission.cuh:112-124; here in FP32 arithmetic from
- * plain device memory where the reference fetches through the texture unit, whose weights have 8
- * fractional bits).  SO_FLOW_NOISE_INLINE evaluates the sheared fBm noise at every flow step (the
- * reference's turb_nt = 0 path) and frees the slices.  No effect on other plasma models.  The
- * batched frames (so_batch_*) and so_radio_flux_noalloc always evaluate the noise in place. */
-enum { SO_FLOW_NOISE_BAKED = 0, SO_FLOW_NOISE_INLINE = 1 };
+ * factors on (phi, ln R, z/R) (453 MB of device memory, render.cu:449-460, 679-682) held as 3-D
+ * arrays, and each flow step reads two of them through the texture unit with the reference's sampler
+ * and interpolates in time (emission.cuh:112-124): the reference's own fetch, trilinear weights with 8
+ * fractional bits.  SO_FLOW_NOISE_BAKED_FP32 keeps the slices in plain device memory and
+ * interpolates them in FP32 with a fixed operation order, which the CPU oracle repeats exactly.
+ * SO_FLOW_NOISE_INLINE evaluates the sheared fBm noise at every flow step (the reference's
+ * turb_nt = 0 path) and frees the slices.  No effect on other plasma models.  The batched frames
+ * (so_batch_*) and so_radio_flux_noalloc always evaluate the noise in place. */
+enum { SO_FLOW_NOISE_BAKED = 0, SO_FLOW_NOISE_INLINE = 1, SO_FLOW_NOISE_BAKED_FP32 = 2 };
 int so_set_flow_noise(so_renderer* r, int mode);
 
 /* Precision and plasma extensions (no reference counterpart: the reference has one FP64 path and

@@ -251,7 +251,8 @@ class Renderer:
         _check(lib().so_set_sky(self.h, t.shape[1], t.shape[0], t.ctypes.data_as(C.c_void_p)), self.h)
 
     def set_flow_noise(self, mode):
-        """Reference flow turbulence: abi.SO_FLOW_NOISE_BAKED (default) or abi.SO_FLOW_NOISE_INLINE."""
+        """Reference flow turbulence: abi.SO_FLOW_NOISE_BAKED (default: baked slices through the texture
+        unit), abi.SO_FLOW_NOISE_BAKED_FP32 (baked, FP32 trilinear as the oracle) or abi.SO_FLOW_NOISE_INLINE."""
         _check(lib().so_set_flow_noise(self.h, mode), self.h)
 
     def set_plasma(self, plasma, modes=None):

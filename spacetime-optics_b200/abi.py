@@ -13,7 +13,7 @@ SO_MODE_VISIBLE, SO_MODE_RADIO = 0, 1
 SO_FATE_LIMIT, SO_FATE_ESCAPED, SO_FATE_CAPTURED = 0, 1, -1
 SO_PREC_FP64, SO_PREC_MIXED = 0, 1
 SO_PLASMA_REFERENCE, SO_PLASMA_TORUS = 0, 1
-SO_FLOW_NOISE_BAKED, SO_FLOW_NOISE_INLINE = 0, 1
+SO_FLOW_NOISE_BAKED, SO_FLOW_NOISE_INLINE, SO_FLOW_NOISE_BAKED_FP32 = 0, 1, 2
 SO_MAX_MODES = 1024
 
 
@@ -89,7 +89,8 @@ class Stats(C.Structure):
                 ("redo_limit", C.c_longlong), ("ms_fp32_trace", C.c_double), ("ms_turb", C.c_double),
                 ("turb_records", C.c_longlong), ("redo_records", C.c_longlong), ("record_waves", C.c_longlong),
                 ("ms_rec64", C.c_double), ("ms_sum64", C.c_double), ("ms_replay64", C.c_double),
-                ("rec64_slots", C.c_longlong), ("rec64_short", C.c_longlong), ("rec64_records", C.c_longlong)]
+                ("rec64_slots", C.c_longlong), ("rec64_short", C.c_longlong), ("rec64_records", C.c_longlong),
+                ("ms_emit64", C.c_double), ("emit64", C.c_int)]
 
 
 class RaysOut(C.Structure):

@@ -47,6 +47,54 @@ __device__ __forceinline__ void pixel_point(const TraceLaunch& L, const so_frame
     sample_point(L.W, L.H, L.jitter, F, q, s, x, yv);
 }
 
+// Where a job of the launch lands: its frame, pixel, first sample and number of samples.
+struct JobPlace {
+    long long pix;
+    int fidx, sbase, jobs_n;
+};
+__device__ __forceinline__ JobPlace job_place(const TraceLaunch& L, long long job) {
+    JobPlace q;
+    q.pix = 0;
+    q.fidx = 0;
+    q.sbase = 0;
+    q.jobs_n = 1;
+    if (L.kind == RAYS_LIST) {
+        q.fidx = L.list_frames > 0 ? (int)(job % L.list_frames) : 0;
+    } else if (L.kind == RAYS_SAMPLES) {
+        const long long sid = (long long)__ldg(L.list + job);
+        q.pix = sid / L.spp;
+        q.sbase = (int)(sid % L.spp);
+    } else if (L.kind == RAYS_PIXELS) {
+        const long long npix = (long long)L.W * L.H;
+        if (L.interleave && L.nframes > 1) {
+            // consecutive tiles of `tile` pixels cycle through the frames: cheap and expensive frames
+            // (different spins, zooms) mix in every warp instead of queueing up (the host keeps tile
+            // a divisor of W * H)
+            const long long T = L.tile > 1 ? L.tile : 1;
+            const long long t = job / T;
+            q.fidx = (int)(t % L.nframes);
+            q.pix = (t / L.nframes) * T + job % T;
+        } else {
+            q.fidx = (int)(job / npix);
+            q.pix = job % npix;
+        }
+        q.sbase = L.sample0;
+        q.jobs_n = L.spp;
+    } else {
+        // upper bound of job in the exclusive scan: the pixel owning chunk `job`
+        long long lo = 0, hi = (long long)L.W * L.H;
+        while (lo < hi) {
+            long long mid = (lo + hi) >> 1;
+            if ((long long)__ldg(L.offsets + mid) <= job) lo = mid + 1;
+            else hi = mid;
+        }
+        q.pix = lo - 1;
+        q.sbase = L.sample0 + (int)(job - (long long)__ldg(L.offsets + q.pix)) * L.chunk;
+        q.jobs_n = L.chunk;
+    }
+    return q;
+}
+
 template <int VAR>
 __device__ __forceinline__ void ray_init(Ray64& R, const so_scene& S, const so_frame& F, double x, double yv) {
     so_vec3 d = view_dir(F, x, yv);
@@ -164,20 +212,22 @@ __device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const so_
                                           const TorusParams& tp, double delta, bool emit,
                                           const double* yn, const double* k7, double hc, double err, int* fate,
                                           double* th, double* ph) {
-    if (VAR == VAR_RADIO && emit && S.flow_on && yn[0] < S.r_flow_max) {
-        double dI, dtau;
-        flow_step(S, F, field, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+    if (VAR == VAR_RADIO && S.flow_on && yn[0] < S.r_flow_max) {
         ++R.nflow;
-        float cc = (float)(R.trans * dI);
-        int n = (int)(R.psi * (1.0 / PI));
-        R.acc[0] += cc;
-        if (n == 1) R.acc[1] += cc;
-        else if (n == 2) R.acc[2] += cc;
-        else if (n >= 3) R.acc[3] += cc;
-        R.trans *= exp(-dtau);
-        if (R.trans < 1e-5) {
-            *fate = -1;
-            return 1;
+        if (emit) {
+            double dI, dtau;
+            flow_step(S, F, field, tp, delta, yn[0], yn[2], yn[4], yn[5], R.c.lam, R.c.E, hc, &dI, &dtau);
+            float cc = (float)(R.trans * dI);
+            int n = (int)(R.psi * (1.0 / PI));
+            R.acc[0] += cc;
+            if (n == 1) R.acc[1] += cc;
+            else if (n == 2) R.acc[2] += cc;
+            else if (n >= 3) R.acc[3] += cc;
+            R.trans *= exp(-dtau);
+            if (R.trans < 1e-5) {
+                *fate = -1;
+                return 1;
+            }
         }
     }
 #pragma unroll
@@ -206,26 +256,27 @@ __device__ __forceinline__ int ray_commit(Ray64& R, const so_scene& S, const so_
 // order.  Every mode read from shared memory feeds four independent branch-free cosines (cos_turns),
 // so the FP64 pipe has independent work while each chain waits on its previous operation.  All 32
 // lanes must call this.
-__device__ __forceinline__ void warp_sums4(const ModesSmem& md, int n, const double* px, const double* py,
-                                           const double* pz, double* acc) {
+template <int P>
+__device__ __forceinline__ void warp_sums(const ModesSmem& md, int n, const double* px, const double* py,
+                                          const double* pz, double* acc) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[j] = 0.0;
+    for (int j = 0; j < P; ++j) acc[j] = 0.0;
 #pragma unroll 1
     for (int i = lane; i < n; i += 32) {
         const double kx = md.kx[i], ky = md.ky[i], kz = md.kz[i], p0 = md.ph[i], w = md.amp[i];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < P; ++j)
             acc[j] = fma(w, cos_turns(fma(kz, pz[j], fma(ky, py[j], fma(kx, px[j], p0)))), acc[j]);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[j] += __shfl_xor_sync(FULL, acc[j], o);
+        for (int j = 0; j < P; ++j) acc[j] += __shfl_xor_sync(FULL, acc[j], o);
     }
 }
 
-// The sums of the lanes in `want` (at their own X, Y, Z), four lanes' positions per warp_sums4 pass.
+// The sums of the lanes in `want` (at their own X, Y, Z), four lanes' positions per warp_sums pass.
 // All 32 lanes must call this; it returns at once when no lane wants a sum.
 __device__ __forceinline__ double warp_turbulence64(const ModesSmem& md, int n, bool want, double X, double Y,
                                                     double Z) {
@@ -246,7 +297,7 @@ __device__ __forceinline__ double warp_turbulence64(const ModesSmem& md, int n, 
             py[j] = __shfl_sync(FULL, Y, src[j]);
             pz[j] = __shfl_sync(FULL, Z, src[j]);
         }
-        warp_sums4(md, n, px, py, pz, acc);
+        warp_sums<4>(md, n, px, py, pz, acc);
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (lane == src[j]) mine = acc[j];
@@ -312,12 +363,17 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // against the compiler's free choice (194 registers, two CTAs): the plain FP64 synchrotron frame
 // runs 1.29x faster with a few spilled registers and 50 % more warps.
 // DEFER (deferred FP64 torus turbulence, radio torus only): 0 = sums in the tracer, 1 = recording pass
-// (geometry only: no emission code, so fewer registers and four CTAs per SM), 2 = replay pass.
+// (geometry only: no emission code), 2 = replay pass.  Both passes run four CTAs per SM (128
+// registers): measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against
+// 205 ms at three CTAs (168 registers, fewer spills); the recording pass 58 against 62 ms.
 template <int VAR, bool EMIT32, int DEFER>
-__global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const TraceLaunch L) {
+__global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const TraceLaunch L) {
     extern __shared__ double smem[];
     constexpr int defer = (VAR == VAR_RADIO && !EMIT32) ? DEFER : 0;
     constexpr bool emit = defer != 1;
+    // the replay pass behind the deferred emission runs only when the recording pass left samples
+    // without records (the same value for every thread: the whole grid returns)
+    if (defer == 2 && L.replay_if_short && *(volatile unsigned long long*)&L.rec64_ctl[1] == 0ull) return;
     TorusParams tp;
     tp.on = VAR == VAR_RADIO && L.torus;
     tp.n_modes = tp.on ? L.n_modes : 0;
@@ -364,10 +420,10 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
     const so_frame* F = nullptr;
     const bool radio_lum = VAR == VAR_RADIO;  // sample_lum, render.cu:87
     const bool rec = L.kind == RAYS_LIST && L.record_cross;
-    // deferred FP64 turbulence: the lane's place in its job's record chain (segment, slots used in it,
-    // first segment) and whether the job's sums are in place (pass 1: the pool ran out; pass 2: the
-    // job's records are incomplete)
-    int rseg = -1, rcnt = REC_SEG, rhead = -1;
+    // deferred FP64 turbulence: the lane's place in its sample's record chain (segment, slots used in
+    // it, first segment, records so far) and whether the sample's sums are in place (pass 1: the pool
+    // ran out; pass 2: the sample's records are incomplete)
+    int rseg = -1, rcnt = REC_SEG, rhead = -1, rtot = 0;
     bool rinline = false;
     long long job = 0, pix = 0;
     int sample = 0, fidx = 0, sbase = 0, jobs_n = 1;
@@ -377,6 +433,7 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
         if (defer == 1) {
             rseg = rhead = -1;
             rcnt = REC_SEG;  // the first record opens a segment
+            rtot = 0;
             rinline = false;
         } else {
             rhead = L.job_head64[job * jobs_n + s];
@@ -414,49 +471,17 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
                     job = (long long)j;
                     active = true;
                     sample = 0;
+                    const JobPlace q = job_place(L, job);
+                    fidx = q.fidx;
+                    pix = q.pix;
+                    sbase = q.sbase;
+                    jobs_n = q.jobs_n;
                     double x, yv;
                     if (L.kind == RAYS_LIST) {
-                        fidx = L.list_frames > 0 ? (int)(job % L.list_frames) : 0;
                         x = L.x[job];
                         yv = L.y[job];
-                        jobs_n = 1;
-                    } else if (L.kind == RAYS_SAMPLES) {
-                        const long long sid = (long long)__ldg(L.list + job);
-                        fidx = 0;
-                        pix = sid / L.spp;
-                        sbase = (int)(sid % L.spp);
-                        jobs_n = 1;
-                        pixel_point(L, L.frames[0], pix, sbase, &x, &yv);
-                    } else if (L.kind == RAYS_PIXELS) {
-                        const long long npix = (long long)L.W * L.H;
-                        if (L.interleave && L.nframes > 1) {
-                            // consecutive tiles of `tile` pixels cycle through the frames: cheap and
-                            // expensive frames (different spins, zooms) mix in every warp instead of
-                            // queueing up (the host keeps tile a divisor of W * H)
-                            const long long T = L.tile > 1 ? L.tile : 1;
-                            const long long t = job / T;
-                            fidx = (int)(t % L.nframes);
-                            pix = (t / L.nframes) * T + job % T;
-                        } else {
-                            fidx = (int)(job / npix);
-                            pix = job % npix;
-                        }
-                        sbase = L.sample0;
-                        jobs_n = L.spp;
-                        pixel_point(L, L.frames[fidx], pix, sbase, &x, &yv);
                     } else {
-                        // upper bound of job in the exclusive scan: the pixel owning chunk `job`
-                        long long lo = 0, hi = (long long)L.W * L.H;
-                        while (lo < hi) {
-                            long long mid = (lo + hi) >> 1;
-                            if ((long long)__ldg(L.offsets + mid) <= job) lo = mid + 1;
-                            else hi = mid;
-                        }
-                        fidx = 0;
-                        pix = lo - 1;
-                        sbase = L.sample0 + (int)(job - (long long)__ldg(L.offsets + pix)) * L.chunk;
-                        jobs_n = L.chunk;
-                        pixel_point(L, L.frames[0], pix, sbase, &x, &yv);
+                        pixel_point(L, L.frames[fidx], pix, sbase, &x, &yv);
                     }
                     S = &L.scenes[L.frame_scene[fidx]];
                     F = &L.frames[fidx];
@@ -474,11 +499,15 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
         int fate = 0, stage = ST_REJECTED;
         double yn[6], k7[6], hc = 0.0, err = 0.0;
         bool want = false;
-        double TX = 0.0, TY = 0.0, TZ = 0.0;
+        double TX = 0.0, TY = 0.0, TZ = 0.0;  // the sum's position (recording / replay pass: TX = azimuth)
         if (active) {
             stage = ray_attempt<VAR>(R, *S, emit, yn, k7, &hc, &err, &fate, rec ? cr : nullptr, cg);
-            if (VAR == VAR_RADIO && stage == ST_ACCEPTED && S->flow_on && yn[0] < S->r_flow_max)
-                want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
+            if (VAR == VAR_RADIO && stage == ST_ACCEPTED && S->flow_on && yn[0] < S->r_flow_max) {
+                if (defer == 1 || (defer == 2 && !rinline))
+                    want = torus_phase(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX);
+                else
+                    want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
+            }
         }
         // ---- all lanes: turbulence sums --------------------------------------------------------
         double delta = 0.0;
@@ -486,9 +515,9 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
             if (EMIT32) {
                 delta = warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ);
             } else if (defer == 1) {
-                // recording pass: append (X, Y, Z) to the job's chain; a lane whose segment is full
-                // takes the next one (one atomic per warp); a job the pool cannot hold is summed in
-                // place by the replay pass
+                // recording pass: append the step (r, u, azimuth, h, tag) to the sample's chain; a
+                // lane whose segment is full closes it and takes the next one (one atomic per warp);
+                // a sample the pool cannot hold is summed in place by the replay pass
                 const bool need_seg = want && !rinline && rcnt == REC_SEG;
                 const unsigned ms = __ballot_sync(FULL, need_seg);
                 if (ms) {
@@ -498,6 +527,8 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
                     base = __shfl_sync(FULL, base, leader);
                     if (need_seg) {
                         const unsigned long long idx = base + __popc(ms & ((1u << lane) - 1u));
+                        if (rseg >= 0)
+                            L.seg_meta64[rseg] = make_uint2((uint32_t)(job * jobs_n + sample), (uint32_t)REC_SEG);
                         if (idx >= (unsigned long long)L.seg_cap64) {
                             rinline = true;
                         } else {
@@ -509,11 +540,20 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
                     }
                 }
                 if (want && !rinline) {
-                    double* slot = L.rec64 + 4 * ((long long)rseg * REC_SEG + rcnt);
-                    slot[0] = TX;
-                    slot[1] = TY;
-                    slot[2] = TZ;
+                    // image-order bucket as ray_commit forms it, counts after this step
+                    const int b = (int)(R.psi * (1.0 / PI));
+                    const unsigned long long tag =
+                        (unsigned long long)(b >= 3 ? 3 : (b < 0 ? 0 : b)) | ((unsigned long long)R.natt << 2) |
+                        ((unsigned long long)R.nacc << (2 + REC64_COUNT_BITS)) |
+                        ((unsigned long long)(R.nflow + 1) << (2 + 2 * REC64_COUNT_BITS));
+                    double* slot = L.rec64 + REC64_W * ((long long)rseg * REC_SEG + rcnt);
+                    slot[0] = yn[0];
+                    slot[1] = yn[2];
+                    slot[2] = TX;
+                    slot[3] = hc;
+                    slot[4] = __longlong_as_double((long long)tag);
                     ++rcnt;
+                    ++rtot;
                     ++n_rec;
                 }
             } else {
@@ -527,7 +567,8 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
                     }
                     // both passes take the same flow steps, so the chain always holds the record;
                     // were it ever short, the sum would be NaN (visible), never a read out of bounds
-                    delta = rseg >= 0 ? L.rec64[4 * ((long long)rseg * REC_SEG + rcnt) + 3] : __longlong_as_double(-1ll);
+                    delta = rseg >= 0 ? L.rec64[REC64_W * ((long long)rseg * REC_SEG + rcnt) + 2]
+                                      : __longlong_as_double(-1ll);
                     ++rcnt;
                 }
             }
@@ -540,10 +581,22 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
             continue;
         // sample finished
         if (defer == 1) {
-            // recording pass: no outputs; the sample's chain is closed and the job's next sample, if
-            // any, opens its own
-            L.job_head64[job * jobs_n + sample] = rinline ? -2 : rhead;
+            // recording pass: the sample's chain is closed with its end state, and the job's next
+            // sample, if any, opens its own
+            const long long sid = job * jobs_n + sample;
+            L.job_head64[sid] = rinline ? -2 : rhead;
             if (rinline) atomicAdd(&L.rec64_ctl[1], 1ull);
+            else if (rseg >= 0) L.seg_meta64[rseg] = make_uint2((uint32_t)sid, (uint32_t)rcnt);
+            Sample64 e;
+            e.lam = R.c.lam;
+            e.E = R.c.E;
+            e.nrec = rtot;
+            e.natt = R.natt;
+            e.nacc = R.nacc;
+            e.nflow = R.nflow;
+            e.fate = fate;
+            e.fidx = fidx;
+            L.samp64[sid] = e;
             if ((L.kind == RAYS_PIXELS || L.kind == RAYS_CHUNKS) && ++sample < jobs_n) {
                 double x, yv;
                 pixel_point(L, *F, pix, sbase + sample, &x, &yv);
@@ -630,12 +683,16 @@ __global__ void __launch_bounds__(128, DEFER == 1 ? 4 : 3) k_trace64(const Trace
     }
 }
 
-// Deferred FP64 turbulence: the sum at every record slot written by a recording pass of k_trace64,
-// by the same warp_sums4 arithmetic as the tracer's own sums (so the replay pass reads exactly the
-// value the tracer would have computed).  Each warp takes four consecutive slots at a time, the grid
-// strides over all slots of the segments taken; the slots past a chain's last record hold stale
-// positions whose sums nobody reads.  The whole SM runs this kernel, without the tracer's register
-// load, so many more warps hide the FP64 latency of the cosine chains.
+// Deferred FP64 turbulence: the sum at every record written by a recording pass of k_trace64, by the
+// same warp_sums arithmetic as the tracer's own sums (so the emission reads exactly the value the
+// tracer would have computed).  Each warp takes kTurb64PerPass consecutive slots at a time, the grid
+// strides over all slots of the segments taken; lane j turns slot j's (r, u, azimuth) into its
+// position and the warp shares it, and the slots past a chain's last record (the segment's count)
+// are summed at the origin and left unwritten.  The whole SM runs this kernel, without the tracer's
+// register load, so many more warps hide the FP64 latency of the cosine chains.
+// Records per warp pass: their cosines interleave.  Measured on the 1024^2 synchrotron frame: 2 per
+// pass (42 registers) 212 ms, 4 (62) 201 ms, 8 (118 registers, two 256-thread CTAs per SM) 167 ms.
+constexpr int kTurb64PerPass = 8;
 __global__ void __launch_bounds__(256) k_turb64_records(const TraceLaunch L) {
     extern __shared__ double smem64[];
     const int n = L.n_modes;
@@ -647,21 +704,27 @@ __global__ void __launch_bounds__(256) k_turb64_records(const TraceLaunch L) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long s0 = 4 * warp; s0 < nslots; s0 += 4 * nwarps) {
-        double px[4], py[4], pz[4], acc[4];
+    constexpr int P = kTurb64PerPass;
+    for (long long s0 = P * warp; s0 < nslots; s0 += P * nwarps) {
+        const long long mine_slot = s0 + lane;
+        const bool live = lane < P && mine_slot < nslots &&
+                          (int)(mine_slot % REC_SEG) < (int)L.seg_meta64[mine_slot / REC_SEG].y;
+        double X = 0.0, Y = 0.0, Z = 0.0;
+        double* rec = L.rec64 + REC64_W * (live ? mine_slot : 0);
+        if (live) torus_xyz(rec[0], rec[1], rec[2], &X, &Y, &Z);
+        double px[P], py[P], pz[P], acc[P];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const double* rec = L.rec64 + 4 * min(s0 + j, nslots - 1);
-            px[j] = rec[0];
-            py[j] = rec[1];
-            pz[j] = rec[2];
+        for (int j = 0; j < P; ++j) {
+            px[j] = __shfl_sync(FULL, X, j);
+            py[j] = __shfl_sync(FULL, Y, j);
+            pz[j] = __shfl_sync(FULL, Z, j);
         }
-        warp_sums4(md, n, px, py, pz, acc);
+        warp_sums<P>(md, n, px, py, pz, acc);
         double mine = acc[0];
 #pragma unroll
-        for (int j = 1; j < 4; ++j)
+        for (int j = 1; j < P; ++j)
             if (lane == j) mine = acc[j];
-        if (lane < 4 && s0 + lane < nslots) L.rec64[4 * (s0 + lane) + 3] = mine;
+        if (live) rec[2] = mine;
     }
 }
 
@@ -678,19 +741,146 @@ cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_
     return cudaGetLastError();
 }
 
+// Deferred emission: flow_step at every record after its sum, one thread per slot over the slots
+// of the segments taken (a slot past its chain's last record is skipped).  Writes the step's
+// emission dI over r and its transmission exp(-dtau) over u.  The torus model reads neither the
+// azimuth nor the time of the step, nor the baked field.  Left to the replay pass when a sample ran
+// out of segments.
+__global__ void __launch_bounds__(256) k_emit64_records(const TraceLaunch L) {
+    if (*(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull) return;
+    unsigned long long used = *(volatile unsigned long long*)&L.rec64_ctl[0];
+    if (used > (unsigned long long)L.seg_cap64) used = (unsigned long long)L.seg_cap64;
+    const long long nslots = (long long)used * REC_SEG;
+    TorusParams tp;
+    tp.on = true;
+    tp.n_modes = L.n_modes;
+    tp.ne_index = L.ne_index;
+    tp.te_index = L.te_index;
+    tp.h_sph = L.h_sph;
+    tp.theta_e0 = L.theta_e0;
+    tp.half_var = L.half_var;
+    for (long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x; slot < nslots;
+         slot += (long long)gridDim.x * blockDim.x) {
+        const uint2 m = L.seg_meta64[slot / REC_SEG];
+        if ((int)(slot % REC_SEG) >= (int)m.y) continue;
+        const Sample64& smp = L.samp64[m.x];
+        const int fidx = smp.fidx;
+        double* rec = L.rec64 + REC64_W * slot;
+        double dI, dtau;
+        flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], nullptr, tp, rec[2], rec[0], rec[1], 0.0, 0.0,
+                  smp.lam, smp.E, rec[3], &dI, &dtau);
+        rec[0] = dI;
+        rec[1] = exp(-dtau);
+    }
+}
+
+cudaError_t launch_emit64_records(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_emit64_records, 256, 0);
+    if (e != cudaSuccess) return e;
+    k_emit64_records<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
+// Deferred emission, ordered transfer: one thread per job walks each sample's chain in recording
+// order with ray_commit's arithmetic (intensity into the image-order bucket, transmission, the
+// 1e-5 opacity cut, after which the counts of the cut step stand), then writes the job's outputs
+// and counts as the tracer does.  Flow steps without a record emit nothing and transmit 1, so
+// skipping them changes no bit.  Left to the replay pass when a sample ran out of segments.
+__global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
+    const bool skip = *(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull;
+    const unsigned long long cmask = (1ull << REC64_COUNT_BITS) - 1ull;
+    unsigned long long n_att = 0, n_acc = 0, n_lim = 0, n_flow = 0;
+    const long long total = skip ? 0 : L.nrays;
+    for (long long job = (long long)blockIdx.x * blockDim.x + threadIdx.x; job < total;
+         job += (long long)gridDim.x * blockDim.x) {
+        const JobPlace q = job_place(L, job);
+        float pa[4] = {0.f, 0.f, 0.f, 0.f};
+        float ys = 0.f, yq = 0.f;
+        for (int s = 0; s < q.jobs_n; ++s) {
+            const long long sid = job * q.jobs_n + s;
+            const Sample64 e = L.samp64[sid];
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            double trans = 1.0;
+            int fate = e.fate, natt = e.natt, nacc = e.nacc, nflow = e.nflow;
+            long long seg = L.job_head64[sid];
+            for (int i = 0; i < e.nrec; ++i) {
+                const int k = i % REC_SEG;
+                if (k == 0 && i > 0) seg = (long long)L.seg_next64[seg];
+                if (seg < 0 || seg >= L.seg_cap64) {  // never with a complete chain; visible, not a stray read
+                    acc[0] = __int_as_float(0x7fc00000);
+                    break;
+                }
+                const double* rec = L.rec64 + REC64_W * (seg * REC_SEG + k);
+                const double dI = rec[0], ex = rec[1];
+                const unsigned long long tag = (unsigned long long)__double_as_longlong(rec[4]);
+                const float cc = (float)(trans * dI);
+                const int b = (int)(tag & 3ull);
+                acc[0] += cc;
+                if (b == 1) acc[1] += cc;
+                else if (b == 2) acc[2] += cc;
+                else if (b == 3) acc[3] += cc;
+                trans *= ex;
+                if (trans < 1e-5) {
+                    fate = -1;
+                    natt = (int)((tag >> 2) & cmask);
+                    nacc = (int)((tag >> (2 + REC64_COUNT_BITS)) & cmask);
+                    nflow = (int)((tag >> (2 + 2 * REC64_COUNT_BITS)) & cmask);
+                    break;
+                }
+            }
+            n_att += (unsigned long long)natt;
+            n_acc += (unsigned long long)nacc;
+            n_flow += (unsigned long long)nflow;
+            if (fate == 0) ++n_lim;
+            pa[0] += acc[0];
+            pa[1] += acc[1];
+            pa[2] += acc[2];
+            pa[3] += acc[3];
+            const float Y = acc[0];  // radio: sample_lum is the total intensity
+            ys += Y;
+            yq += Y * Y;
+            if (L.kind == RAYS_SAMPLES) {
+                const long long o = q.pix * L.spp + q.sbase;
+                L.sample_out[o] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+                if (L.sample_fate) L.sample_fate[o] = (int8_t)fate;
+            }
+        }
+        if (L.kind == RAYS_PIXELS) {
+            const long long o = (long long)q.fidx * L.W * L.H + q.pix;
+            reinterpret_cast<float4*>(L.accum)[o] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+            if (L.ystat) reinterpret_cast<float2*>(L.ystat)[o] = make_float2(ys, yq);
+        } else if (L.kind == RAYS_CHUNKS) {
+            reinterpret_cast<float4*>(L.chunk_acc)[job] = make_float4(pa[0], pa[1], pa[2], pa[3]);
+        }
+    }
+    n_att = warp_sum(n_att);
+    n_acc = warp_sum(n_acc);
+    n_lim = warp_sum(n_lim);
+    n_flow = warp_sum(n_flow);
+    if ((threadIdx.x & 31) == 0 && n_att + n_acc + n_lim + n_flow > 0) {
+        atomicAdd(&L.counters->attempts, n_att);
+        atomicAdd(&L.counters->accepted, n_acc);
+        atomicAdd(&L.counters->step_limited, n_lim);
+        atomicAdd(&L.counters->flow_steps, n_flow);
+    }
+}
+
+cudaError_t launch_transfer64(const TraceLaunch& L, int num_sms, cudaStream_t st) {
+    const long long blocks = (L.nrays + 127) / 128;
+    const long long cap = (long long)num_sms * 16;
+    k_transfer64<<<(int)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap), 128, 0, st>>>(L);
+    return cudaGetLastError();
+}
+
 // Host launcher: grid = SMs x resident CTAs per SM (persistent; capped by L.ctas_per_sm), dynamic
 // shared memory for the mode table.  Returns the CUDA error of the launch.
 // Bake of the flow turbulence for the frame in d_frame (k_bake_turb, render.cu:449-460): slice k
 // holds exp(a n - a^2 / 2) of the sheared noise n at the retarded time t_ref(r) + delta_k, on cell
 // centres phi = 2 pi (i + 1/2) / 512, ln R uniform over [lr0, lr1] (192 cells), z / R uniform over
 // [-zmax, zmax] (48 cells).  One thread per cell, phi fastest (coalesced stores).
-__global__ void __launch_bounds__(256) k_bake_turb(const so_scene* __restrict__ Sp, const so_frame* __restrict__ Fp,
-                                                   const TurbBake b, float* __restrict__ field) {
-    const so_scene& S = *Sp;
-    const so_frame& F = *Fp;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int l = blockIdx.z % TURB_NZ, k = blockIdx.z / TURB_NZ;
-    if (i >= TURB_NPHI || j >= TURB_NLR) return;
+__device__ __forceinline__ float bake_texel(const so_scene& S, const so_frame& F, const TurbBake& b, int i, int j,
+                                             int l, int k) {
     const double phi = (i + 0.5) / TURB_NPHI * 2.0 * PI;
     const double R = exp(S.turb_lr0 + (j + 0.5) / TURB_NLR * (S.turb_lr1 - S.turb_lr0));
     const double z = (-1.0 + 2.0 * (l + 0.5) / TURB_NZ) * S.turb_zmax * R;
@@ -698,7 +888,26 @@ __global__ void __launch_bounds__(256) k_bake_turb(const so_scene* __restrict__ 
     const double t = (F.t - (F.r - r + 2.0 * log(F.r / r))) + b.delta[k];
     const float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);
     const float a = S.flow_turb_amp;
-    field[(((size_t)k * TURB_NZ + l) * TURB_NLR + j) * TURB_NPHI + i] = __expf(a * n - 0.5f * a * a);
+    return __expf(a * n - 0.5f * a * a);
+}
+
+__global__ void __launch_bounds__(256) k_bake_turb(const so_scene* __restrict__ Sp, const so_frame* __restrict__ Fp,
+                                                   const TurbBake b, float* __restrict__ field) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z % TURB_NZ, k = blockIdx.z / TURB_NZ;
+    if (i >= TURB_NPHI || j >= TURB_NLR) return;
+    field[(((size_t)k * TURB_NZ + l) * TURB_NLR + j) * TURB_NPHI + i] = bake_texel(*Sp, *Fp, b, i, j, l, k);
+}
+
+// The same texels into slice k's 3-D array through its surface (x = phi, y = ln R, z = z / R), for
+// the texture-unit fetch (render.cu:449-460 writes its slices the same way).
+__global__ void __launch_bounds__(256) k_bake_turb_surf(const so_scene* __restrict__ Sp,
+                                                        const so_frame* __restrict__ Fp, const TurbBake b,
+                                                        const SurfaceSet surf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int l = blockIdx.z % TURB_NZ, k = blockIdx.z / TURB_NZ;
+    if (i >= TURB_NPHI || j >= TURB_NLR) return;
+    surf3Dwrite(bake_texel(*Sp, *Fp, b, i, j, l, k), surf.s[k], i * (int)sizeof(float), j, l);
 }
 
 // Pixel corners (k_corners, render.cu:40-52): corner (x, y) of a W x H frame at tangent-plane point
@@ -758,6 +967,13 @@ cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, c
                              cudaStream_t st) {
     const dim3 block(32, 8), grid(TURB_NPHI / 32, TURB_NLR / 8, TURB_NZ * TURB_NT);
     k_bake_turb<<<grid, block, 0, st>>>(d_scene, d_frame, b, field);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bake_turb_surf(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b,
+                                  const SurfaceSet& surf, cudaStream_t st) {
+    const dim3 block(32, 8), grid(TURB_NPHI / 32, TURB_NLR / 8, TURB_NZ * TURB_NT);
+    k_bake_turb_surf<<<grid, block, 0, st>>>(d_scene, d_frame, b, surf);
     return cudaGetLastError();
 }
 

@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
     const float rcam_hi = (float)F.r, rcam_lo = (float)(F.r - (double)(float)F.r);
     const float risco = (float)S.r_isco, flow_kep = (float)S.flow_kep;
     const float tcam = (float)F.t;
-    const bool baked = VAR == VAR_RADIO && !tp.on && L.turb_field != nullptr && S.flow_turb_amp > 0.f;
+    const bool baked = VAR == VAR_RADIO && !tp.on && baked_on(S, L.turb_field) && S.flow_turb_amp > 0.f;
     const float r_out = (float)L.r_emit;
     const bool radio = VAR == VAR_RADIO;
     C32 c;
@@ -628,9 +628,8 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                             sl = fminf(fmaxf(sl, 0.f), (float)(TURB_NT - 1) - 1e-4f);
                             const int k = (int)sl;
                             const float f = sl - (float)k;
-                            const size_t slice = (size_t)TURB_NPHI * TURB_NLR * TURB_NZ;
-                            const float A = turb_fetch(L.turb_field + (size_t)k * slice, x, y, w);
-                            const float B = turb_fetch(L.turb_field + (size_t)(k + 1) * slice, x, y, w);
+                            const float A = baked_sample(S, L.turb_field, k, x, y, w);
+                            const float B = baked_sample(S, L.turb_field, k + 1, x, y, w);
                             bfac = fmaf(B - A, f, A);
                         }
                     }

@@ -218,9 +218,10 @@ struct ModesSmem {
 // error of the advected phase.
 //
 // Where the torus turbulence is needed for a flow step at (r, u, phi, t): false when flow_step
-// returns before using it; else the advected Cartesian position (X, Y, Z) of the sum.
-__device__ __forceinline__ bool torus_position(const so_scene& S, const TorusParams& tp, double rcam, double r,
-                                               double u, double phi, double t, double* X, double* Y, double* Z) {
+// returns before using it (only those flow steps can change the transfer); else the advected
+// azimuth phc of the sum's position.
+__device__ __forceinline__ bool torus_phase(const so_scene& S, const TorusParams& tp, double rcam, double r, double u,
+                                            double phi, double t, double* phc) {
     if (!tp.on || tp.n_modes <= 0) return false;
     double s2 = fmax(fma(-u, u, 1.0), 1e-12), s = sqrt(s2);
     double R = r * s;
@@ -228,12 +229,24 @@ __device__ __forceinline__ bool torus_position(const so_scene& S, const TorusPar
     double zh = u / tp.h_sph;
     if (exp(-0.5 * zh * zh) < 1e-7) return false;
     double Omf = S.flow_kep * keplerian_omega(S.a, fmax(R, S.r_isco));
-    double phc = phi - Omf * (t + (rcam - r + 2.0 * log(rcam / r)));
+    *phc = phi - Omf * (t + (rcam - r + 2.0 * log(rcam / r)));
+    return true;
+}
+// The Cartesian position (X, Y, Z) of the sum at (r, u) and advected azimuth phc.
+__device__ __forceinline__ void torus_xyz(double r, double u, double phc, double* X, double* Y, double* Z) {
+    double s2 = fmax(fma(-u, u, 1.0), 1e-12), s = sqrt(s2);
+    double R = r * s;
     double sp, cp;
     sincos(phc, &sp, &cp);
     *X = R * cp;
     *Y = R * sp;
     *Z = r * u;
+}
+__device__ __forceinline__ bool torus_position(const so_scene& S, const TorusParams& tp, double rcam, double r,
+                                               double u, double phi, double t, double* X, double* Y, double* Z) {
+    double phc;
+    if (!torus_phase(S, tp, rcam, r, u, phi, t, &phc)) return false;
+    torus_xyz(r, u, phc, X, Y, Z);
     return true;
 }
 
@@ -265,6 +278,18 @@ __device__ __forceinline__ float turb_fetch(const float* __restrict__ slice, flo
     return fmaf(c, w1 - w0, w0);
 }
 
+// The baked turbulence's slices: in plain memory (`field`, FP32 trilinear by turb_fetch, which the CPU
+// oracle repeats) or, when the scene carries their texture handles, through the texture unit with
+// the reference's sampler (emission.cuh:121-122; its trilinear weights have 8 fractional bits).
+__device__ __forceinline__ bool baked_on(const so_scene& S, const float* field) {
+    return field != nullptr || (S.turb_nt > 0 && S.turb_tex[0] != 0);
+}
+__device__ __forceinline__ float baked_sample(const so_scene& S, const float* field, int k, float x, float y,
+                                              float z) {
+    if (field) return turb_fetch(field + (size_t)k * TURB_NPHI * TURB_NLR * TURB_NZ, x, y, z);
+    return tex3D<float>((cudaTextureObject_t)S.turb_tex[k], x, y, z);
+}
+
 // flow_step with the torus turbulence sum `delta` at this point already evaluated (torus_position).
 // With `field` (the frame's baked slices) the reference model's turbulence is sampled as
 // emission.cuh:112-124 does, else its sheared noise is evaluated in place (the turb_nt = 0 path).
@@ -292,7 +317,7 @@ static __device__ void flow_step(const so_scene& S, const so_frame& F, const flo
         if (vert < 1e-7) return;
         ne = S.n0 * exp(-S.n_index * log(r)) * vert;
         if (S.flow_turb_amp > 0.f) {
-            if (field) {
+            if (baked_on(S, field)) {
                 // two slices around the retarded time t - t_ref(r), interpolated (emission.cuh:112-124)
                 const double tref = F.t - (F.r - r + 2.0 * log(F.r / r));
                 const float y = (float)((log(R) - S.turb_lr0) / (S.turb_lr1 - S.turb_lr0));
@@ -302,9 +327,8 @@ static __device__ void flow_step(const so_scene& S, const so_frame& F, const flo
                 sl = fminf(fmaxf(sl, 0.f), (float)(TURB_NT - 1) - 1e-4f);
                 const int k = (int)sl;
                 const float f = sl - (float)k;
-                const size_t slice = (size_t)TURB_NPHI * TURB_NLR * TURB_NZ;
-                const float A = turb_fetch(field + (size_t)k * slice, x, y, w);
-                const float B = turb_fetch(field + (size_t)(k + 1) * slice, x, y, w);
+                const float A = baked_sample(S, field, k, x, y, w);
+                const float B = baked_sample(S, field, k + 1, x, y, w);
                 ne *= fmaf(B - A, f, A);
             } else {
                 float n = sheared_noise(S, R, phi, z, t, S.flow_turb_scale, S.flow_tcorr, S.seed ^ 0x51f15eedu);

@@ -24,7 +24,24 @@ enum Variant : int {
 };
 
 // Device counters of one launch (zeroed before the launch).
-constexpr int REC_SEG = 16;  // flow-step record slots per segment (256 bytes)
+constexpr int REC_SEG = 16;  // flow-step record slots per segment
+
+// Record of the deferred FP64 torus path, REC64_W doubles per slot: [0] r, [1] u = cos theta,
+// [2] advected azimuth of the turbulence position (k_turb64_records overwrites it with the sum
+// delta), [3] the Mino step h, [4] tag.  k_emit64_records then overwrites [0] with the step's
+// emission dI and [1] with its transmission exp(-dtau).  The tag holds the image-order bucket
+// (bits 0-1: psi / pi clamped to 3) and the ray's attempt, accepted-step and flow-step counts after
+// this step (20 bits each from bit 2, 22 and 42; the path needs max_steps < 2^20).
+constexpr int REC64_W = 5;
+constexpr int REC64_COUNT_BITS = 20;
+// End state of one sample after the recording pass.
+struct Sample64 {
+    double lam, E;            // the ray's constants of motion used by the emission
+    int nrec;                 // records in its chain
+    int natt, nacc, nflow;    // attempts, accepted steps, flow steps to its end
+    int fate;                 // 0 step limit, -1 capture, 1 escape
+    int fidx;                 // frame
+};
 
 // Baked flow turbulence (render.cu:447-460, 594-620): per frame, TURB_NT retarded-time slices of
 // TURB_NPHI x TURB_NLR x TURB_NZ density factors on (phi, ln R, z/R), phi fastest, in HBM.
@@ -135,16 +152,21 @@ struct TraceLaunch {
     int ctas_per_sm;          // persistent grid: CTAs per SM (0 = as many as fit)
     int emit32;               // FP64 tracer: torus turbulence sums in FP32 (geometry stays FP64)
     // deferred FP64 torus turbulence: pass 1 (defer64 = 1) integrates the geodesic only and records
-    // the position of every flow step that needs a sum in its job's chain of REC_SEG-slot segments;
-    // k_turb64_records sums the modes at every record; pass 2 (defer64 = 2) integrates again and reads
-    // each sum back in order.  0 = sums in the tracer.
+    // every flow step that can change the transfer in its sample's chain of REC_SEG-slot segments;
+    // k_turb64_records sums the modes at every record.  Then either k_emit64_records evaluates the
+    // emission at every record and k_transfer64 applies them in order per sample, or pass 2
+    // (defer64 = 2) integrates again and reads each sum back in order.  0 = sums in the tracer.
     int defer64;
-    double* rec64;            // record pool: slot s holds X, Y, Z, delta at doubles 4 s .. 4 s + 3
-    uint32_t* seg_next64;     // per segment: the job's next segment
+    double* rec64;            // record pool: slot s at doubles REC64_W s .. (layout at REC64_W)
+    uint32_t* seg_next64;     // per segment: the sample's next segment
+    uint2* seg_meta64;        // per segment: (sample id owning it, records in it)
+    Sample64* samp64;         // per sample id: the recording pass's end state
     int* job_head64;          // per sample of a job (job * samples per job + s): its chain's first segment,
                               // -1 no records, -2 the pool ran out (the replay pass sums in place)
     long long seg_cap64;      // segments in the pool
-    unsigned long long* rec64_ctl;  // [0] segments taken, [1] jobs that ran out of segments, [2] records
+    unsigned long long* rec64_ctl;  // [0] segments taken, [1] samples that ran out of segments, [2] records
+    int replay_if_short;      // pass 2: runs only when a sample of pass 1 ran out of segments (the
+                              // emission / transfer kernels then leave the frame to it)
     const float* band_rho;    // critical-curve radius (M) per image angle bin, band_n bins over 2 pi
     int band_n;
     float4* state;            // parked ray state, 5 float4 per sample id (SoA planes of nsamples)
@@ -179,6 +201,12 @@ cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cu
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st);
 cudaError_t launch_bake_turb(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b, float* field,
                              cudaStream_t st);
+// The same bake into TURB_NT 3-D float arrays through their surface objects (texture-fetch mode).
+struct SurfaceSet {
+    cudaSurfaceObject_t s[TURB_NT];
+};
+cudaError_t launch_bake_turb_surf(const so_scene* d_scene, const so_frame* d_frame, const TurbBake& b,
+                                  const SurfaceSet& surf, cudaStream_t st);
 // Sky: tangent-plane points of the (W + 1) x (H + 1) pixel corners of the frame in d_frame, the
 // corners' escape (u, v) from the tracer's outputs, and one box-filtered half2 mip level.
 cudaError_t launch_corner_points(const so_frame* d_frame, int W, int H, double* x, double* y, cudaStream_t st);
@@ -195,8 +223,11 @@ struct TurbModes {
 };
 void turb_modes_fold(const so_mode* modes, int n, TurbModes* out);
 cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
-// FP64 sums at every record of a defer64 = 1 pass (modes from L.modes, L.n_modes of them).
+// FP64 sums at every record of a defer64 = 1 pass (modes from L.modes, L.n_modes of them), the
+// emission at every record, and the ordered transfer of every job's samples into the outputs.
 cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
+cudaError_t launch_emit64_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
+cudaError_t launch_transfer64(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_sky_escape(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_flow_records(const TraceLaunch& L, int num_sms, cudaStream_t st);
 cudaError_t launch_gather_samples(const TraceLaunch& L, cudaStream_t st);

@@ -104,7 +104,10 @@ struct so_renderer {
     uint32_t* d_esc_list = nullptr;  // star-map frames on the mixed path: escaped FP32 rays
     long long esc_cap = 0;
     // baked flow turbulence (reference flow model with turbulence, radio mode): the frame's slices
-    float* d_turb = nullptr;
+    float* d_turb = nullptr;                       // SO_FLOW_NOISE_BAKED_FP32: the slices in plain memory
+    cudaArray_t turb_arr[TURB_NT] = {};            // SO_FLOW_NOISE_BAKED: the slices as 3-D arrays,
+    cudaSurfaceObject_t turb_surf[TURB_NT] = {};   // written through surfaces by the bake
+    cudaTextureObject_t turb_texo[TURB_NT] = {};   // and read through the texture unit
     int flow_noise = SO_FLOW_NOISE_BAKED;
     TurbBake tb{};
     double approach_key[6] = {-1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -137,19 +140,22 @@ struct so_renderer {
     LumScratch lum{};
     LumStat* h_lum = nullptr;
     // deferred FP64 torus turbulence of the plain tracer: record pool (segments of REC_SEG slots of
-    // X, Y, Z, delta), per-job chain heads, the recording pass's counters, and the pool's use
+    // REC64_W doubles, each segment's link and owner), per-sample chain heads and end states, the
+    // recording pass's counters, and the pool's use
     double* d_rec64 = nullptr;
     uint32_t* d_seg_next64 = nullptr;
+    uint2* d_seg_meta64 = nullptr;
+    Sample64* d_samp64 = nullptr;
     int* d_job_head64 = nullptr;
-    unsigned long long* d_rec64_ctl = nullptr;  // [0] segments taken, [1] jobs that ran short, [2] records
+    unsigned long long* d_rec64_ctl = nullptr;  // [0] segments taken, [1] samples that ran short, [2] records
     Counters* d_cnt64 = nullptr;
     long long seg_cap64 = 0, job_cap64 = 0, pool64_target = -1;
     double rec_per_sample64 = 320.0;           // pool size per sample (records), doubled after a shortage
     unsigned long long* h_rec64 = nullptr;     // pinned copy of d_rec64_ctl after the last deferred trace
     cudaEvent_t ev_rec64 = nullptr;
     bool rec64_pending = false;
-    cudaEvent_t ev64[4] = {nullptr, nullptr, nullptr, nullptr};  // recording pass, sums, replay pass
-    bool last_defer64 = false;
+    cudaEvent_t ev64[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // recording, sums, emission, replay
+    bool last_defer64 = false, last_emit64 = false;
     std::string err;
 };
 
@@ -178,6 +184,17 @@ int variant_of(const so_scene& S) {
     if (S.mode == SO_MODE_RADIO) return VAR_RADIO;
     if (S.disk_on) return VAR_DISK;
     return VAR_VACUUM;
+}
+
+void free_turb_arrays(so_renderer* r) {
+    for (int k = 0; k < TURB_NT; ++k) {
+        if (r->turb_texo[k]) cudaDestroyTextureObject(r->turb_texo[k]);
+        if (r->turb_surf[k]) cudaDestroySurfaceObject(r->turb_surf[k]);
+        if (r->turb_arr[k]) cudaFreeArray(r->turb_arr[k]);
+        r->turb_texo[k] = 0;
+        r->turb_surf[k] = 0;
+        r->turb_arr[k] = nullptr;
+    }
 }
 
 void free_all(so_renderer* r) {
@@ -212,7 +229,9 @@ void free_all(so_renderer* r) {
     delete r->turb_modes;
     if (r->ev_fork) cudaEventDestroy(r->ev_fork);
     if (r->ev_join) cudaEventDestroy(r->ev_join);
-    void* p64[] = {r->d_rec64, r->d_seg_next64, r->d_job_head64, r->d_rec64_ctl, r->d_cnt64};
+    free_turb_arrays(r);
+    void* p64[] = {r->d_rec64, r->d_seg_next64, r->d_seg_meta64, r->d_samp64, r->d_job_head64, r->d_rec64_ctl,
+                   r->d_cnt64};
     for (void* p : p64)
         if (p) cudaFree(p);
     if (r->h_rec64) cudaFreeHost(r->h_rec64);
@@ -272,21 +291,54 @@ int upload_scene(so_renderer* r) {
 // Baked flow turbulence as Renderer::init sets it up (render.cu:594-620): for a radio scene with
 // the hot flow and its turbulence, TURB_NT slices over ln R in [ln(0.8 r+), ln(1.05 r_flow_max)],
 // z / R within +-min(2, 5 h_r), retarded-time offsets -250 + 260 k / (TURB_NT - 1).  Otherwise (or
-// with SO_FLOW_NOISE_INLINE) turb_nt = 0 and the kernels evaluate the sheared noise in place.  The
-// texture handles of so_scene stay zero: the slices are plain device memory here.
+// with SO_FLOW_NOISE_INLINE) turb_nt = 0 and the kernels evaluate the sheared noise in place.
+// SO_FLOW_NOISE_BAKED keeps the slices as the reference does: 3-D float arrays written through
+// surfaces and read through texture objects with its sampler (normalised coordinates, linear
+// filtering, phi wrapped, ln R and z / R clamped), whose handles go into so_scene.turb_tex.
+// SO_FLOW_NOISE_BAKED_FP32 keeps them in plain device memory for the FP32 trilinear fetch that the
+// CPU oracle repeats; turb_tex stays zero then.
 int turb_setup(so_renderer* r) {
     so_scene& S = r->S;
     for (int k = 0; k < 24; ++k) S.turb_tex[k] = 0;
     const bool bake = S.flow_on && S.mode == SO_MODE_RADIO && S.flow_turb_amp > 0.f &&
-                      r->flow_noise == SO_FLOW_NOISE_BAKED;
-    if (!bake) {
-        S.turb_nt = 0;
+                      (r->flow_noise == SO_FLOW_NOISE_BAKED || r->flow_noise == SO_FLOW_NOISE_BAKED_FP32);
+    const bool tex = bake && r->flow_noise == SO_FLOW_NOISE_BAKED;
+    if (!bake || tex) {
         if (r->d_turb) cudaFree(r->d_turb);
         r->d_turb = nullptr;
+    }
+    if (!tex) free_turb_arrays(r);
+    if (!bake) {
+        S.turb_nt = 0;
         return SO_OK;
     }
-    if (!r->d_turb && dalloc(&r->d_turb, (size_t)TURB_NT * TURB_NPHI * TURB_NLR * TURB_NZ) != cudaSuccess)
+    if (tex) {
+        cudaChannelFormatDesc fd = cudaCreateChannelDesc<float>();
+        for (int k = 0; k < TURB_NT; ++k) {
+            if (r->turb_arr[k]) continue;
+            if (cudaMalloc3DArray(&r->turb_arr[k], &fd, make_cudaExtent(TURB_NPHI, TURB_NLR, TURB_NZ),
+                                  cudaArraySurfaceLoadStore) != cudaSuccess) {
+                free_turb_arrays(r);
+                return fail(r, SO_ERR_ALLOC, "baked turbulence: 3-D array allocation");
+            }
+            cudaResourceDesc rd;
+            std::memset(&rd, 0, sizeof rd);
+            rd.resType = cudaResourceTypeArray;
+            rd.res.array.array = r->turb_arr[k];
+            cudaTextureDesc td;
+            std::memset(&td, 0, sizeof td);
+            td.addressMode[0] = cudaAddressModeWrap;
+            td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+            td.filterMode = cudaFilterModeLinear;
+            td.readMode = cudaReadModeElementType;
+            td.normalizedCoords = 1;
+            SO_CK(r, cudaCreateSurfaceObject(&r->turb_surf[k], &rd));
+            SO_CK(r, cudaCreateTextureObject(&r->turb_texo[k], &rd, &td, nullptr));
+        }
+        for (int k = 0; k < TURB_NT; ++k) S.turb_tex[k] = (unsigned long long)r->turb_texo[k];
+    } else if (!r->d_turb && dalloc(&r->d_turb, (size_t)TURB_NT * TURB_NPHI * TURB_NLR * TURB_NZ) != cudaSuccess) {
         return fail(r, SO_ERR_ALLOC, "baked turbulence: device allocation");
+    }
     S.turb_nt = TURB_NT;
     S.turb_lr0 = (float)std::log(0.8 * S.rh);
     S.turb_lr1 = (float)std::log(S.r_flow_max * 1.05);
@@ -297,10 +349,18 @@ int turb_setup(so_renderer* r) {
     return SO_OK;
 }
 
-// Re-bake of the turbulence for the frame just uploaded to d_frame (render.cu:679-682), queued on
-// the renderer's stream, and the slices given to the tracer launch L.
+// The frame's bake (k_bake_turb): into the 3-D arrays (texture fetch) or the plain slices (FP32
+// fetch, passed to the tracers as L.turb_field).
 int bake_turbulence(so_renderer* r, TraceLaunch& L) {
-    if (r->S.turb_nt <= 0 || !r->d_turb) return SO_OK;
+    if (r->S.turb_nt <= 0) return SO_OK;
+    if (r->turb_arr[0]) {
+        SurfaceSet ss;
+        for (int k = 0; k < TURB_NT; ++k) ss.s[k] = r->turb_surf[k];
+        SO_CK(r, launch_bake_turb_surf(r->d_scene, r->d_frame, r->tb, ss, r->st));
+        L.turb_field = nullptr;
+        return SO_OK;
+    }
+    if (!r->d_turb) return SO_OK;
     SO_CK(r, launch_bake_turb(r->d_scene, r->d_frame, r->tb, r->d_turb, r->st));
     L.turb_field = r->d_turb;
     return SO_OK;
@@ -375,8 +435,8 @@ int ensure_side_queue(so_renderer* r) {
 }
 
 // Record pool of the deferred FP64 turbulence for `jobs` tracer jobs of `per_job` samples:
-// rec_per_sample64 records per sample plus one partly filled segment per job, within half of the
-// free device memory and so_mixed_opts.pool_mb.  Jobs that do not fit are summed in place by the
+// rec_per_sample64 records per sample plus one partly filled segment per sample, within half of the
+// free device memory and so_mixed_opts.pool_mb.  Samples that do not fit are summed in place by the
 // replay pass (the same sums, slower); such a shortage doubles the estimate for the next traces.
 int ensure_records64(so_renderer* r, long long jobs, int per_job) {
     if (!r->h_rec64) {
@@ -393,7 +453,7 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
         if (r->h_rec64[1] > 0) r->rec_per_sample64 *= 2.0;
     }
     cudaGetLastError();  // a pending event reports cudaErrorNotReady
-    const double per_seg = REC_SEG * 4 * sizeof(double) + sizeof(uint32_t);
+    const double per_seg = REC_SEG * REC64_W * sizeof(double) + sizeof(uint32_t) + sizeof(uint2);
     const double seg_per_job = (r->rec_per_sample64 / REC_SEG + 1.0) * per_job;  // a partly filled segment per sample
     long long want = std::min<long long>((long long)std::ceil((double)jobs * seg_per_job), 0x7fffffffll);
     if (r->mixed.pool_mb > 0.0)
@@ -402,16 +462,18 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
         SO_CK(r, cudaStreamSynchronize(r->st));
         if (r->d_rec64) cudaFree(r->d_rec64);
         if (r->d_seg_next64) cudaFree(r->d_seg_next64);
+        if (r->d_seg_meta64) cudaFree(r->d_seg_meta64);
         r->d_rec64 = nullptr;
         r->d_seg_next64 = nullptr;
+        r->d_seg_meta64 = nullptr;
         r->seg_cap64 = 0;
         r->pool64_target = -1;
         size_t fr = 0, tot = 0;
         SO_CK(r, cudaMemGetInfo(&fr, &tot));
         const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
         if (cap < 1) return fail(r, SO_ERR_ALLOC, "FP64 record pool: no device memory");
-        if (dalloc(&r->d_rec64, (size_t)cap * REC_SEG * 4) != cudaSuccess ||
-            dalloc(&r->d_seg_next64, (size_t)cap) != cudaSuccess)
+        if (dalloc(&r->d_rec64, (size_t)cap * REC_SEG * REC64_W) != cudaSuccess ||
+            dalloc(&r->d_seg_next64, (size_t)cap) != cudaSuccess || dalloc(&r->d_seg_meta64, (size_t)cap) != cudaSuccess)
             return fail(r, SO_ERR_ALLOC, "FP64 record pool: device allocation");
         r->seg_cap64 = cap;
         r->pool64_target = want;
@@ -419,9 +481,11 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
     const long long heads = jobs * per_job;  // one chain per sample
     if (heads > r->job_cap64) {
         if (r->d_job_head64) cudaFree(r->d_job_head64);
+        if (r->d_samp64) cudaFree(r->d_samp64);
         r->d_job_head64 = nullptr;
+        r->d_samp64 = nullptr;
         r->job_cap64 = 0;
-        if (dalloc(&r->d_job_head64, (size_t)heads) != cudaSuccess)
+        if (dalloc(&r->d_job_head64, (size_t)heads) != cudaSuccess || dalloc(&r->d_samp64, (size_t)heads) != cudaSuccess)
             return fail(r, SO_ERR_ALLOC, "FP64 record pool: chain heads");
         r->job_cap64 = heads;
     }
@@ -429,9 +493,12 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
 }
 
 // Launches of the FP64 tracer.  A torus-plasma launch with FP64 sums and at least kDeferMinJobs
-// host-counted jobs on the renderer's stream runs as recording pass -> k_turb64_records -> replay
-// pass (bit for bit the in-tracer result, with the sums at full occupancy); everything else, and any
-// launch whose pool cannot be had, sums in the tracer.
+// host-counted jobs on the renderer's stream defers its sums: recording pass (geometry only) ->
+// k_turb64_records, then for frame work (pixels, samples, chunks) without a disk the emission too:
+// k_emit64_records -> k_transfer64, with the replay pass behind them running only if the pool ran
+// short; for ray lists (whose per-ray outputs need the geometry up to the opacity cut) and disk
+// scenes the replay pass.  Each is bit for bit the in-tracer result, with the sums and the emission
+// at full occupancy.  Everything else, and any launch whose pool cannot be had, sums in the tracer.
 constexpr long long kDeferMinJobs = 4096;
 
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
@@ -453,9 +520,14 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
             L1.job_head64 = r->d_job_head64;
             L1.seg_cap64 = r->seg_cap64;
             L1.rec64_ctl = r->d_rec64_ctl;
+            L1.seg_meta64 = r->d_seg_meta64;
+            L1.samp64 = r->d_samp64;
+            const bool emit64 = L.kind != RAYS_LIST && !r->S.disk_on &&
+                                r->S.max_steps < (1 << REC64_COUNT_BITS);
             TraceLaunch L2 = L1;
             L2.defer64 = 2;
             L2.counters = L.counters;
+            L2.replay_if_short = emit64 ? 1 : 0;
             cudaEventRecord(r->ev64[0], s);
             cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
             if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
@@ -463,14 +535,24 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
             e = launch_turb64_records(L1, r->num_sms, s);
             if (e != cudaSuccess) return cuda_fail(r, e, "FP64 turbulence sums");
             cudaEventRecord(r->ev64[2], s);
+            if (emit64) {
+                TraceLaunch Le = L1;
+                Le.counters = L.counters;
+                e = launch_emit64_records(Le, r->num_sms, s);
+                if (e != cudaSuccess) return cuda_fail(r, e, "FP64 deferred emission");
+                e = launch_transfer64(Le, r->num_sms, s);
+                if (e != cudaSuccess) return cuda_fail(r, e, "FP64 ordered transfer");
+            }
+            cudaEventRecord(r->ev64[3], s);
             e = launch_trace64(L2, var, r->num_sms, s);
             if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
-            cudaEventRecord(r->ev64[3], s);
+            cudaEventRecord(r->ev64[4], s);
             SO_CK(r, cudaMemcpyAsync(r->h_rec64, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, s));
             SO_CK(r, cudaEventRecord(r->ev_rec64, s));
             r->rec64_pending = true;
             r->last_defer64 = true;
+            r->last_emit64 = emit64;
             return SO_OK;
         }
         r->err.clear();  // no pool: sum in the tracer
@@ -704,10 +786,10 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     // k = floor(t / P) of the raw coordinate time t ~ -r_cam: a relative change eps of the radius moves
     // its phase by ~ (t / P) eps, so any integrator that is not the FP64 one decorrelates it.  Such
     // scenes, and radio scenes with a disk (not in the FP32 tracer), go to FP64 entirely.  A baked
-    // flow field (L.turb_field) is sampled at the position and at t - t_ref(r), both well conditioned,
+    // flow field (turb_nt > 0) is sampled at the position and at t - t_ref(r), both well conditioned,
     // so the FP32 tracer takes those scenes.
     const bool all64 = (r->S.mode == SO_MODE_RADIO && r->S.flow_on && L.torus == 0 && r->S.flow_turb_amp > 0.f &&
-                        !L.turb_field) ||
+                        r->S.turb_nt <= 0) ||
                        (L.sky_uv != nullptr && r->mixed.sky_fp32 == 0) ||  // star map: FP64 unless asked
                        (r->S.disk_on && r->S.disk_turb_amp > 0.f) || (r->S.mode == SO_MODE_RADIO && r->S.disk_on);
     SO_CK(r, launch_route(L, all64 ? 1 : 0, r->st));
@@ -946,16 +1028,20 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->record_waves = 0;
             c.fp64_rays = 0;
         }
-        stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = 0.0;
+        stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = stats->ms_emit64 = 0.0;
         stats->rec64_slots = stats->rec64_short = stats->rec64_records = 0;
+        stats->emit64 = 0;
         if (r->last_defer64) {  // the last tracer launch deferred its FP64 sums (stream synchronised above)
-            float a = 0.f, b = 0.f, c2 = 0.f;
+            float a = 0.f, b = 0.f, c2 = 0.f, d = 0.f;
             cudaEventElapsedTime(&a, r->ev64[0], r->ev64[1]);
             cudaEventElapsedTime(&b, r->ev64[1], r->ev64[2]);
             cudaEventElapsedTime(&c2, r->ev64[2], r->ev64[3]);
+            cudaEventElapsedTime(&d, r->ev64[3], r->ev64[4]);
             stats->ms_rec64 = a;
             stats->ms_sum64 = b;
-            stats->ms_replay64 = c2;
+            stats->ms_emit64 = c2;
+            stats->ms_replay64 = d;
+            stats->emit64 = r->last_emit64 && r->h_rec64[1] == 0 ? 1 : 0;
             const unsigned long long used = std::min<unsigned long long>(r->h_rec64[0], (unsigned long long)r->seg_cap64);
             stats->rec64_slots = (long long)used * REC_SEG;
             stats->rec64_short = (long long)r->h_rec64[1];
@@ -1482,8 +1568,9 @@ int so_set_sky(so_renderer* r, int w, int h, const uint16_t* data) {
 
 int so_set_flow_noise(so_renderer* r, int mode) {
     if (!r) return SO_ERR_ARG;
-    if (mode != SO_FLOW_NOISE_BAKED && mode != SO_FLOW_NOISE_INLINE)
-        return fail(r, SO_ERR_ARG, "so_set_flow_noise: SO_FLOW_NOISE_BAKED or SO_FLOW_NOISE_INLINE");
+    if (mode != SO_FLOW_NOISE_BAKED && mode != SO_FLOW_NOISE_INLINE && mode != SO_FLOW_NOISE_BAKED_FP32)
+        return fail(r, SO_ERR_ARG,
+                    "so_set_flow_noise: SO_FLOW_NOISE_BAKED, SO_FLOW_NOISE_INLINE or SO_FLOW_NOISE_BAKED_FP32");
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
     SO_CK(r, cudaStreamSynchronize(r->st));
     r->flow_noise = mode;

@@ -181,34 +181,44 @@ def test_reference_flow_turbulent_vs_oracle(so, orc):
 
 
 def test_reference_flow_baked_turbulence_vs_oracle(so, orc):
-    """The renderer's default for the turbulent reference flow: 24 retarded-time slices baked per
-    frame and interpolated (render.cu:449-460, emission.cuh:112-124).  Against the oracle, whose
-    texels are the bake formula at each texel centre and whose interpolation repeats the kernel's:
-    geometry exact, intensity within 1e-6 of the maximum.  Switching the mode back reproduces the
-    baked image exactly.  Baked and in-place images are different draws of the same turbulence, not
-    one an approximation of the other: at the camera's coordinate time (t ~ -1e7 M) the sheared
-    noise decorrelates over relative radius changes of ~1e-5, far below the bake's 2 per cent cells
-    (on this 40 x 40 frame the total flux differs by 22 per cent), so only their sizes are compared."""
+    """The turbulent reference flow baked per frame into 24 retarded-time slices (render.cu:449-460,
+    emission.cuh:112-124).  With SO_FLOW_NOISE_BAKED_FP32 (slices in plain memory, FP32 trilinear in
+    a fixed order) against the oracle, whose texels are the bake formula at each texel centre and
+    whose interpolation repeats the kernel's: geometry exact, intensity within 1e-6 of the maximum.
+    The default SO_FLOW_NOISE_BAKED reads the same slices through the texture unit (the reference's
+    own fetch, weights with 8 fractional bits): same geometry, intensity within 2 % of the maximum
+    per ray and 1e-3 in total (the reference's own renderer is matched at rounding level instead:
+    tests/test_gpu_reference_renderer.py).  Switching modes reproduces each image exactly.  Baked and
+    in-place images are different draws of the same turbulence, not one an approximation of the
+    other: at the camera's coordinate time (t ~ -1e7 M) the sheared noise decorrelates over relative
+    radius changes of ~1e-5, far below the bake's 2 per cent cells, so only their sizes are compared."""
     sh = so.Shot("m87_reference_flow.ini", ["camera.width=40", "camera.height=40"])
     r = so.Renderer(sh.scene, sh.tables, sh.settings)
     f = sh.frame(0)
     X, Y = so.pixel_centres(f, 40, 40)
+    kt = r.trace_rays(f, X, Y)  # default: texture fetch
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_BAKED_FP32)
     k = r.trace_rays(f, X, Y)
     o = orc.orc_trace(orc.baked(sh.scene), f, X, Y)
     _cmp_geometry(o, k, rtol_dir=1e-12)
     I0, I1 = o["I"].astype(np.float64), k["I"].astype(np.float64)
     assert I0[:, 0].max() > 0
     assert np.abs(I0 - I1).max() <= 1e-6 * I0[:, 0].max()
+    _cmp_geometry(o, kt, rtol_dir=1e-12)
+    It = kt["I"].astype(np.float64)
+    assert np.abs(It - I1).max() <= 2e-2 * I1[:, 0].max()
+    assert abs(It[:, 0].sum() / I1[:, 0].sum() - 1.0) < 1e-3
     r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
     ki = r.trace_rays(f, X, Y)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_BAKED_FP32)
+    assert np.array_equal(r.trace_rays(f, X, Y)["I"], k["I"])
     r.set_flow_noise(so.abi.SO_FLOW_NOISE_BAKED)
-    kb = r.trace_rays(f, X, Y)
-    assert np.array_equal(kb["I"], k["I"])
+    assert np.array_equal(r.trace_rays(f, X, Y)["I"], kt["I"])
     Ii = ki["I"].astype(np.float64)
     assert not np.array_equal(Ii, I1)
     assert 0.5 < Ii[:, 0].sum() / I1[:, 0].sum() < 2.0
     with pytest.raises(so.TracerError):
-        r.set_flow_noise(2)
+        r.set_flow_noise(3)
     r.close()
 
 
@@ -283,11 +293,11 @@ def test_torus_1024_strided_vs_oracle(so, orc):
 
 
 def test_deferred_fp64_sums_multi_sample_frame(so, orc):
-    """The plain FP64 tracer on a torus frame of >= 4096 pixels defers its turbulence sums (recording
-    pass, k_turb64_records, replay pass), one record chain per sample.  A 64 x 64 frame at 2 samples
-    per pixel equals, bit for bit, the same frame with the record pool capped so that nearly every
-    sample is summed in the tracer instead, and matches the oracle's pass 1 within 1e-6 of the frame
-    maximum."""
+    """The plain FP64 tracer on a torus frame of >= 4096 pixels defers its turbulence sums and its
+    emission (recording pass, k_turb64_records, k_emit64_records, k_transfer64), one record chain
+    per sample.  A 64 x 64 frame at 2 samples per pixel equals, bit for bit, the same frame with the
+    record pool capped so that nearly every sample is summed in the tracer by the replay pass
+    instead, and matches the oracle's pass 1 within 1e-6 of the frame maximum."""
     n = 64
     sh = so.Shot("synchrotron_1024.ini", [f"camera.width={n}", f"camera.height={n}", "render.spp=2",
                                           "render.spp_max=2", "flow.n0=1594262.8"])
@@ -297,7 +307,7 @@ def test_deferred_fp64_sums_multi_sample_frame(so, orc):
     f = sh.frame(0)
     r.set_precision(so.abi.SO_PREC_FP64)
     a, _, sa = r.render(f)
-    assert sa.rec64_slots > 0 and sa.rec64_short == 0 and sa.rec64_records > 0
+    assert sa.rec64_slots > 0 and sa.rec64_short == 0 and sa.rec64_records > 0 and sa.emit64 == 1
     r.set_precision(so.abi.SO_PREC_FP64, pool_mb=0.001)  # two segments: the rest is summed in place
     b, _, sb = r.render(f)
     assert sb.rec64_short > 0.9 * n * n * 2
@@ -309,6 +319,57 @@ def test_deferred_fp64_sums_multi_sample_frame(so, orc):
     assert np.abs(a - ref).max() <= 1e-6 * ref[..., 0].max()
     assert sa.attempts == att
     r.close()
+
+
+def _deferred_pair(so, overrides):
+    """One torus frame rendered twice through the plain FP64 path: with deferred emission
+    (k_emit64_records + k_transfer64) and with the record pool capped to two segments, so that the
+    recording pass runs short and the replay pass (in-tracer emission) renders the frame."""
+    sh = so.Shot("synchrotron_1024.ini", overrides)
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_plasma(sh.plasma())
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    a, _, sa = r.render(f)
+    r.set_precision(so.abi.SO_PREC_FP64, pool_mb=0.001)
+    b, _, sb = r.render(f)
+    r.close()
+    return a, sa, b, sb
+
+
+def _counts(st):
+    return st.attempts, st.accepted, st.flow_steps, st.step_limited, st.samples
+
+
+def test_deferred_fp64_emission_opacity_cut(so):
+    """Deferred emission ends a sample at the transfer's 1e-5 opacity cut with the counts recorded at
+    that step.  At the normalised density and at 1000 times it (where many rays are cut), the frame
+    and every counter equal the replay pass's bit for bit, and the dense frame makes fewer attempts
+    than the same geometry without cuts."""
+    n = 64
+    base = [f"camera.width={n}", f"camera.height={n}", "render.spp=2", "render.spp_max=2"]
+    thin = _deferred_pair(so, base + ["flow.n0=1594262.8"])
+    thick = _deferred_pair(so, base + ["flow.n0=1594262800.0"])
+    for a, sa, b, sb in (thin, thick):
+        assert sa.emit64 == 1 and sa.rec64_short == 0 and sa.ms_emit64 > 0
+        assert sb.emit64 == 0 and sb.rec64_short > 0
+        assert np.array_equal(a, b)
+        assert _counts(sa) == _counts(sb)
+    assert thick[1].attempts < thin[1].attempts
+    print("opacity cut: attempts", thin[1].attempts, "->", thick[1].attempts)
+
+
+def test_deferred_fp64_emission_adaptive_chunks(so):
+    """Adaptive pass 2 on a torus frame (chunks of 8 samples, well over the deferral threshold of
+    4096 jobs): the frame with deferred emission in both passes equals the replay pass's bit for
+    bit, counters included."""
+    n = 128
+    a, sa, b, sb = _deferred_pair(so, [f"camera.width={n}", f"camera.height={n}", "render.spp=2",
+                                       "render.spp_max=34", "render.target_error=0.005", "flow.n0=1594262.8"])
+    assert sa.samples - n * n * 2 >= 4096 * 8, sa.samples  # pass 2 ran at least 4096 chunks
+    assert sa.emit64 == 1 and sb.emit64 == 0
+    assert np.array_equal(a, b)
+    assert _counts(sa) == _counts(sb)
 
 
 def test_torus_plasma_vs_oracle(so, orc):
@@ -352,10 +413,11 @@ def test_thin_disk_vs_oracle_and_golden(so, orc):
 
 def test_render_pass1_jitter_vs_oracle(so, orc):
     """so_render with spp = 2 R2-jittered samples, no adaptive pass and the flow turbulence baked for
-    the frame == oracle pass 1 / spp."""
+    the frame (FP32 fetch, which the oracle repeats) == oracle pass 1 / spp."""
     sh = so.Shot("m87_reference_flow.ini", ["camera.width=32", "camera.height=24", "render.spp=2",
                                             "render.spp_max=2"])
     r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_BAKED_FP32)
     f = sh.frame(0)
     img, hdr, st = r.render(f)
     acc, ys, lim, att = orc.orc_pass1(orc.baked(sh.scene), f)
