@@ -301,9 +301,10 @@ def run_ours(args, so, world, rank, local):
     del host
     # per frame: tracer + resolve (plain); route, approach, band tracer, FP32 tracer, [turbulence sums,
     # transfer,] re-trace, gather, resolve (mixed); spp_max = spp, so no adaptive pass
-    # (plain FP64 with deferred torus sums: recording pass, sums, emission, ordered transfer, the
-    # replay pass that returns at once, resolve; or recording pass, sums, replay pass, resolve)
-    plain_launches = (6 if st.emit64 else 4) if st.rec64_slots else 2
+    # (plain FP64 with deferred passes, per wave: recording pass, [torus sums,] emission, ordered
+    # transfer, the replay launch that returns at once; then resolve)
+    torus_sums = 0 if flow else 1
+    plain_launches = (st.rec64_waves * (2 + torus_sums + (2 if st.emit64 else 0)) + 1) if st.rec64_slots else 2
     gpu_launches = args.steps * ((plain_launches if path == "fp64" else 9 if st.ms_turb > 0 else 7) +
                                  (1 if flow else 0))
     if flow:
@@ -344,21 +345,24 @@ def plain_fp64_record(so, sh, st, ms, ms_frame, clocks, npix, world, local):
     """The plain FP64 path's frames: rate, phase times and rooflines against the measured FP64 FMA
     peak.  With the deferred torus turbulence the frame is recording pass + k_turb64_records +
     k_emit64_records + k_transfer64 (or a replay pass instead of the last two); the sums kernel is
-    the dominant one, its algorithmic FLOPs are the recorded positions x modes x FLOPS_MODE."""
+    the dominant one, its algorithmic FLOPs are the recorded positions x modes x FLOPS_MODE.  The
+    reference flow model's frames defer their emission only (recording pass + k_emit64_records +
+    k_transfer64); their roofline is the whole frame's."""
     fp64_peak, _ = so.probe_fma_peak(local)
     pl = sh.plasma()
     n_modes = pl.n_modes if pl is not None else 0
     flops = (st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT + st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
     kernels = "k_trace64"
     if st.rec64_slots:
-        kernels = ("k_trace64 (recording pass) + k_turb64_records + k_emit64_records + k_transfer64" if st.emit64
-                   else "k_trace64 (recording + replay passes) + k_turb64_records")
+        sums = " + k_turb64_records" if n_modes else ""
+        kernels = (f"k_trace64 (recording pass){sums} + k_emit64_records + k_transfer64" if st.emit64
+                   else f"k_trace64 (recording + replay passes){sums}")
     whole = {"kernels": kernels,
              "ms": round(st.ms_kernel, 3), "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
              "unit": "TFLOP/s", "per_launch": flops}
     rec = {"bound": "fp64", "kernel": "k_trace64", "achieved": whole["achieved"], "peak": round(fp64_peak, 3),
            "unit": "TFLOP/s", "kernel_ms": round(st.ms_kernel, 3), "per_launch": flops}
-    if st.rec64_slots:
+    if st.rec64_slots and n_modes:
         sflops = st.rec64_records * n_modes * FLOPS_MODE
         rec = {"bound": "fp64", "kernel": "k_turb64_records", "achieved": round(sflops / (st.ms_sum64 * 1e-3) / 1e12, 3),
                "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel_ms": round(st.ms_sum64, 3), "per_launch": sflops,

@@ -175,7 +175,8 @@ typedef struct so_stats {
     long long turb_records; /* ... record slots summed (segments in use x 16) */
     long long redo_records; /* ... FP32 rays re-traced in FP64 because the record pool ran out */
     long long record_waves; /* ... waves the FP32 rays were traced in (the pool holds one wave's records) */
-    double ms_rec64;      /* plain FP64, deferred torus turbulence: device time of the recording pass */
+    double ms_rec64;      /* plain FP64, deferred passes (torus plasma; reference flow frames): device
+                             time of the recording pass */
     double ms_sum64;      /* ... of the FP64 turbulence sums over all records (k_turb64_records) */
     double ms_replay64;   /* ... of the replay pass (geodesic again, sums read back, emission); with
                              deferred emission it runs only when the record pool ran out */
@@ -185,6 +186,7 @@ typedef struct so_stats {
     double ms_emit64;     /* ... deferred emission: device time of the emission at every record and the
                              ordered transfer (0 when the replay pass does the emission) */
     int emit64;           /* ... 1 = the last trace deferred its emission too, 0 = replay pass */
+    int rec64_waves;      /* ... waves the last deferred trace ran in (the pool holds one wave) */
 } so_stats;
 
 /* Per-ray outputs of so_trace_rays.  Each pointer is a caller-owned host array, or NULL to skip. */

@@ -90,7 +90,7 @@ class Stats(C.Structure):
                 ("turb_records", C.c_longlong), ("redo_records", C.c_longlong), ("record_waves", C.c_longlong),
                 ("ms_rec64", C.c_double), ("ms_sum64", C.c_double), ("ms_replay64", C.c_double),
                 ("rec64_slots", C.c_longlong), ("rec64_short", C.c_longlong), ("rec64_records", C.c_longlong),
-                ("ms_emit64", C.c_double), ("emit64", C.c_int)]
+                ("ms_emit64", C.c_double), ("emit64", C.c_int), ("rec64_waves", C.c_int)]
 
 
 class RaysOut(C.Structure):

@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
             rtot = 0;
             rinline = false;
         } else {
-            rhead = L.job_head64[job * jobs_n + s];
+            rhead = L.job_head64[(job - L.job0) * jobs_n + s];
             rseg = rhead;
             rcnt = 0;
             rinline = rhead == -2;
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                 if (j >= (unsigned long long)total) {
                     exhausted = true;
                 } else {
-                    job = (long long)j;
+                    job = L.job0 + (long long)j;
                     active = true;
                     sample = 0;
                     const JobPlace q = job_place(L, job);
@@ -503,21 +503,23 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
         if (active) {
             stage = ray_attempt<VAR>(R, *S, emit, yn, k7, &hc, &err, &fate, rec ? cr : nullptr, cg);
             if (VAR == VAR_RADIO && stage == ST_ACCEPTED && S->flow_on && yn[0] < S->r_flow_max) {
-                if (defer == 1 || (defer == 2 && !rinline))
-                    want = torus_phase(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX);
-                else
-                    want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
+                if (tp.n_modes > 0) {
+                    if (defer == 1 || (defer == 2 && !rinline))
+                        want = torus_phase(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX);
+                    else
+                        want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
+                } else if (defer == 1) {
+                    want = flow_wants(*S, yn[0], yn[2]);
+                }
             }
         }
         // ---- all lanes: turbulence sums --------------------------------------------------------
         double delta = 0.0;
-        if (VAR == VAR_RADIO && tp.n_modes > 0) {
-            if (EMIT32) {
-                delta = warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ);
-            } else if (defer == 1) {
-                // recording pass: append the step (r, u, azimuth, h, tag) to the sample's chain; a
-                // lane whose segment is full closes it and takes the next one (one atomic per warp);
-                // a sample the pool cannot hold is summed in place by the replay pass
+        if (VAR == VAR_RADIO && defer == 1) {
+            {
+                // recording pass: append the step (r, u, azimuth or phi, h, tag[, t]) to the sample's
+                // chain; a lane whose segment is full closes it and takes the next one (one atomic per
+                // warp); a sample the pool cannot hold is left to the replay pass
                 const bool need_seg = want && !rinline && rcnt == REC_SEG;
                 const unsigned ms = __ballot_sync(FULL, need_seg);
                 if (ms) {
@@ -528,7 +530,8 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                     if (need_seg) {
                         const unsigned long long idx = base + __popc(ms & ((1u << lane) - 1u));
                         if (rseg >= 0)
-                            L.seg_meta64[rseg] = make_uint2((uint32_t)(job * jobs_n + sample), (uint32_t)REC_SEG);
+                            L.seg_meta64[rseg] =
+                                make_uint2((uint32_t)((job - L.job0) * jobs_n + sample), (uint32_t)REC_SEG);
                         if (idx >= (unsigned long long)L.seg_cap64) {
                             rinline = true;
                         } else {
@@ -546,16 +549,21 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                         (unsigned long long)(b >= 3 ? 3 : (b < 0 ? 0 : b)) | ((unsigned long long)R.natt << 2) |
                         ((unsigned long long)R.nacc << (2 + REC64_COUNT_BITS)) |
                         ((unsigned long long)(R.nflow + 1) << (2 + 2 * REC64_COUNT_BITS));
-                    double* slot = L.rec64 + REC64_W * ((long long)rseg * REC_SEG + rcnt);
+                    double* slot = L.rec64 + (long long)L.rec64_w * ((long long)rseg * REC_SEG + rcnt);
                     slot[0] = yn[0];
                     slot[1] = yn[2];
-                    slot[2] = TX;
+                    slot[2] = tp.n_modes > 0 ? TX : yn[4];
                     slot[3] = hc;
                     slot[4] = __longlong_as_double((long long)tag);
+                    if (tp.n_modes <= 0) slot[5] = yn[5];
                     ++rcnt;
                     ++rtot;
                     ++n_rec;
                 }
+            }
+        } else if (VAR == VAR_RADIO && tp.n_modes > 0) {
+            if (EMIT32) {
+                delta = warp_turbulence32(km, kamp, tp.n_modes, want, TX, TY, TZ);
             } else {
                 // in the tracer (defer 0), or in place for the replay pass's incomplete jobs
                 delta = warp_turbulence64(md, tp.n_modes, want && (defer == 0 || rinline), TX, TY, TZ);
@@ -567,7 +575,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                     }
                     // both passes take the same flow steps, so the chain always holds the record;
                     // were it ever short, the sum would be NaN (visible), never a read out of bounds
-                    delta = rseg >= 0 ? L.rec64[REC64_W * ((long long)rseg * REC_SEG + rcnt) + 2]
+                    delta = rseg >= 0 ? L.rec64[(long long)L.rec64_w * ((long long)rseg * REC_SEG + rcnt) + 2]
                                       : __longlong_as_double(-1ll);
                     ++rcnt;
                 }
@@ -583,7 +591,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
         if (defer == 1) {
             // recording pass: the sample's chain is closed with its end state, and the job's next
             // sample, if any, opens its own
-            const long long sid = job * jobs_n + sample;
+            const long long sid = (job - L.job0) * jobs_n + sample;
             L.job_head64[sid] = rinline ? -2 : rhead;
             if (rinline) atomicAdd(&L.rec64_ctl[1], 1ull);
             else if (rseg >= 0) L.seg_meta64[rseg] = make_uint2((uint32_t)sid, (uint32_t)rcnt);
@@ -710,7 +718,7 @@ __global__ void __launch_bounds__(256) k_turb64_records(const TraceLaunch L) {
         const bool live = lane < P && mine_slot < nslots &&
                           (int)(mine_slot % REC_SEG) < (int)L.seg_meta64[mine_slot / REC_SEG].y;
         double X = 0.0, Y = 0.0, Z = 0.0;
-        double* rec = L.rec64 + REC64_W * (live ? mine_slot : 0);
+        double* rec = L.rec64 + (long long)L.rec64_w * (live ? mine_slot : 0);
         if (live) torus_xyz(rec[0], rec[1], rec[2], &X, &Y, &Z);
         double px[P], py[P], pz[P], acc[P];
 #pragma unroll
@@ -741,19 +749,20 @@ cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_
     return cudaGetLastError();
 }
 
-// Deferred emission: flow_step at every record after its sum, one thread per slot over the slots
-// of the segments taken (a slot past its chain's last record is skipped).  Writes the step's
-// emission dI over r and its transmission exp(-dtau) over u.  The torus model reads neither the
-// azimuth nor the time of the step, nor the baked field.  Left to the replay pass when a sample ran
-// out of segments.
+// Deferred emission: flow_step at every record (after its sum, on the torus plasma), one thread per
+// slot over the slots of the segments taken (a slot past its chain's last record is skipped).
+// Writes the step's emission dI over r and its transmission exp(-dtau) over u.  The torus model
+// reads neither the azimuth nor the time of the step, nor the baked field; the reference flow model
+// reads its phi and t and fetches the frame's turbulence as the tracer does.  Left to the replay
+// pass when a sample ran out of segments.
 __global__ void __launch_bounds__(256) k_emit64_records(const TraceLaunch L) {
     if (*(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull) return;
     unsigned long long used = *(volatile unsigned long long*)&L.rec64_ctl[0];
     if (used > (unsigned long long)L.seg_cap64) used = (unsigned long long)L.seg_cap64;
     const long long nslots = (long long)used * REC_SEG;
     TorusParams tp;
-    tp.on = true;
-    tp.n_modes = L.n_modes;
+    tp.on = L.torus && L.n_modes > 0;
+    tp.n_modes = tp.on ? L.n_modes : 0;
     tp.ne_index = L.ne_index;
     tp.te_index = L.te_index;
     tp.h_sph = L.h_sph;
@@ -765,10 +774,14 @@ __global__ void __launch_bounds__(256) k_emit64_records(const TraceLaunch L) {
         if ((int)(slot % REC_SEG) >= (int)m.y) continue;
         const Sample64& smp = L.samp64[m.x];
         const int fidx = smp.fidx;
-        double* rec = L.rec64 + REC64_W * slot;
+        double* rec = L.rec64 + (long long)L.rec64_w * slot;
         double dI, dtau;
-        flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], nullptr, tp, rec[2], rec[0], rec[1], 0.0, 0.0,
-                  smp.lam, smp.E, rec[3], &dI, &dtau);
+        if (tp.on)
+            flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], nullptr, tp, rec[2], rec[0], rec[1], 0.0, 0.0,
+                      smp.lam, smp.E, rec[3], &dI, &dtau);
+        else
+            flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], L.turb_field, tp, 0.0, rec[0], rec[1], rec[2],
+                      rec[5], smp.lam, smp.E, rec[3], &dI, &dtau);
         rec[0] = dI;
         rec[1] = exp(-dtau);
     }
@@ -792,13 +805,14 @@ __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
     const unsigned long long cmask = (1ull << REC64_COUNT_BITS) - 1ull;
     unsigned long long n_att = 0, n_acc = 0, n_lim = 0, n_flow = 0;
     const long long total = skip ? 0 : L.nrays;
-    for (long long job = (long long)blockIdx.x * blockDim.x + threadIdx.x; job < total;
-         job += (long long)gridDim.x * blockDim.x) {
+    for (long long jrel = (long long)blockIdx.x * blockDim.x + threadIdx.x; jrel < total;
+         jrel += (long long)gridDim.x * blockDim.x) {
+        const long long job = L.job0 + jrel;
         const JobPlace q = job_place(L, job);
         float pa[4] = {0.f, 0.f, 0.f, 0.f};
         float ys = 0.f, yq = 0.f;
         for (int s = 0; s < q.jobs_n; ++s) {
-            const long long sid = job * q.jobs_n + s;
+            const long long sid = jrel * q.jobs_n + s;
             const Sample64 e = L.samp64[sid];
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             double trans = 1.0;
@@ -811,7 +825,7 @@ __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
                     acc[0] = __int_as_float(0x7fc00000);
                     break;
                 }
-                const double* rec = L.rec64 + REC64_W * (seg * REC_SEG + k);
+                const double* rec = L.rec64 + (long long)L.rec64_w * (seg * REC_SEG + k);
                 const double dI = rec[0], ex = rec[1];
                 const unsigned long long tag = (unsigned long long)__double_as_longlong(rec[4]);
                 const float cc = (float)(trans * dI);
@@ -1006,8 +1020,8 @@ cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaS
         case VAR_DISK: return go(k_trace64<VAR_DISK, false, 0>);
         default:
             if (emit32) return go(k_trace64<VAR_RADIO, true, 0>);
-            if (torus && L.defer64 == 1) return go(k_trace64<VAR_RADIO, false, 1>);
-            if (torus && L.defer64 == 2) return go(k_trace64<VAR_RADIO, false, 2>);
+            if (L.defer64 == 1) return go(k_trace64<VAR_RADIO, false, 1>);
+            if (L.defer64 == 2) return go(k_trace64<VAR_RADIO, false, 2>);
             return go(k_trace64<VAR_RADIO, false, 0>);
     }
 }

@@ -290,6 +290,17 @@ __device__ __forceinline__ float baked_sample(const so_scene& S, const float* fi
     return tex3D<float>((cudaTextureObject_t)S.turb_tex[k], x, y, z);
 }
 
+// Whether flow_step on the reference flow model (no torus) can change the transfer at (r, u): its
+// first two returns, in its own arithmetic.  A step for which this is false emits nothing and
+// transmits exactly 1.
+__device__ __forceinline__ bool flow_wants(const so_scene& S, double r, double u) {
+    double s2 = fmax(fma(-u, u, 1.0), 1e-12), s = sqrt(s2);
+    double R = r * s, z = r * u;
+    if (r > S.r_flow_max || R < 1e-3) return false;
+    double zh = z / (S.h_r * R);
+    return !(exp(-0.5 * zh * zh) < 1e-7);
+}
+
 // flow_step with the torus turbulence sum `delta` at this point already evaluated (torus_position).
 // With `field` (the frame's baked slices) the reference model's turbulence is sampled as
 // emission.cuh:112-124 does, else its sheared noise is evaluated in place (the turb_nt = 0 path).

@@ -26,13 +26,14 @@ enum Variant : int {
 // Device counters of one launch (zeroed before the launch).
 constexpr int REC_SEG = 16;  // flow-step record slots per segment
 
-// Record of the deferred FP64 torus path, REC64_W doubles per slot: [0] r, [1] u = cos theta,
-// [2] advected azimuth of the turbulence position (k_turb64_records overwrites it with the sum
-// delta), [3] the Mino step h, [4] tag.  k_emit64_records then overwrites [0] with the step's
-// emission dI and [1] with its transmission exp(-dtau).  The tag holds the image-order bucket
-// (bits 0-1: psi / pi clamped to 3) and the ray's attempt, accepted-step and flow-step counts after
-// this step (20 bits each from bit 2, 22 and 42; the path needs max_steps < 2^20).
-constexpr int REC64_W = 5;
+// Flow-step record of the deferred FP64 path, rec64_w doubles per slot: [0] r, [1] u = cos theta,
+// [2] torus plasma: the advected azimuth of the turbulence position (k_turb64_records overwrites
+// it with the sum delta); reference flow: phi, [3] the Mino step h, [4] tag, [5] reference flow
+// only: t.  k_emit64_records then overwrites [0] with the step's emission dI and [1] with its
+// transmission exp(-dtau).  The tag holds the image-order bucket (bits 0-1: psi / pi clamped to 3)
+// and the ray's attempt, accepted-step and flow-step counts after this step (20 bits each from bit
+// 2, 22 and 42; the path needs max_steps < 2^20).
+constexpr int REC64_W_TORUS = 5, REC64_W_FLOW = 6;
 constexpr int REC64_COUNT_BITS = 20;
 // End state of one sample after the recording pass.
 struct Sample64 {
@@ -157,7 +158,11 @@ struct TraceLaunch {
     // emission at every record and k_transfer64 applies them in order per sample, or pass 2
     // (defer64 = 2) integrates again and reads each sum back in order.  0 = sums in the tracer.
     int defer64;
-    double* rec64;            // record pool: slot s at doubles REC64_W s .. (layout at REC64_W)
+    double* rec64;            // record pool: slot s at doubles rec64_w s .. (layout at REC64_W_TORUS)
+    int rec64_w;              // doubles per record: REC64_W_TORUS or REC64_W_FLOW
+    long long job0;           // deferred passes in waves: this launch's jobs are job0 .. job0 + nrays - 1
+                              // of the frame's job numbering (chain heads and sample ends are indexed
+                              // from job0)
     uint32_t* seg_next64;     // per segment: the sample's next segment
     uint2* seg_meta64;        // per segment: (sample id owning it, records in it)
     Sample64* samp64;         // per sample id: the recording pass's end state

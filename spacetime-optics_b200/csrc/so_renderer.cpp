@@ -139,10 +139,11 @@ struct so_renderer {
     // luminance statistics of so_render (device buffers and the pinned result)
     LumScratch lum{};
     LumStat* h_lum = nullptr;
-    // deferred FP64 torus turbulence of the plain tracer: record pool (segments of REC_SEG slots of
-    // REC64_W doubles, each segment's link and owner), per-sample chain heads and end states, the
-    // recording pass's counters, and the pool's use
+    // deferred FP64 passes of the plain tracer: record pool (segments of REC_SEG slots of rec64_w
+    // doubles, each segment's link and owner), per-sample chain heads and end states, the recording
+    // pass's counters, and the pool's use
     double* d_rec64 = nullptr;
+    long long rec64_doubles = 0;               // size of d_rec64; segment arrays hold rec64_doubles / (REC_SEG * 5)
     uint32_t* d_seg_next64 = nullptr;
     uint2* d_seg_meta64 = nullptr;
     Sample64* d_samp64 = nullptr;
@@ -151,10 +152,11 @@ struct so_renderer {
     Counters* d_cnt64 = nullptr;
     long long seg_cap64 = 0, job_cap64 = 0, pool64_target = -1;
     double rec_per_sample64 = 320.0;           // pool size per sample (records), doubled after a shortage
-    unsigned long long* h_rec64 = nullptr;     // pinned copy of d_rec64_ctl after the last deferred trace
+    unsigned long long* h_rec64 = nullptr;     // pinned copies of d_rec64_ctl after each wave of the last deferred trace
     cudaEvent_t ev_rec64 = nullptr;
     bool rec64_pending = false;
-    cudaEvent_t ev64[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // recording, sums, emission, replay
+    std::vector<cudaEvent_t> ev64;             // per wave: recording, sums, emission, replay boundaries (5 each)
+    int waves64 = 0;                           // waves of the last deferred trace
     bool last_defer64 = false, last_emit64 = false;
     std::string err;
 };
@@ -434,31 +436,39 @@ int ensure_side_queue(so_renderer* r) {
     return SO_OK;
 }
 
-// Record pool of the deferred FP64 turbulence for `jobs` tracer jobs of `per_job` samples:
-// rec_per_sample64 records per sample plus one partly filled segment per sample, within half of the
-// free device memory and so_mixed_opts.pool_mb.  Samples that do not fit are summed in place by the
-// replay pass (the same sums, slower); such a shortage doubles the estimate for the next traces.
-int ensure_records64(so_renderer* r, long long jobs, int per_job) {
+// Record pool of the deferred FP64 passes for `jobs` tracer jobs of `per_job` samples, records of
+// `w` doubles: rec_per_sample64 records per sample plus one partly filled segment per sample, within
+// half of the free device memory and so_mixed_opts.pool_mb.  A launch the pool cannot hold at once
+// runs in waves of *wave_jobs jobs (at most kMaxWaves64); where even that would leave waves too
+// small to fill the GPU, it runs as one wave and the samples that do not fit are left to the replay
+// pass (the same result, slower).  A shortage doubles the estimate for the next traces.
+constexpr int kMaxWaves64 = 64;
+constexpr long long kDeferMinJobs = 4096;
+int ensure_records64(so_renderer* r, long long jobs, int per_job, int w, long long* wave_jobs) {
     if (!r->h_rec64) {
-        SO_CK(r, cudaMallocHost((void**)&r->h_rec64, 3 * sizeof(unsigned long long)));
-        r->h_rec64[0] = r->h_rec64[1] = r->h_rec64[2] = 0;
+        SO_CK(r, cudaMallocHost((void**)&r->h_rec64, 3 * kMaxWaves64 * sizeof(unsigned long long)));
+        std::memset(r->h_rec64, 0, 3 * kMaxWaves64 * sizeof(unsigned long long));
         SO_CK(r, cudaEventCreateWithFlags(&r->ev_rec64, cudaEventDisableTiming));
-        for (cudaEvent_t& e : r->ev64) SO_CK(r, cudaEventCreate(&e));
     }
     if (!r->d_rec64_ctl && dalloc(&r->d_rec64_ctl, 3) != cudaSuccess)
         return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
     if (!r->d_cnt64 && dalloc(&r->d_cnt64, 1) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
     if (r->rec64_pending && cudaEventQuery(r->ev_rec64) == cudaSuccess) {
         r->rec64_pending = false;
-        if (r->h_rec64[1] > 0) r->rec_per_sample64 *= 2.0;
+        unsigned long long short_samples = 0;
+        for (int k = 0; k < r->waves64; ++k) short_samples += r->h_rec64[3 * k + 1];
+        if (short_samples > 0) r->rec_per_sample64 *= 2.0;
     }
     cudaGetLastError();  // a pending event reports cudaErrorNotReady
-    const double per_seg = REC_SEG * REC64_W * sizeof(double) + sizeof(uint32_t) + sizeof(uint2);
+    const double seg_doubles = (double)REC_SEG * w;
+    const double per_seg = seg_doubles * sizeof(double) + sizeof(uint32_t) + sizeof(uint2);
     const double seg_per_job = (r->rec_per_sample64 / REC_SEG + 1.0) * per_job;  // a partly filled segment per sample
     long long want = std::min<long long>((long long)std::ceil((double)jobs * seg_per_job), 0x7fffffffll);
     if (r->mixed.pool_mb > 0.0)
         want = std::min<long long>(want, std::max<long long>(1, (long long)(r->mixed.pool_mb * 1048576.0 / per_seg)));
-    if (r->seg_cap64 <= 0 || want > r->pool64_target || (r->mixed.pool_mb > 0.0 && want < r->seg_cap64)) {
+    const long long want_d = (long long)(want * seg_doubles);
+    if (r->rec64_doubles <= 0 || want_d > r->pool64_target ||
+        (r->mixed.pool_mb > 0.0 && want_d < r->rec64_doubles)) {
         SO_CK(r, cudaStreamSynchronize(r->st));
         if (r->d_rec64) cudaFree(r->d_rec64);
         if (r->d_seg_next64) cudaFree(r->d_seg_next64);
@@ -466,19 +476,31 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
         r->d_rec64 = nullptr;
         r->d_seg_next64 = nullptr;
         r->d_seg_meta64 = nullptr;
-        r->seg_cap64 = 0;
+        r->rec64_doubles = 0;
         r->pool64_target = -1;
         size_t fr = 0, tot = 0;
         SO_CK(r, cudaMemGetInfo(&fr, &tot));
-        const long long cap = std::min<long long>(want, (long long)(0.5 * (double)fr / per_seg));
-        if (cap < 1) return fail(r, SO_ERR_ALLOC, "FP64 record pool: no device memory");
-        if (dalloc(&r->d_rec64, (size_t)cap * REC_SEG * REC64_W) != cudaSuccess ||
-            dalloc(&r->d_seg_next64, (size_t)cap) != cudaSuccess || dalloc(&r->d_seg_meta64, (size_t)cap) != cudaSuccess)
+        // segment arrays sized for the narrowest record (REC64_W_TORUS doubles)
+        const double per_double = sizeof(double) + (sizeof(uint32_t) + sizeof(uint2)) / (double)(REC_SEG * REC64_W_TORUS);
+        const long long cap_d = std::min<long long>(want_d, (long long)(0.5 * (double)fr / per_double));
+        const long long nseg = cap_d / (REC_SEG * REC64_W_TORUS);
+        if (nseg < 1) return fail(r, SO_ERR_ALLOC, "FP64 record pool: no device memory");
+        if (dalloc(&r->d_rec64, (size_t)cap_d) != cudaSuccess || dalloc(&r->d_seg_next64, (size_t)nseg) != cudaSuccess ||
+            dalloc(&r->d_seg_meta64, (size_t)nseg) != cudaSuccess)
             return fail(r, SO_ERR_ALLOC, "FP64 record pool: device allocation");
-        r->seg_cap64 = cap;
-        r->pool64_target = want;
+        r->rec64_doubles = cap_d;
+        r->pool64_target = want_d;
     }
-    const long long heads = jobs * per_job;  // one chain per sample
+    r->seg_cap64 = std::min<long long>(r->rec64_doubles / (REC_SEG * w), 0x7fffffffll);
+    if (r->seg_cap64 < 1) return fail(r, SO_ERR_ALLOC, "FP64 record pool: no segment");
+    long long wave = jobs;
+    if ((double)r->seg_cap64 < (double)jobs * seg_per_job) {
+        wave = (long long)((double)r->seg_cap64 / seg_per_job);
+        const long long min_wave = std::max<long long>(kDeferMinJobs, (jobs + kMaxWaves64 - 1) / kMaxWaves64);
+        if (wave < min_wave) wave = jobs;  // one wave; what does not fit goes to the replay pass
+    }
+    *wave_jobs = wave;
+    const long long heads = wave * per_job;  // one chain per sample
     if (heads > r->job_cap64) {
         if (r->d_job_head64) cudaFree(r->d_job_head64);
         if (r->d_samp64) cudaFree(r->d_samp64);
@@ -492,70 +514,91 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job) {
     return SO_OK;
 }
 
-// Launches of the FP64 tracer.  A torus-plasma launch with FP64 sums and at least kDeferMinJobs
-// host-counted jobs on the renderer's stream defers its sums: recording pass (geometry only) ->
-// k_turb64_records, then for frame work (pixels, samples, chunks) without a disk the emission too:
-// k_emit64_records -> k_transfer64, with the replay pass behind them running only if the pool ran
-// short; for ray lists (whose per-ray outputs need the geometry up to the opacity cut) and disk
-// scenes the replay pass.  Each is bit for bit the in-tracer result, with the sums and the emission
-// at full occupancy.  Everything else, and any launch whose pool cannot be had, sums in the tracer.
-constexpr long long kDeferMinJobs = 4096;
-
+// Launches of the FP64 tracer.  A launch of at least kDeferMinJobs host-counted jobs on the
+// renderer's stream defers work out of the tracer when it is a torus-plasma launch with FP64 sums,
+// or frame work on the reference flow model: a recording pass (geometry only, one record per flow
+// step that can emit) -> k_turb64_records (torus: the FP64 sums at every record) -> for frame work
+// (pixels, samples, chunks) without a disk, k_emit64_records (flow_step at every record) ->
+// k_transfer64 (ordered transfer), with a replay pass behind them that runs only if the pool ran
+// short; for torus ray lists (whose per-ray outputs need the geometry up to the opacity cut) and
+// torus disk scenes the replay pass instead of the emission kernels.  Each is bit for bit the
+// in-tracer result, with the sums and the emission at full occupancy.  Everything else, and any
+// launch whose pool cannot be had, runs in the tracer.
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
     const int var = variant_of(r->S);
     const cudaStream_t s = st ? st : r->st;
-    const bool defer = var == VAR_RADIO && L.torus && L.n_modes > 0 && !L.emit32 && !L.nrays_dev &&
-                       L.nrays >= kDeferMinJobs && s == r->st;
+    const bool torus = var == VAR_RADIO && L.torus && L.n_modes > 0;
+    const bool emit_ok = L.kind != RAYS_LIST && !r->S.disk_on && r->S.max_steps < (1 << REC64_COUNT_BITS);
+    const bool flow = var == VAR_RADIO && !torus && r->S.flow_on && emit_ok;
+    const bool defer = ((torus && !L.emit32) || flow) && !L.nrays_dev && L.nrays >= kDeferMinJobs && s == r->st;
     r->last_defer64 = false;
     if (defer) {
         const int per_job = L.kind == RAYS_PIXELS ? L.spp : L.kind == RAYS_CHUNKS ? L.chunk : 1;
-        if (ensure_records64(r, L.nrays, per_job) == SO_OK) {
-            SO_CK(r, cudaMemsetAsync(r->d_rec64_ctl, 0, 3 * sizeof(unsigned long long), s));
-            SO_CK(r, cudaMemsetAsync(r->d_cnt64, 0, sizeof(Counters), s));
-            TraceLaunch L1 = L;
-            L1.defer64 = 1;
-            L1.counters = r->d_cnt64;
-            L1.rec64 = r->d_rec64;
-            L1.seg_next64 = r->d_seg_next64;
-            L1.job_head64 = r->d_job_head64;
-            L1.seg_cap64 = r->seg_cap64;
-            L1.rec64_ctl = r->d_rec64_ctl;
-            L1.seg_meta64 = r->d_seg_meta64;
-            L1.samp64 = r->d_samp64;
-            const bool emit64 = L.kind != RAYS_LIST && !r->S.disk_on &&
-                                r->S.max_steps < (1 << REC64_COUNT_BITS);
-            TraceLaunch L2 = L1;
-            L2.defer64 = 2;
-            L2.counters = L.counters;
-            L2.replay_if_short = emit64 ? 1 : 0;
-            cudaEventRecord(r->ev64[0], s);
-            cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
-            if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
-            cudaEventRecord(r->ev64[1], s);
-            e = launch_turb64_records(L1, r->num_sms, s);
-            if (e != cudaSuccess) return cuda_fail(r, e, "FP64 turbulence sums");
-            cudaEventRecord(r->ev64[2], s);
-            if (emit64) {
-                TraceLaunch Le = L1;
-                Le.counters = L.counters;
-                e = launch_emit64_records(Le, r->num_sms, s);
-                if (e != cudaSuccess) return cuda_fail(r, e, "FP64 deferred emission");
-                e = launch_transfer64(Le, r->num_sms, s);
-                if (e != cudaSuccess) return cuda_fail(r, e, "FP64 ordered transfer");
+        const int w = torus ? REC64_W_TORUS : REC64_W_FLOW;
+        long long wave = 0;
+        if (ensure_records64(r, L.nrays, per_job, w, &wave) == SO_OK) {
+            const int nw = (int)((L.nrays + wave - 1) / wave);
+            while ((int)r->ev64.size() < 5 * nw) {
+                cudaEvent_t e = nullptr;
+                SO_CK(r, cudaEventCreate(&e));
+                r->ev64.push_back(e);
             }
-            cudaEventRecord(r->ev64[3], s);
-            e = launch_trace64(L2, var, r->num_sms, s);
-            if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
-            cudaEventRecord(r->ev64[4], s);
-            SO_CK(r, cudaMemcpyAsync(r->h_rec64, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
-                                     cudaMemcpyDeviceToHost, s));
+            for (int k = 0; k < nw; ++k) {
+                const long long j0 = (long long)k * wave;
+                SO_CK(r, cudaMemsetAsync(r->d_rec64_ctl, 0, 3 * sizeof(unsigned long long), s));
+                SO_CK(r, cudaMemsetAsync(r->d_cnt64, 0, sizeof(Counters), s));
+                TraceLaunch L1 = L;
+                L1.defer64 = 1;
+                L1.counters = r->d_cnt64;
+                L1.rec64 = r->d_rec64;
+                L1.rec64_w = w;
+                L1.job0 = j0;
+                L1.nrays = std::min<long long>(wave, L.nrays - j0);
+                L1.seg_next64 = r->d_seg_next64;
+                L1.seg_meta64 = r->d_seg_meta64;
+                L1.samp64 = r->d_samp64;
+                L1.job_head64 = r->d_job_head64;
+                L1.seg_cap64 = r->seg_cap64;
+                L1.rec64_ctl = r->d_rec64_ctl;
+                TraceLaunch L2 = L1;
+                L2.defer64 = 2;
+                L2.counters = L.counters;
+                L2.replay_if_short = emit_ok ? 1 : 0;
+                cudaEvent_t* ev = &r->ev64[5 * k];
+                cudaEventRecord(ev[0], s);
+                cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
+                if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
+                cudaEventRecord(ev[1], s);
+                if (torus) {
+                    e = launch_turb64_records(L1, r->num_sms, s);
+                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 turbulence sums");
+                }
+                cudaEventRecord(ev[2], s);
+                if (emit_ok) {
+                    TraceLaunch Le = L1;
+                    Le.counters = L.counters;
+                    e = launch_emit64_records(Le, r->num_sms, s);
+                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 deferred emission");
+                    e = launch_transfer64(Le, r->num_sms, s);
+                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 ordered transfer");
+                }
+                cudaEventRecord(ev[3], s);
+                // the replay pass's queue starts at the wave's first job
+                SO_CK(r, cudaMemsetAsync(&L.counters->next, 0, sizeof(unsigned long long), s));
+                e = launch_trace64(L2, var, r->num_sms, s);
+                if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
+                cudaEventRecord(ev[4], s);
+                SO_CK(r, cudaMemcpyAsync(r->h_rec64 + 3 * k, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
+                                         cudaMemcpyDeviceToHost, s));
+            }
             SO_CK(r, cudaEventRecord(r->ev_rec64, s));
             r->rec64_pending = true;
+            r->waves64 = nw;
             r->last_defer64 = true;
-            r->last_emit64 = emit64;
+            r->last_emit64 = emit_ok;
             return SO_OK;
         }
-        r->err.clear();  // no pool: sum in the tracer
+        r->err.clear();  // no pool: run in the tracer
     }
     cudaError_t e = launch_trace64(L, var, r->num_sms, s);
     if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch");
@@ -1031,21 +1074,25 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
         stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = stats->ms_emit64 = 0.0;
         stats->rec64_slots = stats->rec64_short = stats->rec64_records = 0;
         stats->emit64 = 0;
-        if (r->last_defer64) {  // the last tracer launch deferred its FP64 sums (stream synchronised above)
-            float a = 0.f, b = 0.f, c2 = 0.f, d = 0.f;
-            cudaEventElapsedTime(&a, r->ev64[0], r->ev64[1]);
-            cudaEventElapsedTime(&b, r->ev64[1], r->ev64[2]);
-            cudaEventElapsedTime(&c2, r->ev64[2], r->ev64[3]);
-            cudaEventElapsedTime(&d, r->ev64[3], r->ev64[4]);
-            stats->ms_rec64 = a;
-            stats->ms_sum64 = b;
-            stats->ms_emit64 = c2;
-            stats->ms_replay64 = d;
-            stats->emit64 = r->last_emit64 && r->h_rec64[1] == 0 ? 1 : 0;
-            const unsigned long long used = std::min<unsigned long long>(r->h_rec64[0], (unsigned long long)r->seg_cap64);
-            stats->rec64_slots = (long long)used * REC_SEG;
-            stats->rec64_short = (long long)r->h_rec64[1];
-            stats->rec64_records = (long long)r->h_rec64[2];
+        stats->rec64_waves = 0;
+        if (r->last_defer64) {  // the last tracer launch deferred work (stream synchronised above)
+            unsigned long long slots = 0, short_samples = 0, records = 0;
+            for (int k = 0; k < r->waves64; ++k) {
+                float t[4] = {0.f, 0.f, 0.f, 0.f};
+                for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&t[i], r->ev64[5 * k + i], r->ev64[5 * k + i + 1]);
+                stats->ms_rec64 += t[0];
+                stats->ms_sum64 += t[1];
+                stats->ms_emit64 += t[2];
+                stats->ms_replay64 += t[3];
+                slots += std::min<unsigned long long>(r->h_rec64[3 * k], (unsigned long long)r->seg_cap64) * REC_SEG;
+                short_samples += r->h_rec64[3 * k + 1];
+                records += r->h_rec64[3 * k + 2];
+            }
+            stats->emit64 = r->last_emit64 && short_samples == 0 ? 1 : 0;
+            stats->rec64_slots = (long long)slots;
+            stats->rec64_short = (long long)short_samples;
+            stats->rec64_records = (long long)records;
+            stats->rec64_waves = r->waves64;
         }
         float ms1 = 0.f, ms2 = 0.f;
         cudaEventElapsedTime(&ms1, ev[0], ev[1]);

@@ -372,6 +372,55 @@ def test_deferred_fp64_emission_adaptive_chunks(so):
     assert _counts(sa) == _counts(sb)
 
 
+def test_deferred_fp64_waves(so):
+    """A record pool that holds about a third of the frame: the deferred passes run in waves of
+    consecutive jobs, and the frame and every counter equal the single-wave frame's bit for bit."""
+    n = 128
+    ov = [f"camera.width={n}", f"camera.height={n}", "render.spp=2", "render.spp_max=2", "flow.n0=1594262.8"]
+
+    def render(pool_mb):
+        sh = so.Shot("synchrotron_1024.ini", ov)
+        r = so.Renderer(sh.scene, sh.tables, sh.settings)
+        r.set_plasma(sh.plasma())
+        r.set_precision(so.abi.SO_PREC_FP64, pool_mb=pool_mb)
+        img, _, st = r.render(sh.frame(0))
+        r.close()
+        return img, st
+
+    a, sa = render(0.0)
+    b, sb = render(140.0)
+    print("waves:", sa.rec64_waves, "->", sb.rec64_waves, "records", sa.rec64_records, sb.rec64_records)
+    assert sa.rec64_waves == 1 and sb.rec64_waves >= 3
+    assert sa.emit64 == 1 and sb.emit64 == 1 and sb.rec64_short == 0
+    assert sa.rec64_records == sb.rec64_records
+    assert np.array_equal(a, b)
+    assert _counts(sa) == _counts(sb)
+
+
+@pytest.mark.parametrize("noise", ["BAKED", "BAKED_FP32", "INLINE"])
+def test_deferred_fp64_emission_reference_flow(so, noise):
+    """Frames of the reference flow model defer their emission too (recording pass,
+    k_emit64_records, k_transfer64).  For each turbulence fetch (texture unit, FP32 trilinear,
+    in-place noise) the frame and its counters equal the in-tracer frame's (record pool capped to
+    one segment, so the replay pass renders it) bit for bit."""
+    n = 96
+    sh = so.Shot("m87_reference_flow.ini", [f"camera.width={n}", f"camera.height={n}", "render.spp=2",
+                                            "render.spp_max=2"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(getattr(so.abi, "SO_FLOW_NOISE_" + noise))
+    f = sh.frame(0)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    a, _, sa = r.render(f)
+    r.set_precision(so.abi.SO_PREC_FP64, pool_mb=0.001)
+    b, _, sb = r.render(f)
+    r.close()
+    assert sa.emit64 == 1 and sa.rec64_records > 0 and sa.rec64_short == 0 and sa.ms_sum64 < 0.05
+    assert sb.emit64 == 0 and sb.rec64_short > 0
+    assert a[..., 0].max() > 0
+    assert np.array_equal(a, b)
+    assert _counts(sa) == _counts(sb)
+
+
 def test_torus_plasma_vs_oracle(so, orc):
     """Synchrotron torus with 512 Fourier modes (FP64 everywhere), 40 x 40 over the +-12 M field."""
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=40", "camera.height=40"])
