@@ -1,4 +1,4 @@
-"""Coefficients of cos_turns (so_math.cuh; the oracle repeats them): a near-minimax polynomial of
+"""Coefficients of cos_turns (so_kerr.cuh; the oracle repeats them): a near-minimax polynomial of
 degree 8 in z = g^2 for cos(2 pi g) on |g| <= 1/4 turn, from Chebyshev interpolation of
 cos(2 pi sqrt(z)) on [0, 1/16] at 60-digit precision, printed as C hex-float literals (ascending
 powers of z).  Run: python fit_cos_turns.py"""

@@ -362,10 +362,12 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // Register budget: three 128-thread CTAs per SM (at most 170 registers).  Measured on the B200
 // against the compiler's free choice (194 registers, two CTAs): the plain FP64 synchrotron frame
 // runs 1.29x faster with a few spilled registers and 50 % more warps.
-// DEFER (deferred FP64 torus turbulence, radio torus only): 0 = sums in the tracer, 1 = recording pass
-// (geometry only: no emission code), 2 = replay pass.  Both passes run four CTAs per SM (128
-// registers): measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against
-// 205 ms at three CTAs (168 registers, fewer spills); the recording pass 58 against 62 ms.
+// DEFER (deferred FP64 passes, radio only): 0 = emission in the tracer, 1 = recording pass (geometry
+// only: no emission code), 2 = replay pass.  Both passes run four CTAs per SM (128 registers):
+// measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against 205 ms at
+// three CTAs (168 registers, fewer spills); the recording pass 78 ms, against 84 ms at five CTAs
+// (96 registers) and 88 ms at six (80), whose spills cost more than the warps gain (the reference
+// flow frame: 80, 89 and 100 ms).
 template <int VAR, bool EMIT32, int DEFER>
 __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const TraceLaunch L) {
     extern __shared__ double smem[];
