@@ -259,7 +259,7 @@ def run_ours(args, so, world, rank, local):
         roof = {"bound": "fp64", "achieved": round(flops / (st.ms_kernel * 1e-3) / 1e12, 3),
                 "peak": round(fp64_peak, 3), "unit": "TFLOP/s", "kernel": "k_trace64", "kernel_ms": st.ms_kernel,
                 "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
-    elif st.ms_turb > 0:
+    elif st.turb_records > 0:
         # deferred turbulence: the batched mode sums dominate, one SFU cosine per Fourier mode per
         # record slot (the FP32 tracer and the ordered transfer are listed beside it)
         sfu_peak = so.probe_sfu_peak(local)
@@ -283,6 +283,10 @@ def run_ours(args, so, world, rank, local):
                 "unit": "Gop/s", "kernel": "k_trace32", "kernel_ms": st.ms_fp32, "per_launch": ops,
                 "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
                 "fp32_tflops_peak": round(fp32_peak, 3)}
+        if st.record_waves > 0:  # deferred emission without mode sums (reference flow): tracer + transfer
+            roof["kernels"] = "k_trace32 + k_flow_records"
+            roof["tracer_k_trace32_ms"] = round(st.ms_fp32_trace, 3)
+            roof["transfer_k_flow_records_ms"] = round(st.ms_fp32 - st.ms_fp32_trace - st.ms_turb, 3)
     roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
     roof.setdefault("traffic", None)
     # e2e: host buffers through so_render (frame H2D, image D2H inside the timed region)
@@ -305,8 +309,11 @@ def run_ours(args, so, world, rank, local):
     # transfer, the replay launch that returns at once; then resolve)
     torus_sums = 0 if flow else 1
     plain_launches = (st.rec64_waves * (2 + torus_sums + (2 if st.emit64 else 0)) + 1) if st.rec64_slots else 2
-    gpu_launches = args.steps * ((plain_launches if path == "fp64" else 9 if st.ms_turb > 0 else 7) +
-                                 (1 if flow else 0))
+    # mixed: route, approach, band tracer, FP32 tracer, re-trace, gather, resolve, and per wave of
+    # the deferred form an FP32 tracer launch beyond the first, the mode sums (torus) and the transfer
+    waves = max(st.record_waves, 1)
+    mixed_launches = 7 + (waves - 1) + (waves * ((1 if st.turb_records > 0 else 0) + 1) if st.record_waves > 0 else 0)
+    gpu_launches = args.steps * ((plain_launches if path == "fp64" else mixed_launches) + (1 if flow else 0))
     if flow:
         workload = (f"reference flow {W}x{W} (n ~ r^-1.1, fBm turbulence baked per frame into 24 slices of "
                     f"512x192x48), a=0.94, i=163 deg, fov 30 M, 230 GHz, step fraction 0.01, 1 R2-jittered "

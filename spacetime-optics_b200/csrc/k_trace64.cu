@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
         const bool need = !active && !exhausted && (lane & (stride - 1)) == 0;
         const bool grab = need && chunk_left == 0;
         const unsigned m = __ballot_sync(FULL, grab);
-        unsigned long long j = (unsigned long long)job + 1;  // the next job of the lane's grab
+        unsigned long long j = (unsigned long long)(job - L.job0) + 1;  // the next job of the lane's grab
         if (m) {
             const int leader = __ffs(m) - 1;
             unsigned long long base = 0;
