@@ -686,8 +686,10 @@ def cpu_baseline_disk(so, sh, f, W, budget_s=15.0):
 
 def run_wavefront(args, so, world, rank, local):
     """The photon-ring batch: 4 spins x 2 inclinations x 8 turbulence times / zooms of the torus
-    plasma, W x W windows on the critical curve, all frames in one persistent launch replayed from a
-    CUDA graph, launch shape from the autotuner (run on a 128 x 128 copy of the batch)."""
+    plasma, W x W windows on the critical curve, all frames in one job space: a persistent recording
+    pass over every frame, the turbulence sums at its records (FP32 for mixed precision, FP64
+    otherwise), the emission and the ordered transfer, in waves through the record pool, replayed
+    from a CUDA graph; launch shape from the autotuner (run on a 128 x 128 copy of the batch)."""
     import importlib
     import torch
     torch.cuda.set_device(local)
@@ -733,7 +735,9 @@ def run_wavefront(args, so, world, rank, local):
                  st.flow_steps * (FLOPS_FLOW + n_modes * FLOPS_MODE))
         achieved = flops / (ms_step * 1e-3) / 1e12
         roof = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64_peak, 3), "unit": "TFLOP/s",
-                "frac": round(achieved / fp64_peak, 4), "traffic": None, "kernel": "k_trace64",
+                "frac": round(achieved / fp64_peak, 4), "traffic": None,
+                "kernel": ("whole batch: k_trace64 recording pass + k_turb64_records + k_emit64_records + k_transfer64"
+                           if st.rec64_waves else "k_trace64"),
                 "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)"}
     else:
         # FP64 geometry, FP32 turbulence sums: the SFU cosines (one per mode per flow step) dominate
@@ -741,7 +745,9 @@ def run_wavefront(args, so, world, rank, local):
         ops = st.flow_steps * n_modes
         achieved = ops / (ms_step * 1e-3) / 1e9
         roof = {"bound": "sfu", "achieved": round(achieved, 3), "peak": round(sfu_peak, 3), "unit": "Gop/s",
-                "frac": round(achieved / sfu_peak, 4), "traffic": None, "kernel": "k_trace64 (FP32 sums)",
+                "frac": round(achieved / sfu_peak, 4), "traffic": None,
+                "kernel": ("whole batch: k_trace64 recording pass + k_turb32_rec64 + k_emit64_records + k_transfer64"
+                           if st.rec64_waves else "k_trace64 (FP32 sums)"),
                 "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
                 "fp64_geometry_flops": st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT}
     line = {
@@ -750,15 +756,21 @@ def run_wavefront(args, so, world, rank, local):
         "vs_baseline": None, "dtype": "f64" if prec == so.abi.SO_PREC_FP64 else "f64+f32", "data": "synthetic",
         "config": {"workload": f"photon-ring batch: {len(frames)} frames of {W}x{W} (spins 0/0.5/0.9/0.99, "
                                "incl 17/60 deg, 8 turbulence times, zoom 1e3-4e4 on the critical curve), torus "
-                               "plasma with 512 modes, one persistent launch replayed from a CUDA graph",
+                               "plasma with 512 modes, " + (f"deferred sums and emission in {st.rec64_waves} waves"
+                                                            if st.rec64_waves else "one persistent launch") +
+                               " replayed from a CUDA graph",
                    "tune": {"ctas_per_sm": tune.ctas_per_sm, "interleave": tune.interleave, "tile": tune.tile,
                             "queue_chunk": tune.queue_chunk, "tuned_on": "128x128"},
                    "frames_per_s": round(world * len(frames) / (ms_step * 1e-3), 4),
                    "attempts_per_ray": st.attempts / nrays, "flow_steps_per_ray": st.flow_steps / nrays,
+                   "records": st.rec64_records, "record_waves": st.rec64_waves,
+                   "samples_traced_in_place": st.rec64_short,
                    "l2": "inputs (mode table, frame descriptors) are small; no flush (one step is seconds long)"},
         "roofline": roof,
         "e2e": None,
-        "gpu_launches": args.steps * 3,
+        # per wave: recording pass, sums, emission, transfer, replay launch (returns at once); then
+        # resolve; without waves: the persistent tracer and resolve
+        "gpu_launches": args.steps * ((st.rec64_waves * 5 + 1) if st.rec64_waves else 2),
         "clocks": clk.summary(),
     }
     b.close()

@@ -766,6 +766,58 @@ cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_
     return cudaGetLastError();
 }
 
+// The mixed form of the deferred sums (FP64 geometry, FP32 turbulence sums, as the tracer's EMIT32):
+// FP32 SFU cosines at every record of a recording pass, the modes folded to FP32 in constant memory
+// (the kernel parameter), kTurb32RecP positions per thread at slots c0 + t + 256 q of a block's
+// chunk, each position formed in FP64 from (r, u, azimuth) as the tracer forms it and rounded to
+// FP32.  The sum (in mode order) goes to the record's slot [2] as the FP64 sums do.
+constexpr int kTurb32RecP = 8;
+__global__ void __launch_bounds__(256) k_turb32_rec64(const TraceLaunch L, const __grid_constant__ TurbModes M) {
+    unsigned long long used = *(volatile unsigned long long*)&L.rec64_ctl[0];
+    if (used > (unsigned long long)L.seg_cap64) used = (unsigned long long)L.seg_cap64;
+    const long long nslots = (long long)used * REC_SEG;
+    const int nm = M.n;
+    constexpr int P = kTurb32RecP;
+    const long long chunk = 256LL * P;
+    for (long long c0 = (long long)blockIdx.x * chunk; c0 < nslots; c0 += (long long)gridDim.x * chunk) {
+        float x[P], y[P], z[P], acc[P];
+        bool live[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const long long slot = c0 + threadIdx.x + 256LL * q;
+            live[q] = slot < nslots && (int)(slot % REC_SEG) < (int)L.seg_meta64[slot / REC_SEG].y;
+            double X = 0.0, Y = 0.0, Z = 0.0;
+            if (live[q]) {
+                const double* rec = L.rec64 + (long long)L.rec64_w * slot;
+                torus_xyz(rec[0], rec[1], rec[2], &X, &Y, &Z);
+            }
+            x[q] = (float)X;
+            y[q] = (float)Y;
+            z[q] = (float)Z;
+            acc[q] = 0.f;
+        }
+#pragma unroll 2
+        for (int m = 0; m < nm; ++m) {
+            const float4 k = M.k[m];
+            const float am = M.a[m];
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+                acc[q] = fmaf(am, __cosf(fmaf(k.z, z[q], fmaf(k.y, y[q], fmaf(k.x, x[q], k.w)))), acc[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < P; ++q)
+            if (live[q]) L.rec64[(long long)L.rec64_w * (c0 + threadIdx.x + 256LL * q) + 2] = (double)acc[q];
+    }
+}
+
+cudaError_t launch_turb32_rec64(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st) {
+    int per_sm = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_turb32_rec64, 256, 0);
+    if (e != cudaSuccess) return e;
+    k_turb32_rec64<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, st>>>(L, M);
+    return cudaGetLastError();
+}
+
 // Deferred emission: flow_step at every record (after its sum, on the torus plasma), one thread per
 // slot over the slots of the segments taken (a slot past its chain's last record is skipped).
 // Writes the step's emission dI over r and its transmission exp(-dtau) over u.  The torus model

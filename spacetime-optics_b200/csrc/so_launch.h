@@ -228,6 +228,8 @@ struct TurbModes {
 };
 void turb_modes_fold(const so_mode* modes, int n, TurbModes* out);
 cudaError_t launch_turb_records(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
+// FP32 sums (SFU) at every record of a defer64 = 1 pass: the mixed form of launch_turb64_records.
+cudaError_t launch_turb32_rec64(const TraceLaunch& L, const TurbModes& M, int num_sms, cudaStream_t st);
 // FP64 sums at every record of a defer64 = 1 pass (modes from L.modes, L.n_modes of them), the
 // emission at every record, and the ordered transfer of every job's samples into the outputs.
 cudaError_t launch_turb64_records(const TraceLaunch& L, int num_sms, cudaStream_t st);

@@ -157,6 +157,7 @@ struct so_renderer {
     bool rec64_pending = false;
     std::vector<cudaEvent_t> ev64;             // per wave: recording, sums, emission, replay boundaries (5 each)
     int waves64 = 0;                           // waves of the last deferred trace
+    long long samples64 = 0;                   // samples of the last deferred trace (for the estimate)
     bool last_defer64 = false, last_emit64 = false;
     std::string err;
 };
@@ -454,10 +455,15 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job, int w, long lo
         return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
     if (!r->d_cnt64 && dalloc(&r->d_cnt64, 1) != cudaSuccess) return fail(r, SO_ERR_ALLOC, "FP64 record pool: allocation");
     if (r->rec64_pending && cudaEventQuery(r->ev_rec64) == cudaSuccess) {
+        // the last deferred trace's records per sample, with a margin; doubled after a shortage
         r->rec64_pending = false;
-        unsigned long long short_samples = 0;
-        for (int k = 0; k < r->waves64; ++k) short_samples += r->h_rec64[3 * k + 1];
-        if (short_samples > 0) r->rec_per_sample64 *= 2.0;
+        unsigned long long short_samples = 0, records = 0;
+        for (int k = 0; k < r->waves64; ++k) {
+            short_samples += r->h_rec64[3 * k + 1];
+            records += r->h_rec64[3 * k + 2];
+        }
+        const double seen = r->samples64 > 0 ? 1.5 * (double)records / (double)r->samples64 : 0.0;
+        r->rec_per_sample64 = std::max(short_samples > 0 ? 2.0 * r->rec_per_sample64 : r->rec_per_sample64, seen);
     }
     cudaGetLastError();  // a pending event reports cudaErrorNotReady
     const double seg_doubles = (double)REC_SEG * w;
@@ -524,6 +530,76 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job, int w, long lo
 // torus disk scenes the replay pass instead of the emission kernels.  Each is bit for bit the
 // in-tracer result, with the sums and the emission at full occupancy.  Everything else, and any
 // launch whose pool cannot be had, runs in the tracer.
+// The deferred passes of one launch on stream s, in waves of `wave` jobs through the pool that
+// ensure_records64 set up: per wave a recording pass, the sums (sums: 0 none, 1 FP64, 2 FP32), the
+// emission and ordered transfer (emit), and a replay pass that runs when the pool ran short (always,
+// without emit).  With `timed` the phases are bracketed by events (not inside a graph capture).
+// Each wave's pool counters go to h_rec64 for the shortage feedback and the statistics.
+int enqueue_deferred64(so_renderer* r, const TraceLaunch& L, int var, cudaStream_t s, long long wave, int w, int sums,
+                       bool emit, bool timed) {
+    const int nw = (int)((L.nrays + wave - 1) / wave);
+    if (nw > kMaxWaves64) return fail(r, SO_ERR_SIZE, "FP64 record pool: too many waves");
+    if (timed) {
+        while ((int)r->ev64.size() < 5 * nw) {
+            cudaEvent_t e = nullptr;
+            SO_CK(r, cudaEventCreate(&e));
+            r->ev64.push_back(e);
+        }
+    }
+    for (int k = 0; k < nw; ++k) {
+        const long long j0 = (long long)k * wave;
+        SO_CK(r, cudaMemsetAsync(r->d_rec64_ctl, 0, 3 * sizeof(unsigned long long), s));
+        SO_CK(r, cudaMemsetAsync(r->d_cnt64, 0, sizeof(Counters), s));
+        TraceLaunch L1 = L;
+        L1.defer64 = 1;
+        L1.emit32 = 0;
+        L1.counters = r->d_cnt64;
+        L1.rec64 = r->d_rec64;
+        L1.rec64_w = w;
+        L1.job0 = j0;
+        L1.nrays = std::min<long long>(wave, L.nrays - j0);
+        L1.seg_next64 = r->d_seg_next64;
+        L1.seg_meta64 = r->d_seg_meta64;
+        L1.samp64 = r->d_samp64;
+        L1.job_head64 = r->d_job_head64;
+        L1.seg_cap64 = r->seg_cap64;
+        L1.rec64_ctl = r->d_rec64_ctl;
+        TraceLaunch L2 = L1;
+        L2.defer64 = 2;
+        L2.counters = L.counters;
+        L2.replay_if_short = emit ? 1 : 0;
+        L2.emit32 = 0;
+        cudaEvent_t* ev = timed ? &r->ev64[5 * k] : nullptr;
+        if (ev) cudaEventRecord(ev[0], s);
+        cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
+        if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
+        if (ev) cudaEventRecord(ev[1], s);
+        if (sums == 1) e = launch_turb64_records(L1, r->num_sms, s);
+        else if (sums == 2) e = launch_turb32_rec64(L1, *r->turb_modes, r->num_sms, s);
+        if (e != cudaSuccess) return cuda_fail(r, e, "deferred turbulence sums");
+        if (ev) cudaEventRecord(ev[2], s);
+        if (emit) {
+            TraceLaunch Le = L1;
+            Le.counters = L.counters;
+            e = launch_emit64_records(Le, r->num_sms, s);
+            if (e != cudaSuccess) return cuda_fail(r, e, "FP64 deferred emission");
+            e = launch_transfer64(Le, r->num_sms, s);
+            if (e != cudaSuccess) return cuda_fail(r, e, "FP64 ordered transfer");
+        }
+        if (ev) cudaEventRecord(ev[3], s);
+        // the replay pass's queue starts at the wave's first job (it reads each recorded sum back,
+        // whichever form summed it, and sums the samples the pool could not hold in FP64)
+        SO_CK(r, cudaMemsetAsync(&L.counters->next, 0, sizeof(unsigned long long), s));
+        e = launch_trace64(L2, var, r->num_sms, s);
+        if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
+        if (ev) cudaEventRecord(ev[4], s);
+        SO_CK(r, cudaMemcpyAsync(r->h_rec64 + 3 * k, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+    }
+    r->waves64 = nw;
+    return SO_OK;
+}
+
 int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) {
     const int var = variant_of(r->S);
     const cudaStream_t s = st ? st : r->st;
@@ -537,63 +613,10 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
         const int w = torus ? REC64_W_TORUS : REC64_W_FLOW;
         long long wave = 0;
         if (ensure_records64(r, L.nrays, per_job, w, &wave) == SO_OK) {
-            const int nw = (int)((L.nrays + wave - 1) / wave);
-            while ((int)r->ev64.size() < 5 * nw) {
-                cudaEvent_t e = nullptr;
-                SO_CK(r, cudaEventCreate(&e));
-                r->ev64.push_back(e);
-            }
-            for (int k = 0; k < nw; ++k) {
-                const long long j0 = (long long)k * wave;
-                SO_CK(r, cudaMemsetAsync(r->d_rec64_ctl, 0, 3 * sizeof(unsigned long long), s));
-                SO_CK(r, cudaMemsetAsync(r->d_cnt64, 0, sizeof(Counters), s));
-                TraceLaunch L1 = L;
-                L1.defer64 = 1;
-                L1.counters = r->d_cnt64;
-                L1.rec64 = r->d_rec64;
-                L1.rec64_w = w;
-                L1.job0 = j0;
-                L1.nrays = std::min<long long>(wave, L.nrays - j0);
-                L1.seg_next64 = r->d_seg_next64;
-                L1.seg_meta64 = r->d_seg_meta64;
-                L1.samp64 = r->d_samp64;
-                L1.job_head64 = r->d_job_head64;
-                L1.seg_cap64 = r->seg_cap64;
-                L1.rec64_ctl = r->d_rec64_ctl;
-                TraceLaunch L2 = L1;
-                L2.defer64 = 2;
-                L2.counters = L.counters;
-                L2.replay_if_short = emit_ok ? 1 : 0;
-                cudaEvent_t* ev = &r->ev64[5 * k];
-                cudaEventRecord(ev[0], s);
-                cudaError_t e = launch_trace64(L1, var, r->num_sms, s);
-                if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (recording pass)");
-                cudaEventRecord(ev[1], s);
-                if (torus) {
-                    e = launch_turb64_records(L1, r->num_sms, s);
-                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 turbulence sums");
-                }
-                cudaEventRecord(ev[2], s);
-                if (emit_ok) {
-                    TraceLaunch Le = L1;
-                    Le.counters = L.counters;
-                    e = launch_emit64_records(Le, r->num_sms, s);
-                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 deferred emission");
-                    e = launch_transfer64(Le, r->num_sms, s);
-                    if (e != cudaSuccess) return cuda_fail(r, e, "FP64 ordered transfer");
-                }
-                cudaEventRecord(ev[3], s);
-                // the replay pass's queue starts at the wave's first job
-                SO_CK(r, cudaMemsetAsync(&L.counters->next, 0, sizeof(unsigned long long), s));
-                e = launch_trace64(L2, var, r->num_sms, s);
-                if (e != cudaSuccess) return cuda_fail(r, e, "tracer launch (replay pass)");
-                cudaEventRecord(ev[4], s);
-                SO_CK(r, cudaMemcpyAsync(r->h_rec64 + 3 * k, r->d_rec64_ctl, 3 * sizeof(unsigned long long),
-                                         cudaMemcpyDeviceToHost, s));
-            }
+            r->samples64 = L.nrays * per_job;
+            if (int rc = enqueue_deferred64(r, L, var, s, wave, w, torus ? 1 : 0, emit_ok, true)) return rc;
             SO_CK(r, cudaEventRecord(r->ev_rec64, s));
             r->rec64_pending = true;
-            r->waves64 = nw;
             r->last_defer64 = true;
             r->last_emit64 = emit_ok;
             return SO_OK;
@@ -1684,6 +1707,11 @@ struct so_batch {
     cudaGraphExec_t gexec = nullptr;
     float* graph_px = nullptr;  // output buffer baked into the graph
     so_tune graph_tune{-1, -1, 0.0, -1, -1};
+    // deferred passes (torus plasma, frame work without disks): decided and sized before each graph
+    // capture; wave64 = 0 traces in one persistent launch
+    bool defer_ok = false;
+    long long wave64 = 0;
+    int sums64 = 0;  // 1 FP64 sums, 2 FP32 sums (mixed precision)
 };
 
 namespace {
@@ -1713,11 +1741,9 @@ bool same_tune(const so_tune& a, const so_tune& b) {
            a.queue_chunk == b.queue_chunk;
 }
 
-// The launch sequence of one batch: counter reset, persistent tracer over all frames, resolve.
-int batch_enqueue(so_batch* b, float* d_px) {
+// The batch's launch descriptor: all frames, the tuned launch shape.
+void batch_launch_desc(so_batch* b, float* d_px, TraceLaunch& L) {
     so_renderer* r = b->r;
-    SO_CK(r, cudaMemsetAsync(b->d_cnt, 0, sizeof(Counters), r->st));
-    TraceLaunch L;
     launch_common(r, L);
     L.scenes = b->d_scenes;
     L.frames = b->d_frames;
@@ -1738,8 +1764,42 @@ int batch_enqueue(so_batch* b, float* d_px) {
     // mixed precision on a batch: FP64 geometry everywhere (photon-ring windows lie in the critical
     // band), FP32 turbulence sums
     L.emit32 = r->precision == SO_PREC_MIXED;
-    cudaError_t e = launch_trace64(L, b->variant, r->num_sms, r->st);
-    if (e != cudaSuccess) return cuda_fail(r, e, "batch tracer launch");
+}
+
+// Whether and how the batch's next capture defers its turbulence sums and emission: the torus
+// plasma's frame work of at least kDeferMinJobs jobs, through the renderer's record pool (sized
+// here, outside the capture), in waves; FP32 sums for mixed precision, FP64 otherwise.
+void batch_plan(so_batch* b, float* d_px) {
+    so_renderer* r = b->r;
+    b->wave64 = 0;
+    b->sums64 = 0;
+    TraceLaunch L;
+    batch_launch_desc(b, d_px, L);
+    if (!b->defer_ok || b->variant != VAR_RADIO || !L.torus || L.n_modes <= 0 || L.nrays < kDeferMinJobs) return;
+    long long wave = 0;
+    if (ensure_records64(r, L.nrays, b->spp, REC64_W_TORUS, &wave) != SO_OK) {
+        r->err.clear();  // no pool: one persistent launch
+        return;
+    }
+    b->wave64 = wave;
+    b->sums64 = (r->precision == SO_PREC_MIXED && r->turb_modes) ? 2 : 1;
+    r->samples64 = L.nrays * b->spp;
+}
+
+// The launch sequence of one batch: counter reset, the tracer over all frames (one persistent launch,
+// or the deferred passes in waves), resolve.
+int batch_enqueue(so_batch* b, float* d_px) {
+    so_renderer* r = b->r;
+    SO_CK(r, cudaMemsetAsync(b->d_cnt, 0, sizeof(Counters), r->st));
+    TraceLaunch L;
+    batch_launch_desc(b, d_px, L);
+    if (b->wave64 > 0) {
+        if (int rc = enqueue_deferred64(r, L, b->variant, r->st, b->wave64, REC64_W_TORUS, b->sums64, true, false))
+            return rc;
+    } else {
+        cudaError_t e = launch_trace64(L, b->variant, r->num_sms, r->st);
+        if (e != cudaSuccess) return cuda_fail(r, e, "batch tracer launch");
+    }
     SO_CK(r, launch_resolve(reinterpret_cast<float4*>(d_px), reinterpret_cast<const float4*>(d_px), nullptr,
                             (uint32_t)b->spp, L.nrays, r->S.mode == SO_MODE_VISIBLE, r->st));
     return SO_OK;
@@ -1748,6 +1808,7 @@ int batch_enqueue(so_batch* b, float* d_px) {
 int batch_capture(so_batch* b, float* d_px) {
     so_renderer* r = b->r;
     batch_drop_graph(b);
+    batch_plan(b, d_px);
     SO_CK(r, cudaStreamBeginCapture(r->st, cudaStreamCaptureModeRelaxed));
     int rc = batch_enqueue(b, d_px);
     cudaGraph_t g = nullptr;
@@ -1787,6 +1848,10 @@ int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const s
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
     so_batch* b = new so_batch;
     b->r = r;
+    b->defer_ok = true;
+    for (int s = 0; s < nscenes; ++s)
+        b->defer_ok = b->defer_ok && scenes[s].mode == SO_MODE_RADIO && scenes[s].flow_on && !scenes[s].disk_on &&
+                      scenes[s].max_steps < (1 << REC64_COUNT_BITS);
     b->nframes = nframes;
     b->nscenes = nscenes;
     b->W = W;
@@ -1829,6 +1894,16 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
     if (!b || !d_px) return SO_ERR_ARG;
     so_renderer* r = b->r;
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    if (b->gexec && b->wave64 > 0 && r->rec64_pending) {
+        // the previous launch of the deferred graph ran short of records: capture again with a larger
+        // pool (ensure_records64 doubles the estimate)
+        if (cudaEventQuery(r->ev_rec64) == cudaSuccess) {
+            unsigned long long short_samples = 0;
+            for (int k = 0; k < r->waves64; ++k) short_samples += r->h_rec64[3 * k + 1];
+            if (short_samples > 0) batch_drop_graph(b);
+        }
+        cudaGetLastError();  // a pending event reports cudaErrorNotReady
+    }
     if (!b->gexec || b->graph_px != d_px || !same_tune(b->graph_tune, b->tune)) {
         int rc = batch_capture(b, d_px);
         if (rc) return rc;
@@ -1844,6 +1919,10 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
         return cuda_fail(r, e, "so_batch_render graph launch");
+    }
+    if (b->wave64 > 0) {  // the graph copied each wave's pool counters out: note when they are there
+        cudaEventRecord(r->ev_rec64, r->st);
+        r->rec64_pending = true;
     }
     if (stats) {
         cudaEventRecord(e1, r->st);
@@ -1863,6 +1942,19 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
         stats->flow_steps = (long long)c.flow_steps;
         stats->ms_kernel = ms;
         stats->ms_trace = ms;
+        if (b->wave64 > 0) {  // the deferred passes' pool counters, copied out by the graph
+            unsigned long long slots = 0, short_samples = 0, records = 0;
+            for (int k = 0; k < r->waves64; ++k) {
+                slots += std::min<unsigned long long>(r->h_rec64[3 * k], (unsigned long long)r->seg_cap64) * REC_SEG;
+                short_samples += r->h_rec64[3 * k + 1];
+                records += r->h_rec64[3 * k + 2];
+            }
+            stats->rec64_slots = (long long)slots;
+            stats->rec64_short = (long long)short_samples;
+            stats->rec64_records = (long long)records;
+            stats->rec64_waves = r->waves64;
+            stats->emit64 = short_samples == 0 ? 1 : 0;
+        }
     }
     return SO_OK;
 }

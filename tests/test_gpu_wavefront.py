@@ -76,6 +76,60 @@ def test_batch_matches_single_frames(so):
     r.close()
 
 
+def test_batch_deferred_matches_single_frames(so):
+    """A batch of >= 4096 jobs on the torus plasma defers its sums and emission (recording pass over
+    all frames, sums, emission, ordered transfer, in waves through the renderer's record pool,
+    captured in the batch's graph).  FP64: every frame equals the single-frame render (each below
+    the deferral threshold, so traced with the sums in the tracer) bit for bit, with the pool
+    uncapped, capped to a few waves, and too small for a wave (the replay pass renders the batch),
+    for two launch shapes.  Mixed precision (FP32 sums at the
+    records): within 1e-4 relative L1 of the FP64 frames."""
+    import torch
+    wf = _wavefront(so)
+    W = 48
+    shots = wf.photon_ring_shots(so, W, spins=(0.5, 0.94), inclinations=(60.0,), times=(0.0, 150.0, 300.0),
+                                 zooms=(30.0, 100.0, 300.0), tolerance=1e-10, max_steps=20000)
+    sh0 = shots[0]
+    scenes, frames, fs, ref = [], [], [], []
+    for si, sh in enumerate(shots):
+        scenes.append(sh.scene)
+        rr = so.Renderer(sh.scene, sh.tables, sh.settings)
+        rr.set_plasma(sh.plasma())
+        for i in range(sh.nframes()):
+            frames.append(sh.frame(i))
+            fs.append(si)
+            img, _, _ = rr.render(sh.frame(i))
+            ref.append(img)
+        rr.close()
+    ref = np.stack(ref)
+    assert len(frames) * W * W >= 4096 and ref[..., 0].max() > 0
+    r = so.Renderer(sh0.scene, sh0.tables, sh0.settings)
+    r.set_plasma(sh0.plasma())
+    out = torch.zeros((len(frames), W, W, 4), dtype=torch.float32, device="cuda")
+    for pool_mb in (0.0, 64.0, 4.0):  # one wave; a few waves; a pool too small for a wave (replay)
+        r.set_precision(so.abi.SO_PREC_FP64, pool_mb=pool_mb)
+        b = so.Batch(r, scenes, frames, fs, W, W, 1)
+        for inter, ctas, tile, chunk in ((0, 0, 1, 1), (1, 0, 32, 3)):
+            b.set_tune(ctas, inter, tile, chunk)
+            for _ in range(3):  # a run short of records is recaptured with a larger pool
+                out.zero_()
+                st = b.render(out.data_ptr(), stats=True)
+                torch.cuda.synchronize()
+            assert np.array_equal(out.cpu().numpy(), ref), (pool_mb, inter, ctas, tile, chunk)
+            assert st.samples == len(frames) * W * W and st.attempts > 0
+        b.close()
+    r.set_precision(so.abi.SO_PREC_MIXED)
+    b = so.Batch(r, scenes, frames, fs, W, W, 1)
+    out.zero_()
+    b.render(out.data_ptr())
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()[..., 0].astype(np.float64)
+    want = ref[..., 0].astype(np.float64)
+    assert np.abs(got - want).sum() / want.sum() < 1e-4
+    b.close()
+    r.close()
+
+
 def test_batch_rejects_bad_input(so):
     import ctypes as C
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=8", "camera.height=8"])
