@@ -369,7 +369,12 @@ void so_destroy(so_renderer* r);
  * scenes[frame_scene[i]]; every scene must have the same mode and use the renderer's tables (those
  * of so_init: the K2 and blackbody tables do not depend on the scene, the disk table depends on the
  * spin, so disk scenes must share a spin).  The plasma is the renderer's (so_set_plasma).  The launch
- * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed. */
+ * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed.  A batch
+ * of 4096 jobs or more on the torus plasma (no disk) traces in deferred passes instead: a
+ * persistent recording pass over all frames, the turbulence sums at its records (FP32 under
+ * SO_PREC_MIXED, FP64 otherwise), the emission and the ordered transfer, in waves through the
+ * renderer's record pool (sized before the capture, within so_mixed_opts.pool_mb); a batch that ran
+ * short of records is captured again with a larger pool at its next so_batch_render. */
 typedef struct so_batch so_batch;
 /* Launch shape of the batch: resident CTAs per SM of the persistent grid (0 = as many as fit); the
  * job order (0 = frame after frame, 1 = frames interleaved in tiles of `tile` consecutive pixels,
@@ -381,7 +386,8 @@ int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const s
                     const int* frame_scene, int nframes, int W, int H, int spp, so_batch** out);
 /* Traces the batch into d_px (device memory, nframes * W * H * 4 floats, frame after frame) by
  * replaying the batch's CUDA graph on so_stream(r).  With stats: waits, fills the counters and
- * ms_kernel (graph time, CUDA events); without: asynchronous. */
+ * ms_kernel (graph time, CUDA events), and for deferred passes the rec64_* fields; without:
+ * asynchronous. */
 int so_batch_render(so_batch* b, float* d_px, so_stats* stats);
 /* Autotuner: times every launch shape (CTAs per SM from 1 to the occupancy limit, both job orders)
  * on the batch, keeps the fastest for later so_batch_render calls and returns it in *best. */
