@@ -20,6 +20,13 @@
 // the geometry must be FP64 (critical band, photon-ring batches) but the emission needs no more
 // than FP32.
 //
+// Large frames and batches take the emission out of the tracer altogether (DEFER): a recording pass
+// integrates the geodesics and records each flow step that can emit; k_turb64_records /
+// k_turb32_rec64 sum the turbulence at the records, k_emit64_records evaluates flow_step at each,
+// and k_transfer64 applies them in each sample's order.  Every one of those kernels runs with all its
+// lanes on the same kind of work, where inside the tracer the emission ran on the lanes that
+// happened to take a flow step.
+//
 // Compiled with -fmad=false: every fusion is an explicit fma() (so_kerr.cuh), matching the oracle.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
