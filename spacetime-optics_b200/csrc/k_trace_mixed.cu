@@ -824,12 +824,14 @@ __device__ __forceinline__ Torus32 torus32_of(const TraceLaunch& L) {
 // R = r sqrt(max((1-u)(1+u), 1e-12)), x = R cos phi_c, y = R sin phi_c, z = r u), TURB_P positions
 // per thread, the modes read from constant memory (the kernel parameter M, the same address for the
 // whole warp: no shared-memory loads in the MIO queue that feeds the SFU), so every lane does the
-// same work and the SFU
-// cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine and one FMA per mode
-// and position).  Blocks take chunks of TURB_P x 256 slots from a work counter, so SMs that also
-// host the FP64 re-trace (on the other stream) do less of it instead of finishing last.  Slots of
-// a segment past its ray's last record hold stale data; their sums are never read.
-constexpr int TURB_P = 8;
+// same work and the SFU cosine is the bound (three FMAs, the cosine's scaling multiply, the cosine
+// and one FMA per mode and position).  Each mode's constant loads serve TURB_P positions: measured
+// on the 2048^2 frame, 8 positions (64 registers, 4 CTAs / SM) 142.6 ms at 0.85 of the SFU rate, 12
+// (80 registers, 3 CTAs) 134.0 ms at 0.90, 16 (126 registers, 2 CTAs) 142.3 ms.  Blocks take chunks
+// of TURB_P x 256 slots from a work counter, so SMs that also host the FP64 re-trace (on the other
+// stream) do less of it instead of finishing last.  Slots of a segment past its ray's last record
+// hold stale data; their sums are never read.
+constexpr int TURB_P = 12;
 constexpr int TURB_CHUNK = TURB_P * 256;
 __global__ void __launch_bounds__(256) k_turb_records(const TraceLaunch L, const __grid_constant__ TurbModes M) {
     const int nm = M.n;
