@@ -385,9 +385,11 @@ __device__ __forceinline__ void flow_step32(const so_scene& S, const Torus32& tp
 
 // FP32 tracer.  One loop iteration = one DP5(4) attempt for every active lane.  The loop body is
 // split in two around the warp-cooperative turbulence sum, so every lane reaches the shuffles.
-// DEFER (radio torus with Fourier modes): instead of the turbulence sum and the transfer, every
-// emitting flow step is recorded (r, u, advected azimuth, step) in the ray's chain of record
-// segments; k_turb_records and k_flow_records finish the emission.  The geodesic does not depend on
+// DEFER (radio torus with Fourier modes, or the reference flow model): instead of the turbulence
+// sum and the transfer, every emitting flow step is recorded (r, u, advected azimuth, step; for the
+// reference flow the baked turbulence factor, fetched here as the in-line form fetches it, goes to
+// the record's sum slot) in the ray's chain of record segments; k_turb_records (torus) and
+// k_flow_records finish the emission.  The geodesic does not depend on
 // the emission; only the opacity cut (trans < 1e-5) does, and k_flow_records applies it at the
 // record where it happens, so the result is the one of the in-line form to FP32 rounding.
 template <int VAR, int MINB, bool DEFER>
@@ -492,6 +494,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
         float nrh = 0.f, nrl = 0.f, nprh = 0.f, nprl = 0.f, nuh = 0.f, nul = 0.f, npuh = 0.f, npul = 0.f;
         float n0 = 0.f, n1 = 0.f, n2 = 0.f, hc = 0.f, err = 0.f, TX = 0.f, TY = 0.f, TZ = 0.f;
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+        float rec_bf = 1.f;  // reference flow model: the record's baked turbulence factor
         float bfac = 1.f;
         float k7[6], dy[6];
         if (active) {
@@ -611,7 +614,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                             want_turb = true;
                         }
                     }
-                    if (!DEFER && want_flow && baked) {
+                    if (want_flow && baked) {
                         // the reference flow's baked turbulence (emission.cuh:112-124) at the end of
                         // the step, its retarded time t - t_ref(r) from the two-float t
                         float s2 = fmaxf((1.f - n2) * (1.f + n2), 1e-12f);
@@ -631,6 +634,22 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
                             const float A = baked_sample(S, L.turb_field, k, x, y, w);
                             const float B = baked_sample(S, L.turb_field, k + 1, x, y, w);
                             bfac = fmaf(B - A, f, A);
+                        }
+                    }
+                    if (DEFER && want_flow && !tp.on) {
+                        // reference flow model: record the steps flow_step32 does not return at once
+                        // from (its first tests, in its own arithmetic) with their turbulence factor,
+                        // fetched above exactly as the in-line form fetches it
+                        float s2 = fmaxf((1.f - n2) * (1.f + n2), 1e-12f);
+                        float Rc = n0 * sqrtf(s2);
+                        if (Rc >= 1e-3f) {
+                            float zh = __fdividef(n0 * n2, (float)S.h_r * Rc);
+                            if (!(__expf(-0.5f * zh * zh) < 1e-7f)) {
+                                const int nb = min((int)(R.psi * (float)(1.0 / PI)), 3);
+                                rec = make_float4((nb & 1) ? -n0 : n0, n2, 0.f, (nb & 2) ? -hc : hc);
+                                rec_bf = bfac;
+                                want_turb = true;
+                            }
                         }
                     }
                 }
@@ -662,6 +681,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace32(const TraceLaunch L) {
             }
             if (want_turb) {
                 L.rec[(long long)R.seg * REC_SEG + R.cnt] = rec;
+                if (!tp.on) L.rec_delta[(long long)R.seg * REC_SEG + R.cnt] = rec_bf;
                 ++R.cnt;
                 ++R.nrec;
             }
@@ -909,9 +929,11 @@ __global__ void __launch_bounds__(256) k_flow_records(const TraceLaunch L) {
             if (k < nrec) {
                 const long long j = (lane < 16 ? sa : sb) * REC_SEG + (lane & 15);
                 const float4 v = L.rec[j];
+                // torus: the turbulence sum; reference flow: the baked turbulence factor
                 const float delta = L.rec_delta[j];
                 nb = (int)(__float_as_uint(v.x) >> 31) | (int)((__float_as_uint(v.w) >> 31) << 1);
-                flow_step32(S, tp, delta, fabsf(v.x), v.y, lam, E, fabsf(v.w), &dI, &dtau);
+                flow_step32(S, tp, tp.on ? delta : 0.f, fabsf(v.x), v.y, lam, E, fabsf(v.w), &dI, &dtau,
+                            tp.on ? 1.f : delta);
             }
             float incl = dtau;
 #pragma unroll
@@ -1061,7 +1083,7 @@ cudaError_t launch_approach64(const TraceLaunch& L, long long n, int num_sms, cu
 
 cudaError_t launch_trace32(const TraceLaunch& L, long long n, int variant, int num_sms, cudaStream_t st) {
     const bool torus = variant == VAR_RADIO && L.torus && L.n_modes > 0;
-    const bool defer = torus && L.defer;
+    const bool defer = variant == VAR_RADIO && L.defer;
     size_t smem = torus && !defer ? (size_t)L.n_modes * (sizeof(float4) + sizeof(float)) : 0;
     int per_sm = 1;
     cudaError_t e;

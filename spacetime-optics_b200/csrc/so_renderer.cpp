@@ -871,7 +871,9 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     Lb.emit32 = 1;  // FP64 geometry in the band; the emission needs no more than FP32
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
-    const bool defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0 && r->mixed.turbulence == 0;
+    const bool torus_defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0;
+    const bool flow_defer = variant_of(r->S) == VAR_RADIO && !L.torus && r->S.flow_on;
+    const bool defer = (torus_defer || flow_defer) && r->mixed.turbulence == 0;
     L.defer = defer ? 1 : 0;
     if (defer) {
         rc = ensure_records(r, ns);
@@ -918,7 +920,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
         }
         if (defer) {
             SO_CK(r, cudaEventRecord(r->ev_wave[3 * w + 1], r->st));
-            SO_CK(r, launch_turb_records(Lw, *r->turb_modes, r->num_sms, r->st));
+            if (torus_defer) SO_CK(r, launch_turb_records(Lw, *r->turb_modes, r->num_sms, r->st));
             SO_CK(r, cudaEventRecord(r->ev_wave[3 * w + 2], r->st));
             SO_CK(r, launch_flow_records(Lw, r->num_sms, r->st));
         }

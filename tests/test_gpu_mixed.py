@@ -208,6 +208,35 @@ def test_deferred_turbulence_matches_in_tracer_sums(so):
         r.close()
 
 
+@pytest.mark.parametrize("noise,turb", [("BAKED", []), ("BAKED_FP32", []), ("BAKED", ["flow.turbulence=0"])],
+                         ids=["texture", "fp32_fetch", "no_turbulence"])
+def test_deferred_emission_reference_flow(so, noise, turb):
+    """The reference flow model's FP32 rays defer their emission too: the tracer records each flow
+    step with the baked turbulence factor it fetched (as the in-line form fetches it) and the
+    warp-per-ray transfer runs flow_step32 on the records.  The image equals the in-line form's
+    within 1e-5 relative L1 (the scanned transmittance) with the same termination class for every
+    sample, and stays within the mixed path's bar of the FP64 frame."""
+    W = 96
+    sh = so.Shot("m87_reference_flow.ini", [f"camera.width={W}", f"camera.height={W}", "render.spp=1",
+                                            "render.spp_max=1", "render.step_fraction=0.01", *turb])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(getattr(so.abi, "SO_FLOW_NOISE_" + noise))
+    f = sh.frame(0)
+    n = W * W
+    r.set_precision(so.abi.SO_PREC_FP64)
+    img64, _, _ = r.render(f)
+    a, sa, fa = _mixed_fates(so, r, f, n, turbulence=1)
+    b, sb, fb = _mixed_fates(so, r, f, n, turbulence=0)
+    r.close()
+    assert sa.record_waves == 0 and sb.record_waves >= 1 and sb.turb_records == 0 and sb.redo_records == 0
+    assert sb.attempts_fp32 > 0 and b[..., 0].max() > 0
+    l1, flux = _errors(a, b)
+    assert l1 <= 1e-5 and flux <= 1e-5, (l1, flux)
+    assert np.array_equal(fa, fb), int((fa != fb).sum())
+    l1, flux = _errors(img64, b)
+    assert l1 <= 2e-3 and flux <= 1e-3, (l1, flux)
+
+
 def test_deferred_turbulence_record_pool_shortage(so):
     """A record pool far too small for the frame: the rays that find no record slot are re-traced
     in FP64, so the image stays within the mixed path's bar of the FP64 frame, and the next frame's
