@@ -872,7 +872,7 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
     const bool torus_defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0;
-    const bool flow_defer = variant_of(r->S) == VAR_RADIO && !L.torus && r->S.flow_on;
+    const bool flow_defer = variant_of(r->S) == VAR_RADIO && !L.torus && r->S.flow_on && !all64;
     const bool defer = (torus_defer || flow_defer) && r->mixed.turbulence == 0;
     L.defer = defer ? 1 : 0;
     if (defer) {
