@@ -402,20 +402,25 @@ def same_scene_record(args, so, world, rank, local):
     r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
     f = sh.frame(0)
     X, Y = so.pixel_centres(f, W, W)
-    r.trace_rays(f, X[:65536], Y[:65536])  # warm-up
+    r.trace_rays(f, X, Y)  # warm-up: the record pool is sized for the full list here, not in a timed call
     torch.cuda.synchronize()
     t = []
     for _ in range(2):
         t0 = time.perf_counter()
         out = r.trace_rays(f, X, Y)
         t.append(time.perf_counter() - t0)
+    st = r.trace_stats()
     r.close()
     ours = allreduce_max(float(np.mean(t)), world)
     rec = {"workload": f"reference arm's scene: synchrotron geometry {W}x{W}, reference flow model (n ~ r^-1.5, "
                        "Theta 16.86 r^-0.84, h/r 0.3, 0.8 Keplerian, fBm turbulence rms 0.3 in place, n0 1e6), "
                        "every pixel centre, FP64",
            "mrays_s_e2e": round(world * W * W / ours / 1e6, 4), "s_per_frame": round(ours, 3),
-           "api": "so_trace_rays, host arrays in and out", "escaped": int((out["fate"] == 1).sum())}
+           "api": "so_trace_rays, host arrays in and out", "escaped": int((out["fate"] == 1).sum()),
+           "s_calls": [round(x, 3) for x in t],
+           "deferred_emission": bool(st.emit64), "records": st.rec64_records, "waves": st.rec64_waves,
+           "phases_ms": {"recording_pass": round(st.ms_rec64, 3), "emission_and_transfer": round(st.ms_emit64, 3),
+                         "replay_pass": round(st.ms_replay64, 3)}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import _oracle

@@ -316,6 +316,11 @@ int so_radio_flux_noalloc(const so_scene* d_scene, const so_frame* d_frame, int 
 /* Same as so_trace_rays with x, y and the outputs already in device memory (device pointers). */
 int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
                          const so_rays_out* d_out);
+/* Counters of the last so_trace_rays / so_trace_rays_device call (waits for it): samples (its rays),
+ * attempts, accepted, flow_steps, step_limited, and whether and how its emission was deferred
+ * (emit64, rec64_*, ms_rec64 .. ms_replay64); every other field 0.  No reference counterpart.
+ * SO_ERR_STATE when a frame or batch was rendered after it, or no list was traced. */
+int so_trace_stats(so_renderer* r, so_stats* stats);
 /* The star map of Renderer::init's SkyTexture (renderer.hpp:14-17, render.cu:550-593): w x h texels
  * of half2 (brightness s, s T / 1e4) as 16-bit halves, row-major.  Made a mipmapped texture (box-
  * filtered levels down to 1 x 1) sampled as the reference samples it (bilinear and between levels,

@@ -55,6 +55,7 @@ def lib():
         L.so_radio_flux.argtypes = [vp, P(Frame), C.c_int, C.c_double, P(C.c_double)]
         L.so_trace_rays.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
         L.so_trace_rays_device.argtypes = [vp, P(Frame), C.c_int, vp, vp, P(RaysOut)]
+        L.so_trace_stats.argtypes = [vp, P(Stats)]
         L.so_set_precision.argtypes = [vp, C.c_int, P(MixedOpts)]
         L.so_set_plasma.argtypes = [vp, P(Plasma), P(Mode)]
         L.so_set_flow_noise.argtypes = [vp, C.c_int]
@@ -318,6 +319,12 @@ class Renderer:
                                                  "cross_r", "cross_g")])
         _check(lib().so_trace_rays(self.h, C.byref(frame), n, _ptr(x), _ptr(y), C.byref(ro)), self.h)
         return o
+
+    def trace_stats(self):
+        """Counters of the last trace_rays call (so_trace_stats)."""
+        st = Stats()
+        _check(lib().so_trace_stats(self.h, C.byref(st)), self.h)
+        return st
 
     def normalize_flux(self, scene, frame_wide, n, pix_sr, target_jy):
         n0 = C.c_double()

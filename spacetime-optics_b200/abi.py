@@ -186,7 +186,7 @@ LAYOUT_FIELDS = [
 # Every entry point include/so_tracer.h declares (checked against the built library's exports).
 EXPORTS = [
     "so_init", "so_update_scene", "so_render", "so_render_device", "so_radio_flux", "so_trace_rays",
-    "so_trace_rays_device", "so_probe_fma_peak", "so_probe_sfu_peak", "so_probe_cos_turns", "so_radio_flux_noalloc",
+    "so_trace_rays_device", "so_trace_stats", "so_probe_fma_peak", "so_probe_sfu_peak", "so_probe_cos_turns", "so_radio_flux_noalloc",
     "so_batch_create", "so_batch_render", "so_batch_autotune", "so_batch_set_tune", "so_batch_free",
     "so_set_precision", "so_set_plasma", "so_set_flow_noise", "so_set_sky", "so_sky_file", "so_stream", "so_last_error", "so_destroy",
     "so_shot_load", "so_shot_scene", "so_shot_settings", "so_shot_nframes", "so_shot_frame",

@@ -20,10 +20,10 @@
 // the geometry must be FP64 (critical band, photon-ring batches) but the emission needs no more
 // than FP32.
 //
-// Large frames and batches take the emission out of the tracer altogether (DEFER): a recording pass
-// integrates the geodesics and records each flow step that can emit; k_turb64_records /
-// k_turb32_rec64 sum the turbulence at the records, k_emit64_records evaluates flow_step at each,
-// and k_transfer64 applies them in each sample's order.  Every one of those kernels runs with all its
+// Large frames, batches and ray lists take the emission out of the tracer altogether (DEFER): a
+// recording pass integrates the geodesics and records each flow step that can emit;
+// k_turb64_records / k_turb32_rec64 sum the turbulence at the records, k_emit64_records evaluates
+// flow_step at each, and k_transfer64 applies them in each sample's order.  Every one of those kernels runs with all its
 // lanes on the same kind of work, where inside the tracer the emission ran on the lanes that
 // happened to take a flow step.
 //
@@ -123,6 +123,25 @@ __device__ __forceinline__ void ray_init(Ray64& R, const so_scene& S, const so_f
 }
 
 enum Stage : int { ST_REJECTED = 0, ST_ACCEPTED = 1, ST_DONE = 2 };
+
+// A ray list's per-ray outputs but the intensity (trace_ray's results, trace.cuh:57-61, 149-163):
+// fate, crossings (saturated at 127), escape direction of an escaped ray, step counts, and the first
+// three crossings' radius and redshift (cr, cg: 0 past the ray's crossings).
+__device__ __forceinline__ void list_out(const so_rays_out& o, long long job, int fate, int ncross, double th,
+                                         double ph, int nacc, int natt, const double* cr, const double* cg) {
+    if (o.fate) o.fate[job] = (int8_t)fate;
+    if (o.ncross) o.ncross[job] = (int8_t)(ncross > 127 ? 127 : ncross);
+    if (o.theta) o.theta[job] = fate == 1 ? th : 0.0;
+    if (o.phi) o.phi[job] = fate == 1 ? ph : 0.0;
+    if (o.n_accepted) o.n_accepted[job] = nacc;
+    if (o.n_attempts) o.n_attempts[job] = natt;
+    if (o.cross_r) {
+        for (int c = 0; c < 3; ++c) {
+            o.cross_r[3 * job + c] = cr[c];
+            o.cross_g[3 * job + c] = cg[c];
+        }
+    }
+}
 
 // First half of one loop iteration of trace_ray (trace.cuh:81-129): step cap, DP5(4) attempt,
 // controller on rejection, swept angle, equatorial crossing (with the disk).  On acceptance the new
@@ -385,7 +404,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // against the compiler's free choice (194 registers, two CTAs): the plain FP64 synchrotron frame
 // runs 1.29x faster with a few spilled registers and 50 % more warps.
 // DEFER (deferred FP64 passes, radio only): 0 = emission in the tracer, 1 = recording pass (geometry
-// only: no emission code), 2 = replay pass.  Both passes run four CTAs per SM (128 registers):
+// only: no emission code), 2 = replay pass, 3 = recording pass of a ray list (also records each
+// step's crossings and writes the rays' outputs without emission).  Both passes run four CTAs per SM (128 registers):
 // measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against 205 ms at
 // three CTAs (168 registers, fewer spills); the recording pass 78 ms, against 84 ms at five CTAs
 // (96 registers) and 88 ms at six (80), whose spills cost more than the warps gain (the reference
@@ -393,8 +413,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 template <int VAR, bool EMIT32, int DEFER>
 __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const TraceLaunch L) {
     extern __shared__ double smem[];
-    constexpr int defer = (VAR == VAR_RADIO && !EMIT32) ? DEFER : 0;
+    constexpr int defer = (VAR == VAR_RADIO && !EMIT32) ? (DEFER == 3 ? 1 : DEFER) : 0;
     constexpr bool emit = defer != 1;
+    constexpr bool list_rec = defer == 1 && DEFER == 3;  // the recording pass of a ray list
     // the replay pass behind the deferred emission runs only when the recording pass left samples
     // without records (the same value for every thread: the whole grid returns)
     if (defer == 2 && L.replay_if_short && *(volatile unsigned long long*)&L.rec64_ctl[1] == 0ull) return;
@@ -580,6 +601,7 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                     slot[3] = hc;
                     slot[4] = __longlong_as_double((long long)tag);
                     if (tp.n_modes <= 0) slot[5] = yn[5];
+                    if (list_rec) slot[L.rec64_w - 1] = (double)R.ncross;
                     ++rcnt;
                     ++rtot;
                     ++n_rec;
@@ -629,6 +651,9 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
             e.fate = fate;
             e.fidx = fidx;
             L.samp64[sid] = e;
+            // a ray list's outputs of the ray without emission; the transfer writes its intensity and,
+            // where the opacity cut ends it earlier, what the tracer reports for it there
+            if (list_rec) list_out(L.out, job, fate, R.ncross, th, ph, R.nacc, R.natt, cr, cg);
             if ((L.kind == RAYS_PIXELS || L.kind == RAYS_CHUNKS) && ++sample < jobs_n) {
                 double x, yv;
                 pixel_point(L, *F, pix, sbase + sample, &x, &yv);
@@ -655,20 +680,9 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
             R.acc[2] += tf * xyz[2];
         }
         if (L.kind == RAYS_LIST) {
-            const so_rays_out& o = L.out;
-            if (o.fate) o.fate[job] = (int8_t)fate;
-            if (o.ncross) o.ncross[job] = (int8_t)(R.ncross > 127 ? 127 : R.ncross);
-            if (o.theta) o.theta[job] = fate == 1 ? th : 0.0;
-            if (o.phi) o.phi[job] = fate == 1 ? ph : 0.0;
-            if (o.I) reinterpret_cast<float4*>(o.I)[job] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
-            if (o.n_accepted) o.n_accepted[job] = R.nacc;
-            if (o.n_attempts) o.n_attempts[job] = R.natt;
-            if (o.cross_r) {
-                for (int c = 0; c < 3; ++c) {
-                    o.cross_r[3 * job + c] = cr[c];
-                    o.cross_g[3 * job + c] = cg[c];
-                }
-            }
+            list_out(L.out, job, fate, R.ncross, th, ph, R.nacc, R.natt, cr, cg);
+            if (L.out.I)
+                reinterpret_cast<float4*>(L.out.I)[job] = make_float4(R.acc[0], R.acc[1], R.acc[2], R.acc[3]);
             active = false;
         } else {
             pa[0] += R.acc[0];
@@ -876,7 +890,7 @@ cudaError_t launch_emit64_records(const TraceLaunch& L, int num_sms, cudaStream_
 // Deferred emission, ordered transfer: one thread per job walks each sample's chain in recording
 // order with ray_commit's arithmetic (intensity into the image-order bucket, transmission, the
 // 1e-5 opacity cut, after which the counts of the cut step stand), then writes the job's outputs
-// and counts as the tracer does.  Flow steps without a record emit nothing and transmit 1, so
+// and counts as the tracer does (a ray list's cut ray: also its crossings at the cut step).  Flow steps without a record emit nothing and transmit 1, so
 // skipping them changes no bit.  Left to the replay pass when a sample ran out of segments.
 __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
     const bool skip = *(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull;
@@ -894,7 +908,7 @@ __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
             const Sample64 e = L.samp64[sid];
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             double trans = 1.0;
-            int fate = e.fate, natt = e.natt, nacc = e.nacc, nflow = e.nflow;
+            int fate = e.fate, natt = e.natt, nacc = e.nacc, nflow = e.nflow, ncut = -1;
             long long seg = L.job_head64[sid];
             for (int i = 0; i < e.nrec; ++i) {
                 const int k = i % REC_SEG;
@@ -918,6 +932,7 @@ __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
                     natt = (int)((tag >> 2) & cmask);
                     nacc = (int)((tag >> (2 + REC64_COUNT_BITS)) & cmask);
                     nflow = (int)((tag >> (2 + 2 * REC64_COUNT_BITS)) & cmask);
+                    if (L.kind == RAYS_LIST) ncut = (int)rec[L.rec64_w - 1];
                     break;
                 }
             }
@@ -936,6 +951,22 @@ __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
                 const long long o = q.pix * L.spp + q.sbase;
                 L.sample_out[o] = make_float4(acc[0], acc[1], acc[2], acc[3]);
                 if (L.sample_fate) L.sample_fate[o] = (int8_t)fate;
+            } else if (L.kind == RAYS_LIST) {
+                // the recording pass wrote the uncut ray's outputs; a ray cut on its opacity reports
+                // the tracer's values at the cut: captured, no escape direction, the counts and
+                // crossings of that step (later crossings were never reached)
+                const so_rays_out& o = L.out;
+                if (o.I) reinterpret_cast<float4*>(o.I)[job] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+                if (ncut >= 0) {
+                    double cr[3] = {0.0, 0.0, 0.0}, cg[3] = {0.0, 0.0, 0.0};
+                    if (o.cross_r) {
+                        for (int c = 0; c < 3 && c < ncut; ++c) {
+                            cr[c] = o.cross_r[3 * job + c];
+                            cg[c] = o.cross_g[3 * job + c];
+                        }
+                    }
+                    list_out(o, job, -1, ncut, 0.0, 0.0, nacc, natt, cr, cg);
+                }
             }
         }
         if (L.kind == RAYS_PIXELS) {
@@ -1098,7 +1129,8 @@ cudaError_t launch_trace64(const TraceLaunch& L, int variant, int num_sms, cudaS
         case VAR_DISK: return go(k_trace64<VAR_DISK, false, 0>);
         default:
             if (emit32) return go(k_trace64<VAR_RADIO, true, 0>);
-            if (L.defer64 == 1) return go(k_trace64<VAR_RADIO, false, 1>);
+            if (L.defer64 == 1)
+                return L.kind == RAYS_LIST ? go(k_trace64<VAR_RADIO, false, 3>) : go(k_trace64<VAR_RADIO, false, 1>);
             if (L.defer64 == 2) return go(k_trace64<VAR_RADIO, false, 2>);
             return go(k_trace64<VAR_RADIO, false, 0>);
     }

@@ -32,7 +32,9 @@ constexpr int REC_SEG = 16;  // flow-step record slots per segment
 // only: t.  k_emit64_records then overwrites [0] with the step's emission dI and [1] with its
 // transmission exp(-dtau).  The tag holds the image-order bucket (bits 0-1: psi / pi clamped to 3)
 // and the ray's attempt, accepted-step and flow-step counts after this step (20 bits each from bit
-// 2, 22 and 42; the path needs max_steps < 2^20).
+// 2, 22 and 42; the path needs max_steps < 2^20).  A ray list's records carry one more double, last:
+// the ray's equatorial crossings after this step (its ncross output when the opacity cut ends it
+// there).
 constexpr int REC64_W_TORUS = 5, REC64_W_FLOW = 6;
 constexpr int REC64_COUNT_BITS = 20;
 // End state of one sample after the recording pass.
@@ -159,7 +161,7 @@ struct TraceLaunch {
     // (defer64 = 2) integrates again and reads each sum back in order.  0 = sums in the tracer.
     int defer64;
     double* rec64;            // record pool: slot s at doubles rec64_w s .. (layout at REC64_W_TORUS)
-    int rec64_w;              // doubles per record: REC64_W_TORUS or REC64_W_FLOW
+    int rec64_w;              // doubles per record: REC64_W_TORUS or REC64_W_FLOW (+1 for a ray list)
     long long job0;           // deferred passes in waves: this launch's jobs are job0 .. job0 + nrays - 1
                               // of the frame's job numbering (chain heads and sample ends are indexed
                               // from job0)

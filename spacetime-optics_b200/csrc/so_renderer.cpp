@@ -159,6 +159,7 @@ struct so_renderer {
     int waves64 = 0;                           // waves of the last deferred trace
     long long samples64 = 0;                   // samples of the last deferred trace (for the estimate)
     bool last_defer64 = false, last_emit64 = false;
+    long long list_rays = 0;                   // rays of the last so_trace_rays whose counters d_cnt holds
     std::string err;
 };
 
@@ -522,14 +523,14 @@ int ensure_records64(so_renderer* r, long long jobs, int per_job, int w, long lo
 
 // Launches of the FP64 tracer.  A launch of at least kDeferMinJobs host-counted jobs on the
 // renderer's stream defers work out of the tracer when it is a torus-plasma launch with FP64 sums,
-// or frame work on the reference flow model: a recording pass (geometry only, one record per flow
-// step that can emit) -> k_turb64_records (torus: the FP64 sums at every record) -> for frame work
-// (pixels, samples, chunks) without a disk, k_emit64_records (flow_step at every record) ->
-// k_transfer64 (ordered transfer), with a replay pass behind them that runs only if the pool ran
-// short; for torus ray lists (whose per-ray outputs need the geometry up to the opacity cut) and
-// torus disk scenes the replay pass instead of the emission kernels.  Each is bit for bit the
-// in-tracer result, with the sums and the emission at full occupancy.  Everything else, and any
-// launch whose pool cannot be had, runs in the tracer.
+// or a launch on the reference flow model: a recording pass (geometry only, one record per flow
+// step that can emit) -> k_turb64_records (torus: the FP64 sums at every record) -> without a disk,
+// k_emit64_records (flow_step at every record) -> k_transfer64 (ordered transfer; a ray list's ray
+// cut on its opacity gets the fate, counts and crossings of the cut step from its record), with a
+// replay pass behind them that runs only if the pool ran short; for torus disk scenes the replay
+// pass instead of the emission kernels.  Each is bit for bit the in-tracer result, with the sums and
+// the emission at full occupancy.  Everything else, and any launch whose pool cannot be had, runs
+// in the tracer.
 // The deferred passes of one launch on stream s, in waves of `wave` jobs through the pool that
 // ensure_records64 set up: per wave a recording pass, the sums (sums: 0 none, 1 FP64, 2 FP32), the
 // emission and ordered transfer (emit), and a replay pass that runs when the pool ran short (always,
@@ -604,13 +605,13 @@ int run_tracer(so_renderer* r, const TraceLaunch& L, cudaStream_t st = nullptr) 
     const int var = variant_of(r->S);
     const cudaStream_t s = st ? st : r->st;
     const bool torus = var == VAR_RADIO && L.torus && L.n_modes > 0;
-    const bool emit_ok = L.kind != RAYS_LIST && !r->S.disk_on && r->S.max_steps < (1 << REC64_COUNT_BITS);
+    const bool emit_ok = !r->S.disk_on && r->S.max_steps < (1 << REC64_COUNT_BITS);
     const bool flow = var == VAR_RADIO && !torus && r->S.flow_on && emit_ok;
     const bool defer = ((torus && !L.emit32) || flow) && !L.nrays_dev && L.nrays >= kDeferMinJobs && s == r->st;
     r->last_defer64 = false;
     if (defer) {
         const int per_job = L.kind == RAYS_PIXELS ? L.spp : L.kind == RAYS_CHUNKS ? L.chunk : 1;
-        const int w = torus ? REC64_W_TORUS : REC64_W_FLOW;
+        const int w = (torus ? REC64_W_TORUS : REC64_W_FLOW) + (L.kind == RAYS_LIST ? 1 : 0);
         long long wave = 0;
         if (ensure_records64(r, L.nrays, per_job, w, &wave) == SO_OK) {
             r->samples64 = L.nrays * per_job;
@@ -941,6 +942,32 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     return SO_OK;
 }
 
+// The deferred FP64 passes' fields of so_stats for the last tracer launch (its stream synchronised).
+void rec64_stats(so_renderer* r, so_stats* stats) {
+    stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = stats->ms_emit64 = 0.0;
+    stats->rec64_slots = stats->rec64_short = stats->rec64_records = 0;
+    stats->emit64 = 0;
+    stats->rec64_waves = 0;
+    if (!r->last_defer64) return;
+    unsigned long long slots = 0, short_samples = 0, records = 0;
+    for (int k = 0; k < r->waves64; ++k) {
+        float t[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&t[i], r->ev64[5 * k + i], r->ev64[5 * k + i + 1]);
+        stats->ms_rec64 += t[0];
+        stats->ms_sum64 += t[1];
+        stats->ms_emit64 += t[2];
+        stats->ms_replay64 += t[3];
+        slots += std::min<unsigned long long>(r->h_rec64[3 * k], (unsigned long long)r->seg_cap64) * REC_SEG;
+        short_samples += r->h_rec64[3 * k + 1];
+        records += r->h_rec64[3 * k + 2];
+    }
+    stats->emit64 = r->last_emit64 && short_samples == 0 ? 1 : 0;
+    stats->rec64_slots = (long long)slots;
+    stats->rec64_short = (long long)short_samples;
+    stats->rec64_records = (long long)records;
+    stats->rec64_waves = r->waves64;
+}
+
 int read_counters(so_renderer* r, Counters* c) {
     SO_CK(r, cudaMemcpyAsync(c, r->d_cnt, sizeof(Counters), cudaMemcpyDeviceToHost, r->st));
     SO_CK(r, cudaStreamSynchronize(r->st));
@@ -963,6 +990,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
     } guard{ev};
     SO_CK(r, cudaMemcpyAsync(r->d_frame, &f, sizeof f, cudaMemcpyHostToDevice, r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    r->list_rays = 0;
     const long long n = (long long)f.W * f.H;
     TraceLaunch L;
     launch_common(r, L);
@@ -1096,29 +1124,7 @@ int trace_frame(so_renderer* r, const so_frame& f, bool adaptive, so_stats* stat
             stats->record_waves = 0;
             c.fp64_rays = 0;
         }
-        stats->ms_rec64 = stats->ms_sum64 = stats->ms_replay64 = stats->ms_emit64 = 0.0;
-        stats->rec64_slots = stats->rec64_short = stats->rec64_records = 0;
-        stats->emit64 = 0;
-        stats->rec64_waves = 0;
-        if (r->last_defer64) {  // the last tracer launch deferred work (stream synchronised above)
-            unsigned long long slots = 0, short_samples = 0, records = 0;
-            for (int k = 0; k < r->waves64; ++k) {
-                float t[4] = {0.f, 0.f, 0.f, 0.f};
-                for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&t[i], r->ev64[5 * k + i], r->ev64[5 * k + i + 1]);
-                stats->ms_rec64 += t[0];
-                stats->ms_sum64 += t[1];
-                stats->ms_emit64 += t[2];
-                stats->ms_replay64 += t[3];
-                slots += std::min<unsigned long long>(r->h_rec64[3 * k], (unsigned long long)r->seg_cap64) * REC_SEG;
-                short_samples += r->h_rec64[3 * k + 1];
-                records += r->h_rec64[3 * k + 2];
-            }
-            stats->emit64 = r->last_emit64 && short_samples == 0 ? 1 : 0;
-            stats->rec64_slots = (long long)slots;
-            stats->rec64_short = (long long)short_samples;
-            stats->rec64_records = (long long)records;
-            stats->rec64_waves = r->waves64;
-        }
+        rec64_stats(r, stats);
         float ms1 = 0.f, ms2 = 0.f;
         cudaEventElapsedTime(&ms1, ev[0], ev[1]);
         if (cudaEventQuery(ev[3]) == cudaSuccess && cudaEventElapsedTime(&ms2, ev[2], ev[3]) != cudaSuccess) ms2 = 0.f;
@@ -1253,6 +1259,7 @@ int rend_trace_list_frames(so_renderer* r, int n, const double* d_x, const doubl
     if (n <= 0) return SO_OK;
     if (nframes <= 0 || !d_scenes || !d_frames || !d_frame_scene) return fail(r, SO_ERR_ARG, "trace list: frames");
     SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    r->list_rays = 0;
     TraceLaunch L;
     launch_common(r, L);
     L.scenes = d_scenes;
@@ -1445,6 +1452,7 @@ static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const doubl
                            const so_rays_out& d_out) {
     SO_CK(r, cudaMemcpyAsync(r->d_frame, f, sizeof(so_frame), cudaMemcpyHostToDevice, r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
+    r->list_rays = n;
     TraceLaunch L;
     launch_common(r, L);
     if (int brc = bake_turbulence(r, L)) return brc;
@@ -1459,6 +1467,22 @@ static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const doubl
         L.out.cross_g = nullptr;
     }
     return run_tracer(r, L);
+}
+
+int so_trace_stats(so_renderer* r, so_stats* stats) {
+    if (!r || !stats) return fail(r, SO_ERR_ARG, "so_trace_stats: NULL argument");
+    if (r->list_rays <= 0) return fail(r, SO_ERR_STATE, "so_trace_stats: no ray list traced since the last frame");
+    if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    Counters c;
+    if (int rc = read_counters(r, &c)) return rc;
+    std::memset(stats, 0, sizeof *stats);
+    stats->samples = r->list_rays;
+    stats->attempts = (long long)c.attempts;
+    stats->accepted = (long long)c.accepted;
+    stats->flow_steps = (long long)c.flow_steps;
+    stats->step_limited = (long long)c.step_limited;
+    rec64_stats(r, stats);
+    return SO_OK;
 }
 
 int so_trace_rays_device(so_renderer* r, const so_frame* f, int n, const double* d_x, const double* d_y,
@@ -1896,6 +1920,7 @@ int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
     if (!b || !d_px) return SO_ERR_ARG;
     so_renderer* r = b->r;
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
+    r->list_rays = 0;
     if (b->gexec && b->wave64 > 0 && r->rec64_pending) {
         // the previous launch of the deferred graph ran short of records: capture again with a larger
         // pool (ensure_records64 doubles the estimate)

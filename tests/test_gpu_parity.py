@@ -421,6 +421,79 @@ def test_deferred_fp64_emission_reference_flow(so, noise):
     assert _counts(sa) == _counts(sb)
 
 
+_LIST_CASES = {
+    # shot, density override (normal, 1000x), set-up
+    "flow_inline": ("m87_reference_flow.ini", "flow.n0", 3e5,
+                    lambda so, r, sh: r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)),
+    "flow_texture": ("m87_reference_flow.ini", "flow.n0", 3e5, lambda so, r, sh: None),
+    "torus": ("synchrotron_1024.ini", "flow.n0", 1594262.8, lambda so, r, sh: r.set_plasma(sh.plasma())),
+}
+
+
+def _list_pair(so, case, scale, n=72):
+    """n x n pixel centres (over the deferral threshold of 4096 rays) through so_trace_rays twice:
+    with the deferred passes, and with the record pool capped to one segment, so that the replay
+    pass (emission in the tracer) traces the list."""
+    shot, key, n0, setup = _LIST_CASES[case]
+    sh = so.Shot(shot, [f"camera.width={n}", f"camera.height={n}", f"{key}={n0 * scale!r}"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    setup(so, r, sh)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, n, n)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    a = r.trace_rays(f, X, Y, cross=True)
+    sa = r.trace_stats()
+    r.set_precision(so.abi.SO_PREC_FP64, pool_mb=0.001)
+    b = r.trace_rays(f, X, Y, cross=True)
+    sb = r.trace_stats()
+    r.close()
+    return a, sa, b, sb
+
+
+@pytest.mark.parametrize("case", sorted(_LIST_CASES))
+def test_deferred_fp64_ray_list(so, case):
+    """Ray lists defer their emission like frames: the recording pass writes each ray's outputs
+    without emission, and the ordered transfer writes its intensity and, for a ray the 1e-5 opacity
+    cut ends, the tracer's outputs at the cut (captured, no escape direction, that step's counts,
+    winding order and crossings).  At the normal density and at 1000 times it, every per-ray output
+    (fate, winding order, escape direction, intensity, step counts, the first three crossings'
+    radius and redshift) and the counters equal the in-tracer list's bit for bit."""
+    out = {}
+    for scale in (1.0, 1000.0):
+        a, sa, b, sb = _list_pair(so, case, scale)
+        assert sa.emit64 == 1 and sa.rec64_short == 0 and sa.rec64_records > 0 and sa.samples == a["fate"].size
+        assert sb.emit64 == 0 and sb.rec64_short > 0
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (scale, k)
+        assert _counts(sa) == _counts(sb)
+        assert a["I"][:, 0].max() > 0
+        out[scale] = (a, sa)
+    (thin, st), (thick, sk) = out[1.0], out[1000.0]
+    cut = (thick["fate"] == -1) & (thin["fate"] != -1)
+    fewer = thick["ncross"] < thin["ncross"]
+    print(f"{case}: rays cut on their opacity {int(cut.sum())}, crossings dropped {int(fewer.sum())}, "
+          f"attempts {st.attempts} -> {sk.attempts}")
+    assert cut.any() and sk.attempts < st.attempts
+    assert np.all(thick["theta"][cut] == 0) and np.all(thick["n_attempts"] <= thin["n_attempts"])
+
+
+def test_trace_stats_state(so):
+    """so_trace_stats reports the last ray list only: after a frame it is a state error."""
+    sh = so.Shot("shadow_selftest_256.ini", ["camera.width=16", "camera.height=16"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, 16, 16)
+    k = r.trace_rays(f, X, Y)
+    st = r.trace_stats()
+    assert st.samples == 256 and st.accepted == int(k["n_accepted"].sum()) and st.attempts == int(k["n_attempts"].sum())
+    assert st.emit64 == 0 and st.rec64_waves == 0
+    r.render(f)
+    with pytest.raises(so.TracerError) as e:
+        r.trace_stats()
+    assert e.value.code == so.abi.SO_ERR_STATE
+    r.close()
+
+
 def test_torus_plasma_vs_oracle(so, orc):
     """Synchrotron torus with 512 Fourier modes (FP64 everywhere), 40 x 40 over the +-12 M field."""
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=40", "camera.height=40"])

@@ -214,6 +214,7 @@ def test_init_fails_loudly_without_device_or_bad_args(so):
     assert lib.so_init(None, 0, None, None, None) == so.abi.SO_ERR_ARG
     assert lib.so_render(None, None, None, 0.5, None, None) == so.abi.SO_ERR_ARG
     assert lib.so_trace_rays(None, None, 1, None, None, None) == so.abi.SO_ERR_ARG
+    assert lib.so_trace_stats(None, None) == so.abi.SO_ERR_ARG
     assert lib.so_last_error(None)  # message of the last failed init
 
 
