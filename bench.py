@@ -539,6 +539,116 @@ def run_shadow(args, so, world, rank, local):
     return line
 
 
+def run_rays(args, so, world, rank, local):
+    """The drop-in ray-list path on the reference arm's scene: the reference flow model with its fBm
+    turbulence in place, every pixel centre of the W x W synchrotron geometry, one ray each.  `value`:
+    so_trace_rays_device with the coordinates and every per-ray output (fate, winding order, escape
+    direction, the four intensity bins, step counts) resident on the device; `e2e`: so_trace_rays
+    with host arrays, the copies inside the timed region.  The CPU baseline is the reference's own
+    trace_ray on the host cores over a bounded sample of the same pixels."""
+    import torch
+    torch.cuda.set_device(local)
+    W = args.size or 2048
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", *REF_SCENE])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
+    f = rank_frame(sh, rank)
+    X, Y = so.pixel_centres(f, W, W)
+    n = X.size
+    dev = torch.device("cuda", local)
+    dx, dy = torch.from_numpy(X).to(dev), torch.from_numpy(Y).to(dev)
+    outs = {"fate": torch.int8, "ncross": torch.int8, "theta": torch.float64, "phi": torch.float64,
+            "I": torch.float32, "n_accepted": torch.int32, "n_attempts": torch.int32}
+    d = {k: torch.empty((n, 4) if k == "I" else (n,), dtype=t, device=dev) for k, t in outs.items()}
+    ro = so.abi.RaysOut(*[C.c_void_p(d[k].data_ptr()) if k in d else None
+                          for k, _ in so.abi.RaysOut._fields_])
+    lib = so.lib()
+
+    def trace_device():
+        rc = lib.so_trace_rays_device(r.h, C.byref(f), n, C.c_void_p(dx.data_ptr()), C.c_void_p(dy.data_ptr()),
+                                      C.byref(ro))
+        if rc != so.abi.SO_OK:
+            raise so.TracerError(rc, lib.so_last_error(r.h).decode())
+
+    stream = torch.cuda.ExternalStream(r.stream())
+    for _ in range(args.warmup):
+        trace_device()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+                ev[i][0].record(stream)
+            trace_device()
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    st = r.trace_stats()
+    barrier(world)
+    ms_step = allreduce_max(ms_step, world)
+    value = job_rate(world, n, ms_step) / 1e6
+    fp64_peak, _ = so.probe_fma_peak(local)
+    # the recording pass (the geodesics: DP5(4) attempts and accepted steps) is the longest kernel;
+    # the emission at the records (fBm noise in place) and the ordered transfer follow it
+    flops = st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT
+    roof = {"bound": "fp64", "achieved": round(flops / (st.ms_rec64 * 1e-3) / 1e12, 3), "peak": round(fp64_peak, 3),
+            "unit": "TFLOP/s", "kernel": "k_trace64 (recording pass of the ray list)", "kernel_ms": st.ms_rec64,
+            "per_launch": flops, "peak_source": "so_probe_fma_peak (measured FP64 FMA chains on this GPU)",
+            "phases_ms": {"recording_pass": round(st.ms_rec64, 3), "emission_and_transfer": round(st.ms_emit64, 3),
+                          "replay_pass": round(st.ms_replay64, 3)},
+            "traffic": None}
+    roof["frac"] = round(roof["achieved"] / roof["peak"], 4)
+    k = r.trace_rays(f, X, Y)  # warm-up of the host-array form
+    e2e_s = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        k = r.trace_rays(f, X, Y)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_step = allreduce_max(float(np.mean(e2e_s)), world)
+    same = all(np.array_equal(k[key], d[key].cpu().numpy()) for key in outs)
+    line = {
+        "metric": "Mrays/s (so_trace_rays, every per-ray output)", "value": round(value, 4), "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"reference arm's scene: synchrotron geometry {W}x{W}, reference flow model "
+                               "(n ~ r^-1.5, Theta 16.86 r^-0.84, h/r 0.3, 0.8 Keplerian, fBm turbulence rms 0.3 "
+                               "in place, n0 1e6), every pixel centre, one ray each", "path": "fp64",
+                   "api": "so_trace_rays_device (value), so_trace_rays with host arrays (e2e)",
+                   "deferred_emission": bool(st.emit64), "records": st.rec64_records, "waves": st.rec64_waves,
+                   "attempts_per_ray": st.attempts / n, "flow_steps_per_ray": st.flow_steps / n,
+                   "escaped": int((k["fate"] == 1).sum()), "host_and_device_outputs_identical": bool(same),
+                   "l2": "256 MiB buffer written between timed steps"},
+        "roofline": roof,
+        "e2e": {"value": round(world * n / e2e_step / 1e6, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 16 * n,
+                "d2h_bytes_per_step": n * (1 + 1 + 8 + 8 + 16 + 4 + 4)},
+        "gpu_launches": args.steps * 4 * max(st.rec64_waves, 1) if st.rec64_waves else args.steps,
+        "clocks": clk.summary(),
+    }
+    r.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import _oracle
+        if _oracle.have_ref():
+            R = _oracle.RefShot(os.path.join(PKG_DIR, "shots", "synchrotron_1024.ini"),
+                                [f"camera.width={W}", f"camera.height={W}", *REF_SCENE])
+            threads = os.cpu_count() or 1
+            m = 65536
+            idx = np.linspace(0, n - 1, m).astype(np.int64)
+            t0 = time.perf_counter()
+            _oracle.ref_trace(R.scene, R.frame(0), X[idx], Y[idx], threads=threads)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": round(m / dt / 1e6, 6), "unit": "Mrays/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"{m} evenly strided pixel centres, the reference's trace_ray "
+                                              f"(oracle/_ref), {dt:.1f} s"}
+    return line
+
+
 # surrogate network: forward FLOPs per ray (FMA = 2; the head is 16 wide on the tensor cores)
 SUR_FLOPS_RAY = 2 * (128 * 256 + 3 * 256 * 256 + 256 * 16)
 SUR_SIGMA = 0.35           # std of the random Fourier frequencies per unit of the scaled inputs
@@ -863,8 +973,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="synchrotron",
-                    choices=["synchrotron", "surrogate", "wavefront", "shadow", "flow"])
-    ap.add_argument("--size", type=int, default=0, help="frame width (default: synchrotron and shadow 2048, surrogate 4096, wavefront 512, flow 1024)")
+                    choices=["synchrotron", "surrogate", "wavefront", "shadow", "flow", "rays"])
+    ap.add_argument("--size", type=int, default=0, help="frame width (default: synchrotron, shadow and rays 2048, surrogate 4096, wavefront 512, flow 1024)")
     ap.add_argument("--band", type=float, default=0.1, help="surrogate: critical band half-width (M)")
     ap.add_argument("--train-rays", type=int, default=1 << 24)
     ap.add_argument("--train-steps", type=int, default=40000)
@@ -888,6 +998,8 @@ def main():
         line = run_wavefront(args, so, world, rank, local)
     elif args.workload == "shadow":
         line = run_shadow(args, so, world, rank, local)
+    elif args.workload == "rays":
+        line = run_rays(args, so, world, rank, local)
     elif args.workload == "flow":
         args.size = args.size or 1024
         line = run_ours(args, so, world, rank, local)
