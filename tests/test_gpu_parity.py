@@ -477,6 +477,38 @@ def test_deferred_fp64_ray_list(so, case):
     assert np.all(thick["theta"][cut] == 0) and np.all(thick["n_attempts"] <= thin["n_attempts"])
 
 
+def test_deferred_fp64_ray_list_waves(so):
+    """A ray list whose records the pool holds only in part runs the deferred passes in waves of
+    consecutive rays (each writing its rays' outputs at their own indices): 256 x 256 pixel centres
+    on the reference flow model with a pool planned for about 40 % of the rays, every output and
+    counter bit-identical to the single-wave list."""
+    n = 256
+    sh = so.Shot("m87_reference_flow.ini", [f"camera.width={n}", f"camera.height={n}", "flow.n0=3e7"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    r.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, n, n)
+    r.set_precision(so.abi.SO_PREC_FP64)
+    a = r.trace_rays(f, X, Y, cross=True)
+    sa = r.trace_stats()
+    # the pool is planned from the records per ray seen so far (1.5 x, at least 320) plus a partly
+    # filled segment per ray: size it for about 40 % of the rays, segments of 16 records of 7 doubles
+    # with their 12 bytes of links
+    est = max(320.0, 1.5 * sa.rec64_records / (n * n))
+    r.set_precision(so.abi.SO_PREC_FP64, pool_mb=n * n / 2.5 * (est / 16 + 1) * (16 * 7 * 8 + 12) / 2 ** 20)
+    b = r.trace_rays(f, X, Y, cross=True)
+    sb = r.trace_stats()
+    r.close()
+    print("ray list waves:", sa.rec64_waves, "->", sb.rec64_waves, "records", sa.rec64_records, sb.rec64_records,
+          "cut", int((a["fate"] == -1).sum()))
+    assert sa.rec64_waves == 1 and sb.rec64_waves >= 2
+    assert sa.emit64 == 1 and sb.emit64 == 1 and sb.rec64_short == 0
+    assert sa.rec64_records == sb.rec64_records
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert _counts(sa) == _counts(sb)
+
+
 def test_trace_stats_state(so):
     """so_trace_stats reports the last ray list only: after a frame it is a state error."""
     sh = so.Shot("shadow_selftest_256.ini", ["camera.width=16", "camera.height=16"])
