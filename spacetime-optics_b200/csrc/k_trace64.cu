@@ -23,9 +23,9 @@
 // Large frames, batches and ray lists take the emission out of the tracer altogether (DEFER): a
 // recording pass integrates the geodesics and records each flow step that can emit;
 // k_turb64_records / k_turb32_rec64 sum the turbulence at the records, k_emit64_records evaluates
-// flow_step at each, and k_transfer64 applies them in each sample's order.  Every one of those kernels runs with all its
-// lanes on the same kind of work, where inside the tracer the emission ran on the lanes that
-// happened to take a flow step.
+// flow_step at each, and k_transfer64 applies them in each sample's order.  Every one of those
+// kernels runs with all its lanes on the same kind of work, where inside the tracer the emission
+// ran on the lanes that happened to take a flow step.
 //
 // Compiled with -fmad=false: every fusion is an explicit fma() (so_kerr.cuh), matching the oracle.
 #include <cuda_fp16.h>
@@ -405,8 +405,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // runs 1.29x faster with a few spilled registers and 50 % more warps.
 // DEFER (deferred FP64 passes, radio only): 0 = emission in the tracer, 1 = recording pass (geometry
 // only: no emission code), 2 = replay pass, 3 = recording pass of a ray list (also records each
-// step's crossings and writes the rays' outputs without emission).  Both passes run four CTAs per SM (128 registers):
-// measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against 205 ms at
+// step's crossings and writes the rays' outputs without emission).  Both passes run four CTAs per
+// SM (128 registers): measured on the 1024^2 synchrotron frame, the replay pass takes 178 ms there against 205 ms at
 // three CTAs (168 registers, fewer spills); the recording pass 78 ms, against 84 ms at five CTAs
 // (96 registers) and 88 ms at six (80), whose spills cost more than the warps gain (the reference
 // flow frame: 80, 89 and 100 ms).
@@ -890,8 +890,9 @@ cudaError_t launch_emit64_records(const TraceLaunch& L, int num_sms, cudaStream_
 // Deferred emission, ordered transfer: one thread per job walks each sample's chain in recording
 // order with ray_commit's arithmetic (intensity into the image-order bucket, transmission, the
 // 1e-5 opacity cut, after which the counts of the cut step stand), then writes the job's outputs
-// and counts as the tracer does (a ray list's cut ray: also its crossings at the cut step).  Flow steps without a record emit nothing and transmit 1, so
-// skipping them changes no bit.  Left to the replay pass when a sample ran out of segments.
+// and counts as the tracer does (a ray list's cut ray: also its crossings at the cut step).  Flow
+// steps without a record emit nothing and transmit 1, so skipping them changes no bit.  Left to the
+// replay pass when a sample ran out of segments.
 __global__ void __launch_bounds__(128) k_transfer64(const TraceLaunch L) {
     const bool skip = *(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull;
     const unsigned long long cmask = (1ull << REC64_COUNT_BITS) - 1ull;
