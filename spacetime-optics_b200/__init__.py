@@ -310,11 +310,12 @@ class Renderer:
         x = np.ascontiguousarray(x, np.float64)
         y = np.ascontiguousarray(y, np.float64)
         n = x.size
-        o = dict(fate=np.zeros(n, np.int8), ncross=np.zeros(n, np.int8), theta=np.zeros(n), phi=np.zeros(n),
-                 I=np.zeros((n, 4), np.float32), n_accepted=np.zeros(n, np.int32), n_attempts=np.zeros(n, np.int32))
+        # so_trace_rays writes every element of every output it is given
+        o = dict(fate=np.empty(n, np.int8), ncross=np.empty(n, np.int8), theta=np.empty(n), phi=np.empty(n),
+                 I=np.empty((n, 4), np.float32), n_accepted=np.empty(n, np.int32), n_attempts=np.empty(n, np.int32))
         if cross:
-            o["cross_r"] = np.zeros((n, 3))
-            o["cross_g"] = np.zeros((n, 3))
+            o["cross_r"] = np.empty((n, 3))
+            o["cross_g"] = np.empty((n, 3))
         ro = RaysOut(*[_ptr(o.get(k)) for k in ("fate", "ncross", "theta", "phi", "I", "n_accepted", "n_attempts",
                                                  "cross_r", "cross_g")])
         _check(lib().so_trace_rays(self.h, C.byref(frame), n, _ptr(x), _ptr(y), C.byref(ro)), self.h)
