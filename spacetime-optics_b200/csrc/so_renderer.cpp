@@ -1452,7 +1452,7 @@ static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const doubl
                            const so_rays_out& d_out) {
     SO_CK(r, cudaMemcpyAsync(r->d_frame, f, sizeof(so_frame), cudaMemcpyHostToDevice, r->st));
     SO_CK(r, cudaMemsetAsync(r->d_cnt, 0, sizeof(Counters), r->st));
-    r->list_rays = n;
+    r->list_rays = 0;
     TraceLaunch L;
     launch_common(r, L);
     if (int brc = bake_turbulence(r, L)) return brc;
@@ -1466,7 +1466,9 @@ static int trace_rays_impl(so_renderer* r, const so_frame* f, int n, const doubl
         L.out.cross_r = nullptr;
         L.out.cross_g = nullptr;
     }
-    return run_tracer(r, L);
+    const int rc = run_tracer(r, L);
+    if (rc == SO_OK) r->list_rays = n;
+    return rc;
 }
 
 int so_trace_stats(so_renderer* r, so_stats* stats) {
