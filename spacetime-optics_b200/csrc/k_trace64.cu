@@ -554,7 +554,8 @@ __global__ void __launch_bounds__(128, DEFER >= 1 ? 4 : 3) k_trace64(const Trace
                     else
                         want = torus_position(*S, tp, F->r, yn[0], yn[2], yn[4], yn[5], &TX, &TY, &TZ);
                 } else if (defer == 1) {
-                    want = flow_wants(*S, yn[0], yn[2]);
+                    // no turbulence sums: the torus without modes or the reference flow model
+                    want = tp.on ? torus_wants(*S, tp, yn[0], yn[2]) : flow_wants(*S, yn[0], yn[2]);
                 }
             }
         }
@@ -843,17 +844,18 @@ cudaError_t launch_turb32_rec64(const TraceLaunch& L, const TurbModes& M, int nu
 
 // Deferred emission: flow_step at every record (after its sum, on the torus plasma), one thread per
 // slot over the slots of the segments taken (a slot past its chain's last record is skipped).
-// Writes the step's emission dI over r and its transmission exp(-dtau) over u.  The torus model
-// reads neither the azimuth nor the time of the step, nor the baked field; the reference flow model
-// reads its phi and t and fetches the frame's turbulence as the tracer does.  Left to the replay
-// pass when a sample ran out of segments.
+// Writes the step's emission dI over r and its transmission exp(-dtau) over u.  The torus model with
+// turbulence reads the sum, and neither the azimuth nor the time of the step; without modes it takes
+// the flow records' form (phi, t) and reads neither; the reference flow model reads its phi and t
+// and fetches the frame's turbulence as the tracer does.  Left to the replay pass when a sample ran
+// out of segments.
 __global__ void __launch_bounds__(256) k_emit64_records(const TraceLaunch L) {
     if (*(volatile unsigned long long*)&L.rec64_ctl[1] != 0ull) return;
     unsigned long long used = *(volatile unsigned long long*)&L.rec64_ctl[0];
     if (used > (unsigned long long)L.seg_cap64) used = (unsigned long long)L.seg_cap64;
     const long long nslots = (long long)used * REC_SEG;
     TorusParams tp;
-    tp.on = L.torus && L.n_modes > 0;
+    tp.on = L.torus;
     tp.n_modes = tp.on ? L.n_modes : 0;
     tp.ne_index = L.ne_index;
     tp.te_index = L.te_index;
@@ -868,10 +870,10 @@ __global__ void __launch_bounds__(256) k_emit64_records(const TraceLaunch L) {
         const int fidx = smp.fidx;
         double* rec = L.rec64 + (long long)L.rec64_w * slot;
         double dI, dtau;
-        if (tp.on)
+        if (tp.n_modes > 0)
             flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], nullptr, tp, rec[2], rec[0], rec[1], 0.0, 0.0,
                       smp.lam, smp.E, rec[3], &dI, &dtau);
-        else
+        else  // the reference flow model, or the torus without turbulence (flow_step's tp.on branch)
             flow_step(L.scenes[L.frame_scene[fidx]], L.frames[fidx], L.turb_field, tp, 0.0, rec[0], rec[1], rec[2],
                       rec[5], smp.lam, smp.E, rec[3], &dI, &dtau);
         rec[0] = dI;

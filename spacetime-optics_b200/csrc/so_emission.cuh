@@ -301,6 +301,16 @@ __device__ __forceinline__ bool flow_wants(const so_scene& S, double r, double u
     return !(exp(-0.5 * zh * zh) < 1e-7);
 }
 
+// The same for the torus plasma (flow_step's torus branch: outside the flow region, or the vertical
+// profile exp(-(u / h_sph)^2 / 2) below 1e-7).
+__device__ __forceinline__ bool torus_wants(const so_scene& S, const TorusParams& tp, double r, double u) {
+    double s2 = fmax(fma(-u, u, 1.0), 1e-12), s = sqrt(s2);
+    double R = r * s;
+    if (r > S.r_flow_max || R < 1e-3) return false;
+    double zh = u / tp.h_sph;
+    return !(exp(-0.5 * zh * zh) < 1e-7);
+}
+
 // flow_step with the torus turbulence sum `delta` at this point already evaluated (torus_position).
 // With `field` (the frame's baked slices) the reference model's turbulence is sampled as
 // emission.cuh:112-124 does, else its sheared noise is evaluated in place (the turb_nt = 0 path).

@@ -477,6 +477,38 @@ def test_deferred_fp64_ray_list(so, case):
     assert np.all(thick["theta"][cut] == 0) and np.all(thick["n_attempts"] <= thin["n_attempts"])
 
 
+def test_deferred_fp64_torus_without_modes(so, orc):
+    """The torus plasma without turbulence (n_modes = 0) defers its emission through records of the
+    flow form (no sums), with the torus's own vertical profile deciding which steps record and the
+    torus density in the emission: a 96 x 96 frame (2 samples) equals the in-tracer frame bit for
+    bit, counters included, and a 64 x 64 ray list (4096 rays, deferred) equals the oracle (geometry
+    exact, intensity within 1e-6 of the maximum)."""
+    ov = ["so.modes=0", "flow.n0=1594262.8"]
+    a, sa, b, sb = _deferred_pair(so, ["camera.width=96", "camera.height=96", "render.spp=2", "render.spp_max=2", *ov])
+    assert sa.emit64 == 1 and sa.rec64_records > 0 and sa.rec64_short == 0 and sa.ms_sum64 < 0.05
+    assert sb.emit64 == 0 and sb.rec64_short > 0
+    assert a[..., 0].max() > 0
+    assert np.array_equal(a, b)
+    assert _counts(sa) == _counts(sb)
+    n = 64
+    sh = so.Shot("synchrotron_1024.ini", [f"camera.width={n}", f"camera.height={n}", *ov])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    p = sh.plasma()
+    assert p.n_modes == 0
+    r.set_plasma(p)
+    f = sh.frame(0)
+    X, Y = so.pixel_centres(f, n, n)
+    k = r.trace_rays(f, X, Y)
+    st = r.trace_stats()
+    r.close()
+    assert st.emit64 == 1 and st.rec64_short == 0
+    o = orc.orc_trace(sh.scene, f, X, Y, plasma=p, threads=_threads())
+    _cmp_geometry(o, k, rtol_dir=1e-12)
+    I0, I1 = o["I"].astype(np.float64), k["I"].astype(np.float64)
+    assert I0[:, 0].max() > 0
+    assert np.abs(I0 - I1).max() <= 1e-6 * I0[:, 0].max()
+
+
 def test_deferred_fp64_ray_list_waves(so):
     """A ray list whose records the pool holds only in part runs the deferred passes in waves of
     consecutive rays (each writing its rays' outputs at their own indices): 256 x 256 pixel centres
