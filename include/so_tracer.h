@@ -365,6 +365,8 @@ void* so_stream(so_renderer* r);
 /* Message of the last failed call on r.  With r NULL: of the last failed call without a renderer
  * (so_init, so_shot_load, so_radio_flux_noalloc, so_sur_gemm) made by the calling thread. */
 const char* so_last_error(const so_renderer* r);
+/* Frees the renderer.  Batches made on it and not yet freed are detached: so_batch_render and
+ * so_batch_autotune on them return SO_ERR_STATE, and so_batch_free still frees them. */
 void so_destroy(so_renderer* r);
 
 /* ---- batched frames: the persistent wavefront (no reference counterpart) --------------------- */

@@ -160,8 +160,12 @@ struct so_renderer {
     long long samples64 = 0;                   // samples of the last deferred trace (for the estimate)
     bool last_defer64 = false, last_emit64 = false;
     long long list_rays = 0;                   // rays of the last so_trace_rays whose counters d_cnt holds
+    std::vector<so_batch*> batches;            // live batches on this renderer (detached by so_destroy)
     std::string err;
 };
+
+// Clears the renderer pointer of every live batch of r (so_destroy).
+void detach_batches(so_renderer* r);
 
 namespace {
 
@@ -1682,6 +1686,7 @@ const char* so_last_error(const so_renderer* r) { return r ? r->err.c_str() : g_
 
 void so_destroy(so_renderer* r) {
     if (!r) return;
+    detach_batches(r);  // so_batch_free still frees them
     cudaSetDevice(r->device);
     if (r->st) cudaStreamSynchronize(r->st);
     free_all(r);
@@ -1735,12 +1740,18 @@ struct so_batch {
     cudaGraphExec_t gexec = nullptr;
     float* graph_px = nullptr;  // output buffer baked into the graph
     so_tune graph_tune{-1, -1, 0.0, -1, -1};
-    // deferred passes (torus plasma, frame work without disks): decided and sized before each graph
-    // capture; wave64 = 0 traces in one persistent launch
+    // deferred passes (radio frames without disks): decided and sized before each graph capture;
+    // wave64 = 0 traces in one persistent launch
     bool defer_ok = false;
     long long wave64 = 0;
-    int sums64 = 0;  // 1 FP64 sums, 2 FP32 sums (mixed precision)
+    int sums64 = 0;              // 0 none (reference flow, torus without modes), 1 FP64, 2 FP32 (mixed)
+    int w64 = REC64_W_TORUS;     // doubles per record
 };
+
+void detach_batches(so_renderer* r) {
+    for (so_batch* b : r->batches) b->r = nullptr;
+    r->batches.clear();
+}
 
 namespace {
 
@@ -1794,23 +1805,28 @@ void batch_launch_desc(so_batch* b, float* d_px, TraceLaunch& L) {
     L.emit32 = r->precision == SO_PREC_MIXED;
 }
 
-// Whether and how the batch's next capture defers its turbulence sums and emission: the torus
-// plasma's frame work of at least kDeferMinJobs jobs, through the renderer's record pool (sized
-// here, outside the capture), in waves; FP32 sums for mixed precision, FP64 otherwise.
+// Whether and how the batch's next capture defers its turbulence sums and emission: radio frame
+// work of at least kDeferMinJobs jobs, through the renderer's record pool (sized here, outside the
+// capture), in waves.  The torus plasma's sums in FP32 for mixed precision, FP64 otherwise; the
+// reference flow model (its noise in place: a batch bakes no slices) and the torus without modes
+// defer the emission alone.
 void batch_plan(so_batch* b, float* d_px) {
     so_renderer* r = b->r;
     b->wave64 = 0;
     b->sums64 = 0;
     TraceLaunch L;
     batch_launch_desc(b, d_px, L);
-    if (!b->defer_ok || b->variant != VAR_RADIO || !L.torus || L.n_modes <= 0 || L.nrays < kDeferMinJobs) return;
+    if (!b->defer_ok || b->variant != VAR_RADIO || L.nrays < kDeferMinJobs) return;
+    const bool sums = L.torus && L.n_modes > 0;
+    const int w = sums ? REC64_W_TORUS : REC64_W_FLOW;
     long long wave = 0;
-    if (ensure_records64(r, L.nrays, b->spp, REC64_W_TORUS, &wave) != SO_OK) {
+    if (ensure_records64(r, L.nrays, b->spp, w, &wave) != SO_OK) {
         r->err.clear();  // no pool: one persistent launch
         return;
     }
     b->wave64 = wave;
-    b->sums64 = (r->precision == SO_PREC_MIXED && r->turb_modes) ? 2 : 1;
+    b->w64 = w;
+    b->sums64 = !sums ? 0 : (r->precision == SO_PREC_MIXED && r->turb_modes) ? 2 : 1;
     r->samples64 = L.nrays * b->spp;
 }
 
@@ -1822,7 +1838,7 @@ int batch_enqueue(so_batch* b, float* d_px) {
     TraceLaunch L;
     batch_launch_desc(b, d_px, L);
     if (b->wave64 > 0) {
-        if (int rc = enqueue_deferred64(r, L, b->variant, r->st, b->wave64, REC64_W_TORUS, b->sums64, true, false))
+        if (int rc = enqueue_deferred64(r, L, b->variant, r->st, b->wave64, b->w64, b->sums64, true, false))
             return rc;
     } else {
         cudaError_t e = launch_trace64(L, b->variant, r->num_sms, r->st);
@@ -1888,6 +1904,10 @@ int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const s
     b->variant = var;
     std::vector<so_scene> sc(scenes, scenes + nscenes);
     for (so_scene& s : sc) {  // the renderer's device tables
+        // the reference flow's turbulence in place: a batch bakes no per-frame slices, so no scene
+        // may point at textures of another frame's bake
+        s.turb_nt = 0;
+        for (int k = 0; k < 24; ++k) s.turb_tex[k] = 0;
         s.disk_lnT = r->d_disk;
         s.k2_lntab = r->d_k2;
         s.bb_xyz = r->d_bb;
@@ -1914,12 +1934,14 @@ int so_batch_create(so_renderer* r, const so_scene* scenes, int nscenes, const s
         so_batch_free(b);
         return rc;
     }
+    r->batches.push_back(b);
     *out = b;
     return SO_OK;
 }
 
 int so_batch_render(so_batch* b, float* d_px, so_stats* stats) {
     if (!b || !d_px) return SO_ERR_ARG;
+    if (!b->r) return SO_ERR_STATE;  // its renderer was destroyed
     so_renderer* r = b->r;
     if (cudaSetDevice(r->device) != cudaSuccess) return fail(r, SO_ERR_CUDA, "cudaSetDevice");
     r->list_rays = 0;
@@ -2001,6 +2023,7 @@ int so_batch_set_tune(so_batch* b, const so_tune* t) {
 
 int so_batch_autotune(so_batch* b, float* d_px, so_tune* best) {
     if (!b || !d_px) return SO_ERR_ARG;
+    if (!b->r) return SO_ERR_STATE;
     // warm-up with the full grid; then CTAs per SM from 1 up (the launcher caps the value at the
     // kernel's occupancy limit, so the sweep stops once a larger cap no longer helps)
     const int per_sm = 8;
@@ -2051,7 +2074,11 @@ int so_batch_autotune(so_batch* b, float* d_px, so_tune* best) {
 
 void so_batch_free(so_batch* b) {
     if (!b) return;
-    if (b->r) cudaSetDevice(b->r->device);
+    if (b->r) {
+        cudaSetDevice(b->r->device);
+        auto& v = b->r->batches;
+        v.erase(std::remove(v.begin(), v.end(), b), v.end());
+    }
     batch_drop_graph(b);
     void* ps[] = {b->d_scenes, b->d_frames, b->d_frame_scene, b->d_cnt};
     for (void* p : ps)

@@ -130,6 +130,56 @@ def test_batch_deferred_matches_single_frames(so):
     r.close()
 
 
+@pytest.mark.parametrize("plasma", ["reference_flow", "torus_without_modes"])
+def test_batch_deferred_emission_without_sums(so, plasma):
+    """Batches with no mode sums defer their emission alone: the reference flow model (its sheared
+    noise in place, as every batch evaluates it) over three spins, and the torus plasma without
+    turbulence.  Every frame equals its single-frame render (below the deferral threshold, emission in
+    the tracer; the reference model with SO_FLOW_NOISE_INLINE) bit for bit, with the pool uncapped and
+    too small for a wave (the replay pass renders the batch); mixed precision changes nothing here
+    (no FP32 sums to take)."""
+    import torch
+    W = 48
+    if plasma == "reference_flow":
+        shots = [so.Shot("m87_reference_flow.ini", [f"camera.width={W}", f"camera.height={W}", f"bh.spin={a}",
+                                                    "render.spp=1", "render.spp_max=1"]) for a in (0.5, 0.94, 0.99)]
+    else:
+        shots = [so.Shot("synchrotron_1024.ini", [f"camera.width={W}", f"camera.height={W}", f"bh.spin={a}",
+                                                  "so.modes=0", "flow.n0=1594262.8"]) for a in (0.5, 0.94, 0.99)]
+    scenes, frames, fs, ref = [], [], [], []
+    for si, sh in enumerate(shots):
+        scenes.append(sh.scene)
+        rr = so.Renderer(sh.scene, sh.tables, sh.settings)
+        rr.set_plasma(sh.plasma() if plasma != "reference_flow" else None)
+        if plasma == "reference_flow":
+            rr.set_flow_noise(so.abi.SO_FLOW_NOISE_INLINE)
+        frames.append(sh.frame(0))
+        fs.append(si)
+        img, _, _ = rr.render(sh.frame(0))
+        ref.append(img)
+        rr.close()
+    ref = np.stack(ref)
+    assert len(frames) * W * W >= 4096 and ref[..., 0].max() > 0
+    sh0 = shots[0]
+    r = so.Renderer(sh0.scene, sh0.tables, sh0.settings)
+    r.set_plasma(sh0.plasma() if plasma != "reference_flow" else None)
+    out = torch.zeros((len(frames), W, W, 4), dtype=torch.float32, device="cuda")
+    for prec, pool_mb in ((so.abi.SO_PREC_FP64, 0.0), (so.abi.SO_PREC_FP64, 0.001), (so.abi.SO_PREC_MIXED, 0.0)):
+        r.set_precision(prec, pool_mb=pool_mb)
+        b = so.Batch(r, scenes, frames, fs, W, W, 1)
+        for _ in range(2):
+            out.zero_()
+            st = b.render(out.data_ptr(), stats=True)
+            torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), ref), (prec, pool_mb)
+        if pool_mb == 0.0:
+            assert st.emit64 == 1 and st.rec64_records > 0 and st.rec64_short == 0 and st.ms_sum64 < 0.05
+        else:
+            assert st.emit64 == 0 and st.rec64_short > 0
+        b.close()
+    r.close()
+
+
 def test_batch_rejects_bad_input(so):
     import ctypes as C
     sh = so.Shot("synchrotron_1024.ini", ["camera.width=8", "camera.height=8"])
@@ -144,3 +194,22 @@ def test_batch_rejects_bad_input(so):
     h = C.c_void_p()
     assert L.so_batch_create(r.h, None, 0, None, None, 0, 8, 8, 1, C.byref(h)) == so.abi.SO_ERR_ARG
     r.close()
+
+
+def test_batch_after_its_renderer_is_destroyed(so):
+    """A batch whose renderer is destroyed first is detached: rendering it is a state error, freeing
+    it is still safe, and no CUDA error is left behind for the next caller on the thread."""
+    import torch
+    sh = so.Shot("synchrotron_1024.ini", ["camera.width=8", "camera.height=8"])
+    r = so.Renderer(sh.scene, sh.tables, sh.settings)
+    b = so.Batch(r, [sh.scene], [sh.frame(0)], [0], 8, 8, 1)
+    out = torch.zeros((1, 8, 8, 4), dtype=torch.float32, device="cuda")
+    b.render(out.data_ptr())
+    torch.cuda.synchronize()
+    r.close()
+    with pytest.raises(so.TracerError) as e:
+        b.render(out.data_ptr())
+    assert e.value.code == so.abi.SO_ERR_STATE
+    b.close()
+    torch.zeros(4, device="cuda").add_(1.0)
+    torch.cuda.synchronize()
