@@ -376,12 +376,13 @@ void so_destroy(so_renderer* r);
  * scenes[frame_scene[i]]; every scene must have the same mode and use the renderer's tables (those
  * of so_init: the K2 and blackbody tables do not depend on the scene, the disk table depends on the
  * spin, so disk scenes must share a spin).  The plasma is the renderer's (so_set_plasma).  The launch
- * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed.  A batch
- * of 4096 jobs or more on the torus plasma (no disk) traces in deferred passes instead: a
- * persistent recording pass over all frames, the turbulence sums at its records (FP32 under
- * SO_PREC_MIXED, FP64 otherwise), the emission and the ordered transfer, in waves through the
- * renderer's record pool (sized before the capture, within so_mixed_opts.pool_mb); a batch that ran
- * short of records is captured again with a larger pool at its next so_batch_render. */
+ * sequence (counter reset, tracer, resolve) is captured once into a CUDA graph and replayed.  A radio
+ * batch of 4096 jobs or more (no disk) traces in deferred passes instead: a persistent recording
+ * pass over all frames, the torus plasma's turbulence sums at its records (FP32 under
+ * SO_PREC_MIXED, FP64 otherwise; none for the reference flow model, whose noise a batch evaluates
+ * in place), the emission and the ordered transfer, in waves through the renderer's record pool
+ * (sized before the capture, within so_mixed_opts.pool_mb); a batch that ran short of records is
+ * captured again with a larger pool at its next so_batch_render. */
 typedef struct so_batch so_batch;
 /* Launch shape of the batch: resident CTAs per SM of the persistent grid (0 = as many as fit); the
  * job order (0 = frame after frame, 1 = frames interleaved in tiles of `tile` consecutive pixels,
