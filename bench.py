@@ -560,6 +560,7 @@ def run_rays(args, so, world, rank, local):
     outs = {"fate": torch.int8, "ncross": torch.int8, "theta": torch.float64, "phi": torch.float64,
             "I": torch.float32, "n_accepted": torch.int32, "n_attempts": torch.int32}
     d = {k: torch.empty((n, 4) if k == "I" else (n,), dtype=t, device=dev) for k, t in outs.items()}
+    torch.cuda.synchronize()  # the coordinates are on the device before the library's stream reads them
     ro = so.abi.RaysOut(*[C.c_void_p(d[k].data_ptr()) if k in d else None
                           for k, _ in so.abi.RaysOut._fields_])
     lib = so.lib()
