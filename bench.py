@@ -866,6 +866,20 @@ def run_wavefront(args, so, world, rank, local):
                            if st.rec64_waves else "k_trace64 (FP32 sums)"),
                 "peak_source": "so_probe_sfu_peak (measured SFU cosine chains on this GPU)",
                 "fp64_geometry_flops": st.attempts * FLOPS_ATTEMPT + st.accepted * FLOPS_ACCEPT}
+    # e2e: the batch through so_batch_render and every frame read back into pinned host memory (the
+    # frames' descriptors were uploaded once at so_batch_create: no per-step input), at most 2 steps
+    # (the copy runs on torch's stream, ordered after the library's: a pinned buffer used on the
+    # library's stream would keep an event on it past r.close())
+    host = torch.empty((len(frames), W, W, 4), dtype=torch.float32).pin_memory()
+    e2e_s = []
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        b.render(out.data_ptr())
+        torch.cuda.current_stream().wait_stream(stream)
+        host.copy_(out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_step = allreduce_max(float(np.mean(e2e_s)), world)
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
@@ -883,7 +897,8 @@ def run_wavefront(args, so, world, rank, local):
                    "samples_traced_in_place": st.rec64_short,
                    "l2": "inputs (mode table, frame descriptors) are small; no flush (one step is seconds long)"},
         "roofline": roof,
-        "e2e": None,
+        "e2e": {"value": round(world * nrays / e2e_step / 1e6, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": nrays * 16},
         # per wave: recording pass, sums, emission, transfer, replay launch (returns at once); then
         # resolve; without waves: the persistent tracer and resolve
         "gpu_launches": args.steps * ((st.rec64_waves * 5 + 1) if st.rec64_waves else 2),
