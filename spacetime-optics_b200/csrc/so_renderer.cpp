@@ -874,11 +874,14 @@ int trace_pass1_mixed(so_renderer* r, const so_frame& f, TraceLaunch& L) {
     Lb.nrays_dev = &r->d_nlists[1];
     Lb.counters = &r->d_cnt3[0];
     Lb.emit32 = 1;  // FP64 geometry in the band; the emission needs no more than FP32
-    // One CTA per SM for the band and the re-trace: their few rays, some of them very long, would
-    // otherwise keep three 168-register CTAs (every SM's whole register file) resident and hold the
-    // FP32 tracer off those SMs.  Measured: the reference flow frame at 1024^2 72.0 -> 67.5 ms, the
-    // synchrotron frame at 2048^2 unchanged (210 ms), the images identical.
-    Lb.ctas_per_sm = 1;
+    // The band and the re-trace take one CTA per SM, two when their rays carry the torus's
+    // warp-cooperative turbulence sums (throughput work that more warps serve); otherwise their
+    // rays are long latency-bound chains, and the full persistent grid (three 168-register CTAs,
+    // every SM's register file) held the FP32 tracer off those SMs.  Measured, three / two / one
+    // CTAs per SM: the reference flow frame at 1024^2 72.0 / 71.3 / 67.5 ms, the synchrotron frame
+    // at 2048^2 210.3 / 207.4 / 210.3 ms, the vacuum shadow frame at 2048^2 one CTA 122.5 Mrays/s
+    // against 119.8 with two; the images identical.
+    Lb.ctas_per_sm = (L.torus && L.n_modes > 0) ? 2 : 1;
     int rc = run_tracer(r, Lb, r->st2);
     if (rc) return rc;
     const bool torus_defer = variant_of(r->S) == VAR_RADIO && L.torus && L.n_modes > 0;
